@@ -1,0 +1,36 @@
+"""fastlpr_b200: fastLPR's NUFFT path (local polynomial regression with GCV,
+kernel density estimation with LCV) on NVIDIA B200 GPUs.
+
+Public API mirrors the reference package ``fastlpr``:
+
+    from fastlpr_b200 import cv_fastlpr, cv_fastkde, get_hlist
+    regs = cv_fastlpr(x, y, get_hlist(20, [0.01, 1.0]), {"order": 1})
+
+The hot path runs in the in-tree CUDA library ``libfastlpr_b200.so``
+(C ABI: include/fastlpr_b200.h); there is no CPU fallback.
+"""
+from .bandwidth import get_hlist
+from .structures import KDEOutput, RegressionOutput
+from .api import cv_fastkde, cv_fastlpr, cv_fastlpr_device, clear_fastlpr_caches
+
+__version__ = "0.1.0"
+
+
+def fastlpr_predict(regression: RegressionOutput, x_new):
+    """Evaluate a fitted regression at new points (reference predict.py:15-131)."""
+    if regression.fpp_yhat is None:
+        raise ValueError("regression has no interpolant")
+    return regression.fpp_yhat(x_new)
+
+
+__all__ = [
+    "__version__",
+    "cv_fastlpr",
+    "cv_fastkde",
+    "cv_fastlpr_device",
+    "get_hlist",
+    "fastlpr_predict",
+    "RegressionOutput",
+    "KDEOutput",
+    "clear_fastlpr_caches",
+]

@@ -1,0 +1,111 @@
+"""ctypes binding of ``libfastlpr_b200.so`` (the C ABI in include/fastlpr_b200.h).
+
+The library is mandatory: importing the GPU entry points without it raises,
+there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("FASTLPR_B200_LIB", os.path.join(_HERE, "libfastlpr_b200.so"))
+
+FLPR_PREC_F32 = 0
+FLPR_PREC_F64 = 1
+
+# (name, restype, argtypes) for every exported symbol of include/fastlpr_b200.h
+_VP, _I, _I64, _D, _SZ = C.c_void_p, C.c_int, C.c_int64, C.c_double, C.c_size_t
+_PI, _PD = C.POINTER(C.c_int), C.POINTER(C.c_double)
+_PVP = C.POINTER(C.c_void_p)
+SIGNATURES = [
+    ("flpr_last_error", C.c_char_p, []),
+    ("flpr_version", _I, []),
+    ("flpr_launch_count", _I64, []),
+    ("flpr_create", _I, [C.POINTER(_VP), _I]),
+    ("flpr_destroy", _I, [_VP]),
+    ("flpr_point_stats_ws", _SZ, [_I, _I64]),
+    ("flpr_point_stats", _I, [_I, _I64, _VP, _VP, _VP, _SZ, _VP]),
+    ("flpr_spread_ws", _SZ, [_I, _I64, _PI, _I, _I, _I]),
+    ("flpr_spread", _I, [_I, _I64, _VP, _PD, _PI, _I, _PD, _I, _I, _PVP, _VP, _I, _VP, _SZ, _VP]),
+    ("flpr_forward_fft_ws", _SZ, [_VP, _I, _PI, _I, _I]),
+    ("flpr_forward_fft", _I, [_VP, _I, _PI, _I, _VP, _VP, _I, _VP, _SZ, _VP]),
+    ("flpr_kernel_factors_ws", _SZ, [_VP, _I, _PI, _I, _I]),
+    ("flpr_kernel_factors", _I, [_VP, _I, _PI, _PI, _PD, _PD, _I, _VP, _I, _VP, _VP, _VP, _SZ, _VP]),
+    ("flpr_conv_ws", _SZ, [_VP, _I, _PI, _I, _I]),
+    ("flpr_conv", _I, [_VP, _I, _PI, _PI, _PI, _I, _I, _VP, _VP, _I, _PI, _PI, _PI, _D, _I, _VP,
+                       _I, _VP, _SZ, _VP]),
+    ("flpr_solve", _I, [_I, _I, _I, _I, _I64, _I, _VP, _VP, _D, _VP, _VP, _I, _VP]),
+    ("flpr_interp_reduce_ws", _SZ, [_I64, _I, _I, _I]),
+    ("flpr_interp_reduce", _I, [_I, _I64, _VP, _PD, _PI, _I, _I, _I, _VP, _PVP, _PVP, _VP, _VP,
+                                _VP, _VP, _SZ, _VP]),
+    ("flpr_interp_eval", _I, [_I, _I64, _VP, _PD, _PI, _I, _VP, _VP, _VP]),
+    ("flpr_kde_ws", _SZ, [_I64, _I, _I64]),
+    ("flpr_kde_lcv", _I, [_I, _I64, _VP, _PD, _PI, _I, _VP, _D, _PD, _VP, _VP, _VP, _SZ, _VP]),
+    ("flpr_log_shift", _I, [_I64, _VP, _D, _VP, _VP]),
+    ("flpr_exp_weighted_sum", _I, [_I64, _VP, _VP, _VP, _VP]),
+]
+
+
+class FastLPRError(RuntimeError):
+    """Error status returned by the CUDA library."""
+
+
+_lib: Optional[C.CDLL] = None
+_lib_lock = threading.Lock()
+
+
+def load() -> C.CDLL:
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lib_lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    f"fastlpr_b200 CUDA library not found at {LIB_PATH}; build it with "
+                    "`python -m fastlpr_b200.build` (there is no CPU fallback)")
+            lib = C.CDLL(LIB_PATH)
+            for name, res, args in SIGNATURES:
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def check(status: int, what: str = "") -> None:
+    if status != 0:
+        msg = load().flpr_last_error().decode(errors="replace")
+        raise FastLPRError(f"{what} failed with status {status}: {msg}")
+
+
+def ivec(vals: Sequence[int]):
+    a = (C.c_int * max(1, len(vals)))(*[int(v) for v in vals])
+    return a
+
+
+def dvec(vals: Sequence[float]):
+    return (C.c_double * max(1, len(vals)))(*[float(v) for v in vals])
+
+
+def pvec(ptrs: Sequence[int]):
+    return (C.c_void_p * max(1, len(ptrs)))(*[C.c_void_p(int(p)) for p in ptrs])
+
+
+_handles: Dict[int, C.c_void_p] = {}
+
+
+def handle(device: int) -> C.c_void_p:
+    """Per-device library handle (owns the cuFFT plan cache)."""
+    h = _handles.get(device)
+    if h is None:
+        h = C.c_void_p()
+        check(load().flpr_create(C.byref(h), device), "flpr_create")
+        _handles[device] = h
+    return h

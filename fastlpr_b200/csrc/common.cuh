@@ -1,0 +1,150 @@
+// Shared helpers for the fastlpr_b200 CUDA library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "../../include/fastlpr_b200.h"
+
+namespace flpr {
+
+// Per-thread message for flpr_last_error().
+void set_error(const char* fmt, ...);
+
+// Number of kernels this library has launched (flpr_launch_count()).
+void count_launch();
+
+#define FLPR_CHECK_ARG(cond, ...)            \
+  do {                                       \
+    if (!(cond)) {                           \
+      ::flpr::set_error(__VA_ARGS__);        \
+      return FLPR_ERR_ARG;                   \
+    }                                        \
+  } while (0)
+
+#define FLPR_CUDA(call)                                                        \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      ::flpr::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call,             \
+                        cudaGetErrorString(e_));                               \
+      return FLPR_ERR_CUDA;                                                    \
+    }                                                                          \
+  } while (0)
+
+#define FLPR_LAUNCH_CHECK()                                                    \
+  do {                                                                         \
+    ::flpr::count_launch();                                                    \
+    cudaError_t e_ = cudaGetLastError();                                       \
+    if (e_ != cudaSuccess) {                                                   \
+      ::flpr::set_error("%s:%d launch: %s", __FILE__, __LINE__,                \
+                        cudaGetErrorString(e_));                               \
+      return FLPR_ERR_CUDA;                                                    \
+    }                                                                          \
+  } while (0)
+
+#define FLPR_CUFFT(call)                                                       \
+  do {                                                                         \
+    cufftResult r_ = (call);                                                   \
+    if (r_ != CUFFT_SUCCESS) {                                                 \
+      ::flpr::set_error("%s:%d %s: cufft error %d", __FILE__, __LINE__, #call, \
+                        (int)r_);                                              \
+      return FLPR_ERR_CUFFT;                                                   \
+    }                                                                          \
+  } while (0)
+
+#define FLPR_TRY(call)                 \
+  do {                                 \
+    int s_ = (call);                   \
+    if (s_ != FLPR_OK) return s_;      \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline size_t align_up(size_t v, size_t a = 256) { return (v + a - 1) / a * a; }
+
+// Bump allocator over a caller-provided workspace.
+struct Arena {
+  char* base;
+  size_t size;
+  size_t used = 0;
+  Arena(void* b, size_t s) : base(static_cast<char*>(b)), size(s) {}
+  template <typename T>
+  T* take(size_t count) {
+    size_t off = align_up(used);
+    used = off + align_up(count * sizeof(T));
+    if (used > size) return nullptr;
+    return reinterpret_cast<T*>(base + off);
+  }
+};
+
+// Size-only counterpart of Arena for *_ws queries.
+struct ArenaSize {
+  size_t used = 0;
+  template <typename T>
+  void take(size_t count) { used = align_up(used) + align_up(count * sizeof(T)); }
+};
+
+inline int sm_count() {
+  static int cached = -1;
+  if (cached < 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    cached = v;
+  }
+  return cached;
+}
+
+inline int64_t prod(const int* v, int d) {
+  int64_t p = 1;
+  for (int i = 0; i < d; ++i) p *= v[i];
+  return p;
+}
+
+// Round-to-nearest FP64 arithmetic without contraction into FMA; the knot
+// mapping must reproduce the reference's elementwise numpy operations.
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// numpy.mod for float64 (floor-style remainder).
+__device__ __forceinline__ double np_mod(double a, double b) {
+  double r = fmod(a, b);
+  if (r != 0.0) {
+    if ((b < 0.0) != (r < 0.0)) r = dadd(r, b);
+  } else {
+    r = copysign(0.0, b);
+  }
+  return r;
+}
+
+// Per-axis knot map constants, in the order of flpr_spread's h_kmap.
+struct KnotAxis {
+  double mean, std, center, xs_min, xs_scale, ks, r0, shift, hx;
+};
+
+// Knot coordinate of raw coordinate x on one axis (see the header).
+__device__ __forceinline__ double knot_of(double x, const KnotAxis& a) {
+  double xs = dsub(ddiv(dsub(x, a.mean), a.std), a.center);
+  double xn = dadd(dmul(ddiv(dsub(xs, a.xs_min), a.xs_scale), a.ks), a.r0);
+  xn = dadd(xn, 0.5);
+  xn = np_mod(xn, 1.0);
+  double k = dsub(xn, 0.5);
+  k = dadd(k, a.shift);
+  k = dmul(k, 6.283185307179586);  // 2*pi as the float64 numpy computes it
+  return np_mod(k, 6.283185307179586);
+}
+
+}  // namespace flpr

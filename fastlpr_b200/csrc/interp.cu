@@ -1,0 +1,325 @@
+// Grid -> point interpolation, GCV / Hutchinson reductions and KDE LCV.
+#include "common.cuh"
+
+namespace flpr {
+
+constexpr int kMaxRed = 32;  // values reduced per (point, bandwidth)
+
+struct InterpGeom {
+  int d;
+  int G[3];
+  double x0[3], dx[3];
+  int64_t M;
+};
+
+// Cell and fraction on one axis, clamped like interp_optimized.py:60-78.
+__device__ __forceinline__ void axis_cell(double xi, double x0, double dx, int nx, int* ix,
+                                          double* fr) {
+  double t = (xi - x0) / dx;
+  if (t < 0.0) {
+    *ix = 0;
+    *fr = 0.0;
+  } else if (t >= (double)(nx - 1)) {
+    *ix = nx - 2 < 0 ? 0 : nx - 2;
+    *fr = 1.0;
+  } else {
+    int i = (int)t;
+    *ix = i;
+    *fr = t - (double)i;
+  }
+}
+
+// Corner offsets/weights of the multilinear stencil of point i.
+struct Stencil {
+  int64_t base[8];
+  double w[8];
+  int ncorner;
+};
+
+__device__ __forceinline__ void make_stencil(const InterpGeom& g, const double* __restrict__ x,
+                                             int64_t i, Stencil& st) {
+  int ix[3] = {0, 0, 0};
+  double fr[3] = {0, 0, 0};
+  for (int a = 0; a < g.d; ++a) axis_cell(x[i * g.d + a], g.x0[a], g.dx[a], g.G[a], &ix[a], &fr[a]);
+  st.ncorner = 1 << g.d;
+  for (int c = 0; c < st.ncorner; ++c) {
+    int64_t idx = 0;
+    double w = 1.0;
+    for (int a = 0; a < g.d; ++a) {
+      int bit = (c >> (g.d - 1 - a)) & 1;
+      int ia = ix[a] + bit;
+      if (ia >= g.G[a]) ia = g.G[a] - 1;  // single-point axis
+      idx = idx * g.G[a] + ia;
+      w *= bit ? fr[a] : (1.0 - fr[a]);
+    }
+    st.base[c] = idx;
+    st.w[c] = w;
+  }
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += sh[w];
+  return r;  // valid in thread 0
+}
+
+struct ColPtrs {
+  const double* col[kMaxRed];
+};
+
+// blockIdx.y = bandwidth.  m: (H, M, C) with C = ny + R.
+__global__ void interp_reduce_kernel(InterpGeom g, int64_t n, const double* __restrict__ x, int H,
+                                     int ny, int R, const double* __restrict__ m, ColPtrs yc,
+                                     ColPtrs pc, double* __restrict__ rss,
+                                     double* __restrict__ pdot) {
+  __shared__ double sh[32];
+  const int h = blockIdx.y;
+  const int C = ny + R;
+  double acc[kMaxRed];
+#pragma unroll
+  for (int c = 0; c < kMaxRed; ++c) acc[c] = 0.0;
+  const double* mh = m + (int64_t)h * g.M * C;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    Stencil st;
+    make_stencil(g, x, i, st);
+#pragma unroll
+    for (int c = 0; c < kMaxRed; ++c) {
+      if (c < C) {
+        double v = 0.0;
+        for (int k = 0; k < st.ncorner; ++k) v += st.w[k] * mh[st.base[k] * C + c];
+        if (c < ny) {
+          double r = yc.col[c][i] - v;
+          acc[c] += r * r;
+        } else {
+          acc[c] += pc.col[c - ny][i] * v;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < kMaxRed; ++c) {
+    if (c < C) {
+      double s = block_sum(acc[c], sh);
+      if (threadIdx.x == 0) {
+        if (c < ny) atomicAdd(&rss[h * ny + c], s);
+        else atomicAdd(&pdot[(c - ny) * H + h], s);
+      }
+    }
+  }
+}
+
+__global__ void probe_norm_kernel(int64_t n, int R, ColPtrs pc, double* __restrict__ pp) {
+  __shared__ double sh[32];
+  for (int r = 0; r < R; ++r) {
+    double a = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+      double v = pc.col[r][i];
+      a += v * v;
+    }
+    double s = block_sum(a, sh);
+    if (threadIdx.x == 0) atomicAdd(&pp[r], s);
+  }
+}
+
+__global__ void interp_eval_kernel(InterpGeom g, int64_t n, const double* __restrict__ x, int nval,
+                                   const double* __restrict__ vals, double* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    Stencil st;
+    make_stencil(g, x, i, st);
+    for (int v = 0; v < nval; ++v) {
+      const double* vv = vals + (int64_t)v * g.M;
+      double r = 0.0;
+      for (int k = 0; k < st.ncorner; ++k) r += st.w[k] * vv[st.base[k]];
+      out[(int64_t)v * n + i] = r;
+    }
+  }
+}
+
+// ---- KDE -----------------------------------------------------------------
+__global__ void plane_sum_kernel(int64_t M, const double* __restrict__ s, double* __restrict__ sums) {
+  __shared__ double sh[32];
+  const int h = blockIdx.y;
+  const double* p = s + (int64_t)h * M;
+  double a = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M;
+       i += (int64_t)gridDim.x * blockDim.x)
+    a += p[i];
+  double t = block_sum(a, sh);
+  if (threadIdx.x == 0) atomicAdd(&sums[h], t);
+}
+
+__global__ void kde_normalize_kernel(int64_t M, int H, const double* __restrict__ s,
+                                     const double* __restrict__ sums, double dxprod,
+                                     double* __restrict__ f) {
+  const int64_t total = (int64_t)H * M;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int h = (int)(t / M);
+    double tot = sums[h] * dxprod;
+    double v = tot > 0.0 ? s[t] / tot : s[t];
+    f[t] = v > 0.0 ? v : 0.0;
+  }
+}
+
+struct K0s {
+  double k0[256];
+};
+
+__global__ void kde_lcv_kernel(InterpGeom g, int64_t n, const double* __restrict__ x,
+                               const double* __restrict__ f, int h0, K0s k0,
+                               double* __restrict__ lcv) {
+  __shared__ double sh[32];
+  const int h = h0 + blockIdx.y;
+  const double* fh = f + (int64_t)h * g.M;
+  const double k0n = k0.k0[blockIdx.y] / (double)n;
+  const double ratio = (double)n / (double)(n - 1);
+  double s1 = 0.0, s2 = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    Stencil st;
+    make_stencil(g, x, i, st);
+    double v = 0.0;
+    for (int k = 0; k < st.ncorner; ++k) v += st.w[k] * fh[st.base[k]];
+    double fl = ratio * (v - k0n);
+    if (!(fl > 1e-10)) fl = 1e-10;
+    double l = log(fl);
+    s1 += l;
+    s2 += l * l;
+  }
+  double a = block_sum(s1, sh);
+  if (threadIdx.x == 0) atomicAdd(&lcv[2 * h], a);
+  double b = block_sum(s2, sh);
+  if (threadIdx.x == 0) atomicAdd(&lcv[2 * h + 1], b);
+}
+
+static int make_geom(InterpGeom& g, int d, const double* ax, const int* G) {
+  memset(&g, 0, sizeof(g));
+  FLPR_CHECK_ARG(d >= 1 && d <= 3, "interp: d=%d", d);
+  g.d = d;
+  g.M = 1;
+  for (int a = 0; a < d; ++a) {
+    FLPR_CHECK_ARG(G[a] >= 1, "interp: G[%d]=%d", a, G[a]);
+    g.G[a] = G[a];
+    g.x0[a] = ax[2 * a];
+    g.dx[a] = ax[2 * a + 1];
+    g.M *= G[a];
+  }
+  return FLPR_OK;
+}
+
+static int pt_blocks(int64_t n, int per_sm) {
+  int64_t b = (n + 255) / 256;
+  int64_t cap = (int64_t)per_sm * sm_count();
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+}  // namespace flpr
+
+using namespace flpr;
+
+extern "C" {
+
+size_t flpr_interp_reduce_ws(int64_t n, int H, int ny, int R) {
+  (void)n;
+  (void)H;
+  (void)ny;
+  (void)R;
+  return 0;
+}
+
+int flpr_interp_reduce(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G,
+                       int H, int ny, int R, const double* d_m, const double* const* h_ycols,
+                       const double* const* h_pcols, double* d_rss, double* d_pdot, double* d_pp,
+                       void* d_ws, size_t ws_bytes, void* stream) {
+  (void)d_ws;
+  (void)ws_bytes;
+  InterpGeom g;
+  FLPR_TRY(make_geom(g, d, h_ax, h_G));
+  FLPR_CHECK_ARG(n >= 1 && H >= 1 && ny >= 0 && R >= 0 && ny + R >= 1 && ny + R <= kMaxRed,
+                 "interp_reduce: n=%lld H=%d ny=%d R=%d", (long long)n, H, ny, R);
+  cudaStream_t s = as_stream(stream);
+  ColPtrs yc, pc;
+  memset(&yc, 0, sizeof(yc));
+  memset(&pc, 0, sizeof(pc));
+  for (int c = 0; c < ny; ++c) yc.col[c] = h_ycols[c];
+  for (int r = 0; r < R; ++r) pc.col[r] = h_pcols[r];
+  if (ny) FLPR_CUDA(cudaMemsetAsync(d_rss, 0, sizeof(double) * H * ny, s));
+  if (R) {
+    FLPR_CUDA(cudaMemsetAsync(d_pdot, 0, sizeof(double) * H * R, s));
+    FLPR_CUDA(cudaMemsetAsync(d_pp, 0, sizeof(double) * R, s));
+  }
+  int per_h = pt_blocks(n, 4);
+  per_h = (per_h + H - 1) / H * 1;
+  if (per_h < 8) per_h = 8;
+  dim3 grid(per_h, H);
+  interp_reduce_kernel<<<grid, 256, 0, s>>>(g, n, d_x, H, ny, R, d_m, yc, pc, d_rss, d_pdot);
+  FLPR_LAUNCH_CHECK();
+  if (R) {
+    probe_norm_kernel<<<pt_blocks(n, 4), 256, 0, s>>>(n, R, pc, d_pp);
+    FLPR_LAUNCH_CHECK();
+  }
+  return FLPR_OK;
+}
+
+int flpr_interp_eval(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G,
+                     int nval, const double* d_vals, double* d_out, void* stream) {
+  InterpGeom g;
+  FLPR_TRY(make_geom(g, d, h_ax, h_G));
+  FLPR_CHECK_ARG(n >= 1 && nval >= 1, "interp_eval: n=%lld nval=%d", (long long)n, nval);
+  interp_eval_kernel<<<pt_blocks(n, 8), 256, 0, as_stream(stream)>>>(g, n, d_x, nval, d_vals,
+                                                                      d_out);
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
+size_t flpr_kde_ws(int64_t n, int H, int64_t M) {
+  (void)n;
+  (void)M;
+  return align_up(sizeof(double) * (size_t)(H > 0 ? H : 1));
+}
+
+int flpr_kde_lcv(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G, int H,
+                 const double* d_s, double dxprod, const double* h_k0, double* d_f, double* d_lcv,
+                 void* d_ws, size_t ws_bytes, void* stream) {
+  InterpGeom g;
+  FLPR_TRY(make_geom(g, d, h_ax, h_G));
+  FLPR_CHECK_ARG(n >= 2 && H >= 1, "kde_lcv: n=%lld H=%d", (long long)n, H);
+  if (ws_bytes < flpr_kde_ws(n, H, g.M)) {
+    set_error("kde_lcv: workspace too small");
+    return FLPR_ERR_WORKSPACE;
+  }
+  cudaStream_t s = as_stream(stream);
+  double* sums = static_cast<double*>(d_ws);
+  FLPR_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * H, s));
+  FLPR_CUDA(cudaMemsetAsync(d_lcv, 0, sizeof(double) * 2 * H, s));
+  int gb = pt_blocks(g.M, 2);
+  gb = (gb + H - 1) / H;
+  if (gb < 4) gb = 4;
+  plane_sum_kernel<<<dim3(gb, H), 256, 0, s>>>(g.M, d_s, sums);
+  FLPR_LAUNCH_CHECK();
+  kde_normalize_kernel<<<pt_blocks((int64_t)H * g.M, 8), 256, 0, s>>>(g.M, H, d_s, sums, dxprod,
+                                                                      d_f);
+  FLPR_LAUNCH_CHECK();
+  const int per_h = 2 * sm_count() / (H < 8 ? H : 8) + 1;
+  for (int h0 = 0; h0 < H; h0 += 256) {
+    int hn = H - h0 < 256 ? H - h0 : 256;
+    K0s k0;
+    for (int j = 0; j < hn; ++j) k0.k0[j] = h_k0[h0 + j];
+    kde_lcv_kernel<<<dim3(per_h, hn), 256, 0, s>>>(g, n, d_x, d_f, h0, k0, d_lcv);
+    FLPR_LAUNCH_CHECK();
+  }
+  return FLPR_OK;
+}
+
+}  // extern "C"

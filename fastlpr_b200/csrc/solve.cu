@@ -1,0 +1,213 @@
+// Local polynomial solve at every (grid point, bandwidth).
+#include "common.cuh"
+
+namespace flpr {
+
+constexpr int kMaxNt = 10;
+constexpr int kMaxSolveChan = 64;
+
+// Order-preserving map of a double onto an unsigned 64-bit integer.
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double from_ordered(unsigned long long b) {
+  b = (b & 0x8000000000000000ull) ? (b & 0x7fffffffffffffffull) : ~b;
+  return __longlong_as_double((long long)b);
+}
+
+// max over one plane of |S| (use_abs) or S; NaN never wins.
+template <typename Real>
+__global__ void plane_max_kernel(int64_t plane_len, const Real* __restrict__ S, int use_abs,
+                                 unsigned long long* __restrict__ out) {
+  __shared__ unsigned long long sh[256];
+  unsigned long long best = ordered_bits(-INFINITY);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < plane_len;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double v = (double)S[i];
+    if (use_abs) v = fabs(v);
+    unsigned long long b = ordered_bits(v);
+    if (v == v && b > best) best = b;
+  }
+  sh[threadIdx.x] = best;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s && sh[threadIdx.x + s] > sh[threadIdx.x]) sh[threadIdx.x] = sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicMax(out, sh[0]);
+}
+
+__global__ void bits_init_kernel(unsigned long long* bits) { bits[0] = ordered_bits(-INFINITY); }
+
+__global__ void scalar_from_bits_kernel(const unsigned long long* bits, double factor, double* out) {
+  out[0] = from_ordered(bits[0]) * factor;
+}
+
+// z = A^-1 e1 for symmetric A (nt x nt, row-major), LDL' without pivoting;
+// falls back to Gaussian elimination with partial pivoting when a pivot is
+// zero or not finite.  Returns false if A is singular.
+__device__ bool solve_e1(int nt, double A[kMaxNt][kMaxNt], double z[kMaxNt]) {
+  double Lm[kMaxNt][kMaxNt];
+  double D[kMaxNt];
+  bool ok = true;
+  for (int j = 0; j < nt && ok; ++j) {
+    double dj = A[j][j];
+    for (int k = 0; k < j; ++k) dj -= Lm[j][k] * Lm[j][k] * D[k];
+    if (!(fabs(dj) > 0.0) || !isfinite(dj)) {
+      ok = false;
+      break;
+    }
+    D[j] = dj;
+    Lm[j][j] = 1.0;
+    for (int i = j + 1; i < nt; ++i) {
+      double v = A[i][j];
+      for (int k = 0; k < j; ++k) v -= Lm[i][k] * Lm[j][k] * D[k];
+      Lm[i][j] = v / dj;
+    }
+  }
+  if (ok) {
+    // L y = e1 ; D w = y ; L' z = w
+    double y[kMaxNt];
+    for (int i = 0; i < nt; ++i) {
+      double v = (i == 0) ? 1.0 : 0.0;
+      for (int k = 0; k < i; ++k) v -= Lm[i][k] * y[k];
+      y[i] = v;
+    }
+    for (int i = 0; i < nt; ++i) y[i] /= D[i];
+    for (int i = nt - 1; i >= 0; --i) {
+      double v = y[i];
+      for (int k = i + 1; k < nt; ++k) v -= Lm[k][i] * z[k];
+      z[i] = v;
+    }
+    return true;
+  }
+  // Gaussian elimination with partial pivoting on [A | e1]
+  double B[kMaxNt][kMaxNt + 1];
+  for (int i = 0; i < nt; ++i) {
+    for (int j = 0; j < nt; ++j) B[i][j] = A[i][j];
+    B[i][nt] = (i == 0) ? 1.0 : 0.0;
+  }
+  for (int c = 0; c < nt; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < nt; ++r)
+      if (fabs(B[r][c]) > fabs(B[piv][c])) piv = r;
+    if (!(fabs(B[piv][c]) > 0.0)) return false;
+    if (piv != c)
+      for (int j = 0; j <= nt; ++j) {
+        double t = B[c][j];
+        B[c][j] = B[piv][j];
+        B[piv][j] = t;
+      }
+    for (int r = c + 1; r < nt; ++r) {
+      double f = B[r][c] / B[c][c];
+      for (int j = c; j <= nt; ++j) B[r][j] -= f * B[c][j];
+    }
+  }
+  for (int i = nt - 1; i >= 0; --i) {
+    double v = B[i][nt];
+    for (int k = i + 1; k < nt; ++k) v -= B[i][k] * z[k];
+    z[i] = v / B[i][i];
+  }
+  return true;
+}
+
+// Thread per (bandwidth, grid point) for the first HT bandwidths.
+// S: (ns, H, M); T: (nt, C, HT, M); m: (HT, M, C) float64.
+template <typename Real>
+__global__ void solve_kernel(int order, int nt, int H, int HT, int64_t M, int C,
+                             const Real* __restrict__ S, const Real* __restrict__ T, double reg,
+                             const double* __restrict__ scalar, double* __restrict__ m) {
+  const int64_t HM = (int64_t)H * M;
+  const int64_t HTM = (int64_t)HT * M;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < HTM;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    double* mo = m + t * C;
+    if (order == 0) {
+      double thr = scalar[0] * reg;
+      double s = (double)S[t];
+      double den = s > thr ? s : thr;
+      for (int c = 0; c < C; ++c) mo[c] = (double)T[(int64_t)c * HTM + t] / den;
+      continue;
+    }
+    const double lam = scalar[0];
+    double A[kMaxNt][kMaxNt];
+    int k = 0;
+    for (int j = 0; j < nt; ++j)
+      for (int i = j; i < nt; ++i) {
+        double v = (double)S[(int64_t)k * HM + t];
+        A[i][j] = v;
+        A[j][i] = v;
+        ++k;
+      }
+    for (int i = 0; i < nt; ++i) A[i][i] += lam;
+    double z[kMaxNt];
+    bool ok = solve_e1(nt, A, z);
+    for (int c = 0; c < C; ++c) {
+      double v = 0.0;
+      if (ok) {
+        for (int i = 0; i < nt; ++i) v += z[i] * (double)T[((int64_t)i * C + c) * HTM + t];
+      } else {
+        v = NAN;
+      }
+      mo[c] = v;
+    }
+  }
+}
+
+static int blocks_for(int64_t total, int per_sm) {
+  int64_t b = (total + 255) / 256;
+  int64_t cap = (int64_t)per_sm * sm_count();
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+}  // namespace flpr
+
+using namespace flpr;
+
+extern "C" {
+
+int flpr_solve(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,
+               const void* d_T, double reg, double* d_m, double* d_scalar, int prec,
+               void* stream) {
+  FLPR_CHECK_ARG(order >= 0 && order <= 2, "solve: order=%d", order);
+  FLPR_CHECK_ARG(nt >= 1 && nt <= kMaxNt, "solve: nt=%d", nt);
+  FLPR_CHECK_ARG(order > 0 || nt == 1, "solve: order 0 needs nt=1");
+  FLPR_CHECK_ARG(H >= 1 && M >= 1 && C >= 1 && C <= kMaxSolveChan, "solve: H=%d M=%lld C=%d", H,
+                 (long long)M, C);
+  FLPR_CHECK_ARG(HT >= 1 && HT <= H, "solve: HT=%d not in [1, H=%d]", HT, H);
+  cudaStream_t s = as_stream(stream);
+  // d_scalar first holds the running maximum as ordered bits, then the
+  // scalar itself: lambda = 1e-6 * max |diag S| (order >= 1, regression.py:243-267)
+  // or max S (order 0, regression.py:207-212).
+  unsigned long long* bits = reinterpret_cast<unsigned long long*>(d_scalar);
+  bits_init_kernel<<<1, 1, 0, s>>>(bits);
+  FLPR_LAUNCH_CHECK();
+  const int64_t plane = (int64_t)H * M;
+  const int nb = blocks_for(plane, 4);
+  for (int k = 0; k < nt; ++k) {
+    const int64_t off = (int64_t)(k * nt - k * (k - 1) / 2) * plane;  // diagonal element k
+    if (prec == FLPR_PREC_F32) {
+      plane_max_kernel<float><<<nb, 256, 0, s>>>(plane, (const float*)d_S + off, order > 0, bits);
+    } else {
+      plane_max_kernel<double><<<nb, 256, 0, s>>>(plane, (const double*)d_S + off, order > 0, bits);
+    }
+    FLPR_LAUNCH_CHECK();
+  }
+  scalar_from_bits_kernel<<<1, 1, 0, s>>>(bits, order > 0 ? 1e-6 : 1.0, d_scalar);
+  FLPR_LAUNCH_CHECK();
+  int sb = blocks_for((int64_t)HT * M, 8);
+  if (prec == FLPR_PREC_F32) {
+    solve_kernel<float><<<sb, 256, 0, s>>>(order, nt, H, HT, M, C, (const float*)d_S,
+                                           (const float*)d_T, reg, d_scalar, d_m);
+  } else {
+    solve_kernel<double><<<sb, 256, 0, s>>>(order, nt, H, HT, M, C, (const double*)d_S,
+                                            (const double*)d_T, reg, d_scalar, d_m);
+  }
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
+}  // extern "C"

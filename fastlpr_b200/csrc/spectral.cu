@@ -1,0 +1,345 @@
+// Forward FFT of the spread grids, separable kernel-moment spectra and the
+// batched spectral multiply + inverse FFT + crop.
+#include "common.cuh"
+#include "plans.cuh"
+
+namespace flpr {
+
+template <typename T>
+struct Cplx;
+template <>
+struct Cplx<float> {
+  using type = float2;
+};
+template <>
+struct Cplx<double> {
+  using type = double2;
+};
+
+// ---- kernel factors -------------------------------------------------------
+struct FactorArgs {
+  int d;
+  int G[3], L[3];
+  int64_t off[3];  // start of axis a in d_F (elements)
+  double lo[3], hi[3];
+  int H, npow;
+};
+
+// One block per (axis, h, pow): sample exp(-u^2/2) u^p / h on the linspace
+// grid, zero padded with floor((L-G)/2)+1 leading zeros.
+__global__ void factor_sample_kernel(FactorArgs fa, const double* __restrict__ h,
+                                     double2* __restrict__ F, double* __restrict__ sum0) {
+  const int row = blockIdx.x;  // (a, hi, p)
+  const int per_axis = fa.H * fa.npow;
+  const int a = row / per_axis;
+  const int r = row - a * per_axis;
+  const int hidx = r / fa.npow;
+  const int p = r - hidx * fa.npow;
+  const int G = fa.G[a], L = fa.L[a];
+  const int before = (L - G) / 2 + 1;
+  const double hv = h[hidx * fa.d + a];
+  const double lo = fa.lo[a], hi = fa.hi[a];
+  const double step = G > 1 ? (hi - lo) / (double)(G - 1) : 0.0;
+  double2* out = F + fa.off[a] + (int64_t)r * L;
+  __shared__ double sh[256];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < L; i += blockDim.x) {
+    int k = i - before;
+    double v = 0.0;
+    if (k >= 0 && k < G) {
+      double g = (k == G - 1 && G > 1) ? hi : dadd(dmul((double)k, step), lo);
+      double u = ddiv(g, hv);
+      double e = exp(dmul(-0.5, dmul(u, u)));
+      double pw = 1.0;
+      for (int q = 0; q < p; ++q) pw = dmul(pw, u);
+      v = ddiv(dmul(e, pw), hv);
+      if (p == 0) acc += v;
+    }
+    out[i] = make_double2(v, 0.0);
+  }
+  if (p == 0) {
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) sum0[a * fa.H + hidx] = sh[0];
+  }
+}
+
+// ---- products -------------------------------------------------------------
+struct ProdDesc {
+  int chan;
+  int hidx;
+  int pw[3];
+};
+
+constexpr int kMaxBatch = 128;
+
+struct ProdBatch {
+  ProdDesc p[kMaxBatch];
+};
+
+struct ConvArgs {
+  int d;
+  int L[3];
+  int G[3];
+  int qout[3];
+  int H, npow;
+  int64_t half;   // elements of one half spectrum
+  int64_t cells;  // prod(L)
+  int64_t M;      // prod(G)
+  int64_t foff[3];
+  double scale;
+};
+
+template <typename Real>
+__global__ void product_kernel(ConvArgs ca, int nb, ProdBatch desc,
+                               const typename Cplx<Real>::type* __restrict__ spec,
+                               const double2* __restrict__ F,
+                               typename Cplx<Real>::type* __restrict__ out) {
+  using C = typename Cplx<Real>::type;
+  const int64_t total = (int64_t)nb * ca.half;
+  const int Llast_half = ca.L[ca.d - 1] / 2 + 1;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int b = (int)(t / ca.half);
+    int64_t w = t - (int64_t)b * ca.half;
+    const ProdDesc pd = desc.p[b];
+    // decode frequency index (row-major, last axis half length)
+    int om[3] = {0, 0, 0};
+    {
+      int64_t r = w;
+      om[ca.d - 1] = (int)(r % Llast_half);
+      r /= Llast_half;
+      for (int a = ca.d - 2; a >= 0; --a) {
+        om[a] = (int)(r % ca.L[a]);
+        r /= ca.L[a];
+      }
+    }
+    double kr = ca.scale, ki = 0.0;
+    for (int a = 0; a < ca.d; ++a) {
+      double2 f = F[ca.foff[a] + ((int64_t)pd.hidx * ca.npow + pd.pw[a]) * ca.L[a] + om[a]];
+      double nr = kr * f.x - ki * f.y;
+      double ni = kr * f.y + ki * f.x;
+      kr = nr;
+      ki = ni;
+    }
+    C s = spec[(int64_t)pd.chan * ca.half + w];
+    C o;
+    o.x = (Real)((double)s.x * kr - (double)s.y * ki);
+    o.y = (Real)((double)s.x * ki + (double)s.y * kr);
+    out[t] = o;
+  }
+}
+
+template <typename Real>
+__global__ void crop_kernel(ConvArgs ca, int nb, int p0, const Real* __restrict__ full,
+                            int add_eps, Real* __restrict__ out) {
+  const int64_t total = (int64_t)nb * ca.M;
+  const double eps = 2.220446049250313e-16;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int b = (int)(t / ca.M);
+    int64_t g = t - (int64_t)b * ca.M;
+    int gc[3] = {0, 0, 0};
+    for (int a = ca.d - 1; a >= 0; --a) {
+      gc[a] = (int)(g % ca.G[a]);
+      g /= ca.G[a];
+    }
+    int64_t src = 0;
+    for (int a = 0; a < ca.d; ++a) src = src * ca.L[a] + (gc[a] + ca.qout[a]);
+    Real v = full[(int64_t)b * ca.cells + src];
+    if (add_eps) v = (Real)((double)v + eps);
+    out[(int64_t)(p0 + b) * ca.M + (t - (int64_t)b * ca.M)] = v;
+  }
+}
+
+static int conv_batch(int d, const int* L, int nprod, int prec) {
+  int64_t cells = prod(L, d);
+  int64_t half = cells / L[d - 1] * (L[d - 1] / 2 + 1);
+  size_t es = prec == FLPR_PREC_F32 ? 4 : 8;
+  size_t per = (size_t)half * 2 * es + (size_t)cells * es;
+  size_t budget = (size_t)1536 << 20;
+  int64_t b = (int64_t)(budget / per);
+  if (b < 1) b = 1;
+  if (b > nprod) b = nprod;
+  if (b > kMaxBatch) b = kMaxBatch;
+  return (int)b;
+}
+
+static int grid_blocks(int64_t total) {
+  int64_t b = (total + 255) / 256;
+  int64_t cap = 32 * (int64_t)sm_count();
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+}  // namespace flpr
+
+using namespace flpr;
+
+extern "C" {
+
+size_t flpr_forward_fft_ws(flpr_handle_t handle, int d, const int* h_L, int nchan, int prec) {
+  size_t w = 0;
+  PlanKey k = grid_plan(d, h_L, prec == FLPR_PREC_F32 ? CUFFT_R2C : CUFFT_D2Z, nchan);
+  if (plans_of(handle).work_size(k, &w) != FLPR_OK) return 0;
+  return align_up(w);
+}
+
+int flpr_forward_fft(flpr_handle_t handle, int d, const int* h_L, int nchan, void* d_grid,
+                     void* d_spec, int prec, void* d_ws, size_t ws_bytes, void* stream) {
+  FLPR_CHECK_ARG(d >= 1 && d <= 3, "forward_fft: d=%d", d);
+  FLPR_CHECK_ARG(nchan >= 1, "forward_fft: nchan=%d", nchan);
+  PlanKey k = grid_plan(d, h_L, prec == FLPR_PREC_F32 ? CUFFT_R2C : CUFFT_D2Z, nchan);
+  return plans_of(handle).exec(k, d_grid, d_spec, d_ws, ws_bytes, as_stream(stream));
+}
+
+static PlanKey factor_plan(int L, int batch) {
+  PlanKey k{};
+  k.rank = 1;
+  k.n[0] = L;
+  k.type = CUFFT_Z2Z;
+  k.batch = batch;
+  k.idist = L;
+  k.odist = L;
+  return k;
+}
+
+size_t flpr_kernel_factors_ws(flpr_handle_t handle, int d, const int* h_L, int H, int npow) {
+  size_t mx = 0;
+  for (int a = 0; a < d; ++a) {
+    size_t w = 0;
+    if (plans_of(handle).work_size(factor_plan(h_L[a], H * npow), &w) != FLPR_OK) return 0;
+    if (w > mx) mx = w;
+  }
+  return align_up(mx);
+}
+
+int flpr_kernel_factors(flpr_handle_t handle, int d, const int* h_G, const int* h_L,
+                        const double* h_lo, const double* h_hi, int H, const double* d_h,
+                        int npow, void* d_F, double* d_sum0, void* d_ws, size_t ws_bytes,
+                        void* stream) {
+  FLPR_CHECK_ARG(d >= 1 && d <= 3, "kernel_factors: d=%d", d);
+  FLPR_CHECK_ARG(H >= 1 && npow >= 1 && npow <= 8, "kernel_factors: H=%d npow=%d", H, npow);
+  FactorArgs fa{};
+  fa.d = d;
+  fa.H = H;
+  fa.npow = npow;
+  int64_t off = 0;
+  for (int a = 0; a < d; ++a) {
+    FLPR_CHECK_ARG(h_G[a] >= 1 && h_L[a] >= h_G[a] + 1, "kernel_factors: G=%d L=%d", h_G[a],
+                   h_L[a]);
+    fa.G[a] = h_G[a];
+    fa.L[a] = h_L[a];
+    fa.lo[a] = h_lo[a];
+    fa.hi[a] = h_hi[a];
+    fa.off[a] = off;
+    off += (int64_t)H * npow * h_L[a];
+  }
+  cudaStream_t s = as_stream(stream);
+  factor_sample_kernel<<<d * H * npow, 256, 0, s>>>(fa, d_h, (double2*)d_F, d_sum0);
+  FLPR_LAUNCH_CHECK();
+  for (int a = 0; a < d; ++a) {
+    double2* base = (double2*)d_F + fa.off[a];
+    FLPR_TRY(plans_of(handle).exec(factor_plan(h_L[a], H * npow), base, base, d_ws, ws_bytes, s));
+  }
+  return FLPR_OK;
+}
+
+size_t flpr_conv_ws(flpr_handle_t handle, int d, const int* h_L, int nprod, int prec) {
+  if (d < 1 || d > 3 || nprod < 1) return 0;
+  int B = conv_batch(d, h_L, nprod, prec);
+  int64_t cells = prod(h_L, d);
+  int64_t half = cells / h_L[d - 1] * (h_L[d - 1] / 2 + 1);
+  size_t es = prec == FLPR_PREC_F32 ? 4 : 8;
+  ArenaSize ar;
+  ar.take<char>((size_t)B * half * 2 * es);
+  ar.take<char>((size_t)B * cells * es);
+  int type = prec == FLPR_PREC_F32 ? CUFFT_C2R : CUFFT_Z2D;
+  size_t w1 = 0, w2 = 0;
+  if (plans_of(handle).work_size(grid_plan(d, h_L, type, B), &w1) != FLPR_OK) return 0;
+  int tail = nprod % B;
+  if (tail && plans_of(handle).work_size(grid_plan(d, h_L, type, tail), &w2) != FLPR_OK) return 0;
+  ar.take<char>(w1 > w2 ? w1 : w2);
+  return ar.used;
+}
+
+int flpr_conv(flpr_handle_t handle, int d, const int* h_G, const int* h_L, const int* h_qout,
+              int H, int npow, const void* d_spec, const void* d_F, int nprod,
+              const int* h_chan, const int* h_hidx, const int* h_pow, double scale, int add_eps,
+              void* d_out, int prec, void* d_ws, size_t ws_bytes, void* stream) {
+  FLPR_CHECK_ARG(d >= 1 && d <= 3, "conv: d=%d", d);
+  FLPR_CHECK_ARG(nprod >= 1, "conv: nprod=%d", nprod);
+  ConvArgs ca{};
+  ca.d = d;
+  ca.H = H;
+  ca.npow = npow;
+  ca.scale = scale;
+  int64_t off = 0;
+  for (int a = 0; a < d; ++a) {
+    FLPR_CHECK_ARG(h_qout[a] >= 0 && h_qout[a] + h_G[a] <= h_L[a], "conv: crop window");
+    ca.L[a] = h_L[a];
+    ca.G[a] = h_G[a];
+    ca.qout[a] = h_qout[a];
+    ca.foff[a] = off;
+    off += (int64_t)H * npow * h_L[a];
+  }
+  ca.cells = prod(h_L, d);
+  ca.M = prod(h_G, d);
+  ca.half = ca.cells / h_L[d - 1] * (h_L[d - 1] / 2 + 1);
+  for (int p = 0; p < nprod; ++p) {
+    FLPR_CHECK_ARG(h_hidx[p] >= 0 && h_hidx[p] < H, "conv: hidx[%d]=%d", p, h_hidx[p]);
+    for (int a = 0; a < d; ++a)
+      FLPR_CHECK_ARG(h_pow[p * d + a] >= 0 && h_pow[p * d + a] < npow, "conv: pow out of range");
+  }
+  if (ws_bytes < flpr_conv_ws(handle, d, h_L, nprod, prec)) {
+    set_error("conv: workspace too small");
+    return FLPR_ERR_WORKSPACE;
+  }
+  const int B = conv_batch(d, h_L, nprod, prec);
+  const size_t es = prec == FLPR_PREC_F32 ? 4 : 8;
+  Arena ar(d_ws, ws_bytes);
+  char* pbuf = ar.take<char>((size_t)B * ca.half * 2 * es);
+  char* rbuf = ar.take<char>((size_t)B * ca.cells * es);
+  size_t work_bytes = ar.size - align_up(ar.used);
+  char* work = ar.take<char>(1);
+  cudaStream_t s = as_stream(stream);
+  ProdBatch batch;
+  const int ctype = prec == FLPR_PREC_F32 ? CUFFT_C2R : CUFFT_Z2D;
+  for (int p0 = 0; p0 < nprod; p0 += B) {
+    int nb = nprod - p0 < B ? nprod - p0 : B;
+    for (int b = 0; b < nb; ++b) {
+      ProdDesc pd{};
+      pd.chan = h_chan[p0 + b];
+      pd.hidx = h_hidx[p0 + b];
+      for (int a = 0; a < 3; ++a) pd.pw[a] = a < d ? h_pow[(p0 + b) * d + a] : 0;
+      batch.p[b] = pd;
+    }
+    int blocks = grid_blocks((int64_t)nb * ca.half);
+    if (prec == FLPR_PREC_F32) {
+      product_kernel<float><<<blocks, 256, 0, s>>>(ca, nb, batch, (const float2*)d_spec,
+                                                   (const double2*)d_F, (float2*)pbuf);
+    } else {
+      product_kernel<double><<<blocks, 256, 0, s>>>(ca, nb, batch, (const double2*)d_spec,
+                                                    (const double2*)d_F, (double2*)pbuf);
+    }
+    FLPR_LAUNCH_CHECK();
+    FLPR_TRY(plans_of(handle).exec(grid_plan(d, h_L, ctype, nb), pbuf, rbuf, work, work_bytes, s));
+    int cb = grid_blocks((int64_t)nb * ca.M);
+    if (prec == FLPR_PREC_F32) {
+      crop_kernel<float><<<cb, 256, 0, s>>>(ca, nb, p0, (const float*)rbuf, add_eps,
+                                            (float*)d_out);
+    } else {
+      crop_kernel<double><<<cb, 256, 0, s>>>(ca, nb, p0, (const double*)rbuf, add_eps,
+                                             (double*)d_out);
+    }
+    FLPR_LAUNCH_CHECK();
+  }
+  return FLPR_OK;
+}
+
+}  // extern "C"

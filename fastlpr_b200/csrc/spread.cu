@@ -1,0 +1,527 @@
+// Gaussian-gridding spread (NUFFT type-1 spreading) of many channels.
+//
+// Pipeline (all on one stream):
+//   1. bin_count   : knot mapping per point, home cell -> tile id, tile
+//                    histogram; per-channel sum |v| (sets the fixed-point
+//                    scale of the FP32 path).
+//   2. tile_scan   : exclusive scans of the histogram and of the number of
+//                    work items per tile (a tile is split into chunks of at
+//                    most kItemPoints points).
+//   3. bin_scatter : point indices sorted by tile.
+//   4. tile_accumulate : one CTA per work item; every point of the chunk is
+//                    spread into a shared-memory copy of its tile plus a
+//                    halo of msp cells (one warp per point, lanes over taps),
+//                    then the tile is added to the global accumulator with
+//                    one atomic per non-zero cell.
+//   5. finalize    : accumulator -> real grid (float or double) times 1/n.
+//
+// FLPR_PREC_F32 accumulates 64-bit fixed point: integer addition is
+// associative, so the result does not depend on the order of the atomics
+// and the grid is deterministic.  FLPR_PREC_F64 accumulates float64.
+#include "common.cuh"
+
+namespace flpr {
+
+constexpr int kItemPoints = 4096;
+constexpr int kSpreadThreads = 256;
+constexpr int kMaxTaps1 = 13;  // 2*msp+1 for msp <= 6
+constexpr int kWarpScratch = 3 * kMaxTaps1 + 32;
+
+struct SpreadGeom {
+  int d;
+  int L[3];
+  int T[3];        // tile extent per axis
+  int ntile[3];    // tiles per axis
+  int W[3];        // tile + halo extent per axis
+  int msp;
+  int ntaps1;      // 2*msp+1
+  int64_t cells;   // prod(L)
+  int tile_cells;  // prod(W)
+  int ntiles;
+  double four_tau[3];
+  KnotAxis ax[3];
+};
+
+struct ChanPtrs {
+  const double* col[FLPR_MAX_CHANNELS];
+};
+
+// Home cell and tile of a point; also its unwrapped knot index m.
+__device__ __forceinline__ int point_tile(const SpreadGeom& g, const double* __restrict__ x,
+                                          int64_t i, int* m_out, double* k_out) {
+  int tile = 0;
+  for (int a = 0; a < g.d; ++a) {
+    double k = knot_of(x[i * g.d + a], g.ax[a]);
+    int m = (int)rint(ddiv(k, g.ax[a].hx));
+    int home = m % g.L[a];
+    if (home < 0) home += g.L[a];
+    tile = tile * g.ntile[a] + home / g.T[a];
+    if (m_out) m_out[a] = m;
+    if (k_out) k_out[a] = k;
+  }
+  return tile;
+}
+
+__global__ void bin_count_kernel(SpreadGeom g, int64_t n, const double* __restrict__ x,
+                                 int* __restrict__ point_tile_out, int* __restrict__ counts,
+                                 int nchan, int ones_channel, ChanPtrs cp,
+                                 double* __restrict__ absum) {
+  __shared__ double sh_abs[FLPR_MAX_CHANNELS];
+  for (int c = threadIdx.x; c < nchan; c += blockDim.x) sh_abs[c] = 0.0;
+  __syncthreads();
+  int nv = nchan - ones_channel;
+  double local[8];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int t = point_tile(g, x, i, nullptr, nullptr);
+    point_tile_out[i] = t;
+    atomicAdd(&counts[t], 1);
+  }
+  if (absum != nullptr) {
+    // per-channel sum of |v| in chunks of 8 channels per sweep
+    for (int c0 = 0; c0 < nv; c0 += 8) {
+      int cn = min(8, nv - c0);
+      for (int c = 0; c < 8; ++c) local[c] = 0.0;
+      for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+           i += (int64_t)gridDim.x * blockDim.x)
+        for (int c = 0; c < cn; ++c) local[c] += fabs(cp.col[c0 + c][i]);
+      for (int c = 0; c < cn; ++c) {
+        double v = local[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&sh_abs[ones_channel + c0 + c], v);
+      }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < nchan; c += blockDim.x) {
+      if (ones_channel && c == 0) {
+        if (blockIdx.x == 0) atomicAdd(&absum[0], (double)n);
+      } else {
+        atomicAdd(&absum[c], sh_abs[c]);
+      }
+    }
+  }
+}
+
+// Single-block exclusive scans over the tile histogram.
+__global__ void tile_scan_kernel(int ntiles, const int* __restrict__ counts,
+                                 int* __restrict__ offsets, int* __restrict__ items,
+                                 int* __restrict__ cursor) {
+  __shared__ int sh_a[1024];
+  __shared__ int sh_b[1024];
+  __shared__ int carry_a, carry_b;
+  if (threadIdx.x == 0) {
+    carry_a = 0;
+    carry_b = 0;
+  }
+  __syncthreads();
+  for (int base = 0; base < ntiles; base += blockDim.x) {
+    int t = base + threadIdx.x;
+    int c = t < ntiles ? counts[t] : 0;
+    int a = c;
+    int b = (c + kItemPoints - 1) / kItemPoints;
+    sh_a[threadIdx.x] = a;
+    sh_b[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = 1; s < blockDim.x; s <<= 1) {
+      int va = threadIdx.x >= s ? sh_a[threadIdx.x - s] : 0;
+      int vb = threadIdx.x >= s ? sh_b[threadIdx.x - s] : 0;
+      __syncthreads();
+      sh_a[threadIdx.x] += va;
+      sh_b[threadIdx.x] += vb;
+      __syncthreads();
+    }
+    if (t < ntiles) {
+      offsets[t] = carry_a + sh_a[threadIdx.x] - a;
+      items[t] = carry_b + sh_b[threadIdx.x] - b;
+      cursor[t] = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) {
+      carry_a += sh_a[threadIdx.x];
+      carry_b += sh_b[threadIdx.x];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    offsets[ntiles] = carry_a;
+    items[ntiles] = carry_b;
+  }
+}
+
+__global__ void bin_scatter_kernel(int64_t n, const int* __restrict__ point_tile_in,
+                                   const int* __restrict__ offsets, int* __restrict__ cursor,
+                                   int* __restrict__ sorted) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int t = point_tile_in[i];
+    int pos = offsets[t] + atomicAdd(&cursor[t], 1);
+    sorted[pos] = (int)i;
+  }
+}
+
+template <typename Acc>
+struct AccOps;
+
+template <>
+struct AccOps<long long> {
+  __device__ static void add_shared(long long* p, double v, double scale) {
+    long long q = __double2ll_rn(v * scale);
+    if (q != 0) atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)q);
+  }
+  __device__ static void add_global(long long* p, long long v) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)v);
+  }
+};
+
+template <>
+struct AccOps<double> {
+  __device__ static void add_shared(double* p, double v, double) { atomicAdd(p, v); }
+  __device__ static void add_global(double* p, double v) { atomicAdd(p, v); }
+};
+
+// Fixed-point scale 2^e per channel so that |sum| over any subset of
+// contributions stays below 2^62 (each point adds at most |v| to a cell when
+// the taps do not wrap onto the same cell).
+__device__ __forceinline__ double fixed_scale(double absum, int margin_bits) {
+  if (!(absum > 0.0)) return 1.0;
+  int e = 0;
+  frexp(absum, &e);  // absum < 2^e
+  return ldexp(1.0, 62 - e - margin_bits);
+}
+
+template <typename Acc>
+__global__ void __launch_bounds__(kSpreadThreads)
+tile_accumulate_kernel(SpreadGeom g, const double* __restrict__ x, int nchan, int ones_channel,
+                       ChanPtrs cp, int cgroup, const int* __restrict__ sorted,
+                       const int* __restrict__ offsets, const int* __restrict__ items,
+                       const double* __restrict__ absum, int margin_bits,
+                       Acc* __restrict__ gacc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Acc* acc = reinterpret_cast<Acc*>(smem_raw);
+  const int c_begin = blockIdx.y * cgroup;
+  const int c_end = min(nchan, c_begin + cgroup);
+  const int nc = c_end - c_begin;
+  const int tc = g.tile_cells;
+  double* wscr = reinterpret_cast<double*>(smem_raw + sizeof(Acc) * (size_t)cgroup * tc);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  double* my_w = wscr + warp * kWarpScratch;   // per-axis weights
+  double* my_v = my_w + 3 * kMaxTaps1;          // channel values of the point
+
+  const int item = blockIdx.x;
+  const int total_items = items[g.ntiles];
+  if (item >= total_items) return;
+  // tile owning this item: largest t with items[t] <= item
+  int lo = 0, hi = g.ntiles;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (items[mid] <= item) lo = mid; else hi = mid;
+  }
+  const int tile = lo;
+  const int chunk = item - items[tile];
+  const int p_begin = offsets[tile] + chunk * kItemPoints;
+  const int p_end = min(offsets[tile + 1], p_begin + kItemPoints);
+
+  int tcoord[3] = {0, 0, 0};
+  {
+    int r = tile;
+    for (int a = g.d - 1; a >= 0; --a) {
+      tcoord[a] = r % g.ntile[a];
+      r /= g.ntile[a];
+    }
+  }
+  for (int i = threadIdx.x; i < nc * tc; i += blockDim.x) acc[i] = Acc(0);
+
+  double scale[32];
+  for (int c = 0; c < nc; ++c) scale[c] = fixed_scale(absum ? absum[c_begin + c] : 0.0, margin_bits);
+  __syncthreads();
+
+  const int ntap1 = g.ntaps1;
+  int ntaps = ntap1;
+  for (int a = 1; a < g.d; ++a) ntaps *= ntap1;
+  const int W1 = g.W[1], W2 = g.W[2];
+
+  for (int p = p_begin + warp; p < p_end; p += nwarps) {
+    const int i = sorted[p];
+    int m[3];
+    double k[3];
+    point_tile(g, x, i, m, k);
+    // local origin of the taps inside the smem tile
+    int base[3] = {0, 0, 0};
+    for (int a = 0; a < g.d; ++a) {
+      int home = m[a] % g.L[a];
+      if (home < 0) home += g.L[a];
+      int origin = tcoord[a] * g.T[a] + (m[a] - home);  // unwrapped tile origin
+      base[a] = m[a] - origin;                          // local index of tap j=-msp
+    }
+    // per-axis weights exp(-diff^2/(4 tau)), diff = k - hx*(m+j)
+    for (int t = lane; t < g.d * ntap1; t += 32) {
+      int a = t / ntap1, j = t % ntap1 - g.msp;
+      double diff = dsub(k[a], dmul(g.ax[a].hx, (double)(m[a] + j)));
+      my_w[a * kMaxTaps1 + j + g.msp] = exp(-ddiv(dmul(diff, diff), g.four_tau[a]));
+    }
+    if (lane < nc) {
+      int c = c_begin + lane;
+      my_v[lane] = (ones_channel && c == 0) ? 1.0 : cp.col[c - ones_channel][i];
+    }
+    __syncwarp();
+    for (int t = lane; t < ntaps; t += 32) {
+      int j0, j1 = 0, j2 = 0;
+      if (g.d == 1) {
+        j0 = t;
+      } else if (g.d == 2) {
+        j0 = t / ntap1;
+        j1 = t - j0 * ntap1;
+      } else {
+        j0 = t / (ntap1 * ntap1);
+        int r = t - j0 * ntap1 * ntap1;
+        j1 = r / ntap1;
+        j2 = r - j1 * ntap1;
+      }
+      double w = my_w[j0];
+      int cell = base[0] + j0;
+      if (g.d >= 2) {
+        w *= my_w[kMaxTaps1 + j1];
+        cell = cell * W1 + base[1] + j1;
+      }
+      if (g.d == 3) {
+        w *= my_w[2 * kMaxTaps1 + j2];
+        cell = cell * W2 + base[2] + j2;
+      }
+      for (int c = 0; c < nc; ++c)
+        AccOps<Acc>::add_shared(&acc[c * tc + cell], my_v[c] * w, scale[c]);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // flush: one global atomic per non-zero cell of the tile + halo
+  for (int idx = threadIdx.x; idx < nc * tc; idx += blockDim.x) {
+    Acc v = acc[idx];
+    if (v == Acc(0)) continue;
+    int c = idx / tc;
+    int r = idx - c * tc;
+    int64_t gi = 0;
+    int loc[3] = {0, 0, 0};
+    for (int a = g.d - 1; a >= 0; --a) {
+      loc[a] = r % g.W[a];
+      r /= g.W[a];
+    }
+    for (int a = 0; a < g.d; ++a) {
+      int gc = tcoord[a] * g.T[a] + loc[a] - g.msp;
+      gc %= g.L[a];
+      if (gc < 0) gc += g.L[a];
+      gi = gi * g.L[a] + gc;
+    }
+    AccOps<Acc>::add_global(&gacc[(int64_t)(c_begin + c) * g.cells + gi], v);
+  }
+}
+
+template <typename Acc, typename Out, bool kFixed>
+__global__ void finalize_kernel(int nchan, int64_t cells, const Acc* __restrict__ gacc,
+                                const double* __restrict__ absum, int margin_bits, double inv_n,
+                                Out* __restrict__ out) {
+  int64_t total = (int64_t)nchan * cells;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int c = (int)(i / cells);
+    double v;
+    if (kFixed) {
+      v = (double)gacc[i] / fixed_scale(absum[c], margin_bits);
+    } else {
+      v = (double)gacc[i];
+    }
+    out[i] = (Out)(v * inv_n);
+  }
+}
+
+static void make_geom(SpreadGeom& g, int d, const int* L, int msp, const double* tau,
+                      const double* kmap) {
+  memset(&g, 0, sizeof(g));
+  g.d = d;
+  g.msp = msp;
+  g.ntaps1 = 2 * msp + 1;
+  static const int tile2[3] = {32, 32, 1};
+  static const int tile3[3] = {8, 8, 8};
+  g.cells = 1;
+  g.tile_cells = 1;
+  g.ntiles = 1;
+  for (int a = 0; a < 3; ++a) {
+    if (a < d) {
+      g.L[a] = L[a];
+      int T = d == 1 ? 512 : (d == 2 ? tile2[a] : tile3[a]);
+      if (T > L[a]) T = L[a];
+      g.T[a] = T;
+      g.ntile[a] = (L[a] + T - 1) / T;
+      g.W[a] = T + 2 * msp;
+      g.cells *= L[a];
+      g.tile_cells *= g.W[a];
+      g.ntiles *= g.ntile[a];
+      g.four_tau[a] = 4.0 * tau[a];
+      const double* k = kmap + 9 * a;
+      g.ax[a] = KnotAxis{k[0], k[1], k[2], k[3], k[4], k[5], k[6], k[7], k[8]};
+    } else {
+      g.L[a] = 1;
+      g.T[a] = 1;
+      g.ntile[a] = 1;
+      g.W[a] = 1;
+    }
+  }
+}
+
+static int margin_bits_for(const SpreadGeom& g) {
+  int m = 1;
+  for (int a = 0; a < g.d; ++a)
+    if (g.L[a] < g.ntaps1) m += 4;  // taps wrap onto the same cell
+  return m;
+}
+
+static int channel_group(const SpreadGeom& g, int nchan, size_t acc_bytes) {
+  size_t budget = 200 * 1024 - (size_t)(kSpreadThreads / 32) * kWarpScratch * sizeof(double);
+  int cg = (int)(budget / (acc_bytes * (size_t)g.tile_cells));
+  if (cg > 32) cg = 32;
+  if (cg > nchan) cg = nchan;
+  return cg;
+}
+
+struct SpreadWs {
+  int* point_tile;
+  int* counts;
+  int* offsets;
+  int* items;
+  int* cursor;
+  int* sorted;
+  double* absum;
+  void* gacc;
+};
+
+template <typename A>
+static void spread_layout(A& ar, int64_t n, int ntiles, int nchan, int64_t cells,
+                          SpreadWs* w) {
+  auto p0 = ar.template take<int>(n);
+  auto p1 = ar.template take<int>(ntiles);
+  auto p2 = ar.template take<int>(ntiles + 1);
+  auto p3 = ar.template take<int>(ntiles + 1);
+  auto p4 = ar.template take<int>(ntiles);
+  auto p5 = ar.template take<int>(n);
+  auto p6 = ar.template take<double>(FLPR_MAX_CHANNELS);
+  auto p7 = ar.template take<double>((size_t)nchan * cells);
+  if (w) {
+    w->point_tile = (int*)p0;
+    w->counts = (int*)p1;
+    w->offsets = (int*)p2;
+    w->items = (int*)p3;
+    w->cursor = (int*)p4;
+    w->sorted = (int*)p5;
+    w->absum = (double*)p6;
+    w->gacc = (void*)p7;
+  }
+}
+
+struct SizeArena {
+  size_t used = 0;
+  template <typename T>
+  T* take(size_t count) {
+    used = align_up(used) + align_up(count * sizeof(T));
+    return nullptr;
+  }
+};
+
+}  // namespace flpr
+
+using namespace flpr;
+
+extern "C" {
+
+size_t flpr_spread_ws(int d, int64_t n, const int* h_L, int msp, int nchan, int prec) {
+  (void)prec;
+  if (d < 1 || d > 3 || n < 1 || nchan < 1) return 0;
+  SpreadGeom g;
+  double tau[3] = {1, 1, 1}, kmap[27] = {0};
+  make_geom(g, d, h_L, msp, tau, kmap);
+  SizeArena ar;
+  spread_layout(ar, n, g.ntiles, nchan, g.cells, nullptr);
+  return ar.used;
+}
+
+int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const int* h_L,
+                int msp, const double* h_tau, int nchan, int ones_channel,
+                const double* const* h_cols, void* d_grid_out, int prec, void* d_ws,
+                size_t ws_bytes, void* stream) {
+  FLPR_CHECK_ARG(d >= 1 && d <= 3, "spread: d=%d not in [1,3]", d);
+  FLPR_CHECK_ARG(n >= 1 && n < (int64_t)1 << 31, "spread: n=%lld out of range", (long long)n);
+  FLPR_CHECK_ARG(msp >= 0 && 2 * msp + 1 <= kMaxTaps1, "spread: msp=%d not in [0,6]", msp);
+  FLPR_CHECK_ARG(nchan >= 1 && nchan <= FLPR_MAX_CHANNELS, "spread: nchan=%d", nchan);
+  FLPR_CHECK_ARG(ones_channel == 0 || ones_channel == 1, "spread: ones_channel must be 0/1");
+  FLPR_CHECK_ARG(prec == FLPR_PREC_F32 || prec == FLPR_PREC_F64, "spread: bad precision");
+  for (int a = 0; a < d; ++a) FLPR_CHECK_ARG(h_L[a] >= 1, "spread: L[%d]=%d", a, h_L[a]);
+  if (ws_bytes < flpr_spread_ws(d, n, h_L, msp, nchan, prec)) {
+    set_error("spread: workspace too small");
+    return FLPR_ERR_WORKSPACE;
+  }
+  cudaStream_t s = as_stream(stream);
+  SpreadGeom g;
+  make_geom(g, d, h_L, msp, h_tau, h_kmap);
+  ChanPtrs cp;
+  memset(&cp, 0, sizeof(cp));
+  for (int c = 0; c < nchan - ones_channel; ++c) cp.col[c] = h_cols[c];
+  Arena ar(d_ws, ws_bytes);
+  SpreadWs w;
+  spread_layout(ar, n, g.ntiles, nchan, g.cells, &w);
+
+  const bool fixed = (prec == FLPR_PREC_F32);
+  const int margin = margin_bits_for(g);
+  FLPR_CUDA(cudaMemsetAsync(w.counts, 0, sizeof(int) * g.ntiles, s));
+  FLPR_CUDA(cudaMemsetAsync(w.absum, 0, sizeof(double) * FLPR_MAX_CHANNELS, s));
+  FLPR_CUDA(cudaMemsetAsync(w.gacc, 0, sizeof(double) * (size_t)nchan * g.cells, s));
+
+  int nb = (int)((n + 255) / 256);
+  if (nb > 8 * sm_count()) nb = 8 * sm_count();
+  bin_count_kernel<<<nb, 256, 0, s>>>(g, n, d_x, w.point_tile, w.counts, nchan, ones_channel, cp,
+                                      fixed ? w.absum : nullptr);
+  FLPR_LAUNCH_CHECK();
+  tile_scan_kernel<<<1, 1024, 0, s>>>(g.ntiles, w.counts, w.offsets, w.items, w.cursor);
+  FLPR_LAUNCH_CHECK();
+  bin_scatter_kernel<<<nb, 256, 0, s>>>(n, w.point_tile, w.offsets, w.cursor, w.sorted);
+  FLPR_LAUNCH_CHECK();
+
+  const size_t acc_bytes = 8;
+  int cg = channel_group(g, nchan, acc_bytes);
+  FLPR_CHECK_ARG(cg >= 1, "spread: tile does not fit shared memory");
+  int ngroups = (nchan + cg - 1) / cg;
+  size_t smem = acc_bytes * (size_t)cg * g.tile_cells +
+                (size_t)(kSpreadThreads / 32) * kWarpScratch * sizeof(double);
+  int64_t max_items = (int64_t)g.ntiles + (n + kItemPoints - 1) / kItemPoints;
+  dim3 grid((unsigned)max_items, (unsigned)ngroups);
+  if (fixed) {
+    FLPR_CUDA(cudaFuncSetAttribute(tile_accumulate_kernel<long long>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    tile_accumulate_kernel<long long><<<grid, kSpreadThreads, smem, s>>>(
+        g, d_x, nchan, ones_channel, cp, cg, w.sorted, w.offsets, w.items, w.absum, margin,
+        (long long*)w.gacc);
+  } else {
+    FLPR_CUDA(cudaFuncSetAttribute(tile_accumulate_kernel<double>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    tile_accumulate_kernel<double><<<grid, kSpreadThreads, smem, s>>>(
+        g, d_x, nchan, ones_channel, cp, cg, w.sorted, w.offsets, w.items, nullptr, margin,
+        (double*)w.gacc);
+  }
+  FLPR_LAUNCH_CHECK();
+
+  int64_t total = (int64_t)nchan * g.cells;
+  int fb = (int)((total + 255) / 256);
+  if (fb > 16 * sm_count()) fb = 16 * sm_count();
+  double inv_n = 1.0 / (double)n;
+  if (fixed) {
+    finalize_kernel<long long, float, true><<<fb, 256, 0, s>>>(nchan, g.cells, (long long*)w.gacc,
+                                                         w.absum, margin, inv_n,
+                                                         (float*)d_grid_out);
+  } else {
+    finalize_kernel<double, double, false><<<fb, 256, 0, s>>>(nchan, g.cells, (double*)w.gacc, nullptr,
+                                                       margin, inv_n, (double*)d_grid_out);
+  }
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
+}  // extern "C"

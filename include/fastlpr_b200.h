@@ -1,0 +1,198 @@
+/*
+ * fastlpr_b200 -- C ABI of the B200 implementation of fastLPR's NUFFT path
+ * (local polynomial regression with GCV, kernel density estimation with LCV).
+ *
+ * Conventions for every entry point:
+ *   - returns int status: FLPR_OK (0) or a negative FLPR_ERR_* code;
+ *     flpr_last_error() gives a message for the calling thread;
+ *   - pointers named d_* are device pointers, h_* host pointers;
+ *   - `stream` is a cudaStream_t passed as void*; work is only enqueued,
+ *     the call does not synchronise unless its comment says so;
+ *   - the library allocates no device memory: callers pass workspaces whose
+ *     size they obtain from the matching *_ws query.
+ *
+ * Reference paths cited below are relative to fastLPR_py/src/fastlpr/.
+ */
+#ifndef FASTLPR_B200_H
+#define FASTLPR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FLPR_OK 0
+#define FLPR_ERR_ARG (-1)         /* invalid argument or unsupported shape */
+#define FLPR_ERR_CUDA (-2)        /* CUDA runtime error */
+#define FLPR_ERR_CUFFT (-3)       /* cuFFT error */
+#define FLPR_ERR_WORKSPACE (-4)   /* workspace smaller than the query said */
+#define FLPR_ERR_TIMEOUT (-5)     /* a bounded device-side wait ran out */
+
+#define FLPR_PREC_F32 0           /* FP32 grids/FFT/products, FP64 solve and reductions */
+#define FLPR_PREC_F64 1           /* FP64 throughout */
+
+#define FLPR_MAX_DIMS 3
+#define FLPR_MAX_CHANNELS 64
+
+typedef struct flpr_handle_s* flpr_handle_t;
+
+const char* flpr_last_error(void);
+int flpr_version(void);
+/* Number of CUDA kernels launched by this library since it was loaded
+ * (cuFFT's own kernels are not counted). */
+int64_t flpr_launch_count(void);
+
+/* Handle: owns cuFFT plans (without work areas) for one device. */
+int flpr_create(flpr_handle_t* out, int device);
+int flpr_destroy(flpr_handle_t handle);
+
+/* ---------------------------------------------------------------------
+ * (1) Point statistics.  Replaces the numpy reductions of model.py:58-68
+ * (mean, std ddof=1, min, max per axis) and api.py:1025 (column sums).
+ * d_x: (n, d) row-major float64.  d_stats receives 4*d doubles:
+ * [min(d), max(d), mean(d), M2(d)] with M2 = sum (x - mean)^2.
+ * --------------------------------------------------------------------- */
+size_t flpr_point_stats_ws(int d, int64_t n);
+int flpr_point_stats(int d, int64_t n, const double* d_x, double* d_stats,
+                     void* d_ws, size_t ws_bytes, void* stream);
+
+/* ---------------------------------------------------------------------
+ * (2) Gaussian-gridding spread of every channel onto the periodic L^d grid
+ * (NUFFT type-1 spreading).  Replaces fused_spreading_dispatch
+ * (spreading_fused.py:310-332) and nufft_accumulate_cython
+ * (_nufft_accel.pyx:32-76), including the knot mapping of
+ * convolution.py:176-213 and scale_knots (nufftn_type1.py:140-176).
+ *
+ * h_kmap: per axis 9 doubles {mean, std, center, xs_min, xs_scale,
+ *   knot_scale, knot_r0, knot_shift, hx}; the kernel applies
+ *   xs = (x-mean)/std - center;  xn = (xs-xs_min)/xs_scale*knot_scale + r0;
+ *   xn = mod(xn+0.5, 1) - 0.5;  k = mod((xn+shift)*2pi, 2pi);
+ *   m = rint(k/hx); taps j in [-msp, msp], weight exp(-sum diff^2/(4 tau)).
+ * Channels: if ones_channel, channel 0 is the constant 1; the remaining
+ *   nchan-ones_channel channels are h_cols[i] (device float64 arrays of n).
+ * d_grid_out: (nchan, L...) real, float (FLPR_PREC_F32) or double, scaled
+ *   by 1/n (the 1/M of nufftn_type1.py:709-711).
+ * Accumulation is per-tile in shared memory after binning the points by
+ * tile; FLPR_PREC_F32 accumulates in 64-bit fixed point (order independent,
+ * deterministic), FLPR_PREC_F64 in float64.
+ * --------------------------------------------------------------------- */
+size_t flpr_spread_ws(int d, int64_t n, const int* h_L, int msp, int nchan, int prec);
+int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap,
+                const int* h_L, int msp, const double* h_tau,
+                int nchan, int ones_channel, const double* const* h_cols,
+                void* d_grid_out, int prec, void* d_ws, size_t ws_bytes, void* stream);
+
+/* ---------------------------------------------------------------------
+ * (3) Forward FFT of the spread grids: real-to-complex over all axes,
+ * batched over channels.  Replaces the fft/fftshift/ifftshift chain of
+ * nufftn_type1.py:701-711 and convolution.py:235-236 (the shifts cancel).
+ * d_spec: (nchan, L0, .., L_{d-1}/2+1) complex (float2 or double2).
+ * --------------------------------------------------------------------- */
+size_t flpr_forward_fft_ws(flpr_handle_t handle, int d, const int* h_L, int nchan, int prec);
+int flpr_forward_fft(flpr_handle_t handle, int d, const int* h_L, int nchan,
+                     void* d_grid, void* d_spec, int prec,
+                     void* d_ws, size_t ws_bytes, void* stream);
+
+/* ---------------------------------------------------------------------
+ * (4) Per-axis kernel-moment spectra.  The Gaussian kernel of
+ * kernel.py:330-357 is separable, so the spectrum of K(u)*u^a on the padded
+ * grid (convolution.py:318-794, design_matrix_optimized.py:216-436) is
+ * (1/sqrt(2 pi)) * prod_d F[d][h][a_d].  This computes F for
+ * a = 0..npow-1: the 1-D factor exp(-u^2/2) u^a / h_d sampled on
+ * linspace(lo_d, hi_d, G_d), zero padded with floor((L-G)/2)+1 leading
+ * zeros, FFT of length L_d.  d_F: per axis d, (H, npow, L_d) double2,
+ * axes stacked.  d_sum0: (d, H) sums of the a=0 factor over the grid (used
+ * for the "too small bandwidth" filter of convolution.py:542-605).
+ * --------------------------------------------------------------------- */
+size_t flpr_kernel_factors_ws(flpr_handle_t handle, int d, const int* h_L, int H, int npow);
+int flpr_kernel_factors(flpr_handle_t handle, int d, const int* h_G, const int* h_L,
+                        const double* h_lo, const double* h_hi, int H, const double* d_h,
+                        int npow, void* d_F, double* d_sum0,
+                        void* d_ws, size_t ws_bytes, void* stream);
+
+/* ---------------------------------------------------------------------
+ * (5) Spectral multiply + inverse FFT + crop for a list of products.
+ * Product p multiplies channel chan[p] by the kernel spectrum of bandwidth
+ * hidx[p] and per-axis exponents pow[p*d .. p*d+d-1], inverts, keeps the
+ * real part and crops [qout0_d, qout0_d + G_d) per axis.  Replaces
+ * nufft_convolve (convolution.py:904-951).  Output plane p goes to
+ * d_out + p * prod(G) elements (float or double, per prec); when
+ * add_eps is set the float64 machine epsilon is added (regression.py:116).
+ * h_scale: global factor applied to every product (1/(sqrt(2pi) prod L)).
+ * --------------------------------------------------------------------- */
+size_t flpr_conv_ws(flpr_handle_t handle, int d, const int* h_L, int nprod, int prec);
+int flpr_conv(flpr_handle_t handle, int d, const int* h_G, const int* h_L, const int* h_qout,
+              int H, int npow, const void* d_spec, const void* d_F,
+              int nprod, const int* h_chan, const int* h_hidx, const int* h_pow,
+              double scale, int add_eps, void* d_out, int prec,
+              void* d_ws, size_t ws_bytes, void* stream);
+
+/* ---------------------------------------------------------------------
+ * (6) Local polynomial solve at every grid point and bandwidth.
+ * Replaces solve_regression_system (regression.py:162-277) and the
+ * closed forms of lwp_formulas.py.  d_S: ns planes of (H, M) (M = prod G),
+ * packed lower-triangular column-major; d_T: nt*C planes ordered [i][c] of
+ * (HT, M) for the first HT <= H bandwidths.  Order 0:
+ * m = t / max(s, max(s)*reg).  Order >= 1: lambda = 1e-6 * max |diag S|
+ * over all points and all H bandwidths, m = e1' (S + lambda I)^-1 T by an
+ * FP64 LDL' factorisation per (point, bandwidth) (partial-pivoting
+ * elimination where a pivot vanishes).  d_m: (HT, M, C) float64.
+ * d_scalar: one double of device scratch (receives lambda or max(s)).
+ * --------------------------------------------------------------------- */
+int flpr_solve(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,
+               const void* d_T, double reg, double* d_m, double* d_scalar, int prec,
+               void* stream);
+
+/* ---------------------------------------------------------------------
+ * (7) Interpolation + GCV / Hutchinson reductions over the points.
+ * Replaces the yhat interpolation and RSS of api.py:645-741 /
+ * regression.py:280-471 and the probe interpolation and p'phat, p'p sums of
+ * regression.py:1256-1300.  Multilinear clamped interpolation on the raw
+ * grid (interp_optimized.py:60-130).  h_ax: per axis {x0, dx} with
+ * dx = axis[1]-axis[0]; h_G grid sizes.  d_m: (H, M, C) float64 with
+ * C = ny + R: the first ny channels are the response columns, the next R
+ * the probes.  h_ycols: ny device float64 arrays (n); h_pcols: R arrays.
+ * d_rss: (H, ny) sums of (y - yhat)^2; d_pdot: (R, H) sums of p*phat;
+ * d_pp: (R) sums of p*p.  Outputs are overwritten.
+ * --------------------------------------------------------------------- */
+size_t flpr_interp_reduce_ws(int64_t n, int H, int ny, int R);
+int flpr_interp_reduce(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G,
+                       int H, int ny, int R, const double* d_m,
+                       const double* const* h_ycols, const double* const* h_pcols,
+                       double* d_rss, double* d_pdot, double* d_pp,
+                       void* d_ws, size_t ws_bytes, void* stream);
+
+/* (8) Evaluate one grid (values (M) float64 at every grid point, times
+ * nval interleaved value sets, layout (nval, M)) at n points: d_out (nval, n).
+ * Clamped multilinear interpolation (interp_optimized.py:60-130); this is
+ * the fpp_yhat / fpp interpolant and the final yhat of api.py:760-763. */
+int flpr_interp_eval(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G,
+                     int nval, const double* d_vals, double* d_out, void* stream);
+
+/* ---------------------------------------------------------------------
+ * (9) KDE normalisation and LCV.  Replaces api.py:1059-1133.
+ * d_s: (H, M) density sums (float64, epsilon already added).  For each
+ * bandwidth: f = max(s / (sum(s) * dxprod), 0) (no division if the sum is
+ * not positive), written to d_f (H, M) float64; then f is interpolated at
+ * the raw points and the LCV terms log(max(n/(n-1) (f - K0_h/n), 1e-10))
+ * are summed: d_lcv (H, 2) = {sum log, sum log^2}.  h_k0: (H) K0_h values.
+ * --------------------------------------------------------------------- */
+size_t flpr_kde_ws(int64_t n, int H, int64_t M);
+int flpr_kde_lcv(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G,
+                 int H, const double* d_s, double dxprod, const double* h_k0,
+                 double* d_f, double* d_lcv, void* d_ws, size_t ws_bytes, void* stream);
+
+/* (10) Small elementwise helpers used by the variance mode of
+ * api.py:390-396 and api.py:771-786. */
+int flpr_log_shift(int64_t n, const double* d_in, double shift, double* d_out, void* stream);
+/* d_acc[0] = sum_i yraw_i * exp(-yhat_i) */
+int flpr_exp_weighted_sum(int64_t n, const double* d_yraw, const double* d_yhat,
+                          double* d_acc, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTLPR_B200_H */

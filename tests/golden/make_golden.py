@@ -1,0 +1,239 @@
+"""Generate golden fixtures by running the reference fastLPR Python package.
+
+This script is the only committed file that executes the reference.  It
+imports ``fastlpr`` from a read-only checkout (default
+``/root/reference/fastLPR_py/src``, override with ``FASTLPR_REF_SRC``), runs
+it on small seeded inputs and stores inputs and outputs as ``.npz`` files
+next to this script.  The fixtures pin the CPU oracle (``oracle/``) and the
+GPU path without needing the reference at test time.
+
+Two patches are applied to the reference, both to its FP64 configuration:
+
+* ``fastlpr.nufftn_type1.get_complex_dtype`` returns ``complex128`` so the
+  whole chain (spreading grid, FFT, kernel multiply, solve) runs in FP64
+  without changing the spreading width or Gaussian width
+  (``py/nufftn_type1.py:550-557``, ``py/type_utils.py:158-168``).
+* The 2-D order-2 closed form reads a data file that the package does not
+  ship (``py/lwp_formulas.py:436-444``).  It is replaced by a batched
+  ``numpy.linalg.solve`` of ``e1' (S + lambda I)^-1 T`` -- the definition the
+  closed form implements (``py/lwp_formulas.py:12-14``).
+
+Run:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+import warnings
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SRC = os.environ.get("FASTLPR_REF_SRC", "/root/reference/fastLPR_py/src")
+
+
+def _import_reference():
+    os.environ.setdefault("FASTLPR_QUIET", "1")
+    os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")
+    sys.path.insert(0, REF_SRC)
+    import fastlpr  # noqa: F401
+    import fastlpr.nufftn_type1 as nt
+    import fastlpr.lwp_formulas as lf
+
+    nt.get_complex_dtype = lambda acc: np.complex128
+
+    def _solve_2d_order2(s, t):
+        s_b, t_s = lf._prepare_broadcasting(s, t)
+        nt_ = 6
+        shape = np.broadcast_shapes(*[a.shape for a in s_b], *[a.shape for a in t_s])
+        dtype = np.result_type(*s_b, *t_s)
+        S = np.empty(shape + (nt_, nt_), dtype=np.result_type(*s_b))
+        k = 0
+        for j in range(nt_):
+            for i in range(j, nt_):
+                S[..., i, j] = np.broadcast_to(s_b[k], shape)
+                S[..., j, i] = np.broadcast_to(s_b[k], shape)
+                k += 1
+        T = np.stack([np.broadcast_to(a, shape) for a in t_s], axis=-1).astype(dtype)
+        beta = np.linalg.solve(S.astype(dtype), T[..., None])[..., 0]
+        return beta[..., 0]
+
+    lf._lwp_2d_order2_real = _solve_2d_order2
+    return fastlpr
+
+
+def _lpr_case(fastlpr, name, x, y, h, opts, extra=None):
+    from fastlpr import cv_fastlpr
+
+    fastlpr.clear_fastlpr_caches()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        r = cv_fastlpr(x, y, h, dict(opts))
+    g = r.gcv_yhat
+    out = dict(
+        kind="lpr",
+        x=x,
+        y=y,
+        h=np.asarray(h, dtype=float),
+        opts=repr(opts),
+        yhat=np.asarray(r.yhat),
+        h_sel=np.asarray(r.h),
+        grid_values=np.asarray(r.fpp_yhat.values),
+        gcv_m=np.asarray(g["gcv_m"]),
+        gcv_sd=np.asarray(g["gcv_sd"]),
+        dof=np.asarray(g["dof"]),
+        dof_stderr=np.asarray(g["dof_stderr"]),
+        idmin=int(g["idmin"]),
+        id1se=int(g["id1se"]),
+        bandwidths=np.asarray(g["bandwidths"]),
+        s0=np.asarray(r.s0),
+        d_norm=np.nan if r.d is None else float(r.d),
+        mean=np.asarray(r.metadata["mean"]),
+        std=np.asarray(r.metadata["std"]),
+    )
+    for k, ax in enumerate(r.grid):
+        out[f"axis{k}"] = np.asarray(ax)
+    if extra:
+        out.update(extra)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"{name}: N={x.shape[0]} d={x.shape[1]} H={len(h)} id1se={out['id1se']}")
+
+
+def _kde_case(fastlpr, name, x, h, opts):
+    from fastlpr import cv_fastkde
+
+    fastlpr.clear_fastlpr_caches()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        k = cv_fastkde(x, h, dict(opts))
+    out = dict(
+        kind="kde",
+        x=x,
+        h=np.asarray(h, dtype=float),
+        opts=repr(opts),
+        fhat=np.asarray(k.fhat),
+        fhat_all=np.asarray(k.metadata["fhat_all"]),
+        h_sel=np.asarray(k.h),
+        lcv_m=np.asarray(k.lcv["lcv_m"]),
+        lcv_sd=np.asarray(k.lcv["lcv_sd"]),
+        idmax=int(k.lcv["idmax"]),
+        id1se=int(k.lcv["id1se"]),
+    )
+    for j, ax in enumerate(k.grid):
+        out[f"axis{j}"] = np.asarray(ax)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"{name}: N={x.shape[0]} d={x.shape[1]} H={len(h)} id1se={out['id1se']}")
+
+
+def _intermediates_case(fastlpr, name):
+    """Spread spectra and design-matrix planes for a 2-D order-1 problem."""
+    from fastlpr.model import create_regression_model
+    from fastlpr.convolution import nufft_transform, compute_kernel_fourier
+    from fastlpr.regression import compute_design_matrix
+
+    rng = np.random.default_rng(11)
+    n = 3000
+    x = rng.random((n, 2))
+    y = np.sin(2 * np.pi * x[:, 0]) * np.cos(2 * np.pi * x[:, 1]) + 0.1 * rng.standard_normal(n)
+    hv = np.array([0.05, 0.1, 0.3])
+    h = np.column_stack([hv, hv])
+    G = np.array([32, 32])
+    opts = {"order": 1, "N": [32, 32]}
+    fastlpr.clear_fastlpr_caches()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        model = create_regression_model(x, y[:, None], h, opts)
+        kd, prm = compute_kernel_fourier(model.x_scaled, h, G, order=1)
+        spec_ones = nufft_transform(model.x_scaled, np.ones(n), prm["L"], eval_grid_shape=G,
+                                    qin=prm["qin"], accuracy=4)
+        spec_y = nufft_transform(model.x_scaled, y, prm["L"], eval_grid_shape=G,
+                                 qin=prm["qin"], accuracy=4)
+        S, _ = compute_design_matrix(model.x_scaled, h, G, order=1, accuracy=4)
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"),
+        kind="intermediates",
+        x=x, y=y, h=h, G=G,
+        x_scaled=model.x_scaled,
+        L=np.asarray(prm["L"]), qin=np.asarray(prm["qin"]), qout=np.asarray(prm["qout"]),
+        kdf=np.stack([np.asarray(k) for k in kd], axis=0),
+        spec_ones=spec_ones, spec_y=spec_y,
+        S=np.stack([np.asarray(s) for s in S], axis=0),
+    )
+    print(f"{name}: intermediates L={prm['L']}")
+
+
+def main():
+    fastlpr = _import_reference()
+    from fastlpr import get_hlist
+
+    rng = np.random.default_rng(2024)
+
+    # 1-D, orders 0/1/2, real response (tests/e2e/test_e2e_lpr_1d.py shapes).
+    n = 3000
+    x1 = rng.random((n, 1))
+    y1 = np.sin(2 * np.pi * x1[:, 0]) + 0.1 * rng.standard_normal(n)
+    h1 = get_hlist(8, [0.02, 0.8])
+    for order in (0, 1, 2):
+        _lpr_case(fastlpr, f"lpr1d_o{order}", x1, y1, h1, {"order": order, "N": 256})
+
+    # 1-D with a bandwidth far below the grid spacing: exercises the
+    # "too small" filter of py/convolution.py:542-566.
+    h1b = np.vstack([[1e-4], h1])
+    _lpr_case(fastlpr, "lpr1d_o1_badh", x1, y1, h1b, {"order": 1, "N": 128})
+
+    # 1-D complex response (tests/e2e/test_e2e_complex.py).
+    yc = np.exp(2j * np.pi * x1[:, 0]) + 0.1 * (rng.standard_normal(n) + 1j * rng.standard_normal(n))
+    _lpr_case(fastlpr, "lpr1d_o1_complex", x1, yc, h1, {"order": 1, "N": 256})
+
+    # 1-D non-power-of-two padding and fewer probes.
+    _lpr_case(fastlpr, "lpr1d_o1_nopow2", x1, y1, h1,
+              {"order": 1, "N": 200, "flag_power2": False, "num_dof_sample": 4})
+
+    # 2-D, orders 0/1/2 (N >= 5000 keeps the linear GCV/DoF interpolation).
+    n2 = 6000
+    x2 = rng.random((n2, 2))
+    y2 = np.sin(2 * np.pi * x2[:, 0]) * np.cos(2 * np.pi * x2[:, 1]) + 0.1 * rng.standard_normal(n2)
+    hv = np.logspace(np.log10(0.02), np.log10(0.5), 6)
+    h2 = np.column_stack([hv, hv])
+    for order in (0, 1, 2):
+        _lpr_case(fastlpr, f"lpr2d_o{order}", x2, y2, h2, {"order": order, "N": [48, 40]})
+
+    # 2-D anisotropic bandwidth grid from get_hlist (Fortran ordering).
+    h2a = get_hlist([3, 2], [[0.05, 0.4], [0.08, 0.3]])
+    _lpr_case(fastlpr, "lpr2d_o1_aniso", x2, y2, h2a, {"order": 1, "N": [32, 32]})
+
+    # 2-D heteroscedastic variance fit (examples/example_hetero.py pattern).
+    sig = 0.05 + 0.1 * x2[:, 0]
+    y2h = np.sin(2 * np.pi * x2[:, 0]) * np.cos(2 * np.pi * x2[:, 1]) + sig * rng.standard_normal(n2)
+    from fastlpr import cv_fastlpr
+    fastlpr.clear_fastlpr_caches()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        r_mean = cv_fastlpr(x2, y2h, h2, {"order": 1, "N": [32, 32]})
+    res2 = (y2h - r_mean.yhat) ** 2
+    _lpr_case(fastlpr, "lpr2d_o1_variance", x2, res2, h2,
+              {"order": 1, "N": [32, 32], "y_type_out": "variance"})
+
+    # 3-D order 1.
+    n3 = 6000
+    x3 = rng.random((n3, 3))
+    y3 = np.sin(2 * np.pi * x3[:, 0]) + x3[:, 1] * x3[:, 2] + 0.1 * rng.standard_normal(n3)
+    hv3 = np.array([0.1, 0.2, 0.4])
+    h3 = np.column_stack([hv3, hv3, hv3])
+    _lpr_case(fastlpr, "lpr3d_o1", x3, y3, h3, {"order": 1, "N": [16, 16, 16]})
+
+    # KDE 1-D / 2-D / 3-D.
+    xk1 = np.concatenate([rng.normal(-1, 0.3, (1500, 1)), rng.normal(1.5, 0.6, (1500, 1))])
+    _kde_case(fastlpr, "kde1d", xk1, get_hlist(10, [0.05, 1.0]), {"N": 256})
+    xk2 = rng.standard_normal((4000, 2)) * np.array([1.0, 0.5])
+    hk = np.logspace(np.log10(0.05), np.log10(0.8), 6)
+    _kde_case(fastlpr, "kde2d", xk2, np.column_stack([hk, hk]), {"N": [40, 40]})
+    xk3 = rng.standard_normal((5000, 3))
+    hk3 = np.array([0.1, 0.2, 0.4, 0.8])
+    _kde_case(fastlpr, "kde3d", xk3, np.column_stack([hk3, hk3, hk3]), {"N": [16, 16, 16]})
+
+    _intermediates_case(fastlpr, "inter2d_o1")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,211 @@
+"""GPU parity: the CUDA path through the C ABI against the reference (golden
+fixtures made by running it) and against the CPU oracle.
+
+Tolerances: the FP64 path must match within 1e-9 relative, the FP32 path
+(FP32 grids/FFT/products, FP64 solve and reductions) within 1e-5 relative;
+max-normalised for arrays, element-wise for GCV/LCV scores.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import elem_rel_err, golden_files, load_golden, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-9, "fp32": 1e-5}
+
+
+def _fastlpr():
+    import fastlpr_b200
+    return fastlpr_b200
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("path", golden_files("lpr"), ids=os.path.basename)
+def test_lpr_matches_reference(cuda_ok, path, prec):
+    z = load_golden(path)
+    opts = dict(z["opts"], precision=prec)
+    r = _fastlpr().cv_fastlpr(z["x"], z["y"], z["h"], opts)
+    tol = TOL[prec]
+    g = r.gcv_yhat
+    np.testing.assert_array_equal(g["bandwidths"], z["bandwidths"])
+    assert rel_err(r.yhat, z["yhat"]) < tol
+    assert rel_err(r.fpp_yhat.values, z["grid_values"]) < tol
+    assert elem_rel_err(g["gcv_m"], z["gcv_m"]) < tol
+    assert rel_err(g["gcv_sd"], z["gcv_sd"]) < max(tol, 1e-9) * 10
+    assert rel_err(g["dof"], z["dof"]) < tol
+    assert rel_err(r.s0, z["s0"]) < tol
+    assert g["id1se"] == z["id1se"]
+    assert g["idmin"] == z["idmin"]
+    if not np.isnan(z["d_norm"]):
+        assert abs(r.d - z["d_norm"]) / abs(z["d_norm"]) < tol
+    for k in range(z["x"].shape[1]):
+        np.testing.assert_allclose(r.grid[k], z[f"axis{k}"], rtol=1e-14)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("path", golden_files("kde"), ids=os.path.basename)
+def test_kde_matches_reference(cuda_ok, path, prec):
+    z = load_golden(path)
+    k = _fastlpr().cv_fastkde(z["x"], z["h"], dict(z["opts"], precision=prec))
+    tol = TOL[prec]
+    assert rel_err(k.metadata["fhat_all"], z["fhat_all"]) < tol
+    assert elem_rel_err(k.lcv["lcv_m"], z["lcv_m"]) < tol
+    assert elem_rel_err(k.lcv["lcv_sd"], z["lcv_sd"]) < tol * 10
+    assert k.lcv["id1se"] == z["id1se"]
+    assert k.lcv["idmax"] == z["idmax"]
+    for j in range(z["x"].shape[1]):
+        np.testing.assert_allclose(k.grid[j], z[f"axis{j}"], rtol=1e-13)
+
+
+def _spread_via_abi(x_scaled_ref, x_raw, cols, G, prec):
+    """Call flpr_spread directly; returns the (C, L...) grid times n."""
+    import torch
+    from fastlpr_b200 import _lib, api
+    n, d = x_raw.shape
+    ctx = api._Ctx(torch.device("cuda", 0))
+    stats = api._point_stats(ctx, ctx.upload(x_raw), n, d)
+    geom = api._make_geom(stats, n, d, np.asarray(G), 4, True)
+    dcols = [ctx.upload(np.ascontiguousarray(c)) for c in cols.T]
+    spec_dt = torch.float32 if prec == _lib.FLPR_PREC_F32 else torch.float64
+    C = 1 + len(dcols)
+    grid = ctx.empty((C, int(np.prod(geom.L))), dtype=spec_dt)
+    ws = ctx.ws(ctx.lib.flpr_spread_ws(d, n, _lib.ivec(geom.L), geom.msp, C, prec))
+    dx = ctx.upload(x_raw)
+    _lib.check(ctx.lib.flpr_spread(d, n, dx.data_ptr(), _lib.dvec(geom.kmap.ravel()),
+                                   _lib.ivec(geom.L), geom.msp, _lib.dvec(geom.tau), C, 1,
+                                   _lib.pvec([c.data_ptr() for c in dcols]), grid.data_ptr(), prec,
+                                   ws.data_ptr(), ws.numel(), ctx.stream), "spread")
+    torch.cuda.synchronize()
+    return grid.double().cpu().numpy().reshape((C,) + tuple(geom.L)) * n, geom
+
+
+@pytest.mark.parametrize("d,G", [(1, [300]), (2, [48, 40]), (3, [12, 16, 10])])
+def test_spread_kernel_matches_oracle(cuda_ok, d, G):
+    from fastlpr_b200 import _lib
+    rng = np.random.default_rng(10 + d)
+    n = 4000
+    x = rng.random((n, d)) * 2.0 - 0.3
+    vals = np.column_stack([np.sin(3 * x[:, 0]), rng.standard_normal(n)])
+    for prec, tol in ((_lib.FLPR_PREC_F64, 1e-12), (_lib.FLPR_PREC_F32, 2e-7)):
+        g, geom = _spread_via_abi(None, x, vals, G, prec)
+        xs = (x - geom.mean) / geom.std - geom.center
+        xmod = oracle.knot_coordinates(xs, geom.L, np.asarray(G), geom.qin)
+        ref = oracle.spread_grid(xmod, np.column_stack([np.ones(n), vals]), geom.L, geom.msp,
+                                 geom.tau)
+        for c in range(ref.shape[0]):
+            assert rel_err(g[c], ref[c]) < tol, (prec, c)
+
+
+def test_fp32_spread_is_deterministic(cuda_ok):
+    from fastlpr_b200 import _lib
+    rng = np.random.default_rng(7)
+    x = rng.random((20000, 2))
+    v = rng.standard_normal((20000, 3))
+    a, _ = _spread_via_abi(None, x, v, [64, 64], _lib.FLPR_PREC_F32)
+    b, _ = _spread_via_abi(None, x, v, [64, 64], _lib.FLPR_PREC_F32)
+    np.testing.assert_array_equal(a, b)
+
+
+def _compare_to_oracle(r, o, tol):
+    assert rel_err(r.yhat, o["yhat"]) < tol
+    assert elem_rel_err(r.gcv_yhat["gcv_m"], o["gcv_m"]) < tol
+    assert rel_err(r.gcv_yhat["dof"], o["dof_all"]) < tol
+    assert r.gcv_yhat["id1se"] == o["id1se"]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_multi_response_and_aggregation(cuda_ok, prec):
+    rng = np.random.default_rng(21)
+    n = 4000
+    x = rng.random((n, 1))
+    y = np.column_stack([np.sin(2 * np.pi * x[:, 0]), np.cos(3 * x[:, 0])])
+    y = y + 0.1 * rng.standard_normal(y.shape)
+    h = oracle.get_hlist(6, [0.03, 0.5])
+    for agg in ("first", "average", "sum"):
+        opts = {"order": 1, "N": 128, "gcv_selection": agg}
+        o = oracle.cv_fastlpr(x, y, h, opts)
+        r = _fastlpr().cv_fastlpr(x, y, h, dict(opts, precision=prec))
+        _compare_to_oracle(r, o, TOL[prec])
+        assert r.yhat.shape == (n, 2)
+
+
+def test_random_matrix_and_dstd_options(cuda_ok):
+    rng = np.random.default_rng(22)
+    n = 3000
+    x = rng.random((n, 1))
+    y = np.sin(2 * np.pi * x[:, 0]) + 0.2 * rng.standard_normal(n)
+    h = oracle.get_hlist(7, [0.02, 0.6])
+    rm = rng.standard_normal((n, 5))
+    opts = {"order": 2, "N": 200, "random_matrix": rm, "dstd": 1.0}
+    o = oracle.cv_fastlpr(x, y, h, opts)
+    r = _fastlpr().cv_fastlpr(x, y, h, dict(opts, precision="fp64"))
+    _compare_to_oracle(r, o, 1e-9)
+
+
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_fast_path_without_dof(cuda_ok, order):
+    rng = np.random.default_rng(23)
+    n = 3000
+    x = rng.random((n, 2))
+    y = x[:, 0] * np.sin(4 * x[:, 1]) + 0.05 * rng.standard_normal(n)
+    h = np.array([[0.3, 0.3], [0.1, 0.1], [0.6, 0.6]])
+    opts = {"order": order, "N": [40, 40], "calc_dof": False}
+    o = oracle.cv_fastlpr(x, y, h, opts)
+    r = _fastlpr().cv_fastlpr(x, y, h, dict(opts, precision="fp64"))
+    assert rel_err(r.yhat, o["yhat"]) < 1e-9
+    assert rel_err(r.s0, o["s0"]) < 1e-9
+    assert np.isnan(r.dof)
+
+
+def test_metric_shape_against_oracle(cuda_ok):
+    """2-D local-linear GCV sweep with the metric's shape at a size the oracle
+    finishes quickly (N=1e5, grid 128^2, 8 bandwidths)."""
+    rng = np.random.default_rng(0)
+    n = 100_000
+    x = rng.random((n, 2))
+    y = np.sin(2 * np.pi * x[:, 0]) * np.cos(2 * np.pi * x[:, 1]) + 0.1 * rng.standard_normal(n)
+    hv = np.logspace(np.log10(0.005), np.log10(0.5), 8)
+    h = np.column_stack([hv, hv])
+    opts = {"order": 1, "N": [128, 128]}
+    o = oracle.cv_fastlpr(x, y, h, opts)
+    for prec in ("fp64", "fp32"):
+        r = _fastlpr().cv_fastlpr(x, y, h, dict(opts, precision=prec))
+        _compare_to_oracle(r, o, TOL[prec])
+
+
+def test_fp32_and_fp64_paths_agree_at_full_metric_size(cuda_ok):
+    """Size-independent check at N=1e6, grid 512^2, 32 bandwidths: the FP32
+    path stays within 1e-5 of the FP64 path and selects the same bandwidth."""
+    rng = np.random.default_rng(0)
+    n = 1_000_000
+    x = rng.random((n, 2))
+    y = np.sin(2 * np.pi * x[:, 0]) * np.cos(2 * np.pi * x[:, 1]) + 0.1 * rng.standard_normal(n)
+    hv = np.logspace(np.log10(0.005), np.log10(0.5), 32)
+    h = np.column_stack([hv, hv])
+    opts = {"order": 1, "N": [512, 512]}
+    r64 = _fastlpr().cv_fastlpr(x, y, h, dict(opts, precision="fp64"))
+    r32 = _fastlpr().cv_fastlpr(x, y, h, dict(opts, precision="fp32"))
+    assert rel_err(r32.yhat, r64.yhat) < 1e-5
+    assert elem_rel_err(r32.gcv_yhat["gcv_m"], r64.gcv_yhat["gcv_m"]) < 1e-5
+    assert r32.gcv_yhat["id1se"] == r64.gcv_yhat["id1se"]
+    # a constant response is reproduced (up to the 1e-6 ridge)
+    rc = _fastlpr().cv_fastlpr(x, np.full(n, 2.5), h[::8], dict(opts, precision="fp64"))
+    assert np.max(np.abs(rc.yhat - 2.5)) < 1e-4
+
+
+def test_interpolant_and_predict(cuda_ok):
+    rng = np.random.default_rng(24)
+    n = 2000
+    x = rng.random((n, 1))
+    y = np.sin(2 * np.pi * x[:, 0]) + 0.1 * rng.standard_normal(n)
+    fl = _fastlpr()
+    r = fl.cv_fastlpr(x, y, fl.get_hlist(5, [0.05, 0.5]), {"order": 1, "N": 128})
+    xn = np.linspace(0, 1, 50).reshape(-1, 1)
+    p = fl.fastlpr_predict(r, xn)
+    ref = oracle.linear_interp(r.grid, r.fpp_yhat.values, xn)
+    assert rel_err(p, ref) < 1e-14
+    assert np.allclose(r.fpp_yhat(x), r.yhat)

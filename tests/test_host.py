@@ -1,0 +1,152 @@
+"""Host-side logic of fastlpr_b200 that needs no GPU: bandwidth grids, input
+validation, grid geometry, knot constants, selection and GCV assembly."""
+import numpy as np
+import pytest
+
+import oracle
+from fastlpr_b200 import api, get_hlist
+
+
+def test_get_hlist_matches_oracle_and_known_values():
+    h = get_hlist(5, [0.1, 1.0])
+    np.testing.assert_allclose(h[:, 0], np.logspace(-1, 0, 5))
+    h2 = get_hlist([3, 2], [[0.1, 1.0], [0.2, 2.0]])
+    assert h2.shape == (6, 2)
+    # first axis varies fastest (MATLAB ndgrid order)
+    np.testing.assert_allclose(h2[:3, 1], 0.2)
+    np.testing.assert_allclose(h2[3:, 1], 2.0)
+    np.testing.assert_array_equal(h2, oracle.get_hlist([3, 2], [[0.1, 1.0], [0.2, 2.0]]))
+    np.testing.assert_array_equal(get_hlist(1, [0.5, 0.5]), np.array([[0.5]]))
+    lin = get_hlist(5, [0.5, 1.0], spacing=np.linspace)
+    np.testing.assert_allclose(np.diff(lin[:, 0]), 0.125)
+    with pytest.raises(ValueError):
+        get_hlist([2, 2], [[0.1, 1.0]])
+
+
+@pytest.mark.parametrize("bad", [np.nan, np.inf])
+def test_validation_rejects_nonfinite(bad):
+    x = np.random.default_rng(0).random((20, 1))
+    y = np.sin(x[:, 0])
+    xb = x.copy()
+    xb[3, 0] = bad
+    with pytest.raises(ValueError):
+        api.cv_fastlpr(xb, y, [[0.2]], {"order": 1})
+    yb = y.copy()
+    yb[4] = bad
+    with pytest.raises(ValueError):
+        api.cv_fastlpr(x, yb, [[0.2]], {"order": 1})
+    with pytest.raises(ValueError):
+        api.cv_fastkde(xb, [[0.2]])
+
+
+def test_validation_shapes_and_options():
+    rng = np.random.default_rng(1)
+    x = rng.random((30, 1))
+    y = rng.random(30)
+    with pytest.raises(ValueError):
+        api.cv_fastlpr(x, y[:20], [[0.2]])
+    with pytest.raises(ValueError):
+        api.cv_fastlpr(x, np.zeros((30, 1, 1)), [[0.2]])
+    for order in (-1, 3, 5):
+        with pytest.raises(ValueError):
+            api.cv_fastlpr(x, y, [[0.2]], {"order": order})
+    for h in ([[-0.1]], [[0.0]], [[0.1], [-0.2]]):
+        with pytest.raises(ValueError):
+            api.cv_fastlpr(x, y, h)
+    with pytest.raises(ValueError):
+        api.cv_fastlpr(x, y, [[0.2, 0.3]])
+    with pytest.raises(ValueError):
+        api.cv_fastlpr(rng.random((40, 11)), rng.random(40), [[0.2] * 11])
+    with pytest.raises(ValueError):
+        api.cv_fastkde(np.array([[1.0]]))
+    with pytest.raises(ValueError):
+        api.cv_fastlpr(np.zeros((0, 1)), np.zeros(0), [[0.2]])
+
+
+def test_unsupported_paths_raise_not_implemented():
+    rng = np.random.default_rng(2)
+    x = rng.random((50, 4))
+    with pytest.raises(NotImplementedError):
+        api.cv_fastlpr(x, rng.random(50), [[0.3] * 4], {"calc_dof": False})
+    x1 = rng.random((50, 1))
+    with pytest.raises(NotImplementedError):
+        api.cv_fastlpr(x1, rng.random(50), [[0.3]], {"accuracy": 8})
+    with pytest.raises(NotImplementedError):
+        api.cv_fastlpr(x1, rng.random(50), [[0.3]], {"kernel_type": "epanechnikov"})
+
+
+@pytest.mark.parametrize("G,p2", [(np.array([64]), True), (np.array([512, 512]), True),
+                                  (np.array([200]), False), (np.array([16, 24, 9]), True)])
+def test_grid_params_match_oracle(G, p2):
+    L, qin, qout = api._grid_params(G, p2)
+    Lo, qino, qouto = oracle.grid_params(G, p2)
+    np.testing.assert_array_equal(L, Lo)
+    np.testing.assert_array_equal(qin, qino)
+    np.testing.assert_array_equal(qout, qouto)
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_knot_constants_reproduce_oracle_knots(d):
+    """The per-axis constants handed to the spread kernel reproduce the
+    oracle's knot coordinates bit for bit when applied in the same order."""
+    rng = np.random.default_rng(3 + d)
+    n = 5000
+    x = rng.random((n, d)) * np.array([1.0, 3.0, 0.5])[:d] + np.array([-2.0, 5.0, 0.1])[:d]
+    G = np.array([64, 40, 16])[:d]
+    stats = np.stack([x.min(0), x.max(0), x.mean(0), ((x - x.mean(0)) ** 2).sum(0)])
+    geom = api._make_geom(stats, n, d, G, 4, True)
+    xs = (x - geom.mean) / geom.std - geom.center
+    xmod_o = oracle.knot_coordinates(xs, geom.L, G, geom.qin)
+    for a in range(d):
+        mean, std, center, lo, scale, ks, r0, shift, hx = geom.kmap[a]
+        v = (x[:, a] - mean) / std - center
+        xn = (v - lo) / scale * ks + r0
+        xn = np.mod(xn + 0.5, 1.0) - 0.5
+        k = np.mod((xn + shift) * (2 * np.pi), 2 * np.pi)
+        np.testing.assert_array_equal(k, xmod_o[:, a])
+        assert hx == 2 * np.pi / geom.L[a]
+    np.testing.assert_allclose(geom.lo, xs.min(0), rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("d,order", [(1, 0), (1, 1), (1, 2), (2, 1), (2, 2), (3, 1)])
+def test_element_powers_match_oracle(d, order):
+    assert api._element_powers(d, order) == oracle.lpr.element_powers(d, order)
+    assert api._design_powers(d, order) == oracle.design_powers(d, order)
+
+
+def test_one_se_rule_cases():
+    bw = np.array([[0.1], [0.2], [0.3], [0.4]])
+    s = np.array([3.0, 1.0, 1.05, 2.0])
+    e = np.array([0.1, 0.1, 0.1, 0.1])
+    assert api._one_se_rule(s, e, bw, True, dstd=0.0) == 1
+    assert api._one_se_rule(s, e, bw, True, dstd=1.0) == 2
+    assert api._one_se_rule(np.array([np.nan, 2.0, 1.0, np.inf]), e, bw, True, 0.0) == 2
+    with pytest.raises(ValueError):
+        api._one_se_rule(np.array([np.nan, np.nan]), e[:2], bw[:2], True)
+    ll = np.array([-10.0, -5.0, -5.5, -20.0])
+    assert api._one_se_rule(ll, np.array([1.0, 1.0, 1.0, 1.0]), bw, False, 1.0) == 2
+    for _ in range(20):
+        rng = np.random.default_rng(_)
+        sc = rng.random(7)
+        er = rng.random(7) * 0.2
+        hb = rng.random((7, 2))
+        for pref in (True, False):
+            assert api._one_se_rule(sc, er, hb, pref, 1.0) == oracle.one_se_rule(sc, er, hb, pref, 1.0)
+
+
+def test_gcv_from_sums_matches_oracle_formulas():
+    rng = np.random.default_rng(5)
+    n, H, R = 1000, 6, 10
+    p = rng.standard_normal((n, R))
+    phat = rng.standard_normal((n, H, R)) * 0.1 + p[:, None, :] * rng.random((1, H, 1))
+    y = rng.standard_normal((n, 1))
+    yhat = y[:, None, :] + 0.3 * rng.standard_normal((n, H, 1))
+    rss = np.sum((y[:, None, :] - yhat) ** 2, axis=0)  # (H, 1)
+    pdot = np.einsum("nr,nhr->rh", p, phat)
+    pp = np.sum(p * p, axis=0)
+    out = api._gcv_from_sums(n, rss, pdot, pp, 1, False, {"gcv_selection": "first"})
+    tr = np.clip(n * pdot / pp[:, None], 0, n)
+    pen = 1.0 / np.maximum(np.clip(1 - tr / n, 0, 1), 0.01) ** 2
+    np.testing.assert_allclose(out["dof"], tr.mean(0))
+    np.testing.assert_allclose(out["gcv_m"], rss[:, 0] / n * pen.mean(0))
+    np.testing.assert_allclose(out["gcv_sd"], rss[:, 0] / n * pen.std(0, ddof=1))

@@ -1,0 +1,56 @@
+"""The CPU oracle reproduces the reference (run in its FP64 configuration by
+tests/golden/make_golden.py) on every golden fixture."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import elem_rel_err, golden_files, load_golden, rel_err
+
+
+@pytest.mark.parametrize("path", golden_files("lpr"), ids=os.path.basename)
+def test_oracle_lpr_matches_reference(path):
+    z = load_golden(path)
+    o = oracle.cv_fastlpr(z["x"], z["y"], z["h"], z["opts"])
+    assert o["id1se"] == z["id1se"]
+    assert o["idmin"] == z["idmin"]
+    np.testing.assert_allclose(o["bandwidths"], z["bandwidths"], rtol=0, atol=0)
+    assert rel_err(o["yhat"], z["yhat"]) < 1e-12
+    assert rel_err(o["grid_values"], z["grid_values"]) < 1e-12
+    assert elem_rel_err(o["gcv_m"], z["gcv_m"]) < 1e-10
+    assert rel_err(o["gcv_sd"], z["gcv_sd"]) < 1e-10
+    assert rel_err(o["dof_all"], z["dof"]) < 1e-11
+    assert rel_err(o["s0"], z["s0"]) < 1e-12
+    for k in range(len(z["h"][0])):
+        np.testing.assert_allclose(o["axes_raw"][k], z[f"axis{k}"], rtol=1e-15)
+
+
+@pytest.mark.parametrize("path", golden_files("kde"), ids=os.path.basename)
+def test_oracle_kde_matches_reference(path):
+    z = load_golden(path)
+    o = oracle.cv_fastkde(z["x"], z["h"], z["opts"])
+    assert o["id1se"] == z["id1se"]
+    assert o["idmax"] == z["idmax"]
+    assert rel_err(o["fhat_all"], z["fhat_all"]) < 1e-12
+    assert elem_rel_err(o["lcv_m"], z["lcv_m"]) < 1e-12
+    assert elem_rel_err(o["lcv_sd"], z["lcv_sd"]) < 1e-10
+
+
+def test_oracle_intermediates_match_reference():
+    z = load_golden(os.path.join(os.path.dirname(__file__), "golden", "inter2d_o1.npz"))
+    G = z["G"]
+    spectra, prm = oracle.kernel_spectra(z["x_scaled"], z["h"], G, 1)
+    np.testing.assert_array_equal(prm["L"], z["L"])
+    np.testing.assert_array_equal(prm["qin"], z["qin"])
+    np.testing.assert_array_equal(prm["qout"], z["qout"])
+    assert rel_err(np.stack(spectra), z["kdf"]) < 1e-13
+    L, qin = prm["L"], prm["qin"]
+    msp, tau, _ = oracle.lpr.spread_params(L, 4)
+    xmod = oracle.knot_coordinates(z["x_scaled"], L, G, qin)
+    grid = oracle.spread_grid(xmod, np.column_stack([np.ones(len(z["y"])), z["y"]]), L, msp, tau)
+    spec = oracle.nufft_spectra(grid, len(z["y"]))
+    assert rel_err(spec[0], z["spec_ones"]) < 1e-13
+    assert rel_err(spec[1], z["spec_y"]) < 1e-13
+    S = [oracle.lpr.convolve(np.moveaxis(spec[:1], 0, -1), k, prm["qout"], G)[..., 0] for k in spectra]
+    assert rel_err(np.stack(S), z["S"][..., 0]) < 1e-12
