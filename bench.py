@@ -208,7 +208,11 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    x, y, h, opts = workload(1000 + rank)
+    x, y, h, opts = workload(1000 + rank, args.points)
+    if args.grid:
+        opts["N"] = [args.grid, args.grid]
+    if args.bandwidths:
+        h = h[np.linspace(0, N_H - 1, args.bandwidths).round().astype(int)]
     opts = dict(opts, precision="fp32", device=str(dev))
     # resident inputs
     xd = torch.from_numpy(x).to(dev)
@@ -268,8 +272,8 @@ def run_ours(args):
     value = world * 1000.0 / per_step_ms
     e2e_value = world * 1000.0 / (ms_e2e / args.steps)
     h2d = x.nbytes + y.nbytes
-    d2h = y.nbytes  # fitted values; plus O(H) scalars and the selected grid
-    d2h += int(np.prod(GRID)) * 8 * 2
+    # fitted values, selected grid (float64) and s0 plane (float32)
+    d2h = y.nbytes + int(np.prod(opts["N"])) * (8 + 4)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -307,6 +311,9 @@ def run_ours(args):
         "phase_ms": {k: round(v, 3) for k, v in phases.items()},
         "clocks": clk,
     }
+    if args.points != N_POINTS or args.grid or args.bandwidths:
+        line["config"]["workload"] = (f"profiling case: N={args.points}, grid {opts['N']}, "
+                                      f"{len(h)} bandwidths (not the benchmark workload)")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(h_sample=2)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -325,6 +332,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--points", type=int, default=N_POINTS,
+                    help="points per fit (profiling of smaller cases only)")
+    ap.add_argument("--grid", type=int, default=0, help="grid per axis (default 512)")
+    ap.add_argument("--bandwidths", type=int, default=0, help="subset of the 32 bandwidths")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -422,8 +422,13 @@ def _conv(ctx: _Ctx, geom: _Geom, spec, F, Hf: int, npow: int, prods, prec: int,
 def _precision(opts) -> int:
     p = opts.get("precision", None)
     if p is None:
-        # the reference grids are complex64 below accuracy 5 (type_utils.py:158-168)
-        return _lib.FLPR_PREC_F32 if int(opts["accuracy"]) < 5 else _lib.FLPR_PREC_F64
+        # The reference grids are complex64 below accuracy 5 (type_utils.py:158-168).
+        # Local-quadratic (order 2) moment systems are ill-conditioned when h
+        # approaches the grid spacing: FP32 S or T planes then lose ~1e-2 in m,
+        # so order 2 keeps its grids in FP64 by default.
+        if int(opts["accuracy"]) < 5 and int(opts.get("order", 0)) < 2:
+            return _lib.FLPR_PREC_F32
+        return _lib.FLPR_PREC_F64
     p = str(p).lower()
     if p in ("fp32", "float32", "single"):
         return _lib.FLPR_PREC_F32
