@@ -450,6 +450,20 @@ def _check_supported(dims: int, opts) -> None:
         raise NotImplementedError(f"kernel_type={kt!r}: only the Gaussian kernel is supported")
 
 
+def _check_interp_methods(opts, dims: int, n: int) -> None:
+    """The GPU path interpolates linearly.  The reference defaults to cubic
+    GCV/DoF interpolation for 2-D+ data with n < 5000 (api.py:594-600,
+    api.py:651-657); that case warns, an explicit 'cubic' raises."""
+    for key in ("gcv_interp_method", "dof_interp_method", "interp_method"):
+        m = opts.get(key, None)
+        if m is not None and str(m) != "linear":
+            raise NotImplementedError(f"{key}={m!r}: only linear interpolation is implemented")
+    if dims >= 2 and n < 5000 and bool(opts.get("calc_dof", True)) and \
+            opts.get("gcv_interp_method") is None:
+        warnings.warn("n < 5000 in 2-D+: the reference interpolates GCV/DoF cubically here; "
+                      "fastlpr_b200 uses linear interpolation", UserWarning, stacklevel=3)
+
+
 def _grid_shape(opts, n, dims) -> np.ndarray:
     N = opts.get("N", None)
     if N is None:
@@ -553,6 +567,7 @@ def cv_fastlpr(x, y, h=None, options: Optional[dict] = None) -> RegressionOutput
     y_is_complex = bool(np.iscomplexobj(y_arr))
     if variance and y_is_complex:
         raise NotImplementedError("variance mode needs a real response")
+    _check_interp_methods(opts, dims, n)
     prec = _precision(opts)
     ctx = _Ctx(_device(opts))
     with torch.cuda.device(ctx.device):
