@@ -30,6 +30,7 @@ SIGNATURES = [
     ("flpr_destroy", _I, [_VP]),
     ("flpr_point_stats_ws", _SZ, [_I, _I64]),
     ("flpr_point_stats", _I, [_I, _I64, _VP, _VP, _VP, _SZ, _VP]),
+    ("flpr_point_stats_noalloc", _I, [_I, _I64, _VP, _VP, _VP]),
     ("flpr_spread_ws", _SZ, [_I, _I64, _PI, _I, _I, _I]),
     ("flpr_spread", _I, [_I, _I64, _VP, _PD, _PI, _I, _PD, _I, _I, _PVP, _VP, _I, _VP, _SZ, _VP]),
     ("flpr_forward_fft_ws", _SZ, [_VP, _I, _PI, _I, _I]),

@@ -102,11 +102,58 @@ __global__ void exp_weighted_sum_kernel(int64_t n, const double* __restrict__ yr
   if (threadIdx.x == 0) atomicAdd(acc, sh[0]);
 }
 
+// ---- allocation-free variant of the point statistics ----------------------
+// Scratch of flpr_point_stats_noalloc: one Moments record per (block, axis),
+// kNoAllocMaxBlocks x kNoAllocMaxDims records (320 KiB).  It lives in the
+// library's own device data, so every GPU that loads the library holds it
+// until the process exits.
+constexpr int kNoAllocMaxBlocks = 1024;
+constexpr int kNoAllocMaxDims = 8;
+static __device__ __align__(256) Moments g_noalloc_partials[kNoAllocMaxBlocks * kNoAllocMaxDims];
+
+// Device address of g_noalloc_partials per device ordinal.  Host code must not
+// pass the symbol itself to a kernel: on the host it is only a stand-in.
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static Moments* g_noalloc_addr[kNoAllocMaxDevices] = {nullptr};
+
+static int noalloc_scratch(Moments** out) {
+  int dev = 0;
+  FLPR_CUDA(cudaGetDevice(&dev));
+  FLPR_CHECK_ARG(dev >= 0 && dev < kNoAllocMaxDevices, "point_stats_noalloc: device %d", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_addr[dev] == nullptr) {
+    void* p = nullptr;
+    FLPR_CUDA(cudaGetSymbolAddress(&p, g_noalloc_partials));
+    g_noalloc_addr[dev] = static_cast<Moments*>(p);
+  }
+  *out = g_noalloc_addr[dev];
+  return FLPR_OK;
+}
+
 }  // namespace flpr
 
 using namespace flpr;
 
 extern "C" {
+
+int flpr_point_stats_noalloc(int d, int64_t n, const double* d_x, double* d_stats, void* stream) {
+  FLPR_CHECK_ARG(d >= 1 && d <= kNoAllocMaxDims,
+                 "point_stats_noalloc: d=%d exceeds the static scratch (max %d axes)", d,
+                 kNoAllocMaxDims);
+  FLPR_CHECK_ARG(n >= 1, "point_stats_noalloc: n=%lld", (long long)n);
+  int nb = stat_blocks(n);
+  if (nb > kNoAllocMaxBlocks) nb = kNoAllocMaxBlocks;  // grid-stride loop covers any n
+  Moments* part = nullptr;
+  FLPR_TRY(noalloc_scratch(&part));
+  // every block writes its record for every axis before point_stats_final
+  // reads it, so nothing in the scratch has to start at zero
+  point_stats_partial<<<nb, kStatThreads, 0, as_stream(stream)>>>(d, n, d_x, part);
+  FLPR_LAUNCH_CHECK();
+  point_stats_final<<<1, kStatThreads, 0, as_stream(stream)>>>(d, nb, part, d_stats);
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
 
 size_t flpr_point_stats_ws(int d, int64_t n) {
   return align_up(sizeof(Moments) * (size_t)stat_blocks(n) * (size_t)(d > 0 ? d : 1));

@@ -58,6 +58,26 @@ size_t flpr_point_stats_ws(int d, int64_t n);
 int flpr_point_stats(int d, int64_t n, const double* d_x, double* d_stats,
                      void* d_ws, size_t ws_bytes, void* stream);
 
+/* (1b) The same point statistics without any device allocation by the
+ * caller or the library.  This entry point has no counterpart in the
+ * reference.  It is for callers that cannot allocate device memory at the
+ * point where they need the statistics: code running under a host
+ * application that owns every device buffer through its own pool (a
+ * plugin or FFI caller that may not call cudaMalloc/cudaFree), or a caller
+ * that must not trigger the implicit device synchronisation of an
+ * allocation.  The caller still passes d_x and d_stats.
+ * The per-block partial results go to a static device array inside the
+ * library (1024 blocks x 8 axes x 40 bytes = 320 KiB, held by every GPU that
+ * loads the library until the process exits).  Limits: d <= 8 (larger d is
+ * rejected with FLPR_ERR_ARG and a message); any n.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress), so
+ * make the first call on each device before any stream capture begins.
+ * All calls share the array: two calls whose kernels overlap on the GPU
+ * (different streams, no ordering between them) race and may return wrong
+ * statistics; calls on one stream are ordered and safe. */
+int flpr_point_stats_noalloc(int d, int64_t n, const double* d_x, double* d_stats,
+                             void* stream);
+
 /* ---------------------------------------------------------------------
  * (2) Gaussian-gridding spread of every channel onto the periodic L^d grid
  * (NUFFT type-1 spreading).  Replaces fused_spreading_dispatch
