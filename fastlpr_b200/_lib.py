@@ -41,6 +41,10 @@ SIGNATURES = [
     ("flpr_conv", _I, [_VP, _I, _PI, _PI, _PI, _I, _I, _VP, _VP, _I, _PI, _PI, _PI, _D, _I, _VP,
                        _I, _VP, _SZ, _VP]),
     ("flpr_solve", _I, [_I, _I, _I, _I, _I64, _I, _VP, _VP, _D, _VP, _VP, _I, _VP]),
+    ("flpr_solve_reduce", _I, [_I, _I, _I, _I, _I64, _I, _VP, _VP, _D, _I, _VP, _VP, _VP, _VP,
+                               _I, _VP]),
+    ("flpr_deposit", _I, [_I, _I64, _VP, _PD, _PI, _I, _PVP, _VP, _VP, _VP, _VP]),
+    ("flpr_stencil_quad", _I, [_I, _PI, _I, _I, _VP, _VP, _VP, _VP]),
     ("flpr_interp_reduce_ws", _SZ, [_I64, _I, _I, _I]),
     ("flpr_interp_reduce", _I, [_I, _I64, _VP, _PD, _PI, _I, _I, _I, _VP, _PVP, _PVP, _VP, _VP,
                                 _VP, _VP, _SZ, _VP]),

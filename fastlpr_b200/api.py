@@ -678,31 +678,63 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
               prec, False)
     ev.mark("conv_T")
     M = geom.M
-    # lambda (order >= 1) / max(s) (order 0) is taken over every kept bandwidth;
-    # without DoF only the first bandwidth's T is needed.
-    m = ctx.empty((Ht, M, Cv))
-    scalar = ctx.empty(1)
-    ctx.check(lib.flpr_solve(order, nt, H, Ht, M, Cv, S.data_ptr(), T.data_ptr(),
-                             float(opts["regularization"]), m.data_ptr(), scalar.data_ptr(),
-                             prec, ctx.stream), "flpr_solve")
-    ev.mark("solve")
     axes_raw = _raw_axes(geom, opts)
     ax_arg = _lib.dvec(_axes_arg(axes_raw))
     G_arg = _lib.ivec(geom.G)
     bw_k = bw[keep]
-    if calc_dof:
-        rss = ctx.empty((H, ny))
-        pdot = ctx.empty((max(R, 1), H))
-        pp = ctx.empty(max(R, 1))
-        ctx.check(lib.flpr_interp_reduce(d, n, dx.data_ptr(), ax_arg, G_arg, H, ny, R,
-                                         m.data_ptr(), _lib.pvec([c.data_ptr() for c in ycols]),
-                                         _lib.pvec([c.data_ptr() for c in pcols]),
-                                         rss.data_ptr(), pdot.data_ptr(), pp.data_ptr(),
-                                         None, 0, ctx.stream), "flpr_interp_reduce")
+    scalar = ctx.empty(1)
+    reg = float(opts["regularization"])
+    # lambda (order >= 1) / max(s) (order 0) is taken over every kept bandwidth;
+    # without DoF only the first bandwidth's T is needed.
+    if calc_dof and ny <= 4 and not opts.get("_direct_reduce", False):
+        # dual form: grid-domain dot products with the adjoint deposits
+        npair = (2 ** d) * (2 ** d + 1) // 2
+        Q = ctx.empty((M, Cv))
+        Bst = ctx.empty((M, npair))
+        sq = ctx.empty(Cv)
+        ctx.check(lib.flpr_deposit(d, n, dx.data_ptr(), ax_arg, G_arg, Cv,
+                                   _lib.pvec([c.data_ptr() for c in ycols + pcols]),
+                                   Q.data_ptr(), Bst.data_ptr(), sq.data_ptr(), ctx.stream),
+                  "flpr_deposit")
+        ev.mark("deposit")
+        m = ctx.empty((H, M, ny))
+        dots = ctx.empty((Cv, H))
+        ctx.check(lib.flpr_solve_reduce(order, nt, H, H, M, Cv, S.data_ptr(), T.data_ptr(), reg,
+                                        ny, m.data_ptr(), Q.data_ptr(), dots.data_ptr(),
+                                        scalar.data_ptr(), prec, ctx.stream), "flpr_solve_reduce")
+        ev.mark("solve")
+        quad = ctx.empty((H, ny))
+        ctx.check(lib.flpr_stencil_quad(d, G_arg, H, ny, m.data_ptr(), Bst.data_ptr(),
+                                        quad.data_ptr(), ctx.stream), "flpr_stencil_quad")
         ev.mark("interp_reduce")
-        rss_h = rss.cpu().numpy()
-        pdot_h = pdot.cpu().numpy()[:R]
-        pp_h = pp.cpu().numpy()[:R]
+        sq_h = sq.cpu().numpy()
+        dots_h = dots.cpu().numpy()
+        quad_h = quad.cpu().numpy()
+        rss_h = sq_h[None, :ny] - 2.0 * dots_h[:ny].T + quad_h
+        pdot_h = dots_h[ny:]
+        pp_h = sq_h[ny:]
+        mstride = ny
+    else:
+        m = ctx.empty((Ht, M, Cv))
+        ctx.check(lib.flpr_solve(order, nt, H, Ht, M, Cv, S.data_ptr(), T.data_ptr(), reg,
+                                 m.data_ptr(), scalar.data_ptr(), prec, ctx.stream), "flpr_solve")
+        ev.mark("solve")
+        mstride = Cv
+        if calc_dof:
+            rss = ctx.empty((H, ny))
+            pdot = ctx.empty((max(R, 1), H))
+            pp = ctx.empty(max(R, 1))
+            ctx.check(lib.flpr_interp_reduce(d, n, dx.data_ptr(), ax_arg, G_arg, H, ny, R,
+                                             m.data_ptr(),
+                                             _lib.pvec([c.data_ptr() for c in ycols]),
+                                             _lib.pvec([c.data_ptr() for c in pcols]),
+                                             rss.data_ptr(), pdot.data_ptr(), pp.data_ptr(),
+                                             None, 0, ctx.stream), "flpr_interp_reduce")
+            ev.mark("interp_reduce")
+            rss_h = rss.cpu().numpy()
+            pdot_h = pdot.cpu().numpy()[:R]
+            pp_h = pp.cpu().numpy()[:R]
+    if calc_dof:
         gcv = _gcv_from_sums(n, rss_h, pdot_h, pp_h, dy, y_is_complex, opts)
         dstd = float(opts.get("dstd", 0.0))
         sel = _one_se_rule(gcv["gcv_m"], gcv["gcv_sd"], bw_k, prefer_smaller=True, dstd=dstd)
@@ -712,7 +744,7 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
         sel = 0
         msel = 0
     # selected grid values and fitted values
-    mv = m[msel]                                     # (M, Cv)
+    mv = m[msel]                                     # (M, mstride)
     gv_dev = mv[:, :ny].t().contiguous()             # (ny, M)
     yhat_dev = ctx.empty((ny, n))
     ctx.check(lib.flpr_interp_eval(d, n, dx.data_ptr(), ax_arg, G_arg, ny, gv_dev.data_ptr(),

@@ -201,6 +201,93 @@ __global__ void kde_lcv_kernel(InterpGeom g, int64_t n, const double* __restrict
   if (threadIdx.x == 0) atomicAdd(&lcv[2 * h + 1], b);
 }
 
+// ---- adjoint of the interpolation (dual form of the GCV/Hutchinson sums) --
+// p . interp(m) = sum_g m(g) Q(g) with Q = sum_i w_ig p_i, and
+// sum_i interp(m)_i^2 = sum_b sum_{corner pairs} B_b,pair m(b+c) m(b+c'),
+// so the point-wise interpolation of every (bandwidth, channel) reduces to
+// grid-domain dot products with h-independent deposits Q and B.
+__host__ __device__ constexpr int corner_pairs(int d) { return (1 << d) * ((1 << d) + 1) / 2; }
+
+__global__ void deposit_kernel(InterpGeom g, int64_t n, const double* __restrict__ x, int C,
+                               ColPtrs vals, double* __restrict__ Q, double* __restrict__ B,
+                               double* __restrict__ sq) {
+  __shared__ double sh[32];
+  const int npair = corner_pairs(g.d);
+  double s2[kMaxRed];
+#pragma unroll
+  for (int c = 0; c < kMaxRed; ++c) s2[c] = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    Stencil st;
+    make_stencil(g, x, i, st);
+#pragma unroll
+    for (int c = 0; c < kMaxRed; ++c) {
+      if (c < C) {
+        const double v = vals.col[c][i];
+        s2[c] += v * v;
+        for (int k = 0; k < st.ncorner; ++k) atomicAdd(&Q[st.base[k] * C + c], st.w[k] * v);
+      }
+    }
+    int p = 0;
+    double* Bb = B + st.base[0] * npair;
+    for (int k = 0; k < st.ncorner; ++k)
+      for (int k2 = k; k2 < st.ncorner; ++k2, ++p)
+        atomicAdd(&Bb[p], (k == k2 ? 1.0 : 2.0) * st.w[k] * st.w[k2]);
+  }
+#pragma unroll
+  for (int c = 0; c < kMaxRed; ++c) {
+    if (c < C) {
+      double s = block_sum(s2[c], sh);
+      if (threadIdx.x == 0) atomicAdd(&sq[c], s);
+    }
+  }
+}
+
+// quad[h][c] = sum_b sum_pairs B[b][pair] m(b+c_k) m(b+c_k2); m: (H, M, ny).
+__global__ void stencil_quad_kernel(InterpGeom g, int ny, const double* __restrict__ m,
+                                    const double* __restrict__ B, double* __restrict__ quad) {
+  __shared__ double sh[32];
+  const int h = blockIdx.y;
+  const int npair = corner_pairs(g.d);
+  const int nc = 1 << g.d;
+  const double* mh = m + (int64_t)h * g.M * ny;
+  int64_t coff[8];
+  for (int k = 0; k < nc; ++k) {
+    int64_t o = 0;
+    for (int a = 0; a < g.d; ++a) o = o * g.G[a] + ((k >> (g.d - 1 - a)) & 1);
+    coff[k] = o;
+  }
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < g.M;
+       b += (int64_t)gridDim.x * blockDim.x) {
+    // only base cells with every corner inside the grid carry weight
+    bool inside = true;
+    {
+      int64_t r = b;
+      for (int a = g.d - 1; a >= 0; --a) {
+        int ia = (int)(r % g.G[a]);
+        r /= g.G[a];
+        if (ia >= g.G[a] - 1) inside = false;
+      }
+    }
+    if (!inside) continue;
+    const double* Bb = B + b * npair;
+    for (int c = 0; c < ny && c < 4; ++c) {
+      double mv[8];
+      for (int k = 0; k < nc; ++k) mv[k] = mh[(b + coff[k]) * ny + c];
+      double s = 0.0;
+      int p = 0;
+      for (int k = 0; k < nc; ++k)
+        for (int k2 = k; k2 < nc; ++k2, ++p) s += Bb[p] * mv[k] * mv[k2];
+      acc[c] += s;
+    }
+  }
+  for (int c = 0; c < ny && c < 4; ++c) {
+    double s = block_sum(acc[c], sh);
+    if (threadIdx.x == 0) atomicAdd(&quad[h * ny + c], s);
+  }
+}
+
 static int make_geom(InterpGeom& g, int d, const double* ax, const int* G) {
   memset(&g, 0, sizeof(g));
   FLPR_CHECK_ARG(d >= 1 && d <= 3, "interp: d=%d", d);
@@ -279,6 +366,40 @@ int flpr_interp_eval(int d, int64_t n, const double* d_x, const double* h_ax, co
   FLPR_CHECK_ARG(n >= 1 && nval >= 1, "interp_eval: n=%lld nval=%d", (long long)n, nval);
   interp_eval_kernel<<<pt_blocks(n, 8), 256, 0, as_stream(stream)>>>(g, n, d_x, nval, d_vals,
                                                                       d_out);
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
+int flpr_deposit(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G, int C,
+                 const double* const* h_cols, double* d_Q, double* d_B, double* d_sq,
+                 void* stream) {
+  InterpGeom g;
+  FLPR_TRY(make_geom(g, d, h_ax, h_G));
+  FLPR_CHECK_ARG(n >= 1 && C >= 1 && C <= kMaxRed, "deposit: n=%lld C=%d", (long long)n, C);
+  for (int a = 0; a < d; ++a) FLPR_CHECK_ARG(h_G[a] >= 2, "deposit: G[%d]=%d < 2", a, h_G[a]);
+  cudaStream_t s = as_stream(stream);
+  ColPtrs vc;
+  memset(&vc, 0, sizeof(vc));
+  for (int c = 0; c < C; ++c) vc.col[c] = h_cols[c];
+  FLPR_CUDA(cudaMemsetAsync(d_Q, 0, sizeof(double) * (size_t)g.M * C, s));
+  FLPR_CUDA(cudaMemsetAsync(d_B, 0, sizeof(double) * (size_t)g.M * corner_pairs(d), s));
+  FLPR_CUDA(cudaMemsetAsync(d_sq, 0, sizeof(double) * C, s));
+  deposit_kernel<<<pt_blocks(n, 8), 256, 0, s>>>(g, n, d_x, C, vc, d_Q, d_B, d_sq);
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
+int flpr_stencil_quad(int d, const int* h_G, int H, int ny, const double* d_m, const double* d_B,
+                      double* d_quad, void* stream) {
+  InterpGeom g;
+  double ax[6] = {0, 1, 0, 1, 0, 1};
+  FLPR_TRY(make_geom(g, d, ax, h_G));
+  FLPR_CHECK_ARG(H >= 1 && ny >= 1 && ny <= 4, "stencil_quad: H=%d ny=%d", H, ny);
+  cudaStream_t s = as_stream(stream);
+  FLPR_CUDA(cudaMemsetAsync(d_quad, 0, sizeof(double) * H * ny, s));
+  int per_h = (pt_blocks(g.M, 4) + H - 1) / H;
+  if (per_h < 4) per_h = 4;
+  stencil_quad_kernel<<<dim3(per_h, H), 256, 0, s>>>(g, ny, d_m, d_B, d_quad);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }

@@ -5,6 +5,7 @@ namespace flpr {
 
 constexpr int kMaxNt = 10;
 constexpr int kMaxSolveChan = 64;
+constexpr int kMaxDotChan = 32;
 
 // Order-preserving map of a double onto an unsigned 64-bit integer.
 __device__ __forceinline__ unsigned long long ordered_bits(double v) {
@@ -155,6 +156,80 @@ __global__ void solve_kernel(int order, int nt, int H, int HT, int64_t M, int C,
   }
 }
 
+// Solve fused with the dual-form reductions.  blockIdx.y = bandwidth h < HT.
+// Writes m for the first nkeep channels to mkeep (HT, M, nkeep) and adds
+// dots[c][h] += sum_g m_c(g) Q[g][c] for every channel c < C.
+template <typename Real>
+__global__ void solve_reduce_kernel(int order, int nt, int H, int HT, int64_t M, int C,
+                                    const Real* __restrict__ S, const Real* __restrict__ T,
+                                    double reg, const double* __restrict__ scalar, int nkeep,
+                                    double* __restrict__ mkeep, const double* __restrict__ Q,
+                                    double* __restrict__ dots) {
+  __shared__ double sh[32];
+  const int h = blockIdx.y;
+  const int64_t HM = (int64_t)H * M;
+  const int64_t HTM = (int64_t)HT * M;
+  double acc[kMaxDotChan];
+#pragma unroll
+  for (int c = 0; c < kMaxDotChan; ++c) acc[c] = 0.0;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < M;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = (int64_t)h * M + g;
+    double z[kMaxNt];
+    bool ok = true;
+    double den = 1.0;
+    if (order == 0) {
+      double thr = scalar[0] * reg;
+      double s = (double)S[t];
+      den = s > thr ? s : thr;
+    } else {
+      double A[kMaxNt][kMaxNt];
+      int k = 0;
+      for (int j = 0; j < nt; ++j)
+        for (int i = j; i < nt; ++i) {
+          double v = (double)S[(int64_t)k * HM + t];
+          A[i][j] = v;
+          A[j][i] = v;
+          ++k;
+        }
+      for (int i = 0; i < nt; ++i) A[i][i] += scalar[0];
+      ok = solve_e1(nt, A, z);
+    }
+    const double* q = Q + g * C;
+#pragma unroll
+    for (int c = 0; c < kMaxDotChan; ++c) {
+      if (c < C) {
+        double v;
+        if (order == 0) {
+          v = (double)T[(int64_t)c * HTM + t] / den;
+        } else if (ok) {
+          v = 0.0;
+          for (int i = 0; i < nt; ++i) v += z[i] * (double)T[((int64_t)i * C + c) * HTM + t];
+        } else {
+          v = NAN;
+        }
+        if (c < nkeep) mkeep[t * nkeep + c] = v;
+        acc[c] += v * q[c];
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < kMaxDotChan; ++c) {
+    if (c < C) {
+      double v = acc[c];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      __syncthreads();
+      if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sh[w];
+        atomicAdd(&dots[(int64_t)c * HT + h], s);
+      }
+    }
+  }
+}
+
 static int blocks_for(int64_t total, int per_sm) {
   int64_t b = (total + 255) / 256;
   int64_t cap = (int64_t)per_sm * sm_count();
@@ -168,6 +243,55 @@ static int blocks_for(int64_t total, int per_sm) {
 using namespace flpr;
 
 extern "C" {
+
+static int global_scalar(int order, int nt, int H, int64_t M, const void* d_S, double* d_scalar,
+                         int prec, cudaStream_t s) {
+  unsigned long long* bits = reinterpret_cast<unsigned long long*>(d_scalar);
+  bits_init_kernel<<<1, 1, 0, s>>>(bits);
+  FLPR_LAUNCH_CHECK();
+  const int64_t plane = (int64_t)H * M;
+  const int nb = blocks_for(plane, 4);
+  for (int k = 0; k < nt; ++k) {
+    const int64_t off = (int64_t)(k * nt - k * (k - 1) / 2) * plane;  // diagonal element k
+    if (prec == FLPR_PREC_F32) {
+      plane_max_kernel<float><<<nb, 256, 0, s>>>(plane, (const float*)d_S + off, order > 0, bits);
+    } else {
+      plane_max_kernel<double><<<nb, 256, 0, s>>>(plane, (const double*)d_S + off, order > 0, bits);
+    }
+    FLPR_LAUNCH_CHECK();
+  }
+  scalar_from_bits_kernel<<<1, 1, 0, s>>>(bits, order > 0 ? 1e-6 : 1.0, d_scalar);
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
+int flpr_solve_reduce(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,
+                      const void* d_T, double reg, int nkeep, double* d_mkeep, const double* d_Q,
+                      double* d_dots, double* d_scalar, int prec, void* stream) {
+  FLPR_CHECK_ARG(order >= 0 && order <= 2, "solve_reduce: order=%d", order);
+  FLPR_CHECK_ARG(nt >= 1 && nt <= kMaxNt, "solve_reduce: nt=%d", nt);
+  FLPR_CHECK_ARG(order > 0 || nt == 1, "solve_reduce: order 0 needs nt=1");
+  FLPR_CHECK_ARG(H >= 1 && M >= 1 && C >= 1 && C <= kMaxDotChan, "solve_reduce: H=%d C=%d", H, C);
+  FLPR_CHECK_ARG(HT >= 1 && HT <= H, "solve_reduce: HT=%d", HT);
+  FLPR_CHECK_ARG(nkeep >= 0 && nkeep <= C, "solve_reduce: nkeep=%d", nkeep);
+  cudaStream_t s = as_stream(stream);
+  FLPR_TRY(global_scalar(order, nt, H, M, d_S, d_scalar, prec, s));
+  FLPR_CUDA(cudaMemsetAsync(d_dots, 0, sizeof(double) * (size_t)C * HT, s));
+  int per_h = (blocks_for(M * HT, 4) + HT - 1) / HT;
+  if (per_h < 2) per_h = 2;
+  dim3 grid(per_h, HT);
+  if (prec == FLPR_PREC_F32) {
+    solve_reduce_kernel<float><<<grid, 256, 0, s>>>(order, nt, H, HT, M, C, (const float*)d_S,
+                                                    (const float*)d_T, reg, d_scalar, nkeep,
+                                                    d_mkeep, d_Q, d_dots);
+  } else {
+    solve_reduce_kernel<double><<<grid, 256, 0, s>>>(order, nt, H, HT, M, C, (const double*)d_S,
+                                                     (const double*)d_T, reg, d_scalar, nkeep,
+                                                     d_mkeep, d_Q, d_dots);
+  }
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
 
 int flpr_solve(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,
                const void* d_T, double reg, double* d_m, double* d_scalar, int prec,

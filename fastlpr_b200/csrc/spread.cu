@@ -148,14 +148,31 @@ __global__ void tile_scan_kernel(int ntiles, const int* __restrict__ counts,
   }
 }
 
-__global__ void bin_scatter_kernel(int64_t n, const int* __restrict__ point_tile_in,
+// Sorted structure-of-arrays records, one slot per point in tile order:
+//   rec_base[pos]          local base cell of the point inside its tile,
+//                          packed 10 bits per axis (T <= 1024);
+//   rec_frac[a * n + pos]  k_a - hx_a * m_a (offset of the knot from its cell);
+//   rec_val[c * n + pos]   value of channel c (ones channel excluded).
+template <typename Real>
+__global__ void bin_scatter_kernel(SpreadGeom g, int64_t n, const double* __restrict__ x,
                                    const int* __restrict__ offsets, int* __restrict__ cursor,
-                                   int* __restrict__ sorted) {
+                                   int nv, ChanPtrs cp, int* __restrict__ rec_base,
+                                   Real* __restrict__ rec_frac, Real* __restrict__ rec_val) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    int t = point_tile_in[i];
-    int pos = offsets[t] + atomicAdd(&cursor[t], 1);
-    sorted[pos] = (int)i;
+    int m[3];
+    double k[3];
+    const int t = point_tile(g, x, i, m, k);
+    const int pos = offsets[t] + atomicAdd(&cursor[t], 1);
+    int packed = 0;
+    for (int a = 0; a < g.d; ++a) {
+      int home = m[a] % g.L[a];
+      if (home < 0) home += g.L[a];
+      packed |= (home % g.T[a]) << (10 * a);
+      rec_frac[(int64_t)a * n + pos] = (Real)dsub(k[a], dmul(g.ax[a].hx, (double)m[a]));
+    }
+    rec_base[pos] = packed;
+    for (int c = 0; c < nv; ++c) rec_val[(int64_t)c * n + pos] = (Real)cp.col[c][i];
   }
 }
 
@@ -164,8 +181,10 @@ struct AccOps;
 
 template <>
 struct AccOps<long long> {
-  __device__ static void add_shared(long long* p, double v, double scale) {
-    long long q = __double2ll_rn(v * scale);
+  template <typename Real>
+  __device__ static void add_shared(long long* p, Real v, Real scale) {
+    long long q = (sizeof(Real) == 4) ? __float2ll_rn((float)(v * scale))
+                                      : __double2ll_rn((double)(v * scale));
     if (q != 0) atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)q);
   }
   __device__ static void add_global(long long* p, long long v) {
@@ -175,7 +194,8 @@ struct AccOps<long long> {
 
 template <>
 struct AccOps<double> {
-  __device__ static void add_shared(double* p, double v, double) { atomicAdd(p, v); }
+  template <typename Real>
+  __device__ static void add_shared(double* p, Real v, Real) { atomicAdd(p, (double)v); }
   __device__ static void add_global(double* p, double v) { atomicAdd(p, v); }
 };
 
@@ -189,39 +209,38 @@ __device__ __forceinline__ double fixed_scale(double absum, int margin_bits) {
   return ldexp(1.0, 62 - e - margin_bits);
 }
 
-template <typename Acc>
+__device__ __forceinline__ float fexp(float v) { return expf(v); }
+__device__ __forceinline__ double fexp(double v) { return exp(v); }
+
+// One CTA per work item (a tile, or a chunk of at most kItemPoints points of
+// a tile).  Threads take (point, tap row) pairs: a tap row fixes the tap
+// offsets of all axes but the last, and the thread walks the NT1 taps of the
+// last axis, adding every channel of the point into the shared-memory copy of
+// the tile plus its halo of msp cells.  The tile is then added to the global
+// accumulator with one atomic per non-zero cell.
+template <typename Acc, typename Real, int NT1>
 __global__ void __launch_bounds__(kSpreadThreads)
-tile_accumulate_kernel(SpreadGeom g, const double* __restrict__ x, int nchan, int ones_channel,
-                       ChanPtrs cp, int cgroup, const int* __restrict__ sorted,
+tile_accumulate_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, int cgroup,
                        const int* __restrict__ offsets, const int* __restrict__ items,
-                       const double* __restrict__ absum, int margin_bits,
-                       Acc* __restrict__ gacc) {
+                       const int* __restrict__ rec_base, const Real* __restrict__ rec_frac,
+                       const Real* __restrict__ rec_val, const double* __restrict__ absum,
+                       int margin_bits, Acc* __restrict__ gacc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Acc* acc = reinterpret_cast<Acc*>(smem_raw);
   const int c_begin = blockIdx.y * cgroup;
-  const int c_end = min(nchan, c_begin + cgroup);
-  const int nc = c_end - c_begin;
+  const int nc = min(nchan, c_begin + cgroup) - c_begin;
   const int tc = g.tile_cells;
-  double* wscr = reinterpret_cast<double*>(smem_raw + sizeof(Acc) * (size_t)cgroup * tc);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nwarps = blockDim.x >> 5;
-  double* my_w = wscr + warp * kWarpScratch;   // per-axis weights
-  double* my_v = my_w + 3 * kMaxTaps1;          // channel values of the point
 
   const int item = blockIdx.x;
-  const int total_items = items[g.ntiles];
-  if (item >= total_items) return;
-  // tile owning this item: largest t with items[t] <= item
-  int lo = 0, hi = g.ntiles;
+  if (item >= items[g.ntiles]) return;
+  int lo = 0, hi = g.ntiles;  // tile owning this item: largest t with items[t] <= item
   while (hi - lo > 1) {
     int mid = (lo + hi) >> 1;
     if (items[mid] <= item) lo = mid; else hi = mid;
   }
   const int tile = lo;
-  const int chunk = item - items[tile];
-  const int p_begin = offsets[tile] + chunk * kItemPoints;
+  const int p_begin = offsets[tile] + (item - items[tile]) * kItemPoints;
   const int p_end = min(offsets[tile + 1], p_begin + kItemPoints);
-
   int tcoord[3] = {0, 0, 0};
   {
     int r = tile;
@@ -230,68 +249,58 @@ tile_accumulate_kernel(SpreadGeom g, const double* __restrict__ x, int nchan, in
       r /= g.ntile[a];
     }
   }
+  __shared__ Real scale[32];
   for (int i = threadIdx.x; i < nc * tc; i += blockDim.x) acc[i] = Acc(0);
-
-  double scale[32];
-  for (int c = 0; c < nc; ++c) scale[c] = fixed_scale(absum ? absum[c_begin + c] : 0.0, margin_bits);
+  if (threadIdx.x < 32)
+    scale[threadIdx.x] = (threadIdx.x < nc)
+                             ? (Real)fixed_scale(absum ? absum[c_begin + threadIdx.x] : 0.0, margin_bits)
+                             : Real(1);
   __syncthreads();
 
-  const int ntap1 = g.ntaps1;
-  int ntaps = ntap1;
-  for (int a = 1; a < g.d; ++a) ntaps *= ntap1;
-  const int W1 = g.W[1], W2 = g.W[2];
-
-  for (int p = p_begin + warp; p < p_end; p += nwarps) {
-    const int i = sorted[p];
-    int m[3];
-    double k[3];
-    point_tile(g, x, i, m, k);
-    // local origin of the taps inside the smem tile
-    int base[3] = {0, 0, 0};
-    for (int a = 0; a < g.d; ++a) {
-      int home = m[a] % g.L[a];
-      if (home < 0) home += g.L[a];
-      int origin = tcoord[a] * g.T[a] + (m[a] - home);  // unwrapped tile origin
-      base[a] = m[a] - origin;                          // local index of tap j=-msp
+  constexpr int MSP = (NT1 - 1) / 2;
+  const int d = g.d;
+  const int rows = d == 1 ? 1 : (d == 2 ? NT1 : NT1 * NT1);
+  const int np = p_end - p_begin;
+  const int Wl = g.W[d - 1];
+  const Real hxl = (Real)g.ax[d - 1].hx;
+  const Real ftl = (Real)g.four_tau[d - 1];
+  for (int t = threadIdx.x; t < np * rows; t += blockDim.x) {
+    const int pp = t / rows;
+    const int p = p_begin + pp;
+    const int row = t - pp * rows;
+    const int packed = rec_base[p];
+    int j[2] = {0, 0};
+    if (d == 2) {
+      j[0] = row;
+    } else if (d == 3) {
+      j[0] = row / NT1;
+      j[1] = row - j[0] * NT1;
     }
-    // per-axis weights exp(-diff^2/(4 tau)), diff = k - hx*(m+j)
-    for (int t = lane; t < g.d * ntap1; t += 32) {
-      int a = t / ntap1, j = t % ntap1 - g.msp;
-      double diff = dsub(k[a], dmul(g.ax[a].hx, (double)(m[a] + j)));
-      my_w[a * kMaxTaps1 + j + g.msp] = exp(-ddiv(dmul(diff, diff), g.four_tau[a]));
+    // weight and local cell of the tap row (all axes but the last)
+    Real wrow = Real(1);
+    int cell = 0;
+    for (int a = 0; a < d - 1; ++a) {
+      const Real fr = rec_frac[(int64_t)a * n + p];
+      const Real diff = fr - (Real)g.ax[a].hx * (Real)(j[a] - MSP);
+      wrow *= fexp(-(diff * diff) / (Real)g.four_tau[a]);
+      cell = cell * g.W[a] + ((packed >> (10 * a)) & 1023) + j[a];
     }
-    if (lane < nc) {
-      int c = c_begin + lane;
-      my_v[lane] = (ones_channel && c == 0) ? 1.0 : cp.col[c - ones_channel][i];
+    cell = cell * Wl + ((packed >> (10 * (d - 1))) & 1023);
+    const Real frl = rec_frac[(int64_t)(d - 1) * n + p];
+    Real w[NT1];
+#pragma unroll
+    for (int jl = 0; jl < NT1; ++jl) {
+      const Real diff = frl - hxl * (Real)(jl - MSP);
+      w[jl] = wrow * fexp(-(diff * diff) / ftl);
     }
-    __syncwarp();
-    for (int t = lane; t < ntaps; t += 32) {
-      int j0, j1 = 0, j2 = 0;
-      if (g.d == 1) {
-        j0 = t;
-      } else if (g.d == 2) {
-        j0 = t / ntap1;
-        j1 = t - j0 * ntap1;
-      } else {
-        j0 = t / (ntap1 * ntap1);
-        int r = t - j0 * ntap1 * ntap1;
-        j1 = r / ntap1;
-        j2 = r - j1 * ntap1;
-      }
-      double w = my_w[j0];
-      int cell = base[0] + j0;
-      if (g.d >= 2) {
-        w *= my_w[kMaxTaps1 + j1];
-        cell = cell * W1 + base[1] + j1;
-      }
-      if (g.d == 3) {
-        w *= my_w[2 * kMaxTaps1 + j2];
-        cell = cell * W2 + base[2] + j2;
-      }
-      for (int c = 0; c < nc; ++c)
-        AccOps<Acc>::add_shared(&acc[c * tc + cell], my_v[c] * w, scale[c]);
+    for (int c = 0; c < nc; ++c) {
+      const int ch = c_begin + c;
+      const Real v = (ones_channel && ch == 0) ? Real(1) : rec_val[(int64_t)(ch - ones_channel) * n + p];
+      const Real sc = scale[c];
+      Acc* dst = acc + c * tc + cell;
+#pragma unroll
+      for (int jl = 0; jl < NT1; ++jl) AccOps<Acc>::add_shared(dst + jl, v * w[jl], sc);
     }
-    __syncwarp();
   }
   __syncthreads();
 
@@ -341,7 +350,7 @@ static void make_geom(SpreadGeom& g, int d, const int* L, int msp, const double*
   g.d = d;
   g.msp = msp;
   g.ntaps1 = 2 * msp + 1;
-  static const int tile2[3] = {32, 32, 1};
+  static const int tile2[3] = {16, 16, 1};
   static const int tile3[3] = {8, 8, 8};
   g.cells = 1;
   g.tile_cells = 1;
@@ -349,7 +358,7 @@ static void make_geom(SpreadGeom& g, int d, const int* L, int msp, const double*
   for (int a = 0; a < 3; ++a) {
     if (a < d) {
       g.L[a] = L[a];
-      int T = d == 1 ? 512 : (d == 2 ? tile2[a] : tile3[a]);
+      int T = d == 1 ? 256 : (d == 2 ? tile2[a] : tile3[a]);
       if (T > L[a]) T = L[a];
       g.T[a] = T;
       g.ntile[a] = (L[a] + T - 1) / T;
@@ -377,9 +386,10 @@ static int margin_bits_for(const SpreadGeom& g) {
 }
 
 static int channel_group(const SpreadGeom& g, int nchan, size_t acc_bytes) {
-  size_t budget = 200 * 1024 - (size_t)(kSpreadThreads / 32) * kWarpScratch * sizeof(double);
+  // 1-D/2-D: four CTAs per SM; 3-D tiles are larger: two CTAs per SM
+  size_t budget = (g.d == 3 ? 110 : 55) * 1024;
   int cg = (int)(budget / (acc_bytes * (size_t)g.tile_cells));
-  if (cg > 32) cg = 32;
+  if (cg > 32) cg = 32;  // fixed-point scales of one group live in 32 shared slots
   if (cg > nchan) cg = nchan;
   return cg;
 }
@@ -390,31 +400,37 @@ struct SpreadWs {
   int* offsets;
   int* items;
   int* cursor;
-  int* sorted;
+  int* rec_base;
+  void* rec_frac;
+  void* rec_val;
   double* absum;
   void* gacc;
 };
 
 template <typename A>
-static void spread_layout(A& ar, int64_t n, int ntiles, int nchan, int64_t cells,
-                          SpreadWs* w) {
+static void spread_layout(A& ar, int d, int64_t n, int ntiles, int nchan, int64_t cells,
+                          size_t real_bytes, SpreadWs* w) {
   auto p0 = ar.template take<int>(n);
   auto p1 = ar.template take<int>(ntiles);
   auto p2 = ar.template take<int>(ntiles + 1);
   auto p3 = ar.template take<int>(ntiles + 1);
   auto p4 = ar.template take<int>(ntiles);
   auto p5 = ar.template take<int>(n);
-  auto p6 = ar.template take<double>(FLPR_MAX_CHANNELS);
-  auto p7 = ar.template take<double>((size_t)nchan * cells);
+  auto p6 = ar.template take<char>((size_t)d * n * real_bytes);
+  auto p7 = ar.template take<char>((size_t)(nchan > 1 ? nchan - 1 : 1) * n * real_bytes);
+  auto p8 = ar.template take<double>(FLPR_MAX_CHANNELS);
+  auto p9 = ar.template take<double>((size_t)nchan * cells);
   if (w) {
     w->point_tile = (int*)p0;
     w->counts = (int*)p1;
     w->offsets = (int*)p2;
     w->items = (int*)p3;
     w->cursor = (int*)p4;
-    w->sorted = (int*)p5;
-    w->absum = (double*)p6;
-    w->gacc = (void*)p7;
+    w->rec_base = (int*)p5;
+    w->rec_frac = (void*)p6;
+    w->rec_val = (void*)p7;
+    w->absum = (double*)p8;
+    w->gacc = (void*)p9;
   }
 }
 
@@ -427,6 +443,29 @@ struct SizeArena {
   }
 };
 
+template <int NT1>
+static int launch_accumulate(const SpreadGeom& g, int64_t n, int nchan, int ones_channel, int cg,
+                             const SpreadWs& w, bool fixed, int margin, size_t smem, dim3 grid,
+                             cudaStream_t s) {
+  if (fixed) {
+    auto k = tile_accumulate_kernel<long long, float, NT1>;
+    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, kSpreadThreads, smem, s>>>(g, n, nchan, ones_channel, cg, w.offsets, w.items,
+                                         w.rec_base, (const float*)w.rec_frac,
+                                         (const float*)w.rec_val, w.absum, margin,
+                                         (long long*)w.gacc);
+  } else {
+    auto k = tile_accumulate_kernel<double, double, NT1>;
+    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, kSpreadThreads, smem, s>>>(g, n, nchan, ones_channel, cg, w.offsets, w.items,
+                                         w.rec_base, (const double*)w.rec_frac,
+                                         (const double*)w.rec_val, nullptr, margin,
+                                         (double*)w.gacc);
+  }
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
 }  // namespace flpr
 
 using namespace flpr;
@@ -434,13 +473,12 @@ using namespace flpr;
 extern "C" {
 
 size_t flpr_spread_ws(int d, int64_t n, const int* h_L, int msp, int nchan, int prec) {
-  (void)prec;
   if (d < 1 || d > 3 || n < 1 || nchan < 1) return 0;
   SpreadGeom g;
   double tau[3] = {1, 1, 1}, kmap[27] = {0};
   make_geom(g, d, h_L, msp, tau, kmap);
   SizeArena ar;
-  spread_layout(ar, n, g.ntiles, nchan, g.cells, nullptr);
+  spread_layout(ar, d, n, g.ntiles, nchan, g.cells, prec == FLPR_PREC_F32 ? 4 : 8, nullptr);
   return ar.used;
 }
 
@@ -467,10 +505,10 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
   for (int c = 0; c < nchan - ones_channel; ++c) cp.col[c] = h_cols[c];
   Arena ar(d_ws, ws_bytes);
   SpreadWs w;
-  spread_layout(ar, n, g.ntiles, nchan, g.cells, &w);
-
   const bool fixed = (prec == FLPR_PREC_F32);
+  spread_layout(ar, d, n, g.ntiles, nchan, g.cells, fixed ? 4 : 8, &w);
   const int margin = margin_bits_for(g);
+  const int nv = nchan - ones_channel;
   FLPR_CUDA(cudaMemsetAsync(w.counts, 0, sizeof(int) * g.ntiles, s));
   FLPR_CUDA(cudaMemsetAsync(w.absum, 0, sizeof(double) * FLPR_MAX_CHANNELS, s));
   FLPR_CUDA(cudaMemsetAsync(w.gacc, 0, sizeof(double) * (size_t)nchan * g.cells, s));
@@ -482,31 +520,35 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
   FLPR_LAUNCH_CHECK();
   tile_scan_kernel<<<1, 1024, 0, s>>>(g.ntiles, w.counts, w.offsets, w.items, w.cursor);
   FLPR_LAUNCH_CHECK();
-  bin_scatter_kernel<<<nb, 256, 0, s>>>(n, w.point_tile, w.offsets, w.cursor, w.sorted);
+  if (fixed) {
+    bin_scatter_kernel<float><<<nb, 256, 0, s>>>(g, n, d_x, w.offsets, w.cursor, nv, cp,
+                                                 w.rec_base, (float*)w.rec_frac,
+                                                 (float*)w.rec_val);
+  } else {
+    bin_scatter_kernel<double><<<nb, 256, 0, s>>>(g, n, d_x, w.offsets, w.cursor, nv, cp,
+                                                  w.rec_base, (double*)w.rec_frac,
+                                                  (double*)w.rec_val);
+  }
   FLPR_LAUNCH_CHECK();
 
   const size_t acc_bytes = 8;
   int cg = channel_group(g, nchan, acc_bytes);
   FLPR_CHECK_ARG(cg >= 1, "spread: tile does not fit shared memory");
   int ngroups = (nchan + cg - 1) / cg;
-  size_t smem = acc_bytes * (size_t)cg * g.tile_cells +
-                (size_t)(kSpreadThreads / 32) * kWarpScratch * sizeof(double);
+  size_t smem = acc_bytes * (size_t)cg * g.tile_cells;
   int64_t max_items = (int64_t)g.ntiles + (n + kItemPoints - 1) / kItemPoints;
   dim3 grid((unsigned)max_items, (unsigned)ngroups);
-  if (fixed) {
-    FLPR_CUDA(cudaFuncSetAttribute(tile_accumulate_kernel<long long>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    tile_accumulate_kernel<long long><<<grid, kSpreadThreads, smem, s>>>(
-        g, d_x, nchan, ones_channel, cp, cg, w.sorted, w.offsets, w.items, w.absum, margin,
-        (long long*)w.gacc);
-  } else {
-    FLPR_CUDA(cudaFuncSetAttribute(tile_accumulate_kernel<double>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    tile_accumulate_kernel<double><<<grid, kSpreadThreads, smem, s>>>(
-        g, d_x, nchan, ones_channel, cp, cg, w.sorted, w.offsets, w.items, nullptr, margin,
-        (double*)w.gacc);
+  int status = FLPR_OK;
+  switch (g.ntaps1) {
+    case 3: status = launch_accumulate<3>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
+    case 5: status = launch_accumulate<5>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
+    case 7: status = launch_accumulate<7>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
+    case 9: status = launch_accumulate<9>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
+    case 11: status = launch_accumulate<11>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
+    case 13: status = launch_accumulate<13>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
+    default: set_error("spread: msp=%d not supported (1..6)", g.msp); return FLPR_ERR_ARG;
   }
-  FLPR_LAUNCH_CHECK();
+  if (status != FLPR_OK) return status;
 
   int64_t total = (int64_t)nchan * g.cells;
   int fb = (int)((total + 255) / 256);

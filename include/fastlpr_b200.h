@@ -165,6 +165,15 @@ int flpr_solve(int order, int nt, int H, int HT, int64_t M, int C, const void* d
                const void* d_T, double reg, double* d_m, double* d_scalar, int prec,
                void* stream);
 
+/* (6b) flpr_solve fused with the dual-form reductions: the same lambda
+ * and solve, but m is written only for the first nkeep channels
+ * (d_mkeep: (HT, M, nkeep)) and d_dots[c][h] = sum_g m_c(g) Q[g][c] is
+ * accumulated for every channel c < C (C <= 32; d_dots (C, HT) overwritten)
+ * with Q from flpr_deposit. */
+int flpr_solve_reduce(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,
+                      const void* d_T, double reg, int nkeep, double* d_mkeep, const double* d_Q,
+                      double* d_dots, double* d_scalar, int prec, void* stream);
+
 /* ---------------------------------------------------------------------
  * (7) Interpolation + GCV / Hutchinson reductions over the points.
  * Replaces the yhat interpolation and RSS of api.py:645-741 /
@@ -183,6 +192,25 @@ int flpr_interp_reduce(int d, int64_t n, const double* d_x, const double* h_ax, 
                        const double* const* h_ycols, const double* const* h_pcols,
                        double* d_rss, double* d_pdot, double* d_pp,
                        void* d_ws, size_t ws_bytes, void* stream);
+
+/* (7b) Dual form of (7): the adjoint of the interpolation.
+ * For channel values v_c (h_cols[c], c < C) at the raw points this deposits
+ * Q[g][c] = sum_i w_ig v_ic (d_Q: (M, C)), the stencil weights of
+ * sum_i interp(m)_i^2 (d_B: (M, P) with P = 2^d (2^d + 1) / 2 corner pairs per
+ * base cell) and d_sq[c] = sum_i v_ic^2, so that
+ *   sum_i v_ic interp(m)_i = sum_g m(g) Q[g][c]   and
+ *   sum_i interp(m)_i^2    = sum_b sum_pairs B[b][p] m(b+c_k) m(b+c_k').
+ * Same weights and clamping as flpr_interp_reduce (interp_optimized.py:60-130);
+ * the RSS and p'phat of regression.py:1256-1300 and api.py:645-741 then cost
+ * grid-domain dot products instead of one interpolation per point,
+ * bandwidth and channel.  Outputs are overwritten.  G >= 2 per axis. */
+int flpr_deposit(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G, int C,
+                 const double* const* h_cols, double* d_Q, double* d_B, double* d_sq,
+                 void* stream);
+/* quad[h][c] = sum_b sum_pairs B[b][p] m(b+c_k) m(b+c_k') for m (H, M, ny),
+ * ny <= 4; d_quad (H, ny) overwritten. */
+int flpr_stencil_quad(int d, const int* h_G, int H, int ny, const double* d_m, const double* d_B,
+                      double* d_quad, void* stream);
 
 /* (8) Evaluate one grid (values (M) float64 at every grid point, times
  * nval interleaved value sets, layout (nval, M)) at n points: d_out (nval, n).

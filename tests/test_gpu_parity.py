@@ -226,3 +226,21 @@ def test_interpolant_and_predict(cuda_ok):
     ref = oracle.linear_interp(r.grid, r.fpp_yhat.values, xn)
     assert rel_err(p, ref) < 1e-14
     assert np.allclose(r.fpp_yhat(x), r.yhat)
+
+
+@pytest.mark.parametrize("d,G", [(1, [256]), (2, [64, 48]), (3, [16, 16, 12])])
+def test_dual_form_reductions_match_pointwise(cuda_ok, d, G):
+    """GCV/Hutchinson sums from the adjoint deposits equal the point-wise
+    interpolation of every (bandwidth, channel)."""
+    rng = np.random.default_rng(30 + d)
+    n = 20000
+    x = rng.random((n, d))
+    y = np.sin(2 * np.pi * x[:, 0]) + 0.2 * rng.standard_normal(n)
+    hv = np.array([0.05, 0.15, 0.5])
+    h = np.column_stack([hv] * d)
+    opts = {"order": 1, "N": G, "precision": "fp64"}
+    a = _fastlpr().cv_fastlpr(x, y, h, opts)
+    b = _fastlpr().cv_fastlpr(x, y, h, dict(opts, _direct_reduce=True))
+    assert elem_rel_err(a.gcv_yhat["gcv_m"], b.gcv_yhat["gcv_m"]) < 1e-11
+    assert rel_err(a.gcv_yhat["dof"], b.gcv_yhat["dof"]) < 1e-11
+    assert rel_err(a.yhat, b.yhat) < 1e-14
