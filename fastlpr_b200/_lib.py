@@ -45,6 +45,10 @@ SIGNATURES = [
                                _I, _VP]),
     ("flpr_deposit", _I, [_I, _I64, _VP, _PD, _PI, _I, _PVP, _VP, _VP, _VP, _VP]),
     ("flpr_stencil_quad", _I, [_I, _PI, _I, _I, _VP, _VP, _VP, _VP]),
+    ("flpr_lpr2d_fused_supported", _I, [_PI, _PI, _PI, _I, _I, _I]),
+    ("flpr_lpr2d_fused_ws", _SZ, [_PI, _PI, _PI, _I, _I, _I]),
+    ("flpr_lpr2d_fused", _I, [_PI, _PI, _PI, _I, _I, _I, _I, _I, _VP, _VP, _D, _VP, _D, _VP, _VP,
+                              _VP, _VP, _VP, _SZ, _VP]),
     ("flpr_interp_reduce_ws", _SZ, [_I64, _I, _I, _I]),
     ("flpr_interp_reduce", _I, [_I, _I64, _VP, _PD, _PI, _I, _I, _I, _VP, _PVP, _PVP, _VP, _VP,
                                 _VP, _VP, _SZ, _VP]),

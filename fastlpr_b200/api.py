@@ -360,6 +360,9 @@ def _filter_bandwidths(ctx, geom, bw, npow):
     if np.any(ihbad) and not np.all(ihbad):
         warnings.warn(f"{int(np.sum(ihbad))} bandwidth(s) are too small for this grid and "
                       "will be removed", stacklevel=3)
+        bw = bw[keep]
+        F, _ = _kernel_factors(ctx, geom, bw, npow)
+        keep = np.arange(bw.shape[0])
     elif np.all(ihbad):
         d = geom.d
         hs = (4.0 / (d + 2) / geom.n) ** (1.0 / (d + 4))
@@ -669,14 +672,20 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
     nt = 1 if order == 0 else len(_design_powers(d, order))
     h_t = list(keep) if calc_dof else [int(keep[0])]
     Ht = len(h_t)
-    S = _conv(ctx, geom, spec, F, Hf, npow,
-              [(0, int(hk), epw[k]) for k in range(ns) for hk in keep], prec, order == 0)
-    ev.mark("conv_S")
     Cv = ny + R
-    T = _conv(ctx, geom, spec, F, Hf, npow,
-              [(1 + c, int(hk), epw[i]) for i in range(nt) for c in range(Cv) for hk in h_t],
-              prec, False)
-    ev.mark("conv_T")
+    M = geom.M
+    Lq = (_lib.ivec(geom.G), _lib.ivec(geom.L), _lib.ivec(geom.qout[0]))
+    use_fused = (prec == _lib.FLPR_PREC_F32 and d == 2 and calc_dof and ny <= 4
+                 and not opts.get("_no_fused", False) and not opts.get("_direct_reduce", False)
+                 and lib.flpr_lpr2d_fused_supported(*Lq, H, order, Cv) == 1)
+    if not use_fused:
+        S = _conv(ctx, geom, spec, F, Hf, npow,
+                  [(0, int(hk), epw[k]) for k in range(ns) for hk in keep], prec, order == 0)
+        ev.mark("conv_S")
+        T = _conv(ctx, geom, spec, F, Hf, npow,
+                  [(1 + c, int(hk), epw[i]) for i in range(nt) for c in range(Cv) for hk in h_t],
+                  prec, False)
+        ev.mark("conv_T")
     M = geom.M
     axes_raw = _raw_axes(geom, opts)
     ax_arg = _lib.dvec(_axes_arg(axes_raw))
@@ -699,10 +708,23 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
         ev.mark("deposit")
         m = ctx.empty((H, M, ny))
         dots = ctx.empty((Cv, H))
-        ctx.check(lib.flpr_solve_reduce(order, nt, H, H, M, Cv, S.data_ptr(), T.data_ptr(), reg,
-                                        ny, m.data_ptr(), Q.data_ptr(), dots.data_ptr(),
-                                        scalar.data_ptr(), prec, ctx.stream), "flpr_solve_reduce")
-        ev.mark("solve")
+        if use_fused:
+            S = ctx.empty((ns, H, M), dtype=torch.float32)
+            scale = 1.0 / (SQRT_2PI * float(np.prod(geom.L.astype(float))))
+            ws = ctx.ws(lib.flpr_lpr2d_fused_ws(*Lq, H, order, Cv))
+            ctx.check(lib.flpr_lpr2d_fused(*Lq, H, npow, order, Cv, ny, spec.data_ptr(),
+                                           F.data_ptr(), scale, Q.data_ptr(), reg, S.data_ptr(),
+                                           m.data_ptr(), dots.data_ptr(), scalar.data_ptr(),
+                                           ws.data_ptr(), ws.numel(), ctx.stream),
+                      "flpr_lpr2d_fused")
+            del ws
+            ev.mark("conv_solve")
+        else:
+            ctx.check(lib.flpr_solve_reduce(order, nt, H, H, M, Cv, S.data_ptr(), T.data_ptr(),
+                                            reg, ny, m.data_ptr(), Q.data_ptr(), dots.data_ptr(),
+                                            scalar.data_ptr(), prec, ctx.stream),
+                      "flpr_solve_reduce")
+            ev.mark("solve")
         quad = ctx.empty((H, ny))
         ctx.check(lib.flpr_stencil_quad(d, G_arg, H, ny, m.data_ptr(), Bst.data_ptr(),
                                         quad.data_ptr(), ctx.stream), "flpr_stencil_quad")

@@ -1,9 +1,9 @@
 // Local polynomial solve at every (grid point, bandwidth).
 #include "common.cuh"
+#include "linalg.cuh"
 
 namespace flpr {
 
-constexpr int kMaxNt = 10;
 constexpr int kMaxSolveChan = 64;
 constexpr int kMaxDotChan = 32;
 
@@ -43,74 +43,6 @@ __global__ void bits_init_kernel(unsigned long long* bits) { bits[0] = ordered_b
 
 __global__ void scalar_from_bits_kernel(const unsigned long long* bits, double factor, double* out) {
   out[0] = from_ordered(bits[0]) * factor;
-}
-
-// z = A^-1 e1 for symmetric A (nt x nt, row-major), LDL' without pivoting;
-// falls back to Gaussian elimination with partial pivoting when a pivot is
-// zero or not finite.  Returns false if A is singular.
-__device__ bool solve_e1(int nt, double A[kMaxNt][kMaxNt], double z[kMaxNt]) {
-  double Lm[kMaxNt][kMaxNt];
-  double D[kMaxNt];
-  bool ok = true;
-  for (int j = 0; j < nt && ok; ++j) {
-    double dj = A[j][j];
-    for (int k = 0; k < j; ++k) dj -= Lm[j][k] * Lm[j][k] * D[k];
-    if (!(fabs(dj) > 0.0) || !isfinite(dj)) {
-      ok = false;
-      break;
-    }
-    D[j] = dj;
-    Lm[j][j] = 1.0;
-    for (int i = j + 1; i < nt; ++i) {
-      double v = A[i][j];
-      for (int k = 0; k < j; ++k) v -= Lm[i][k] * Lm[j][k] * D[k];
-      Lm[i][j] = v / dj;
-    }
-  }
-  if (ok) {
-    // L y = e1 ; D w = y ; L' z = w
-    double y[kMaxNt];
-    for (int i = 0; i < nt; ++i) {
-      double v = (i == 0) ? 1.0 : 0.0;
-      for (int k = 0; k < i; ++k) v -= Lm[i][k] * y[k];
-      y[i] = v;
-    }
-    for (int i = 0; i < nt; ++i) y[i] /= D[i];
-    for (int i = nt - 1; i >= 0; --i) {
-      double v = y[i];
-      for (int k = i + 1; k < nt; ++k) v -= Lm[k][i] * z[k];
-      z[i] = v;
-    }
-    return true;
-  }
-  // Gaussian elimination with partial pivoting on [A | e1]
-  double B[kMaxNt][kMaxNt + 1];
-  for (int i = 0; i < nt; ++i) {
-    for (int j = 0; j < nt; ++j) B[i][j] = A[i][j];
-    B[i][nt] = (i == 0) ? 1.0 : 0.0;
-  }
-  for (int c = 0; c < nt; ++c) {
-    int piv = c;
-    for (int r = c + 1; r < nt; ++r)
-      if (fabs(B[r][c]) > fabs(B[piv][c])) piv = r;
-    if (!(fabs(B[piv][c]) > 0.0)) return false;
-    if (piv != c)
-      for (int j = 0; j <= nt; ++j) {
-        double t = B[c][j];
-        B[c][j] = B[piv][j];
-        B[piv][j] = t;
-      }
-    for (int r = c + 1; r < nt; ++r) {
-      double f = B[r][c] / B[c][c];
-      for (int j = c; j <= nt; ++j) B[r][j] -= f * B[c][j];
-    }
-  }
-  for (int i = nt - 1; i >= 0; --i) {
-    double v = B[i][nt];
-    for (int k = i + 1; k < nt; ++k) v -= B[i][k] * z[k];
-    z[i] = v / B[i][i];
-  }
-  return true;
 }
 
 // Thread per (bandwidth, grid point) for the first HT bandwidths.
@@ -238,14 +170,8 @@ static int blocks_for(int64_t total, int per_sm) {
   return (int)b;
 }
 
-}  // namespace flpr
-
-using namespace flpr;
-
-extern "C" {
-
-static int global_scalar(int order, int nt, int H, int64_t M, const void* d_S, double* d_scalar,
-                         int prec, cudaStream_t s) {
+int global_scalar(int order, int nt, int H, int64_t M, const void* d_S, double* d_scalar,
+                  int prec, cudaStream_t s) {
   unsigned long long* bits = reinterpret_cast<unsigned long long*>(d_scalar);
   bits_init_kernel<<<1, 1, 0, s>>>(bits);
   FLPR_LAUNCH_CHECK();
@@ -264,6 +190,12 @@ static int global_scalar(int order, int nt, int H, int64_t M, const void* d_S, d
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
+
+}  // namespace flpr
+
+using namespace flpr;
+
+extern "C" {
 
 int flpr_solve_reduce(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,
                       const void* d_T, double reg, int nkeep, double* d_mkeep, const double* d_Q,

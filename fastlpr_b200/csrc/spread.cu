@@ -448,11 +448,11 @@ static int launch_accumulate(const SpreadGeom& g, int64_t n, int nchan, int ones
                              const SpreadWs& w, bool fixed, int margin, size_t smem, dim3 grid,
                              cudaStream_t s) {
   if (fixed) {
-    auto k = tile_accumulate_kernel<long long, float, NT1>;
+    auto k = tile_accumulate_kernel<long long, double, NT1>;
     FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<grid, kSpreadThreads, smem, s>>>(g, n, nchan, ones_channel, cg, w.offsets, w.items,
-                                         w.rec_base, (const float*)w.rec_frac,
-                                         (const float*)w.rec_val, w.absum, margin,
+                                         w.rec_base, (const double*)w.rec_frac,
+                                         (const double*)w.rec_val, w.absum, margin,
                                          (long long*)w.gacc);
   } else {
     auto k = tile_accumulate_kernel<double, double, NT1>;
@@ -478,7 +478,7 @@ size_t flpr_spread_ws(int d, int64_t n, const int* h_L, int msp, int nchan, int 
   double tau[3] = {1, 1, 1}, kmap[27] = {0};
   make_geom(g, d, h_L, msp, tau, kmap);
   SizeArena ar;
-  spread_layout(ar, d, n, g.ntiles, nchan, g.cells, prec == FLPR_PREC_F32 ? 4 : 8, nullptr);
+  spread_layout(ar, d, n, g.ntiles, nchan, g.cells, 8, nullptr);
   return ar.used;
 }
 
@@ -506,7 +506,7 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
   Arena ar(d_ws, ws_bytes);
   SpreadWs w;
   const bool fixed = (prec == FLPR_PREC_F32);
-  spread_layout(ar, d, n, g.ntiles, nchan, g.cells, fixed ? 4 : 8, &w);
+  spread_layout(ar, d, n, g.ntiles, nchan, g.cells, 8, &w);
   const int margin = margin_bits_for(g);
   const int nv = nchan - ones_channel;
   FLPR_CUDA(cudaMemsetAsync(w.counts, 0, sizeof(int) * g.ntiles, s));
@@ -520,15 +520,12 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
   FLPR_LAUNCH_CHECK();
   tile_scan_kernel<<<1, 1024, 0, s>>>(g.ntiles, w.counts, w.offsets, w.items, w.cursor);
   FLPR_LAUNCH_CHECK();
-  if (fixed) {
-    bin_scatter_kernel<float><<<nb, 256, 0, s>>>(g, n, d_x, w.offsets, w.cursor, nv, cp,
-                                                 w.rec_base, (float*)w.rec_frac,
-                                                 (float*)w.rec_val);
-  } else {
-    bin_scatter_kernel<double><<<nb, 256, 0, s>>>(g, n, d_x, w.offsets, w.cursor, nv, cp,
-                                                  w.rec_base, (double*)w.rec_frac,
-                                                  (double*)w.rec_val);
-  }
+  // records and tap weights are float64 in both precisions: FP32 weights
+  // lose ~1e-6 on the far taps (exponents near 8), which ill-conditioned
+  // local systems in sparse corners amplify; only the accumulator differs
+  bin_scatter_kernel<double><<<nb, 256, 0, s>>>(g, n, d_x, w.offsets, w.cursor, nv, cp,
+                                                w.rec_base, (double*)w.rec_frac,
+                                                (double*)w.rec_val);
   FLPR_LAUNCH_CHECK();
 
   const size_t acc_bytes = 8;

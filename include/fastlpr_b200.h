@@ -174,6 +174,31 @@ int flpr_solve_reduce(int order, int nt, int H, int HT, int64_t M, int C, const 
                       const void* d_T, double reg, int nkeep, double* d_mkeep, const double* d_Q,
                       double* d_dots, double* d_scalar, int prec, void* stream);
 
+/* (6c) Fused 2-D FP32 convolution + solve + dual-form reductions: the
+ * whole inverse-transform / solve stage of a 2-D GCV sweep in one call,
+ * replacing flpr_conv (S and T) + flpr_solve_reduce for FLPR_PREC_F32.
+ * Separable kernel spectrum: a column pass (axis-0 factor, inverse FFT,
+ * crop) shared by all moments with the same axis-0 exponent, then a row
+ * pass (axis-1 factor, C2R, crop) fused with the FP64 solve; two real row
+ * products share one complex transform.  Replaces nufft_convolve
+ * (convolution.py:904-951) for S (regression.py:130-145) and T
+ * (regression.py:802-817, 1516-1533) plus solve_regression_system.
+ * d_spec: (1 + C, L0, L1/2+1) float2 from flpr_forward_fft (channel 0 = ones,
+ * then C value channels of which the first ny are responses); d_F from
+ * flpr_kernel_factors for these H bandwidths; d_Q (M, C) from flpr_deposit.
+ * Outputs: d_S (ns, H, M) float (S planes), d_my (H, M, ny) fitted grids,
+ * d_dots (C, H) = sum_g m_c(g) Q[g][c], d_scalar (lambda or max s).
+ * Supported when flpr_lpr2d_fused_supported() returns 1: L0, L1 powers of
+ * two in [64, 1024], C <= 32, order <= 2 (shared-memory limits). */
+int flpr_lpr2d_fused_supported(const int* h_G, const int* h_L, const int* h_qout, int H, int order,
+                               int C);
+size_t flpr_lpr2d_fused_ws(const int* h_G, const int* h_L, const int* h_qout, int H, int order,
+                           int C);
+int flpr_lpr2d_fused(const int* h_G, const int* h_L, const int* h_qout, int H, int npow, int order,
+                     int C, int ny, const void* d_spec, const void* d_F, double scale,
+                     const double* d_Q, double reg, float* d_S, double* d_my, double* d_dots,
+                     double* d_scalar, void* d_ws, size_t ws_bytes, void* stream);
+
 /* ---------------------------------------------------------------------
  * (7) Interpolation + GCV / Hutchinson reductions over the points.
  * Replaces the yhat interpolation and RSS of api.py:645-741 /

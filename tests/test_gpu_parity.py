@@ -244,3 +244,32 @@ def test_dual_form_reductions_match_pointwise(cuda_ok, d, G):
     assert elem_rel_err(a.gcv_yhat["gcv_m"], b.gcv_yhat["gcv_m"]) < 1e-11
     assert rel_err(a.gcv_yhat["dof"], b.gcv_yhat["dof"]) < 1e-11
     assert rel_err(a.yhat, b.yhat) < 1e-14
+
+
+@pytest.mark.parametrize("order", [0, 1, 2])
+@pytest.mark.parametrize("G", [[48, 40], [64, 64], [200, 120]])
+def test_fused_2d_path_matches_cufft_path_and_oracle(cuda_ok, order, G):
+    """The fused column/row-pass FFT + solve kernels (2-D FP32) agree with the
+    cuFFT-based product/C2R/crop path and with the oracle."""
+    rng = np.random.default_rng(40 + order)
+    n = 20000
+    x = rng.random((n, 2))
+    y = np.sin(2 * np.pi * x[:, 0]) * np.cos(2 * np.pi * x[:, 1]) + 0.1 * rng.standard_normal(n)
+    hv = np.array([0.04, 0.08, 0.2, 0.5])
+    h = np.column_stack([hv, 0.8 * hv])
+    opts = {"order": order, "N": G, "precision": "fp32"}
+    from fastlpr_b200 import _lib
+    import fastlpr_b200.api as api
+    L, qin, qout = api._grid_params(np.array(G), True)
+    assert _lib.load().flpr_lpr2d_fused_supported(_lib.ivec(G), _lib.ivec(L), _lib.ivec(qout[0]),
+                                                  4, order, 11) == 1
+    fused = _fastlpr().cv_fastlpr(x, y, h, opts)
+    plain = _fastlpr().cv_fastlpr(x, y, h, dict(opts, _no_fused=True))
+    o = oracle.cv_fastlpr(x, y, h, {"order": order, "N": G})
+    tol = 1e-5 if order < 2 else 1e-4
+    for r in (fused, plain):
+        assert rel_err(r.yhat, o["yhat"]) < tol
+        assert elem_rel_err(r.gcv_yhat["gcv_m"], o["gcv_m"]) < tol
+        assert rel_err(r.gcv_yhat["dof"], o["dof_all"]) < tol
+        assert rel_err(r.s0, o["s0"]) < 1e-5
+    assert rel_err(fused.yhat, plain.yhat) < tol
