@@ -176,6 +176,34 @@ colpass_kernel(ColArgs ca, const float2* __restrict__ Yt, const double2* __restr
   }
 }
 
+// Solve vectors z = (S + lam I)^-1 e1 per (bandwidth, grid point); order 0
+// stores 1/max(s, max(s) reg).  S: (ns, H, M) float; z: (H, M, NT) double.
+template <int NT>
+__global__ void zvec_kernel(int order, int H, int64_t M, const float* __restrict__ S,
+                            const double* __restrict__ scalar, double reg, double* __restrict__ z) {
+  constexpr int NS = NT * (NT + 1) / 2;
+  const int64_t HM = (int64_t)H * M;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < HM;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    double zz[NT];
+    if (order == 0) {
+      const double thr = scalar[0] * reg;
+      const double s = (double)S[t];
+      zz[0] = 1.0 / (s > thr ? s : thr);
+    } else {
+      double Ap[NS];
+#pragma unroll
+      for (int k = 0; k < NS; ++k) Ap[k] = (double)S[(int64_t)k * HM + t];
+      if (!solve_e1_fixed<NT>(Ap, scalar[0], zz)) {
+#pragma unroll
+        for (int i = 0; i < NT; ++i) zz[i] = NAN;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NT; ++i) z[t * NT + i] = zz[i];
+  }
+}
+
 struct RowJob {
   short slot_a, pow_a, out_a;
   short slot_b, pow_b, out_b;  // slot_b < 0: single product
@@ -279,10 +307,9 @@ template <int E>
 __global__ void __launch_bounds__(kFusedThreads)
 rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
                        const double2* __restrict__ F1, const float2* __restrict__ tw,
-                       const float2* __restrict__ tw2, int order, int nt, int C, int ny,
-                       const float* __restrict__ S, const double* __restrict__ scalar,
-                       double reg, const double* __restrict__ Q, double* __restrict__ my,
-                       double* __restrict__ dots) {
+                       const float2* __restrict__ tw2, int nt, int C, int ny,
+                       const double* __restrict__ zg, const double* __restrict__ Q,
+                       double* __restrict__ my, double* __restrict__ dots) {
   constexpr int N = 32 * E;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* s_tw = reinterpret_cast<float2*>(smem_raw);
@@ -294,23 +321,10 @@ rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   const int r = blockIdx.x, hz = blockIdx.y, h = ra.hbase + hz;
   const int64_t M = (int64_t)ra.G0 * ra.G1;
-  const int64_t HM = (int64_t)H * M;
-  const int ns = nt * (nt + 1) / 2;
-  // phase 1: solve vector per x1
-  for (int x = threadIdx.x; x < ra.G1; x += blockDim.x) {
-    const int64_t g = (int64_t)r * ra.G1 + x;
-    const int64_t t = (int64_t)h * M + g;
-    double* z = zsm + (size_t)x * nt;
-    if (order == 0) {
-      const double thr = scalar[0] * reg;
-      const double s = (double)S[t];
-      z[0] = 1.0 / (s > thr ? s : thr);
-    } else {
-      double Ap[55];
-      for (int k = 0; k < ns; ++k) Ap[k] = (double)S[(int64_t)k * HM + t];
-      if (!solve_e1_packed(nt, Ap, scalar[0], z))
-        for (int i = 0; i < nt; ++i) z[i] = NAN;
-    }
+  // phase 1: the row's solve vectors
+  {
+    const double* src = zg + ((int64_t)h * M + (int64_t)r * ra.G1) * nt;
+    for (int i = threadIdx.x; i < ra.G1 * nt; i += blockDim.x) zsm[i] = src[i];
   }
   __syncthreads();
   // phase 2: T products
@@ -390,13 +404,13 @@ static int launch_row_s(const RowArgs& ra, int G0, int Hc, int H, int nslots_w, 
 
 template <int E>
 static int launch_row_t(const RowArgs& ra, int G0, int Hc, int H, int nslots_w, const float2* W,
-                        const double2* F1, const float2* tw, const float2* tw2, int order, int nt,
-                        int C, int ny, const float* S, const double* scalar, double reg,
-                        const double* Q, double* my, double* dots, cudaStream_t s) {
+                        const double2* F1, const float2* tw, const float2* tw2, int nt, int C,
+                        int ny, const double* z, const double* Q, double* my, double* dots,
+                        cudaStream_t s) {
   size_t smem = fused_t_smem(E, ra.G1, nt, C);
   FLPR_TRY(set_smem(rowpass_t_solve_kernel<E>, smem));
   rowpass_t_solve_kernel<E><<<dim3(G0, Hc), kFusedThreads, smem, s>>>(
-      ra, H, nslots_w, W, F1, tw, tw2, order, nt, C, ny, S, scalar, reg, Q, my, dots);
+      ra, H, nslots_w, W, F1, tw, tw2, nt, C, ny, z, Q, my, dots);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
@@ -549,7 +563,7 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
                      int ny, const float2* spec, const double2* F, double scale, const double* Q,
                      double reg, float* S, double* my, double* dots, double* scalar, float2* Yt,
                      float2* W, float2* tw0, float2* tw20, float2* tw1, float2* tw21,
-                     cudaStream_t s) {
+                     double* zbuf, cudaStream_t s) {
   const int nt = tb.nt;
   const double2* F0 = F;
   const double2* F1 = F + (size_t)H * npow * fg.L0;
@@ -586,6 +600,18 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
   }
   FLPR_TRY(global_scalar(order, nt, H, fg.M, S, scalar, FLPR_PREC_F32, s));
   FLPR_CUDA(cudaMemsetAsync(dots, 0, sizeof(double) * (size_t)C * H, s));
+  {
+    const int64_t HM = (int64_t)H * fg.M;
+    int nb = (int)((HM + 255) / 256);
+    if (nb > 16 * sm_count()) nb = 16 * sm_count();
+    switch (nt) {
+      case 1: zvec_kernel<1><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, zbuf); break;
+      case 3: zvec_kernel<3><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, zbuf); break;
+      case 6: zvec_kernel<6><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, zbuf); break;
+      default: set_error("fused2d: nt=%d", nt); return FLPR_ERR_ARG;
+    }
+    FLPR_LAUNCH_CHECK();
+  }
   // T pass fused with the solve
   ca = tb.t_col;
   ca.L0 = fg.L0;
@@ -607,8 +633,8 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
     ca.hbase = h0;
     ra.hbase = h0;
     FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.t_nslots, hc, Yt, F0, tw0, tw20, W, s));
-    FLPR_TRY(launch_row_t<E1>(ra, fg.G0, hc, H, hc, W, F1, tw1, tw21, order, nt, C, ny, S, scalar,
-                              reg, Q, my, dots, s));
+    FLPR_TRY(launch_row_t<E1>(ra, fg.G0, hc, H, hc, W, F1, tw1, tw21, nt, C, ny, zbuf, Q, my,
+                              dots, s));
   }
   return FLPR_OK;
 }
@@ -618,11 +644,11 @@ static int dispatch_e1(int E1, const FusedTables& tb, const FusedGeom& fg, int H
                        int order, int C, int ny, const float2* spec, const double2* F,
                        double scale, const double* Q, double reg, float* S, double* my,
                        double* dots, double* scalar, float2* Yt, float2* W, float2* tw0,
-                       float2* tw20, float2* tw1, float2* tw21, cudaStream_t s) {
+                       float2* tw20, float2* tw1, float2* tw21, double* zbuf, cudaStream_t s) {
 #define FLPR_E1(V)                                                                            \
   case V:                                                                                     \
     return run_fused<E0, V>(tb, fg, H, npow, order, C, ny, spec, F, scale, Q, reg, S, my,     \
-                            dots, scalar, Yt, W, tw0, tw20, tw1, tw21, s);
+                            dots, scalar, Yt, W, tw0, tw20, tw1, tw21, zbuf, s);
   switch (E1) {
     FLPR_E1(2)
     FLPR_E1(4)
@@ -676,6 +702,7 @@ size_t flpr_lpr2d_fused_ws(const int* h_G, const int* h_L, const int* h_qout, in
   ar.take<float2>(fg.w_elems);
   ar.take<float2>(2 * (size_t)fg.L0);
   ar.take<float2>(2 * (size_t)fg.L1);
+  ar.take<double>((size_t)H * fg.M * tb.nt);
   return ar.used;
 }
 
@@ -697,6 +724,7 @@ int flpr_lpr2d_fused(const int* h_G, const int* h_L, const int* h_qout, int H, i
   float2* W = ar.take<float2>(fg.w_elems);
   float2* tw0 = ar.take<float2>(2 * (size_t)fg.L0);
   float2* tw1 = ar.take<float2>(2 * (size_t)fg.L1);
+  double* zbuf = ar.take<double>((size_t)H * fg.M * tb.nt);
   float2* tw20 = tw0 + fg.L0;
   float2* tw21 = tw1 + fg.L1;
   cudaStream_t s = as_stream(stream);
@@ -706,7 +734,7 @@ int flpr_lpr2d_fused(const int* h_G, const int* h_L, const int* h_qout, int H, i
 #define FLPR_E0(V)                                                                              \
   case V:                                                                                       \
     return dispatch_e1<V>(fg.L1 / 32, tb, fg, H, npow, order, C, ny, spec, F, scale, d_Q, reg,  \
-                          d_S, d_my, d_dots, d_scalar, Yt, W, tw0, tw20, tw1, tw21, s);
+                          d_S, d_my, d_dots, d_scalar, Yt, W, tw0, tw20, tw1, tw21, zbuf, s);
     FLPR_E0(2)
     FLPR_E0(4)
     FLPR_E0(8)

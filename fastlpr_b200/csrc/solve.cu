@@ -45,45 +45,42 @@ __global__ void scalar_from_bits_kernel(const unsigned long long* bits, double f
   out[0] = from_ordered(bits[0]) * factor;
 }
 
+// Solve vector z = (S + lam I)^-1 e1 at element t of the (H, M) planes, or
+// 1/max(s, max(s) reg) for order 0.  Returns false if singular.
+template <typename Real, int NT>
+__device__ __forceinline__ bool zvec_at(int order, int64_t HM, int64_t t, const Real* __restrict__ S,
+                                        double scal, double reg, double (&z)[NT]) {
+  if (order == 0) {
+    const double thr = scal * reg;
+    const double s = (double)S[t];
+    z[0] = 1.0 / (s > thr ? s : thr);
+    return true;
+  }
+  constexpr int NS = NT * (NT + 1) / 2;
+  double Ap[NS];
+#pragma unroll
+  for (int k = 0; k < NS; ++k) Ap[k] = (double)S[(int64_t)k * HM + t];
+  return solve_e1_fixed<NT>(Ap, scal, z);
+}
+
 // Thread per (bandwidth, grid point) for the first HT bandwidths.
 // S: (ns, H, M); T: (nt, C, HT, M); m: (HT, M, C) float64.
-template <typename Real>
-__global__ void solve_kernel(int order, int nt, int H, int HT, int64_t M, int C,
+template <typename Real, int NT>
+__global__ void solve_kernel(int order, int H, int HT, int64_t M, int C,
                              const Real* __restrict__ S, const Real* __restrict__ T, double reg,
                              const double* __restrict__ scalar, double* __restrict__ m) {
   const int64_t HM = (int64_t)H * M;
   const int64_t HTM = (int64_t)HT * M;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < HTM;
        t += (int64_t)gridDim.x * blockDim.x) {
+    double z[NT];
+    const bool ok = zvec_at<Real, NT>(order, HM, t, S, scalar[0], reg, z);
     double* mo = m + t * C;
-    if (order == 0) {
-      double thr = scalar[0] * reg;
-      double s = (double)S[t];
-      double den = s > thr ? s : thr;
-      for (int c = 0; c < C; ++c) mo[c] = (double)T[(int64_t)c * HTM + t] / den;
-      continue;
-    }
-    const double lam = scalar[0];
-    double A[kMaxNt][kMaxNt];
-    int k = 0;
-    for (int j = 0; j < nt; ++j)
-      for (int i = j; i < nt; ++i) {
-        double v = (double)S[(int64_t)k * HM + t];
-        A[i][j] = v;
-        A[j][i] = v;
-        ++k;
-      }
-    for (int i = 0; i < nt; ++i) A[i][i] += lam;
-    double z[kMaxNt];
-    bool ok = solve_e1(nt, A, z);
     for (int c = 0; c < C; ++c) {
       double v = 0.0;
-      if (ok) {
-        for (int i = 0; i < nt; ++i) v += z[i] * (double)T[((int64_t)i * C + c) * HTM + t];
-      } else {
-        v = NAN;
-      }
-      mo[c] = v;
+#pragma unroll
+      for (int i = 0; i < NT; ++i) v += z[i] * (double)T[((int64_t)i * C + c) * HTM + t];
+      mo[c] = ok ? v : NAN;
     }
   }
 }
@@ -91,8 +88,8 @@ __global__ void solve_kernel(int order, int nt, int H, int HT, int64_t M, int C,
 // Solve fused with the dual-form reductions.  blockIdx.y = bandwidth h < HT.
 // Writes m for the first nkeep channels to mkeep (HT, M, nkeep) and adds
 // dots[c][h] += sum_g m_c(g) Q[g][c] for every channel c < C.
-template <typename Real>
-__global__ void solve_reduce_kernel(int order, int nt, int H, int HT, int64_t M, int C,
+template <typename Real, int NT>
+__global__ void solve_reduce_kernel(int order, int H, int HT, int64_t M, int C,
                                     const Real* __restrict__ S, const Real* __restrict__ T,
                                     double reg, const double* __restrict__ scalar, int nkeep,
                                     double* __restrict__ mkeep, const double* __restrict__ Q,
@@ -107,39 +104,16 @@ __global__ void solve_reduce_kernel(int order, int nt, int H, int HT, int64_t M,
   for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < M;
        g += (int64_t)gridDim.x * blockDim.x) {
     const int64_t t = (int64_t)h * M + g;
-    double z[kMaxNt];
-    bool ok = true;
-    double den = 1.0;
-    if (order == 0) {
-      double thr = scalar[0] * reg;
-      double s = (double)S[t];
-      den = s > thr ? s : thr;
-    } else {
-      double A[kMaxNt][kMaxNt];
-      int k = 0;
-      for (int j = 0; j < nt; ++j)
-        for (int i = j; i < nt; ++i) {
-          double v = (double)S[(int64_t)k * HM + t];
-          A[i][j] = v;
-          A[j][i] = v;
-          ++k;
-        }
-      for (int i = 0; i < nt; ++i) A[i][i] += scalar[0];
-      ok = solve_e1(nt, A, z);
-    }
+    double z[NT];
+    const bool ok = zvec_at<Real, NT>(order, HM, t, S, scalar[0], reg, z);
     const double* q = Q + g * C;
 #pragma unroll
     for (int c = 0; c < kMaxDotChan; ++c) {
       if (c < C) {
-        double v;
-        if (order == 0) {
-          v = (double)T[(int64_t)c * HTM + t] / den;
-        } else if (ok) {
-          v = 0.0;
-          for (int i = 0; i < nt; ++i) v += z[i] * (double)T[((int64_t)i * C + c) * HTM + t];
-        } else {
-          v = NAN;
-        }
+        double v = 0.0;
+#pragma unroll
+        for (int i = 0; i < NT; ++i) v += z[i] * (double)T[((int64_t)i * C + c) * HTM + t];
+        if (!ok) v = NAN;
         if (c < nkeep) mkeep[t * nkeep + c] = v;
         acc[c] += v * q[c];
       }
@@ -154,12 +128,45 @@ __global__ void solve_reduce_kernel(int order, int nt, int H, int HT, int64_t M,
       if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
       __syncthreads();
       if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sh[w];
-        atomicAdd(&dots[(int64_t)c * HT + h], s);
+        double sum = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += sh[w];
+        atomicAdd(&dots[(int64_t)c * HT + h], sum);
       }
     }
   }
+}
+
+template <int NT>
+static int launch_solve_reduce(int order, int H, int HT, int64_t M, int C, const void* d_S,
+                               const void* d_T, double reg, const double* scalar, int nkeep,
+                               double* mkeep, const double* Q, double* dots, int prec, dim3 grid,
+                               cudaStream_t s) {
+  if (prec == FLPR_PREC_F32) {
+    solve_reduce_kernel<float, NT><<<grid, 256, 0, s>>>(order, H, HT, M, C, (const float*)d_S,
+                                                        (const float*)d_T, reg, scalar, nkeep,
+                                                        mkeep, Q, dots);
+  } else {
+    solve_reduce_kernel<double, NT><<<grid, 256, 0, s>>>(order, H, HT, M, C, (const double*)d_S,
+                                                         (const double*)d_T, reg, scalar, nkeep,
+                                                         mkeep, Q, dots);
+  }
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
+template <int NT>
+static int launch_solve(int order, int H, int HT, int64_t M, int C, const void* d_S,
+                        const void* d_T, double reg, const double* scalar, double* m, int prec,
+                        int nb, cudaStream_t s) {
+  if (prec == FLPR_PREC_F32) {
+    solve_kernel<float, NT><<<nb, 256, 0, s>>>(order, H, HT, M, C, (const float*)d_S,
+                                               (const float*)d_T, reg, scalar, m);
+  } else {
+    solve_kernel<double, NT><<<nb, 256, 0, s>>>(order, H, HT, M, C, (const double*)d_S,
+                                                (const double*)d_T, reg, scalar, m);
+  }
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
 }
 
 static int blocks_for(int64_t total, int per_sm) {
@@ -212,17 +219,21 @@ int flpr_solve_reduce(int order, int nt, int H, int HT, int64_t M, int C, const 
   int per_h = (blocks_for(M * HT, 4) + HT - 1) / HT;
   if (per_h < 2) per_h = 2;
   dim3 grid(per_h, HT);
-  if (prec == FLPR_PREC_F32) {
-    solve_reduce_kernel<float><<<grid, 256, 0, s>>>(order, nt, H, HT, M, C, (const float*)d_S,
-                                                    (const float*)d_T, reg, d_scalar, nkeep,
-                                                    d_mkeep, d_Q, d_dots);
-  } else {
-    solve_reduce_kernel<double><<<grid, 256, 0, s>>>(order, nt, H, HT, M, C, (const double*)d_S,
-                                                     (const double*)d_T, reg, d_scalar, nkeep,
-                                                     d_mkeep, d_Q, d_dots);
+  switch (nt) {
+#define FLPR_NT(V)                                                                           \
+  case V:                                                                                    \
+    return launch_solve_reduce<V>(order, H, HT, M, C, d_S, d_T, reg, d_scalar, nkeep, d_mkeep, \
+                                  d_Q, d_dots, prec, grid, s);
+    FLPR_NT(1)
+    FLPR_NT(2)
+    FLPR_NT(3)
+    FLPR_NT(4)
+    FLPR_NT(6)
+#undef FLPR_NT
+    default:
+      set_error("solve_reduce: nt=%d not supported", nt);
+      return FLPR_ERR_ARG;
   }
-  FLPR_LAUNCH_CHECK();
-  return FLPR_OK;
 }
 
 int flpr_solve(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,
@@ -235,35 +246,24 @@ int flpr_solve(int order, int nt, int H, int HT, int64_t M, int C, const void* d
                  (long long)M, C);
   FLPR_CHECK_ARG(HT >= 1 && HT <= H, "solve: HT=%d not in [1, H=%d]", HT, H);
   cudaStream_t s = as_stream(stream);
-  // d_scalar first holds the running maximum as ordered bits, then the
-  // scalar itself: lambda = 1e-6 * max |diag S| (order >= 1, regression.py:243-267)
-  // or max S (order 0, regression.py:207-212).
-  unsigned long long* bits = reinterpret_cast<unsigned long long*>(d_scalar);
-  bits_init_kernel<<<1, 1, 0, s>>>(bits);
-  FLPR_LAUNCH_CHECK();
-  const int64_t plane = (int64_t)H * M;
-  const int nb = blocks_for(plane, 4);
-  for (int k = 0; k < nt; ++k) {
-    const int64_t off = (int64_t)(k * nt - k * (k - 1) / 2) * plane;  // diagonal element k
-    if (prec == FLPR_PREC_F32) {
-      plane_max_kernel<float><<<nb, 256, 0, s>>>(plane, (const float*)d_S + off, order > 0, bits);
-    } else {
-      plane_max_kernel<double><<<nb, 256, 0, s>>>(plane, (const double*)d_S + off, order > 0, bits);
-    }
-    FLPR_LAUNCH_CHECK();
-  }
-  scalar_from_bits_kernel<<<1, 1, 0, s>>>(bits, order > 0 ? 1e-6 : 1.0, d_scalar);
-  FLPR_LAUNCH_CHECK();
+  // lambda = 1e-6 * max |diag S| (order >= 1, regression.py:243-267) or
+  // max S (order 0, regression.py:207-212), over every bandwidth
+  FLPR_TRY(global_scalar(order, nt, H, M, d_S, d_scalar, prec, s));
   int sb = blocks_for((int64_t)HT * M, 8);
-  if (prec == FLPR_PREC_F32) {
-    solve_kernel<float><<<sb, 256, 0, s>>>(order, nt, H, HT, M, C, (const float*)d_S,
-                                           (const float*)d_T, reg, d_scalar, d_m);
-  } else {
-    solve_kernel<double><<<sb, 256, 0, s>>>(order, nt, H, HT, M, C, (const double*)d_S,
-                                            (const double*)d_T, reg, d_scalar, d_m);
+  switch (nt) {
+#define FLPR_NT(V)                                                                               \
+  case V:                                                                                        \
+    return launch_solve<V>(order, H, HT, M, C, d_S, d_T, reg, d_scalar, d_m, prec, sb, s);
+    FLPR_NT(1)
+    FLPR_NT(2)
+    FLPR_NT(3)
+    FLPR_NT(4)
+    FLPR_NT(6)
+#undef FLPR_NT
+    default:
+      set_error("solve: nt=%d not supported", nt);
+      return FLPR_ERR_ARG;
   }
-  FLPR_LAUNCH_CHECK();
-  return FLPR_OK;
 }
 
 }  // extern "C"
