@@ -13,6 +13,7 @@ CUDA library through its C ABI (``_lib``):
 from __future__ import annotations
 
 import math
+import time
 import warnings
 from dataclasses import dataclass
 from typing import Dict, List, Optional, Sequence, Tuple
@@ -156,6 +157,13 @@ class _Ctx:
         _lib.check(status, what)
 
 
+def _to_host(t: torch.Tensor) -> torch.Tensor:
+    """Asynchronous copy of a device tensor into fresh pinned host memory."""
+    out = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    out.copy_(t, non_blocking=True)
+    return out
+
+
 class _PhaseEvents:
     """Optional CUDA-event timing of the pipeline phases (milliseconds per
     phase, accumulated into ``timings``)."""
@@ -169,14 +177,16 @@ class _PhaseEvents:
             return
         e = torch.cuda.Event(enable_timing=True)
         e.record()
-        self.events.append((name, e))
+        self.events.append((name, e, time.perf_counter()))
 
     def finish(self):
         if self.timings is None or len(self.events) < 2:
             return
         self.events[-1][1].synchronize()
-        for (_, a), (name, b) in zip(self.events[:-1], self.events[1:]):
+        for (_, a, ta), (name, b, tb) in zip(self.events[:-1], self.events[1:]):
             self.timings[name] = self.timings.get(name, 0.0) + a.elapsed_time(b)
+            key = "host_" + name
+            self.timings[key] = self.timings.get(key, 0.0) + 1000.0 * (tb - ta)
         self.events = []
 
 
@@ -780,31 +790,36 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
         yhat_dev = torch.exp(yhat_dev) / d_norm
         gv_dev = torch.exp(gv_dev) / d_norm
     ev.mark("final_interp")
-    yh = yhat_dev.cpu().numpy()
-    gvh = gv_dev.cpu().numpy()
+    # residuals on the device; every result is copied into pinned host memory
+    # with one synchronisation (the caching host allocator recycles the pages)
+    if variance:
+        res_dev = y_raw_dev[None, :] - yhat_dev
+    else:
+        res_dev = torch.stack(ycols[:ny], dim=0) - yhat_dev
+    yh = _to_host(yhat_dev)
+    rh = _to_host(res_dev)
+    gvh = _to_host(gv_dev)
+    s0h = _to_host(S.view(ns, H, M)[0, sel])
+    torch.cuda.current_stream(ctx.device).synchronize()
+    yh, rh, gvh = yh.numpy(), rh.numpy(), gvh.numpy()
     gshape = tuple(int(g) for g in geom.G)
     if y_is_complex:
         yh = yh[0::2] + 1j * yh[1::2]
+        rh = rh[0::2] + 1j * rh[1::2]
         gvh = gvh[0::2] + 1j * gvh[1::2]
     if dy == 1:
         yhat = yh[0]
+        residuals = rh[0]
         grid_values = gvh[0].reshape(gshape)
     else:
         yhat = yh.T.copy()
+        residuals = rh.T.copy()
         grid_values = np.moveaxis(gvh.reshape((dy,) + gshape), 0, -1)
-    s0 = S.view(ns, H, M)[0, sel].cpu().numpy().reshape(gshape)
+    s0 = s0h.numpy().reshape(gshape)
     ev.mark("download")
     ev.finish()
     interp = GridInterpolant(axes_raw, grid_values, ctx.device)
     selected = bw_k[sel]
-    if y_arr is None:
-        y_host = torch.stack(ycols, dim=1).cpu().numpy()
-    else:
-        y_host = y_arr
-    if dy == 1:
-        residuals = np.asarray(y_host).ravel() - np.asarray(yhat).ravel()
-    else:
-        residuals = y_host - yhat
     if calc_dof:
         idmin = int(np.argmin(gcv["gcv_m"]))
         gcv_result = {

@@ -133,7 +133,7 @@ struct ColArgs {
 // grid (ceil(L1h/8), nslots, Hc); warp w handles column blockIdx.x*8+w.
 // W layout: [slot][hz][r][w1], r = x0 - q0 in [0, G0).
 template <int E>
-__global__ void __launch_bounds__(kFusedThreads)
+__global__ void __launch_bounds__(kFusedThreads, 3)
 colpass_kernel(ColArgs ca, const float2* __restrict__ Yt, const double2* __restrict__ F0,
                const float2* __restrict__ tw, const float2* __restrict__ tw2,
                float2* __restrict__ W) {
@@ -270,7 +270,7 @@ __device__ __forceinline__ void row_job(const RowArgs& ra, const RowJob& jb, int
 
 // S pass: grid (G0, Hc).  S planes (ns, H, G0*G1) float.
 template <int E>
-__global__ void __launch_bounds__(kFusedThreads)
+__global__ void __launch_bounds__(kFusedThreads, 2)
 rowpass_s_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
                  const double2* __restrict__ F1, const float2* __restrict__ tw,
                  const float2* __restrict__ tw2, float* __restrict__ S) {
@@ -304,7 +304,7 @@ rowpass_s_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
 // Products (c, i) go to Tsm[c * nt + i][x1]; the solve vector z = (S+lam I)^-1 e1
 // (order >= 1) or 1/max(s, thr) (order 0) per x1; m_c = sum_i z_i T_ci.
 template <int E>
-__global__ void __launch_bounds__(kFusedThreads)
+__global__ void __launch_bounds__(kFusedThreads, 2)
 rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
                        const double2* __restrict__ F1, const float2* __restrict__ tw,
                        const float2* __restrict__ tw2, int nt, int C, int ny,
@@ -375,6 +375,9 @@ struct Plan2D {
 template <typename K>
 static int set_smem(K kernel, size_t bytes) {
   FLPR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  // let several CTAs share an SM: take the whole unified L1/shared array as shared memory
+  FLPR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared));
   return FLPR_OK;
 }
 
@@ -547,7 +550,9 @@ static int fused_geom(const int* G, const int* L, const int* qout, int H, const 
   fg->q1 = qout[1];
   fg->M = (int64_t)G[0] * G[1];
   const size_t slab = (size_t)fg->G0 * fg->L1h;  // float2 per (slot, h)
-  const size_t budget_s = (size_t)256 << 20, budget_t = (size_t)64 << 20;
+  // T chunks of a few bandwidths: enough row-pass CTAs to fill the GPU while
+  // the column-pass output stays near the L2 size
+  const size_t budget_s = (size_t)256 << 20, budget_t = (size_t)192 << 20;
   int hs = (int)(budget_s / (sizeof(float2) * slab * t.s_nslots));
   int ht = (int)(budget_t / (sizeof(float2) * slab * t.t_nslots));
   fg->Hc_s = hs < 1 ? 1 : (hs > H ? H : hs);

@@ -450,6 +450,8 @@ static int launch_accumulate(const SpreadGeom& g, int64_t n, int nchan, int ones
   if (fixed) {
     auto k = tile_accumulate_kernel<long long, double, NT1>;
     FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   cudaSharedmemCarveoutMaxShared));
     k<<<grid, kSpreadThreads, smem, s>>>(g, n, nchan, ones_channel, cg, w.offsets, w.items,
                                          w.rec_base, (const double*)w.rec_frac,
                                          (const double*)w.rec_val, w.absum, margin,
@@ -457,6 +459,8 @@ static int launch_accumulate(const SpreadGeom& g, int64_t n, int nchan, int ones
   } else {
     auto k = tile_accumulate_kernel<double, double, NT1>;
     FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   cudaSharedmemCarveoutMaxShared));
     k<<<grid, kSpreadThreads, smem, s>>>(g, n, nchan, ones_channel, cg, w.offsets, w.items,
                                          w.rec_base, (const double*)w.rec_frac,
                                          (const double*)w.rec_val, nullptr, margin,
