@@ -52,6 +52,26 @@ def _as_column_matrix(x) -> np.ndarray:
     return arr.astype(float, copy=False)
 
 
+def _finite_flags(tensors) -> torch.Tensor:
+    """Device-side NaN/Inf scan: [any NaN, any Inf] per tensor, in order."""
+    out = []
+    for t in tensors:
+        out.append(torch.isnan(t).any())
+        out.append(torch.isinf(t).any())
+    return torch.stack(out)
+
+
+def _raise_nonfinite(flags: np.ndarray, names, fn: str) -> None:
+    """ValueError for the first NaN, then Inf, per input (api.py:310-323)."""
+    for k, (what, _) in enumerate(names):
+        if flags[2 * k]:
+            raise ValueError(f"{what} contains NaN values. Please remove or impute NaN values "
+                             f"before calling {fn}.")
+        if flags[2 * k + 1]:
+            raise ValueError(f"{what} contains Inf values. Please remove or handle Inf values "
+                             f"before calling {fn}.")
+
+
 def _default_hrange(points: np.ndarray) -> np.ndarray:
     scale = np.std(points, axis=0, ddof=1)
     scale[scale == 0] = 1.0
@@ -59,11 +79,13 @@ def _default_hrange(points: np.ndarray) -> np.ndarray:
 
 
 def _prepare_bandwidths(h, dims, options, default_range) -> np.ndarray:
-    """api.py:32-70."""
+    """api.py:32-70.  default_range may be a callable (evaluated only when h is None)."""
     if h is None:
         dh = options.get("dh", None)
         if dh is None:
             dh = 20 if dims == 1 else [20] * dims
+        if callable(default_range):
+            default_range = default_range()
         bw = get_hlist(dh, default_range)
     else:
         a = np.asarray(h, dtype=float)
@@ -151,7 +173,9 @@ class _Ctx:
         t = torch.from_numpy(np.ascontiguousarray(arr))
         if t.dtype != dtype:
             t = t.to(dtype)
-        return t.to(self.device, non_blocking=False)
+        # asynchronous from page-locked memory (stream-ordered before every kernel
+        # that reads it; the call returns only after the results are on the host)
+        return t.to(self.device, non_blocking=True)
 
     def check(self, status: int, what: str):
         _lib.check(status, what)
@@ -541,18 +565,7 @@ def cv_fastlpr(x, y, h=None, options: Optional[dict] = None) -> RegressionOutput
             f"y has {y_arr.shape[0]} samples.")
     if x_arr.shape[0] == 0:
         raise ValueError("Input x must have at least one sample.")
-    if np.any(np.isnan(x_arr)):
-        raise ValueError("Input x contains NaN values. Please remove or impute NaN values before "
-                         "calling cv_fastlpr.")
-    if np.any(np.isinf(x_arr)):
-        raise ValueError("Input x contains Inf values. Please remove or handle Inf values before "
-                         "calling cv_fastlpr.")
-    if np.any(np.isnan(y_arr)):
-        raise ValueError("Response y contains NaN values. Please remove or impute NaN values "
-                         "before calling cv_fastlpr.")
-    if np.any(np.isinf(y_arr)):
-        raise ValueError("Response y contains Inf values. Please remove or handle Inf values "
-                         "before calling cv_fastlpr.")
+
     opts = set_defaults(options, order=0, regularization=1e-8, num_dof_sample=10,
                         kernel_type="gaussian", y_type_out="mean", calc_dof=True,
                         gcv_selection="first")
@@ -569,7 +582,7 @@ def cv_fastlpr(x, y, h=None, options: Optional[dict] = None) -> RegressionOutput
     elif dims > 6:
         warnings.warn(f"dx={dims} is high-dimensional and may cause memory issues. "
                       "Consider dimensionality reduction techniques.", UserWarning)
-    bandwidths = _prepare_bandwidths(h, dims, opts, _default_hrange(x_arr))
+    bandwidths = _prepare_bandwidths(h, dims, opts, lambda: _default_hrange(x_arr))
     _check_supported(dims, opts)
     if dims == 3 and order == 2:
         raise ValueError("Order 2 not supported for 3D (max order 1)")
@@ -650,6 +663,11 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
             else:
                 ycols.append(ctx.upload(np.ascontiguousarray(col, dtype=float)))
     y_raw_dev = None
+    flags_h = None
+    if dev_inputs is None:
+        # NaN/Inf checks of the inputs (api.py:310-323) run on the device; the
+        # flags come back with the point statistics' synchronisation
+        flags_h = _to_host(_finite_flags([dx, torch.stack(ycols)]))
     ev.mark("upload")
     if variance:
         y_raw_dev = ycols[0]
@@ -661,6 +679,8 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
 
     G = _grid_shape(opts, n, d)
     stats = _point_stats(ctx, dx, n, d)
+    if flags_h is not None:
+        _raise_nonfinite(flags_h.numpy(), [("Input x", 0), ("Response y", 1)], "cv_fastlpr")
     geom = _make_geom(stats, n, d, G, int(opts["accuracy"]), bool(opts.get("flag_power2", True)))
     npow = 2 * order + 1
     F, bw, keep, _ = _filter_bandwidths(ctx, geom, bandwidths, npow)
@@ -922,12 +942,7 @@ def cv_fastkde(x, h=None, options: Optional[dict] = None) -> KDEOutput:
     n, dims = x_arr.shape
     if n < 2:
         raise ValueError(f"Input x must have at least 2 observations. Got {n} observations.")
-    if np.any(np.isnan(x_arr)):
-        raise ValueError("Input x contains NaN values. Please remove or impute NaN values before "
-                         "calling cv_fastkde.")
-    if np.any(np.isinf(x_arr)):
-        raise ValueError("Input x contains Inf values. Please remove or handle Inf values before "
-                         "calling cv_fastkde.")
+
     opts = set_defaults(options, order=0, calc_dof=False, y_type_out="mean")
     opts = set_defaults(opts, kernel_type="gaussian", verbose=False, dh=20)
     if opts.get("accuracy") is None:
@@ -935,7 +950,7 @@ def cv_fastkde(x, h=None, options: Optional[dict] = None) -> KDEOutput:
     if opts.get("N") is None:
         an = int(np.ceil(n ** (1.0 / dims)))
         opts["N"] = [an] * dims if dims > 1 else an
-    bandwidths = _prepare_bandwidths(h, dims, opts, _default_hrange(x_arr))
+    bandwidths = _prepare_bandwidths(h, dims, opts, lambda: _default_hrange(x_arr))
     _check_supported(dims, opts)
     Nopt = opts["N"]
     gs = Nopt if isinstance(Nopt, int) else (Nopt[0] if dims == 1 else Nopt)
@@ -952,7 +967,9 @@ def _fit_kde(ctx, x_arr, bandwidths, opts, G, prec):
     lib = ctx.lib
     n, d = x_arr.shape
     dx = ctx.upload(x_arr)
+    flags_h = _to_host(_finite_flags([dx]))
     stats = _point_stats(ctx, dx, n, d)
+    _raise_nonfinite(flags_h.numpy(), [("Input x", 0)], "cv_fastkde")
     geom = _make_geom(stats, n, d, G, int(opts["accuracy"]), bool(opts.get("flag_power2", True)))
     F, bw, keep, ihbad = _filter_bandwidths(ctx, geom, bandwidths, 1)
     if len(keep) != bandwidths.shape[0] or bw.shape[0] != bandwidths.shape[0]:

@@ -273,3 +273,22 @@ def test_fused_2d_path_matches_cufft_path_and_oracle(cuda_ok, order, G):
         assert rel_err(r.gcv_yhat["dof"], o["dof_all"]) < tol
         assert rel_err(r.s0, o["s0"]) < 1e-5
     assert rel_err(fused.yhat, plain.yhat) < tol
+
+
+@pytest.mark.parametrize("bad", [np.nan, np.inf])
+def test_validation_rejects_nonfinite(cuda_ok, bad):
+    """NaN/Inf inputs raise the reference's ValueError (checked on the device)."""
+    fl = _fastlpr()
+    x = np.random.default_rng(0).random((200, 1))
+    y = np.sin(x[:, 0])
+    word = "NaN" if np.isnan(bad) else "Inf"
+    xb = x.copy()
+    xb[3, 0] = bad
+    with pytest.raises(ValueError, match=f"Input x contains {word}"):
+        fl.cv_fastlpr(xb, y, [[0.2]], {"order": 1})
+    yb = y.copy()
+    yb[4] = bad
+    with pytest.raises(ValueError, match=f"Response y contains {word}"):
+        fl.cv_fastlpr(x, yb, [[0.2]], {"order": 1})
+    with pytest.raises(ValueError, match=f"Input x contains {word}"):
+        fl.cv_fastkde(xb, [[0.2]])
