@@ -90,7 +90,10 @@ struct Arena {
 struct ArenaSize {
   size_t used = 0;
   template <typename T>
-  void take(size_t count) { used = align_up(used) + align_up(count * sizeof(T)); }
+  T* take(size_t count) {
+    used = align_up(used) + align_up(count * sizeof(T));
+    return nullptr;
+  }
 };
 
 inline int sm_count() {

@@ -5,12 +5,15 @@
 //   column pass: W_{c,a0,h}(x0, w1) = IFFT_0(Y_c(., w1) A0_{h,a0})(x0), x0 cropped,
 //   row pass:    r(x0, x1) = C2R_1(W(x0, .) A1_{h,a1})(x1), x1 cropped,
 // and W is shared by every moment element with the same axis-0 exponent.
-// Each 1-D transform is one warp: a radix-2 DIF over the E = N/32 elements a
-// lane holds (n = 32 s + lane), a twiddle step, and a 32-point DIF across the
-// lanes with shuffles.  Two real row products share one complex transform
-// (both spectra are Hermitian).  The row pass of the T elements is fused
-// with the per-point FP64 solve and the dual-form reductions, so neither the
-// T planes nor the probe fits touch HBM.
+//
+// Each 1-D transform of length N = 32 E is one warp (four-step form,
+// N = E x 32): lane l holds x[32 s + l] in slot s; a radix-2 DIF over the E
+// slots, a twiddle step, a transpose through a per-warp shared-memory
+// buffer, and a second register DFT of length E leave lane t, slot s holding
+// X[t % E + E (t / E + (32 / E) brev(s))].  Two real row products share one
+// complex transform (both spectra are Hermitian).  The row pass of the T
+// elements is fused with the per-point FP64 solve and the dual-form
+// reductions, so neither the T planes nor the probe fits touch HBM.
 #include "common.cuh"
 #include "linalg.cuh"
 #include "plans.cuh"
@@ -20,14 +23,14 @@ namespace flpr {
 int global_scalar(int order, int nt, int H, int64_t M, const void* d_S, double* d_scalar, int prec,
                   cudaStream_t s);
 
-size_t fused_t_smem(int E, int G1, int nt, int C);
-
 namespace {
 
-constexpr int kFusedThreads = 256;
-constexpr int kColBlock = 8;     // columns per column-pass CTA (one per warp)
+constexpr int kColWarps = 8;    // columns per column-pass CTA (one per warp)
+constexpr int kRowWarps = 8;    // (row, job) items per S row-pass CTA (one per warp)
+constexpr int kMaxTWarps = 8;   // warps of a T row-pass CTA
 constexpr int kMaxSlots = 64;
 constexpr int kMaxJobs = 64;
+constexpr size_t kMaxSmem = 227 * 1024;
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -42,65 +45,128 @@ __host__ __device__ constexpr int brev(int x, int bits) {
 }
 __host__ __device__ constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x >> 1); }
 
-// Inverse (unnormalised) FFT of length N = 32 E held by one warp: on entry
-// lane l, slot s holds x[32 s + l]; on exit it holds X[brev_E(s) + E brev_5(l)].
-// tw[k] = exp(2 pi i k / N); tw2[k1 * 32 + l] = exp(2 pi i l k1 / N).
+// Floats of one warp's transpose buffer: E rows of 33 (padded), rounded so
+// that the column-pass write-out (8 warps' buffers read side by side as
+// float2) hits distinct banks: stride = 4 (mod 32) words.
+__host__ __device__ constexpr int warp_buf_stride(int E) { return ((33 * E + 31) / 32) * 32 + 4; }
+
+// Twiddle table of one axis, N + 32 entries: tw2[k1 * 32 + l] = exp(2 pi i l k1 / N)
+// for k1 < E, then tw32[m] = exp(2 pi i m / 32).
+__host__ __device__ constexpr int twiddle_entries(int N) { return N + 32; }
+
+// a * exp(2 pi i m / 32), m known after unrolling: quarter turns are exact.
+__device__ __forceinline__ float2 rot32(float2 a, int m, const float2* __restrict__ tw32) {
+  m &= 31;
+  if (m == 0) return a;
+  if (m == 8) return make_float2(-a.y, a.x);
+  if (m == 16) return make_float2(-a.x, -a.y);
+  if (m == 24) return make_float2(a.y, -a.x);
+  return cmul(a, tw32[m]);
+}
+
+// In-register radix-2 DIF (inverse sign) over the E slots: slot s ends up
+// holding output brev(s).  E <= 32, so every twiddle is a power of W_32.
 template <int E>
-__device__ __forceinline__ void warp_ifft(float2 (&v)[E], const float2* __restrict__ tw,
-                                          const float2* __restrict__ tw2, int lane) {
-  constexpr int N = 32 * E;
-  constexpr int EB = ilog2(E);
+__device__ __forceinline__ void dif_slots(float2 (&v)[E], const float2* __restrict__ tw32) {
 #pragma unroll
   for (int span = E / 2; span >= 1; span >>= 1) {
 #pragma unroll
     for (int s = 0; s < E; ++s) {
       if ((s & span) == 0) {
-        const int i = s & (span - 1);
         const float2 a = v[s], b = v[s + span];
         v[s] = cadd(a, b);
-        v[s + span] = i == 0 ? csub(a, b) : cmul(csub(a, b), tw[i * (N / (2 * span))]);
+        v[s + span] = rot32(csub(a, b), (s & (span - 1)) * (16 / span), tw32);
       }
-    }
-  }
-#pragma unroll
-  for (int s = 0; s < E; ++s) v[s] = cmul(v[s], tw2[brev(s, EB) * 32 + lane]);
-#pragma unroll
-  for (int span = 16; span >= 1; span >>= 1) {
-    const bool upper = (lane & span) != 0;
-    const float2 w = tw[(lane & (span - 1)) * (N / (2 * span))];
-#pragma unroll
-    for (int s = 0; s < E; ++s) {
-      float2 p;
-      p.x = __shfl_xor_sync(0xffffffffu, v[s].x, span);
-      p.y = __shfl_xor_sync(0xffffffffu, v[s].y, span);
-      v[s] = upper ? cmul(csub(p, v[s]), w) : cadd(v[s], p);
     }
   }
 }
 
-// tables for length N (tw: N entries, tw2: 32*N/32 entries) in global memory
-__global__ void twiddle_table_kernel(int N, float2* tw, float2* tw2) {
-  const int E = N / 32;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
-    double sn, cs;
-    sincospi(2.0 * (double)k / (double)N, &sn, &cs);
-    tw[k] = make_float2((float)cs, (float)sn);
-    const int k1 = k / 32, l = k % 32;
-    if (k1 < E) {
-      sincospi(2.0 * (double)((l * k1) % N) / (double)N, &sn, &cs);
-      tw2[k] = make_float2((float)cs, (float)sn);
+// Output index held by lane t, slot s after warp_ifft<E>.
+template <int E>
+__device__ __forceinline__ int out_index(int lane, int s) {
+  constexpr int EB = ilog2(E);
+  constexpr int P = 32 / E;
+  return (lane & (E - 1)) + E * ((lane >> EB) + P * brev(s, EB));
+}
+
+// Inverse (unnormalised) FFT of length N = 32 E held by one warp.  On entry
+// lane l, slot s holds x[32 s + l]; on exit lane t, slot s holds
+// X[out_index<E>(t, s)].  buf: this warp's warp_buf_stride(E) floats, free
+// again when the function returns.
+template <int E>
+__device__ __forceinline__ void warp_ifft(float2 (&v)[E], const float2* __restrict__ tw2,
+                                          const float2* __restrict__ tw32, float* buf, int lane) {
+  constexpr int EB = ilog2(E);
+  constexpr int P = 32 / E;
+  // DFT over n1 (n = 32 n1 + n2) for each n2 = lane
+  dif_slots<E>(v, tw32);
+  // twiddle W_N^(n2 k1), k1 = brev(s)
+#pragma unroll
+  for (int s = 1; s < E; ++s) v[s] = cmul(v[s], tw2[brev(s, EB) * 32 + lane]);
+  // transpose: lane t gathers row k1 = t % E (all 32 n2), real and imaginary
+  // parts in turn through the same E x 33 buffer
+  const int k1 = lane & (E - 1), part = lane >> EB;
+  float ur[32], ui[32];
+#pragma unroll
+  for (int s = 0; s < E; ++s) buf[brev(s, EB) * 33 + lane] = v[s].x;
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 32; ++j) ur[j] = buf[k1 * 33 + j];
+  __syncwarp();
+#pragma unroll
+  for (int s = 0; s < E; ++s) buf[brev(s, EB) * 33 + lane] = v[s].y;
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 32; ++j) ui[j] = buf[k1 * 33 + j];
+  __syncwarp();
+  // 32-point DFT over n2 at k2 = part + P k2': n2 = n2' + E q; the q-sum is a
+  // P-point DFT at frequency `part`, then W_32^(n2' part), then a length-E
+  // DFT over n2'
+#pragma unroll
+  for (int n = 0; n < E; ++n) {
+    float2 z = make_float2(ur[n], ui[n]);
+    if constexpr (P > 1) {
+#pragma unroll
+      for (int q = 1; q < P; ++q)
+        z = cadd(z, cmul(make_float2(ur[n + E * q], ui[n + E * q]), tw32[(E * q * part) & 31]));
+      if (n > 0) z = cmul(z, tw32[(n * part) & 31]);
     }
+    v[n] = z;
+  }
+  dif_slots<E>(v, tw32);
+}
+
+// Twiddle tables of one axis (layout of twiddle_entries).
+__global__ void twiddle_table_kernel(int N, float2* __restrict__ tab) {
+  const int total = twiddle_entries(N);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    double sn, cs;
+    if (k < N) {
+      const int k1 = k / 32, l = k % 32;  // l * k1 < N
+      sincospi(2.0 * (double)(l * k1) / (double)N, &sn, &cs);
+    } else {
+      sincospi(2.0 * (double)(k - N) / 32.0, &sn, &cs);
+    }
+    tab[k] = make_float2((float)cs, (float)sn);
+  }
+}
+
+// Per-axis kernel factor spectra in FP32: F (H, npow, L0) for axis 0 (times
+// `scale`) followed by (H, npow, L1) for axis 1, complex128 -> float2.
+__global__ void factor_f32_kernel(int64_t n0, int64_t ntot, double scale,
+                                  const double2* __restrict__ F, float2* __restrict__ Ff) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ntot;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 f = F[i];
+    const double s = i < n0 ? scale : 1.0;
+    Ff[i] = make_float2((float)(f.x * s), (float)(f.y * s));
   }
 }
 
 template <int E>
-__device__ __forceinline__ void load_twiddles(float2* s_tw, float2* s_tw2, const float2* tw,
-                                              const float2* tw2) {
-  constexpr int N = 32 * E;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    s_tw[i] = tw[i];
-    s_tw2[i] = tw2[i];
-  }
+__device__ __forceinline__ void load_twiddles(float2* s_tab, const float2* __restrict__ tab) {
+  constexpr int T = twiddle_entries(32 * E);
+  for (int i = threadIdx.x; i < T; i += blockDim.x) s_tab[i] = tab[i];
 }
 
 // (C, L0, L1h) -> (C, L1h, L0)
@@ -125,54 +191,52 @@ __global__ void transpose_spec_kernel(int C, int L0, int L1h, const float2* __re
 struct ColArgs {
   int L0, L1h, G0, q0;
   int npow, hbase, nslots;
-  double scale;
   int slot_chan[kMaxSlots];
   int slot_pow[kMaxSlots];
 };
 
 // grid (ceil(L1h/8), nslots, Hc); warp w handles column blockIdx.x*8+w.
-// W layout: [slot][hz][r][w1], r = x0 - q0 in [0, G0).
+// W layout: [slot][hz][r][w1], r = x0 - q0 in [0, G0).  Each warp stages its
+// cropped column in its own transpose buffer; the CTA then writes 8-column
+// row segments.
 template <int E>
-__global__ void __launch_bounds__(kFusedThreads, 3)
-colpass_kernel(ColArgs ca, const float2* __restrict__ Yt, const double2* __restrict__ F0,
-               const float2* __restrict__ tw, const float2* __restrict__ tw2,
-               float2* __restrict__ W) {
+__global__ void __launch_bounds__(kColWarps * 32, 2)
+colpass_kernel(ColArgs ca, const float2* __restrict__ Yt, const float2* __restrict__ F0f,
+               const float2* __restrict__ tab, float2* __restrict__ W) {
   constexpr int N = 32 * E;
-  constexpr int EB = ilog2(E);
+  constexpr int SW = warp_buf_stride(E);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* s_tw = reinterpret_cast<float2*>(smem_raw);
-  float2* s_tw2 = s_tw + N;
-  float2* stage = s_tw2 + N;  // G0 x 8
-  load_twiddles<E>(s_tw, s_tw2, tw, tw2);
+  float2* s_tw2 = reinterpret_cast<float2*>(smem_raw);
+  float2* s_tw32 = s_tw2 + N;
+  float* bufs = reinterpret_cast<float*>(s_tw2 + twiddle_entries(N));
+  load_twiddles<E>(s_tw2, tab);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int slot = blockIdx.y, hz = blockIdx.z, h = ca.hbase + hz;
   const int c = ca.slot_chan[slot], a0 = ca.slot_pow[slot];
-  const int w1 = blockIdx.x * kColBlock + warp;
+  const int w1 = blockIdx.x * kColWarps + warp;
+  float* buf = bufs + warp * SW;
   if (w1 < ca.L1h) {
-    const float2* col = Yt + ((size_t)c * ca.L1h + w1) * N;
-    const double2* f = F0 + ((size_t)h * ca.npow + a0) * N;
+    const float2* col = Yt + ((size_t)c * ca.L1h + w1) * N + lane;
+    const float2* f = F0f + ((size_t)h * ca.npow + a0) * N + lane;
     float2 v[E];
 #pragma unroll
-    for (int s = 0; s < E; ++s) {
-      const int k = 32 * s + lane;
-      const double2 fv = f[k];
-      const float2 y = col[k];
-      v[s] = cmul(y, make_float2((float)(fv.x * ca.scale), (float)(fv.y * ca.scale)));
-    }
-    warp_ifft<E>(v, s_tw, s_tw2, lane);
+    for (int s = 0; s < E; ++s) v[s] = cmul(col[32 * s], f[32 * s]);
+    warp_ifft<E>(v, s_tw2, s_tw32, buf, lane);
+    float2* stage = reinterpret_cast<float2*>(buf);
 #pragma unroll
     for (int s = 0; s < E; ++s) {
-      const int r = brev(s, EB) + E * brev(lane, 5) - ca.q0;
-      if (r >= 0 && r < ca.G0) stage[r * kColBlock + warp] = v[s];
+      const int r = out_index<E>(lane, s) - ca.q0;
+      if (r >= 0 && r < ca.G0) stage[r] = v[s];
     }
   }
   __syncthreads();
   float2* out = W + ((size_t)slot * gridDim.z + hz) * ca.G0 * ca.L1h;
-  for (int i = threadIdx.x; i < ca.G0 * kColBlock; i += blockDim.x) {
-    const int r = i / kColBlock, wl = i - r * kColBlock;
-    const int col = blockIdx.x * kColBlock + wl;
-    if (col < ca.L1h) out[(size_t)r * ca.L1h + col] = stage[i];
+  for (int i = threadIdx.x; i < ca.G0 * kColWarps; i += blockDim.x) {
+    const int r = i / kColWarps, wl = i - r * kColWarps;
+    const int colw = blockIdx.x * kColWarps + wl;
+    if (colw < ca.L1h)
+      out[(size_t)r * ca.L1h + colw] = reinterpret_cast<const float2*>(bufs + wl * SW)[r];
   }
 }
 
@@ -216,161 +280,203 @@ struct RowArgs {
   RowJob jobs[kMaxJobs];
 };
 
-// Hermitian-extended spectrum value k of product W_row * A1 (k in [0, L1)).
-__device__ __forceinline__ float2 herm_product(const float2* __restrict__ wrow,
-                                               const double2* __restrict__ f, int k, int N) {
-  const bool mirror = k > N / 2;
-  const int kk = mirror ? N - k : k;
-  const float2 w = wrow[kk];
-  const double2 a = f[kk];
-  float2 p = cmul(w, make_float2((float)a.x, (float)a.y));
-  if (kk == 0 || 2 * kk == N) p.y = 0.0f;
-  if (mirror) p.y = -p.y;
+// Slot s of the Hermitian extension of the product W_row * A1: element
+// k = 32 s + lane, mirrored (conjugated) above N/2; the DC and Nyquist terms
+// are real.  lo = row + lane, hi = row + N - lane.
+template <int E>
+__device__ __forceinline__ float2 herm_product(const float2* __restrict__ wlo,
+                                               const float2* __restrict__ flo,
+                                               const float2* __restrict__ whi,
+                                               const float2* __restrict__ fhi, int s, int lane) {
+  float2 p;
+  if (s < E / 2) {
+    p = cmul(wlo[32 * s], flo[32 * s]);
+    if (s == 0 && lane == 0) p.y = 0.0f;
+  } else {
+    p = cmul(whi[-32 * s], fhi[-32 * s]);
+    p.y = (s == E / 2 && lane == 0) ? 0.0f : -p.y;
+  }
   return p;
 }
 
-// One warp computes the products of one job for row r and leaves the cropped
-// real results (x1 - q1 in [0, G1)) in out_a / out_b (shared memory rows).
+// One warp: the inverse transform of job jb for row r; on return lane t,
+// slot s holds the products a (real part) and b (imaginary part) at
+// x1 = out_index(t, s).
 template <int E>
-__device__ __forceinline__ void row_job(const RowArgs& ra, const RowJob& jb, int r, int hz, int h,
+__device__ __forceinline__ void row_fft(const RowArgs& ra, const RowJob& jb, int r, int hz, int h,
                                         int nslots_w, const float2* __restrict__ W,
-                                        const double2* __restrict__ F1, const float2* s_tw,
-                                        const float2* s_tw2, int lane, float* out_a,
-                                        float* out_b) {
+                                        const float2* __restrict__ F1f, const float2* s_tw2,
+                                        const float2* s_tw32, float* buf, int lane,
+                                        float2 (&v)[E]) {
   constexpr int N = 32 * E;
-  constexpr int EB = ilog2(E);
   const size_t rowstride = (size_t)ra.L1h;
   const float2* wa = W + (((size_t)jb.slot_a * nslots_w + hz) * ra.G0 + r) * rowstride;
-  const double2* fa = F1 + ((size_t)h * ra.npow + jb.pow_a) * N;
-  const bool pair = jb.slot_b >= 0;
-  const float2* wb = pair ? W + (((size_t)jb.slot_b * nslots_w + hz) * ra.G0 + r) * rowstride : wa;
-  const double2* fb = pair ? F1 + ((size_t)h * ra.npow + jb.pow_b) * N : fa;
-  float2 v[E];
+  const float2* fa = F1f + ((size_t)h * ra.npow + jb.pow_a) * N;
+  if (jb.slot_b >= 0) {
+    const float2* wb = W + (((size_t)jb.slot_b * nslots_w + hz) * ra.G0 + r) * rowstride;
+    const float2* fb = F1f + ((size_t)h * ra.npow + jb.pow_b) * N;
 #pragma unroll
-  for (int s = 0; s < E; ++s) {
-    const int k = 32 * s + lane;
-    const float2 pa = herm_product(wa, fa, k, N);
-    float2 z = pa;
-    if (pair) {
-      const float2 pb = herm_product(wb, fb, k, N);
-      z = make_float2(pa.x - pb.y, pa.y + pb.x);
+    for (int s = 0; s < E; ++s) {
+      const float2 pa = herm_product<E>(wa + lane, fa + lane, wa + N - lane, fa + N - lane, s, lane);
+      const float2 pb = herm_product<E>(wb + lane, fb + lane, wb + N - lane, fb + N - lane, s, lane);
+      v[s] = make_float2(pa.x - pb.y, pa.y + pb.x);
     }
-    v[s] = z;
-  }
-  warp_ifft<E>(v, s_tw, s_tw2, lane);
+  } else {
 #pragma unroll
-  for (int s = 0; s < E; ++s) {
-    const int x = brev(s, EB) + E * brev(lane, 5) - ra.q1;
-    if (x >= 0 && x < ra.G1) {
-      out_a[x] = v[s].x;
-      if (pair) out_b[x] = v[s].y;
-    }
+    for (int s = 0; s < E; ++s)
+      v[s] = herm_product<E>(wa + lane, fa + lane, wa + N - lane, fa + N - lane, s, lane);
   }
+  warp_ifft<E>(v, s_tw2, s_tw32, buf, lane);
 }
 
-// S pass: grid (G0, Hc).  S planes (ns, H, G0*G1) float.
+// S pass: grid (ceil(G0 * njobs / 8), Hc); warp w takes item blockIdx.x*8+w =
+// (row, job).  S planes (ns, H, G0*G1) float, written straight from the
+// registers (consecutive lanes hold consecutive x1).
 template <int E>
-__global__ void __launch_bounds__(kFusedThreads, 2)
+__global__ void __launch_bounds__(kRowWarps * 32, 2)
 rowpass_s_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
-                 const double2* __restrict__ F1, const float2* __restrict__ tw,
-                 const float2* __restrict__ tw2, float* __restrict__ S) {
+                 const float2* __restrict__ F1f, const float2* __restrict__ tab,
+                 float* __restrict__ S) {
   constexpr int N = 32 * E;
+  constexpr int SW = warp_buf_stride(E);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* s_tw = reinterpret_cast<float2*>(smem_raw);
-  float2* s_tw2 = s_tw + N;
-  float* rows = reinterpret_cast<float*>(s_tw2 + N);  // (nwarps, 2, G1)
-  load_twiddles<E>(s_tw, s_tw2, tw, tw2);
+  float2* s_tw2 = reinterpret_cast<float2*>(smem_raw);
+  float2* s_tw32 = s_tw2 + N;
+  float* bufs = reinterpret_cast<float*>(s_tw2 + twiddle_entries(N));
+  load_twiddles<E>(s_tw2, tab);
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  const int r = blockIdx.x, hz = blockIdx.y, h = ra.hbase + hz;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.x * kRowWarps + warp;
+  if (item >= ra.G0 * ra.njobs) return;
+  const int r = item / ra.njobs, j = item - r * ra.njobs;
+  const int hz = blockIdx.y, h = ra.hbase + hz;
   const int64_t M = (int64_t)ra.G0 * ra.G1;
-  float* ra_row = rows + (size_t)warp * 2 * ra.G1;
-  float* rb_row = ra_row + ra.G1;
-  for (int j = warp; j < ra.njobs; j += nwarps) {
-    const RowJob jb = ra.jobs[j];
-    row_job<E>(ra, jb, r, hz, h, nslots_w, W, F1, s_tw, s_tw2, lane, ra_row, rb_row);
-    __syncwarp();
-    float* da = S + ((size_t)jb.out_a * H + h) * M + (size_t)r * ra.G1;
-    for (int x = lane; x < ra.G1; x += 32) da[x] = ra_row[x];
-    if (jb.slot_b >= 0) {
-      float* db = S + ((size_t)jb.out_b * H + h) * M + (size_t)r * ra.G1;
-      for (int x = lane; x < ra.G1; x += 32) db[x] = rb_row[x];
+  const RowJob jb = ra.jobs[j];
+  const bool pair = jb.slot_b >= 0;
+  float2 v[E];
+  row_fft<E>(ra, jb, r, hz, h, nslots_w, W, F1f, s_tw2, s_tw32, bufs + warp * SW, lane, v);
+  float* da = S + ((size_t)jb.out_a * H + h) * M + (size_t)r * ra.G1;
+  float* db = S + ((size_t)(pair ? jb.out_b : jb.out_a) * H + h) * M + (size_t)r * ra.G1;
+#pragma unroll
+  for (int s = 0; s < E; ++s) {
+    const int x = out_index<E>(lane, s) - ra.q1;
+    if (x >= 0 && x < ra.G1) {
+      da[x] = v[s].x;
+      if (pair) db[x] = v[s].y;
     }
-    __syncwarp();
   }
 }
 
-// T pass fused with the solve and the dual-form reductions: grid (G0, Hc).
-// Products (c, i) go to Tsm[c * nt + i][x1]; the solve vector z = (S+lam I)^-1 e1
-// (order >= 1) or 1/max(s, thr) (order 0) per x1; m_c = sum_i z_i T_ci.
-template <int E>
-__global__ void __launch_bounds__(kFusedThreads, 2)
+// Shared memory of the T pass: twiddles, one transpose buffer per warp, and
+// 2*G1 floats for each job that is not the last job of its warp (the last
+// job of warp w leaves its results in w's own buffer).
+inline size_t t_smem_bytes(int E, int nwarps, int njobs, int G1) {
+  const int extra = njobs > nwarps ? njobs - nwarps : 0;
+  return sizeof(float2) * (size_t)twiddle_entries(32 * E) +
+         sizeof(float) * ((size_t)nwarps * warp_buf_stride(E) + (size_t)extra * 2 * G1);
+}
+
+// Warps of a T-pass CTA: as few rounds of at most kMaxTWarps jobs as
+// possible, spread evenly.
+inline int t_warps(int njobs) {
+  const int rounds = (njobs + kMaxTWarps - 1) / kMaxTWarps;
+  return (njobs + rounds - 1) / rounds;
+}
+
+// T pass fused with the solve and the dual-form reductions: grid (G0, Hc),
+// t_warps(njobs) warps.  Warp w computes jobs w, w + nwarps, ...; product
+// p = c * NT + i (job p / 2, half p % 2) stays in shared memory until every
+// job of the row is done; then m_c(x1) = sum_i z_i(x1) T(p, x1) with z the
+// row's solve vectors, the response fits go to `my`, and sum_x1 m_c Q_c goes
+// to one partial per (c, h, row).
+template <int E, int NT>
+__global__ void __launch_bounds__(kMaxTWarps * 32, 2)
 rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
-                       const double2* __restrict__ F1, const float2* __restrict__ tw,
-                       const float2* __restrict__ tw2, int nt, int C, int ny,
-                       const double* __restrict__ zg, const double* __restrict__ Q,
-                       double* __restrict__ my, double* __restrict__ dots) {
+                       const float2* __restrict__ F1f, const float2* __restrict__ tab, int C,
+                       int ny, const double* __restrict__ zg, const double* __restrict__ Q,
+                       double* __restrict__ my, double* __restrict__ dpart) {
   constexpr int N = 32 * E;
+  constexpr int SW = warp_buf_stride(E);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* s_tw = reinterpret_cast<float2*>(smem_raw);
-  float2* s_tw2 = s_tw + N;
-  double* zsm = reinterpret_cast<double*>(s_tw2 + N);          // G1 x nt
-  float* Tsm = reinterpret_cast<float*>(zsm + (size_t)ra.G1 * nt);  // (C*nt) x G1
-  __shared__ double red[kFusedThreads / 32];
-  load_twiddles<E>(s_tw, s_tw2, tw, tw2);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  __shared__ double red[kMaxTWarps * 32];
+  float2* s_tw2 = reinterpret_cast<float2*>(smem_raw);
+  float2* s_tw32 = s_tw2 + N;
+  float* bufs = reinterpret_cast<float*>(s_tw2 + twiddle_entries(N));
+  const int nwarps = blockDim.x >> 5;
+  float* regions = bufs + (size_t)nwarps * SW;
+  load_twiddles<E>(s_tw2, tab);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int r = blockIdx.x, hz = blockIdx.y, h = ra.hbase + hz;
   const int64_t M = (int64_t)ra.G0 * ra.G1;
-  // phase 1: the row's solve vectors
-  {
-    const double* src = zg + ((int64_t)h * M + (int64_t)r * ra.G1) * nt;
-    for (int i = threadIdx.x; i < ra.G1 * nt; i += blockDim.x) zsm[i] = src[i];
-  }
-  __syncthreads();
-  // phase 2: T products
-  for (int j = warp; j < ra.njobs; j += nwarps) {
+  const int G1 = ra.G1, njobs = ra.njobs;
+  const int last0 = njobs - nwarps;  // jobs >= last0 are the last of their warp
+  float* buf = bufs + warp * SW;
+  for (int j = warp; j < njobs; j += nwarps) {
     const RowJob jb = ra.jobs[j];
-    float* oa = Tsm + (size_t)jb.out_a * ra.G1;
-    float* ob = jb.slot_b >= 0 ? Tsm + (size_t)jb.out_b * ra.G1 : oa;
-    row_job<E>(ra, jb, r, hz, h, nslots_w, W, F1, s_tw, s_tw2, lane, oa, ob);
+    const bool pair = jb.slot_b >= 0;
+    float2 v[E];
+    row_fft<E>(ra, jb, r, hz, h, nslots_w, W, F1f, s_tw2, s_tw32, buf, lane, v);
+    float* dst = j >= last0 ? buf : regions + (size_t)j * 2 * G1;
+#pragma unroll
+    for (int s = 0; s < E; ++s) {
+      const int x = out_index<E>(lane, s) - ra.q1;
+      if (x >= 0 && x < G1) {
+        dst[x] = v[s].x;
+        if (pair) dst[G1 + x] = v[s].y;
+      }
+    }
+    __syncwarp();
   }
   __syncthreads();
-  // phase 3: m, fitted grids, dots
   for (int c = 0; c < C; ++c) {
+    const float* src[NT];
+#pragma unroll
+    for (int i = 0; i < NT; ++i) {
+      const int p = c * NT + i, j = p >> 1;
+      src[i] = (j >= last0 ? bufs + (size_t)(j % nwarps) * SW : regions + (size_t)j * 2 * G1) +
+               (p & 1) * G1;
+    }
     double acc = 0.0;
-    for (int x = threadIdx.x; x < ra.G1; x += blockDim.x) {
-      const double* z = zsm + (size_t)x * nt;
+    for (int x = threadIdx.x; x < G1; x += blockDim.x) {
+      const int64_t g = (int64_t)r * G1 + x;
+      const double* z = zg + ((int64_t)h * M + g) * NT;
       double m = 0.0;
-      for (int i = 0; i < nt; ++i) m += z[i] * (double)Tsm[(size_t)(c * nt + i) * ra.G1 + x];
-      const int64_t g = (int64_t)r * ra.G1 + x;
+#pragma unroll
+      for (int i = 0; i < NT; ++i) m += z[i] * (double)src[i][x];
       if (c < ny) my[((int64_t)h * M + g) * ny + c] = m;
       acc += m * Q[g * C + c];
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) red[warp] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double s = 0.0;
-      for (int w = 0; w < nwarps; ++w) s += red[w];
-      atomicAdd(&dots[(int64_t)c * H + h], s);
-    }
+    if (lane == 0) red[c * nwarps + warp] = acc;  // C * nwarps <= 32 * kMaxTWarps
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < C; c += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < nwarps; ++w) s += red[c * nwarps + w];
+    dpart[((int64_t)c * H + h) * ra.G0 + r] = s;
+  }
+}
+
+// dots[c, h] = sum of the row partials (fixed order: deterministic).
+__global__ void dots_reduce_kernel(int CH, int G0, const double* __restrict__ dpart,
+                                   double* __restrict__ dots) {
+  const int ch = blockIdx.x;
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int r = threadIdx.x; r < G0; r += blockDim.x) s += dpart[(int64_t)ch * G0 + r];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
     __syncthreads();
   }
+  if (threadIdx.x == 0 && ch < CH) dots[ch] = sh[0];
 }
 
 }  // namespace
 
-size_t fused_t_smem(int E, int G1, int nt, int C) {
-  return sizeof(float2) * 2 * 32 * (size_t)E + sizeof(double) * (size_t)G1 * nt +
-         sizeof(float) * (size_t)C * nt * G1;
-}
-
 namespace {
-
-struct Plan2D {
-  int L0, L1, L1h, G0, G1, q0, q1, E0, E1;
-  int64_t M;
-};
 
 template <typename K>
 static int set_smem(K kernel, size_t bytes) {
@@ -381,41 +487,56 @@ static int set_smem(K kernel, size_t bytes) {
   return FLPR_OK;
 }
 
+static size_t warp_pass_smem(int E, int nwarps) {
+  return sizeof(float2) * (size_t)twiddle_entries(32 * E) +
+         sizeof(float) * (size_t)nwarps * warp_buf_stride(E);
+}
+
 template <int E>
 static int launch_col(const ColArgs& ca, int ncolblk, int nslots, int Hc, const float2* Yt,
-                      const double2* F0, const float2* tw, const float2* tw2, float2* W,
-                      cudaStream_t s) {
-  constexpr int N = 32 * E;
-  size_t smem = sizeof(float2) * (2 * N + (size_t)ca.G0 * kColBlock);
+                      const float2* F0f, const float2* tab, float2* W, cudaStream_t s) {
+  const size_t smem = warp_pass_smem(E, kColWarps);
   FLPR_TRY(set_smem(colpass_kernel<E>, smem));
-  colpass_kernel<E><<<dim3(ncolblk, nslots, Hc), kFusedThreads, smem, s>>>(ca, Yt, F0, tw, tw2, W);
+  colpass_kernel<E><<<dim3(ncolblk, nslots, Hc), kColWarps * 32, smem, s>>>(ca, Yt, F0f, tab, W);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
 
 template <int E>
-static int launch_row_s(const RowArgs& ra, int G0, int Hc, int H, int nslots_w, const float2* W,
-                        const double2* F1, const float2* tw, const float2* tw2, float* S,
-                        cudaStream_t s) {
-  constexpr int N = 32 * E;
-  size_t smem = sizeof(float2) * 2 * N + sizeof(float) * (kFusedThreads / 32) * 2 * ra.G1;
+static int launch_row_s(const RowArgs& ra, int Hc, int H, int nslots_w, const float2* W,
+                        const float2* F1f, const float2* tab, float* S, cudaStream_t s) {
+  const size_t smem = warp_pass_smem(E, kRowWarps);
   FLPR_TRY(set_smem(rowpass_s_kernel<E>, smem));
-  rowpass_s_kernel<E><<<dim3(G0, Hc), kFusedThreads, smem, s>>>(ra, H, nslots_w, W, F1, tw, tw2, S);
+  const int items = ra.G0 * ra.njobs;
+  rowpass_s_kernel<E><<<dim3((items + kRowWarps - 1) / kRowWarps, Hc), kRowWarps * 32, smem, s>>>(
+      ra, H, nslots_w, W, F1f, tab, S);
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
+template <int E, int NT>
+static int launch_row_t_nt(const RowArgs& ra, int Hc, int H, int nslots_w, const float2* W,
+                           const float2* F1f, const float2* tab, int C, int ny, const double* z,
+                           const double* Q, double* my, double* dpart, cudaStream_t s) {
+  const int nwarps = t_warps(ra.njobs);
+  const size_t smem = t_smem_bytes(E, nwarps, ra.njobs, ra.G1);
+  FLPR_TRY(set_smem(rowpass_t_solve_kernel<E, NT>, smem));
+  rowpass_t_solve_kernel<E, NT><<<dim3(ra.G0, Hc), nwarps * 32, smem, s>>>(
+      ra, H, nslots_w, W, F1f, tab, C, ny, z, Q, my, dpart);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
 
 template <int E>
-static int launch_row_t(const RowArgs& ra, int G0, int Hc, int H, int nslots_w, const float2* W,
-                        const double2* F1, const float2* tw, const float2* tw2, int nt, int C,
-                        int ny, const double* z, const double* Q, double* my, double* dots,
-                        cudaStream_t s) {
-  size_t smem = fused_t_smem(E, ra.G1, nt, C);
-  FLPR_TRY(set_smem(rowpass_t_solve_kernel<E>, smem));
-  rowpass_t_solve_kernel<E><<<dim3(G0, Hc), kFusedThreads, smem, s>>>(
-      ra, H, nslots_w, W, F1, tw, tw2, nt, C, ny, z, Q, my, dots);
-  FLPR_LAUNCH_CHECK();
-  return FLPR_OK;
+static int launch_row_t(int nt, const RowArgs& ra, int Hc, int H, int nslots_w, const float2* W,
+                        const float2* F1f, const float2* tab, int C, int ny, const double* z,
+                        const double* Q, double* my, double* dpart, cudaStream_t s) {
+  switch (nt) {
+    case 1: return launch_row_t_nt<E, 1>(ra, Hc, H, nslots_w, W, F1f, tab, C, ny, z, Q, my, dpart, s);
+    case 3: return launch_row_t_nt<E, 3>(ra, Hc, H, nslots_w, W, F1f, tab, C, ny, z, Q, my, dpart, s);
+    case 6: return launch_row_t_nt<E, 6>(ra, Hc, H, nslots_w, W, F1f, tab, C, ny, z, Q, my, dpart, s);
+    default: set_error("fused2d: nt=%d", nt); return FLPR_ERR_ARG;
+  }
 }
 
 // Slot/job tables of one configuration.
@@ -532,6 +653,7 @@ static int build_tables(int order, int C, FusedTables* t) {
 
 static bool pow2_in(int v, int lo, int hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
 
+
 struct FusedGeom {
   int L0, L1, L1h, G0, G1, q0, q1;
   int64_t M;
@@ -550,7 +672,7 @@ static int fused_geom(const int* G, const int* L, const int* qout, int H, const 
   fg->q1 = qout[1];
   fg->M = (int64_t)G[0] * G[1];
   const size_t slab = (size_t)fg->G0 * fg->L1h;  // float2 per (slot, h)
-  // T chunks of a few bandwidths: enough row-pass CTAs to fill the GPU while
+  // chunks of a few bandwidths: enough row-pass CTAs to fill the GPU while
   // the column-pass output stays near the L2 size
   const size_t budget_s = (size_t)256 << 20, budget_t = (size_t)192 << 20;
   int hs = (int)(budget_s / (sizeof(float2) * slab * t.s_nslots));
@@ -563,23 +685,47 @@ static int fused_geom(const int* G, const int* L, const int* qout, int H, const 
   return FLPR_OK;
 }
 
+// Workspace carve-up, shared by the size query and the run.
+struct FusedBuffers {
+  float2 *Yt, *W, *tab0, *tab1, *Ff;
+  double *z, *dpart;
+};
+
+template <typename A>
+static void carve(A& ar, const FusedTables& tb, const FusedGeom& fg, int H, int npow, int C,
+                  FusedBuffers* b) {
+  b->Yt = ar.template take<float2>((size_t)(1 + C) * fg.L1h * fg.L0);
+  b->W = ar.template take<float2>(fg.w_elems);
+  b->tab0 = ar.template take<float2>(twiddle_entries(fg.L0));
+  b->tab1 = ar.template take<float2>(twiddle_entries(fg.L1));
+  b->Ff = ar.template take<float2>((size_t)H * npow * (fg.L0 + fg.L1));
+  b->z = ar.template take<double>((size_t)H * fg.M * tb.nt);
+  b->dpart = ar.template take<double>((size_t)C * H * fg.G0);
+}
+
 template <int E0, int E1>
 static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow, int order, int C,
                      int ny, const float2* spec, const double2* F, double scale, const double* Q,
-                     double reg, float* S, double* my, double* dots, double* scalar, float2* Yt,
-                     float2* W, float2* tw0, float2* tw20, float2* tw1, float2* tw21,
-                     double* zbuf, cudaStream_t s) {
+                     double reg, float* S, double* my, double* dots, double* scalar,
+                     const FusedBuffers& b, cudaStream_t s) {
   const int nt = tb.nt;
-  const double2* F0 = F;
-  const double2* F1 = F + (size_t)H * npow * fg.L0;
-  twiddle_table_kernel<<<(fg.L0 + 255) / 256, 256, 0, s>>>(fg.L0, tw0, tw20);
+  twiddle_table_kernel<<<(twiddle_entries(fg.L0) + 255) / 256, 256, 0, s>>>(fg.L0, b.tab0);
   FLPR_LAUNCH_CHECK();
-  twiddle_table_kernel<<<(fg.L1 + 255) / 256, 256, 0, s>>>(fg.L1, tw1, tw21);
+  twiddle_table_kernel<<<(twiddle_entries(fg.L1) + 255) / 256, 256, 0, s>>>(fg.L1, b.tab1);
   FLPR_LAUNCH_CHECK();
+  {
+    const int64_t n0 = (int64_t)H * npow * fg.L0, ntot = (int64_t)H * npow * (fg.L0 + fg.L1);
+    int nb = (int)((ntot + 255) / 256);
+    if (nb > 4 * sm_count()) nb = 4 * sm_count();
+    factor_f32_kernel<<<nb, 256, 0, s>>>(n0, ntot, scale, F, b.Ff);
+    FLPR_LAUNCH_CHECK();
+  }
+  const float2* F0f = b.Ff;
+  const float2* F1f = b.Ff + (size_t)H * npow * fg.L0;
   transpose_spec_kernel<<<dim3((fg.L1h + 31) / 32, (fg.L0 + 31) / 32, 1 + C), dim3(32, 8), 0, s>>>(
-      1 + C, fg.L0, fg.L1h, spec, Yt);
+      1 + C, fg.L0, fg.L1h, spec, b.Yt);
   FLPR_LAUNCH_CHECK();
-  const int ncolblk = (fg.L1h + kColBlock - 1) / kColBlock;
+  const int ncolblk = (fg.L1h + kColWarps - 1) / kColWarps;
   // S pass
   ColArgs ca = tb.s_col;
   ca.L0 = fg.L0;
@@ -588,7 +734,6 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
   ca.q0 = fg.q0;
   ca.npow = npow;
   ca.nslots = tb.s_nslots;
-  ca.scale = scale;
   RowArgs ra = tb.s_row;
   ra.L1 = fg.L1;
   ra.L1h = fg.L1h;
@@ -600,19 +745,18 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
     const int hc = H - h0 < fg.Hc_s ? H - h0 : fg.Hc_s;
     ca.hbase = h0;
     ra.hbase = h0;
-    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.s_nslots, hc, Yt, F0, tw0, tw20, W, s));
-    FLPR_TRY(launch_row_s<E1>(ra, fg.G0, hc, H, hc, W, F1, tw1, tw21, S, s));
+    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.s_nslots, hc, b.Yt, F0f, b.tab0, b.W, s));
+    FLPR_TRY(launch_row_s<E1>(ra, hc, H, hc, b.W, F1f, b.tab1, S, s));
   }
   FLPR_TRY(global_scalar(order, nt, H, fg.M, S, scalar, FLPR_PREC_F32, s));
-  FLPR_CUDA(cudaMemsetAsync(dots, 0, sizeof(double) * (size_t)C * H, s));
   {
     const int64_t HM = (int64_t)H * fg.M;
     int nb = (int)((HM + 255) / 256);
     if (nb > 16 * sm_count()) nb = 16 * sm_count();
     switch (nt) {
-      case 1: zvec_kernel<1><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, zbuf); break;
-      case 3: zvec_kernel<3><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, zbuf); break;
-      case 6: zvec_kernel<6><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, zbuf); break;
+      case 1: zvec_kernel<1><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, b.z); break;
+      case 3: zvec_kernel<3><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, b.z); break;
+      case 6: zvec_kernel<6><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, b.z); break;
       default: set_error("fused2d: nt=%d", nt); return FLPR_ERR_ARG;
     }
     FLPR_LAUNCH_CHECK();
@@ -625,7 +769,6 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
   ca.q0 = fg.q0;
   ca.npow = npow;
   ca.nslots = tb.t_nslots;
-  ca.scale = scale;
   ra = tb.t_row;
   ra.L1 = fg.L1;
   ra.L1h = fg.L1h;
@@ -637,10 +780,12 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
     const int hc = H - h0 < fg.Hc_t ? H - h0 : fg.Hc_t;
     ca.hbase = h0;
     ra.hbase = h0;
-    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.t_nslots, hc, Yt, F0, tw0, tw20, W, s));
-    FLPR_TRY(launch_row_t<E1>(ra, fg.G0, hc, H, hc, W, F1, tw1, tw21, nt, C, ny, zbuf, Q, my,
-                              dots, s));
+    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.t_nslots, hc, b.Yt, F0f, b.tab0, b.W, s));
+    FLPR_TRY(launch_row_t<E1>(nt, ra, hc, H, hc, b.W, F1f, b.tab1, C, ny, b.z, Q, my, b.dpart,
+                              s));
   }
+  dots_reduce_kernel<<<C * H, 256, 0, s>>>(C * H, fg.G0, b.dpart, dots);
+  FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
 
@@ -648,12 +793,11 @@ template <int E0>
 static int dispatch_e1(int E1, const FusedTables& tb, const FusedGeom& fg, int H, int npow,
                        int order, int C, int ny, const float2* spec, const double2* F,
                        double scale, const double* Q, double reg, float* S, double* my,
-                       double* dots, double* scalar, float2* Yt, float2* W, float2* tw0,
-                       float2* tw20, float2* tw1, float2* tw21, double* zbuf, cudaStream_t s) {
-#define FLPR_E1(V)                                                                            \
-  case V:                                                                                     \
-    return run_fused<E0, V>(tb, fg, H, npow, order, C, ny, spec, F, scale, Q, reg, S, my,     \
-                            dots, scalar, Yt, W, tw0, tw20, tw1, tw21, zbuf, s);
+                       double* dots, double* scalar, const FusedBuffers& b, cudaStream_t s) {
+#define FLPR_E1(V)                                                                          \
+  case V:                                                                                   \
+    return run_fused<E0, V>(tb, fg, H, npow, order, C, ny, spec, F, scale, Q, reg, S, my,   \
+                            dots, scalar, b, s);
   switch (E1) {
     FLPR_E1(2)
     FLPR_E1(4)
@@ -676,10 +820,14 @@ int fused2d_check(const int* G, const int* L, const int* qout, int H, int order,
   FLPR_CHECK_ARG(G[0] >= 2 && G[1] >= 2 && G[0] <= L[0] && G[1] <= L[1], "fused2d: G");
   FLPR_CHECK_ARG(qout[0] >= 0 && qout[0] + G[0] <= L[0] && qout[1] >= 0 && qout[1] + G[1] <= L[1],
                  "fused2d: crop window");
+  // a warp's cropped output (2 G floats) must fit its transpose buffer
+  FLPR_CHECK_ARG(2 * G[0] <= warp_buf_stride(L[0] / 32) && 2 * G[1] <= warp_buf_stride(L[1] / 32),
+                 "fused2d: grid (%d,%d) too large for padding (%d,%d)", G[0], G[1], L[0], L[1]);
   FLPR_CHECK_ARG(order >= 0 && order <= 2 && C >= 1 && C <= 32 && H >= 1, "fused2d: order/C/H");
   FLPR_CHECK_ARG(build_tables(order, C, tb) == FLPR_OK, "fused2d: too many slots or jobs");
-  FLPR_CHECK_ARG(fused_t_smem(L[1] / 32, G[1], tb->nt, C) <= 200 * 1024,
-                 "fused2d: T tile does not fit shared memory");
+  const int nwarps = t_warps(tb->t_row.njobs);
+  FLPR_CHECK_ARG(t_smem_bytes(L[1] / 32, nwarps, tb->t_row.njobs, G[1]) <= kMaxSmem,
+                 "fused2d: T row tile does not fit shared memory");
   fused_geom(G, L, qout, H, *tb, fg);
   return FLPR_OK;
 }
@@ -703,11 +851,8 @@ size_t flpr_lpr2d_fused_ws(const int* h_G, const int* h_L, const int* h_qout, in
   FusedGeom fg;
   if (fused2d_check(h_G, h_L, h_qout, H, order, C, &tb, &fg) != FLPR_OK) return 0;
   ArenaSize ar;
-  ar.take<float2>((size_t)(1 + C) * fg.L1h * fg.L0);
-  ar.take<float2>(fg.w_elems);
-  ar.take<float2>(2 * (size_t)fg.L0);
-  ar.take<float2>(2 * (size_t)fg.L1);
-  ar.take<double>((size_t)H * fg.M * tb.nt);
+  FusedBuffers b;
+  carve(ar, tb, fg, H, 2 * order + 1, C, &b);
   return ar.used;
 }
 
@@ -720,26 +865,23 @@ int flpr_lpr2d_fused(const int* h_G, const int* h_L, const int* h_qout, int H, i
   FLPR_TRY(fused2d_check(h_G, h_L, h_qout, H, order, C, &tb, &fg));
   FLPR_CHECK_ARG(ny >= 0 && ny <= C, "fused2d: ny=%d", ny);
   FLPR_CHECK_ARG(npow >= 2 * order + 1, "fused2d: npow=%d < 2*order+1", npow);
-  if (ws_bytes < flpr_lpr2d_fused_ws(h_G, h_L, h_qout, H, order, C)) {
-    set_error("fused2d: workspace too small");
+  ArenaSize need;
+  FusedBuffers b;
+  carve(need, tb, fg, H, npow, C, &b);
+  if (ws_bytes < need.used) {
+    set_error("fused2d: workspace too small (%zu < %zu)", ws_bytes, need.used);
     return FLPR_ERR_WORKSPACE;
   }
   Arena ar(d_ws, ws_bytes);
-  float2* Yt = ar.take<float2>((size_t)(1 + C) * fg.L1h * fg.L0);
-  float2* W = ar.take<float2>(fg.w_elems);
-  float2* tw0 = ar.take<float2>(2 * (size_t)fg.L0);
-  float2* tw1 = ar.take<float2>(2 * (size_t)fg.L1);
-  double* zbuf = ar.take<double>((size_t)H * fg.M * tb.nt);
-  float2* tw20 = tw0 + fg.L0;
-  float2* tw21 = tw1 + fg.L1;
+  carve(ar, tb, fg, H, npow, C, &b);
   cudaStream_t s = as_stream(stream);
   const float2* spec = static_cast<const float2*>(d_spec);
   const double2* F = static_cast<const double2*>(d_F);
   switch (fg.L0 / 32) {
-#define FLPR_E0(V)                                                                              \
-  case V:                                                                                       \
-    return dispatch_e1<V>(fg.L1 / 32, tb, fg, H, npow, order, C, ny, spec, F, scale, d_Q, reg,  \
-                          d_S, d_my, d_dots, d_scalar, Yt, W, tw0, tw20, tw1, tw21, zbuf, s);
+#define FLPR_E0(V)                                                                             \
+  case V:                                                                                      \
+    return dispatch_e1<V>(fg.L1 / 32, tb, fg, H, npow, order, C, ny, spec, F, scale, d_Q, reg, \
+                          d_S, d_my, d_dots, d_scalar, b, s);
     FLPR_E0(2)
     FLPR_E0(4)
     FLPR_E0(8)
