@@ -25,7 +25,6 @@ namespace flpr {
 constexpr int kItemPoints = 4096;
 constexpr int kSpreadThreads = 256;
 constexpr int kMaxTaps1 = 13;  // 2*msp+1 for msp <= 6
-constexpr int kWarpScratch = 3 * kMaxTaps1 + 32;
 
 struct SpreadGeom {
   int d;
@@ -326,6 +325,200 @@ tile_accumulate_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, int
   }
 }
 
+// ---- 2-D path: per-cell register accumulation ------------------------------
+// Tiles of 8 x 8 cells.  A CTA takes the points of one work item in batches
+// of kBatch2; each batch is counting-sorted by cell in shared memory and its
+// 2 x NT1 tap weights and scaled channel values are cached there.  A warp
+// then takes one tile row l0 and a block of channel groups: lane
+// (jy, group) walks the points of that row cell by cell and sums, in
+// registers, the contributions of tap row jy to the NT1 + 7 cells of halo row
+// l0 + jy that the 8 cells of the row reach, for kUnitCh channels.  Only
+// those sums reach the shared tile (one atomic each), instead of one atomic
+// per (point, tap, channel).  In the fixed-point accumulator every product
+// is rounded to an integer before it is added, so sums stay exact and the
+// grid does not depend on the order of the points.
+constexpr int kT2 = 8;         // tile edge of the 2-D path
+constexpr int kBatch2 = 256;   // points per batch (one per thread while caching)
+constexpr int kUnitCh = 2;     // channels per lane
+
+template <typename Acc>
+__device__ __forceinline__ void reg_add(Acc& a, double v);
+template <>
+__device__ __forceinline__ void reg_add<long long>(long long& a, double v) {
+  a += __double2ll_rn(v);
+}
+template <>
+__device__ __forceinline__ void reg_add<double>(double& a, double v) {
+  a += v;
+}
+
+__device__ __forceinline__ void shared_add(long long* p, long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)v);
+}
+__device__ __forceinline__ void shared_add(double* p, double v) { atomicAdd(p, v); }
+
+// Halo-row stride (odd) and channel stride (odd) of the shared tile.
+__host__ __device__ constexpr int row_stride2(int nt1) { return (kT2 + nt1 - 1) | 1; }
+__host__ __device__ constexpr int chan_stride2(int w0, int nt1) { return (w0 * row_stride2(nt1)) | 1; }
+
+template <typename Acc, int NT1>
+__global__ void __launch_bounds__(kBatch2, 2)
+tile_accumulate_2d_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, int cgroup,
+                          const int* __restrict__ offsets, const int* __restrict__ items,
+                          const int* __restrict__ rec_base, const double* __restrict__ rec_frac,
+                          const double* __restrict__ rec_val, const double* __restrict__ absum,
+                          int margin_bits, Acc* __restrict__ gacc) {
+  constexpr int MSP = (NT1 - 1) / 2;
+  constexpr int NACC = kT2 + NT1 - 1;  // halo cells one tile row reaches
+  constexpr int RS = row_stride2(NT1);
+  constexpr int GPL = 32 / NT1;        // channel groups per warp
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int cnt[kT2 * kT2];
+  __shared__ int off[kT2 * kT2 + 1];
+  __shared__ double scale[32];
+  const int c_begin = blockIdx.y * cgroup;
+  const int nc = min(nchan, c_begin + cgroup) - c_begin;
+  const int T0 = g.T[0], W0 = g.W[0];
+  const int CS = chan_stride2(W0, NT1);
+  Acc* acc = reinterpret_cast<Acc*>(smem_raw);                       // nc x CS
+  double* wy = reinterpret_cast<double*>(acc + (size_t)nc * CS);     // kBatch2 x NT1
+  double* wx = wy + kBatch2 * NT1;                                   // kBatch2 x NT1
+  double* vs = wx + kBatch2 * NT1;                                   // kBatch2 x nc
+
+  const int item = blockIdx.x;
+  if (item >= items[g.ntiles]) return;
+  int lo = 0, hi = g.ntiles;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (items[mid] <= item) lo = mid; else hi = mid;
+  }
+  const int tile = lo;
+  const int p_begin = offsets[tile] + (item - items[tile]) * kItemPoints;
+  const int p_end = min(offsets[tile + 1], p_begin + kItemPoints);
+  const int tc0 = tile / g.ntile[1], tc1 = tile - tc0 * g.ntile[1];
+
+  for (int i = threadIdx.x; i < nc * CS; i += blockDim.x) acc[i] = Acc(0);
+  if (threadIdx.x < 32)
+    scale[threadIdx.x] =
+        (threadIdx.x < nc && absum != nullptr) ? fixed_scale(absum[c_begin + threadIdx.x], margin_bits)
+                                               : 1.0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int jy = lane % NT1, gsub = lane / NT1;
+  const int ngrp = (nc + kUnitCh - 1) / kUnitCh;
+  const int ngblk = (ngrp + GPL - 1) / GPL;
+  const int nlc = T0 * kT2;
+  const double hx0 = g.ax[0].hx, hx1 = g.ax[1].hx;
+  const double ft0 = g.four_tau[0], ft1 = g.four_tau[1];
+
+  for (int b0 = p_begin; b0 < p_end; b0 += kBatch2) {
+    const int nb = min(kBatch2, p_end - b0);
+    __syncthreads();  // previous batch's readers are done
+    for (int i = threadIdx.x; i < nlc; i += blockDim.x) cnt[i] = 0;
+    __syncthreads();
+    const int q = threadIdx.x;
+    int lc = 0, rank = 0;
+    if (q < nb) {
+      const int packed = rec_base[b0 + q];
+      lc = (packed & 1023) * kT2 + ((packed >> 10) & 1023);
+      rank = atomicAdd(&cnt[lc], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // exclusive scan of the <= 64 cell counts
+      const int i0 = 2 * lane, i1 = 2 * lane + 1;
+      const int a0 = i0 < nlc ? cnt[i0] : 0, a1 = i1 < nlc ? cnt[i1] : 0;
+      int incl = a0 + a1;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const int excl = incl - a0 - a1;
+      if (i0 < nlc) off[i0] = excl;
+      if (i1 < nlc) off[i1] = excl + a0;
+      if (lane == 31) off[nlc] = incl;
+    }
+    __syncthreads();
+    if (q < nb) {
+      const int pos = off[lc] + rank;
+      const int p = b0 + q;
+      const double f0 = rec_frac[p], f1 = rec_frac[n + p];
+#pragma unroll
+      for (int j = 0; j < NT1; ++j) {
+        const double d0 = f0 - hx0 * (double)(j - MSP);
+        const double d1 = f1 - hx1 * (double)(j - MSP);
+        wy[pos * NT1 + j] = exp(-(d0 * d0) / ft0);
+        wx[pos * NT1 + j] = exp(-(d1 * d1) / ft1);
+      }
+      for (int c = 0; c < nc; ++c) {
+        const int ch = c_begin + c;
+        const double v = (ones_channel && ch == 0) ? 1.0 : rec_val[(int64_t)(ch - ones_channel) * n + p];
+        vs[pos * nc + c] = v * scale[c];
+      }
+    }
+    __syncthreads();
+    // warp items: (tile row l0, block of GPL channel groups)
+    for (int wi = warp; wi < T0 * ngblk; wi += nwarps) {
+      const int l0 = wi / ngblk, gb = wi - l0 * ngblk;
+      const int grp = gb * GPL + gsub;
+      const bool active = lane < NT1 * GPL && grp < ngrp;
+      const int c0 = grp * kUnitCh;
+      Acc a[kUnitCh][NACC];
+#pragma unroll
+      for (int k = 0; k < kUnitCh; ++k)
+#pragma unroll
+        for (int j = 0; j < NACC; ++j) a[k][j] = Acc(0);
+      const int rowbase = l0 * kT2;
+#pragma unroll
+      for (int cr = 0; cr < kT2; ++cr) {
+        const int pe = off[rowbase + cr + 1];
+        for (int pp = off[rowbase + cr]; pp < pe; ++pp) {
+          const double wyv = wy[pp * NT1 + jy];
+          double v[kUnitCh];
+#pragma unroll
+          for (int k = 0; k < kUnitCh; ++k)
+            v[k] = (active && c0 + k < nc) ? wyv * vs[pp * nc + c0 + k] : 0.0;
+#pragma unroll
+          for (int jx = 0; jx < NT1; ++jx) {
+            const double w = wx[pp * NT1 + jx];
+#pragma unroll
+            for (int k = 0; k < kUnitCh; ++k) reg_add<Acc>(a[k][cr + jx], v[k] * w);
+          }
+        }
+      }
+      if (active) {
+        Acc* rowp = acc + (size_t)(l0 + jy) * RS;
+#pragma unroll
+        for (int k = 0; k < kUnitCh; ++k) {
+          if (c0 + k >= nc) break;
+#pragma unroll
+          for (int j = 0; j < NACC; ++j)
+            if (a[k][j] != Acc(0)) shared_add(rowp + (size_t)(c0 + k) * CS + j, a[k][j]);
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // flush: one global atomic per non-zero cell of the tile + halo
+  const int W1 = g.W[1];
+  for (int idx = threadIdx.x; idx < nc * W0 * W1; idx += blockDim.x) {
+    const int c = idx / (W0 * W1);
+    const int r = idx - c * (W0 * W1);
+    const int r0 = r / W1, r1 = r - r0 * W1;
+    const Acc v = acc[(size_t)c * CS + r0 * RS + r1];
+    if (v == Acc(0)) continue;
+    int gc0 = (tc0 * kT2 + r0 - g.msp) % g.L[0];
+    if (gc0 < 0) gc0 += g.L[0];
+    int gc1 = (tc1 * kT2 + r1 - g.msp) % g.L[1];
+    if (gc1 < 0) gc1 += g.L[1];
+    AccOps<Acc>::add_global(&gacc[(int64_t)(c_begin + c) * g.cells + (int64_t)gc0 * g.L[1] + gc1], v);
+  }
+}
+
+static size_t smem_2d(int W0, int nt1, int cg) {
+  return sizeof(double) * ((size_t)cg * chan_stride2(W0, nt1) + (size_t)kBatch2 * (2 * nt1 + cg));
+}
+
 template <typename Acc, typename Out, bool kFixed>
 __global__ void finalize_kernel(int nchan, int64_t cells, const Acc* __restrict__ gacc,
                                 const double* __restrict__ absum, int margin_bits, double inv_n,
@@ -344,9 +537,13 @@ __global__ void finalize_kernel(int nchan, int64_t cells, const Acc* __restrict_
   }
 }
 
+// 2-D grids of at least 8 x 8 cells take the per-cell register path.
+static bool use_2d_path(int d, const int* L) { return d == 2 && L[0] >= kT2 && L[1] >= kT2; }
+
 static void make_geom(SpreadGeom& g, int d, const int* L, int msp, const double* tau,
                       const double* kmap) {
   memset(&g, 0, sizeof(g));
+  const bool path2 = use_2d_path(d, L);
   g.d = d;
   g.msp = msp;
   g.ntaps1 = 2 * msp + 1;
@@ -358,7 +555,7 @@ static void make_geom(SpreadGeom& g, int d, const int* L, int msp, const double*
   for (int a = 0; a < 3; ++a) {
     if (a < d) {
       g.L[a] = L[a];
-      int T = d == 1 ? 256 : (d == 2 ? tile2[a] : tile3[a]);
+      int T = d == 1 ? 256 : (d == 2 ? (path2 ? kT2 : tile2[a]) : tile3[a]);
       if (T > L[a]) T = L[a];
       g.T[a] = T;
       g.ntile[a] = (L[a] + T - 1) / T;
@@ -391,6 +588,13 @@ static int channel_group(const SpreadGeom& g, int nchan, size_t acc_bytes) {
   int cg = (int)(budget / (acc_bytes * (size_t)g.tile_cells));
   if (cg > 32) cg = 32;  // fixed-point scales of one group live in 32 shared slots
   if (cg > nchan) cg = nchan;
+  return cg;
+}
+
+static int channel_group_2d(const SpreadGeom& g, int nchan) {
+  // two CTAs per SM
+  int cg = nchan < 32 ? nchan : 32;
+  while (cg > 1 && smem_2d(g.W[0], g.ntaps1, cg) > (size_t)110 * 1024) --cg;
   return cg;
 }
 
@@ -470,6 +674,35 @@ static int launch_accumulate(const SpreadGeom& g, int64_t n, int nchan, int ones
   return FLPR_OK;
 }
 
+template <int NT1>
+static int launch_accumulate_2d(const SpreadGeom& g, int64_t n, int nchan, int ones_channel,
+                                int cg, const SpreadWs& w, bool fixed, int margin, dim3 grid,
+                                cudaStream_t s) {
+  const size_t smem = smem_2d(g.W[0], NT1, cg);
+  if (fixed) {
+    auto k = tile_accumulate_2d_kernel<long long, NT1>;
+    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   cudaSharedmemCarveoutMaxShared));
+    k<<<grid, kBatch2, smem, s>>>(g, n, nchan, ones_channel, cg, w.offsets, w.items, w.rec_base,
+                                  (const double*)w.rec_frac, (const double*)w.rec_val, w.absum,
+                                  margin, (long long*)w.gacc);
+  } else {
+    auto k = tile_accumulate_2d_kernel<double, NT1>;
+    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   cudaSharedmemCarveoutMaxShared));
+    k<<<grid, kBatch2, smem, s>>>(g, n, nchan, ones_channel, cg, w.offsets, w.items, w.rec_base,
+                                  (const double*)w.rec_frac, (const double*)w.rec_val, nullptr,
+                                  margin, (double*)w.gacc);
+  }
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
+static int finalize(const SpreadGeom& g, int64_t n, int nchan, bool fixed, int margin,
+                    const SpreadWs& w, void* d_grid_out, cudaStream_t s);
+
 }  // namespace flpr
 
 using namespace flpr;
@@ -532,12 +765,29 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
                                                 (double*)w.rec_val);
   FLPR_LAUNCH_CHECK();
 
+  int64_t max_items = (int64_t)g.ntiles + (n + kItemPoints - 1) / kItemPoints;
+  if (use_2d_path(d, h_L)) {
+    const int cg2 = channel_group_2d(g, nchan);
+    FLPR_CHECK_ARG(cg2 >= 1, "spread: tile does not fit shared memory");
+    dim3 grid2((unsigned)max_items, (unsigned)((nchan + cg2 - 1) / cg2));
+    int st = FLPR_OK;
+    switch (g.ntaps1) {
+      case 3: st = launch_accumulate_2d<3>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
+      case 5: st = launch_accumulate_2d<5>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
+      case 7: st = launch_accumulate_2d<7>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
+      case 9: st = launch_accumulate_2d<9>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
+      case 11: st = launch_accumulate_2d<11>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
+      case 13: st = launch_accumulate_2d<13>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
+      default: set_error("spread: msp=%d not supported (1..6)", g.msp); return FLPR_ERR_ARG;
+    }
+    if (st != FLPR_OK) return st;
+    return finalize(g, n, nchan, fixed, margin, w, d_grid_out, s);
+  }
   const size_t acc_bytes = 8;
   int cg = channel_group(g, nchan, acc_bytes);
   FLPR_CHECK_ARG(cg >= 1, "spread: tile does not fit shared memory");
   int ngroups = (nchan + cg - 1) / cg;
   size_t smem = acc_bytes * (size_t)cg * g.tile_cells;
-  int64_t max_items = (int64_t)g.ntiles + (n + kItemPoints - 1) / kItemPoints;
   dim3 grid((unsigned)max_items, (unsigned)ngroups);
   int status = FLPR_OK;
   switch (g.ntaps1) {
@@ -550,7 +800,15 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
     default: set_error("spread: msp=%d not supported (1..6)", g.msp); return FLPR_ERR_ARG;
   }
   if (status != FLPR_OK) return status;
+  return finalize(g, n, nchan, fixed, margin, w, d_grid_out, s);
+}
 
+}  // extern "C"
+
+namespace flpr {
+
+static int finalize(const SpreadGeom& g, int64_t n, int nchan, bool fixed, int margin,
+                    const SpreadWs& w, void* d_grid_out, cudaStream_t s) {
   int64_t total = (int64_t)nchan * g.cells;
   int fb = (int)((total + 255) / 256);
   if (fb > 16 * sm_count()) fb = 16 * sm_count();
@@ -567,4 +825,4 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
   return FLPR_OK;
 }
 
-}  // extern "C"
+}  // namespace flpr
