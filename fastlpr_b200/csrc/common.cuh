@@ -5,6 +5,7 @@
 #include <cufft.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <map>

@@ -31,6 +31,8 @@ constexpr int kMaxTWarps = 8;   // warps of a T row-pass CTA
 constexpr int kMaxSlots = 64;
 constexpr int kMaxJobs = 64;
 constexpr size_t kMaxSmem = 227 * 1024;
+// Kernel factor entries below kBandEps of their peak are left out of both passes.
+constexpr double kBandEps = 1e-11;
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -163,6 +165,44 @@ __global__ void factor_f32_kernel(int64_t n0, int64_t ntot, double scale,
   }
 }
 
+// Band limit of the kernel factor spectra: kcut[axis * H + h] is the largest
+// frequency index m <= N/2 (entries k and N - k) at which some power a has
+// |F[h][a][.]| >= eps * max_k |F[h][a][k]|.  Both passes treat the terms
+// beyond it as zero: their share of any output is below eps * N relative.
+// grid (H, 2), one block per (bandwidth, axis).
+__global__ void band_limit_kernel(int H, int npow, int L0, int L1, const double2* __restrict__ F,
+                                  double eps, int* __restrict__ kcut) {
+  __shared__ double smax[32];
+  __shared__ int scut[32];
+  const int h = blockIdx.x, ax = blockIdx.y;
+  const int N = ax == 0 ? L0 : L1;
+  const double2* base = F + (ax == 0 ? 0 : (size_t)H * npow * L0) + (size_t)h * npow * N;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  int best = 0;
+  for (int a = 0; a < npow; ++a) {
+    const double2* f = base + (size_t)a * N;
+    double m = 0.0;
+    for (int k = threadIdx.x; k < N; k += blockDim.x) m = fmax(m, f[k].x * f[k].x + f[k].y * f[k].y);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) smax[warp] = m;
+    __syncthreads();
+    double mx = 0.0;
+    for (int w = 0; w < nw; ++w) mx = fmax(mx, smax[w]);
+    const double thr = eps * eps * mx;
+    int kc = 0;
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+      const double v = f[k].x * f[k].x + f[k].y * f[k].y;
+      if (mx > 0.0 && v >= thr) kc = max(kc, min(k, N - k));
+    }
+    for (int o = 16; o > 0; o >>= 1) kc = max(kc, __shfl_xor_sync(0xffffffffu, kc, o));
+    if (lane == 0) scut[warp] = kc;
+    __syncthreads();
+    for (int w = 0; w < nw; ++w) best = max(best, scut[w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) kcut[ax * H + h] = best;
+}
+
 template <int E>
 __device__ __forceinline__ void load_twiddles(float2* s_tab, const float2* __restrict__ tab) {
   constexpr int T = twiddle_entries(32 * E);
@@ -202,10 +242,14 @@ struct ColArgs {
 template <int E>
 __global__ void __launch_bounds__(kColWarps * 32, 2)
 colpass_kernel(ColArgs ca, const float2* __restrict__ Yt, const float2* __restrict__ F0f,
-               const float2* __restrict__ tab, float2* __restrict__ W) {
+               const float2* __restrict__ tab, const int* __restrict__ kcut1,
+               float2* __restrict__ W) {
   constexpr int N = 32 * E;
   constexpr int SW = warp_buf_stride(E);
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  // columns beyond the axis-1 band limit are never read by the row pass
+  const int kc1 = kcut1[ca.hbase + blockIdx.z];
+  if (blockIdx.x * kColWarps > kc1) return;
   float2* s_tw2 = reinterpret_cast<float2*>(smem_raw);
   float2* s_tw32 = s_tw2 + N;
   float* bufs = reinterpret_cast<float*>(s_tw2 + twiddle_entries(N));
@@ -216,7 +260,7 @@ colpass_kernel(ColArgs ca, const float2* __restrict__ Yt, const float2* __restri
   const int c = ca.slot_chan[slot], a0 = ca.slot_pow[slot];
   const int w1 = blockIdx.x * kColWarps + warp;
   float* buf = bufs + warp * SW;
-  if (w1 < ca.L1h) {
+  if (w1 < ca.L1h && w1 <= kc1) {
     const float2* col = Yt + ((size_t)c * ca.L1h + w1) * N + lane;
     const float2* f = F0f + ((size_t)h * ca.npow + a0) * N + lane;
     float2 v[E];
@@ -235,7 +279,7 @@ colpass_kernel(ColArgs ca, const float2* __restrict__ Yt, const float2* __restri
   for (int i = threadIdx.x; i < ca.G0 * kColWarps; i += blockDim.x) {
     const int r = i / kColWarps, wl = i - r * kColWarps;
     const int colw = blockIdx.x * kColWarps + wl;
-    if (colw < ca.L1h)
+    if (colw < ca.L1h && colw <= kc1)
       out[(size_t)r * ca.L1h + colw] = reinterpret_cast<const float2*>(bufs + wl * SW)[r];
   }
 }
@@ -282,18 +326,21 @@ struct RowArgs {
 
 // Slot s of the Hermitian extension of the product W_row * A1: element
 // k = 32 s + lane, mirrored (conjugated) above N/2; the DC and Nyquist terms
-// are real.  lo = row + lane, hi = row + N - lane.
+// are real; frequencies beyond the band limit kc are zero.
+// lo = row + lane, hi = row + N - lane.
 template <int E>
 __device__ __forceinline__ float2 herm_product(const float2* __restrict__ wlo,
                                                const float2* __restrict__ flo,
                                                const float2* __restrict__ whi,
-                                               const float2* __restrict__ fhi, int s, int lane) {
-  float2 p;
+                                               const float2* __restrict__ fhi, int s, int lane,
+                                               int kc) {
+  constexpr int N = 32 * E;
+  float2 p = make_float2(0.0f, 0.0f);
   if (s < E / 2) {
-    p = cmul(wlo[32 * s], flo[32 * s]);
+    if (32 * s + lane <= kc) p = cmul(wlo[32 * s], flo[32 * s]);
     if (s == 0 && lane == 0) p.y = 0.0f;
   } else {
-    p = cmul(whi[-32 * s], fhi[-32 * s]);
+    if (N - 32 * s - lane <= kc) p = cmul(whi[-32 * s], fhi[-32 * s]);
     p.y = (s == E / 2 && lane == 0) ? 0.0f : -p.y;
   }
   return p;
@@ -306,7 +353,7 @@ template <int E>
 __device__ __forceinline__ void row_fft(const RowArgs& ra, const RowJob& jb, int r, int hz, int h,
                                         int nslots_w, const float2* __restrict__ W,
                                         const float2* __restrict__ F1f, const float2* s_tw2,
-                                        const float2* s_tw32, float* buf, int lane,
+                                        const float2* s_tw32, float* buf, int lane, int kc,
                                         float2 (&v)[E]) {
   constexpr int N = 32 * E;
   const size_t rowstride = (size_t)ra.L1h;
@@ -317,14 +364,16 @@ __device__ __forceinline__ void row_fft(const RowArgs& ra, const RowJob& jb, int
     const float2* fb = F1f + ((size_t)h * ra.npow + jb.pow_b) * N;
 #pragma unroll
     for (int s = 0; s < E; ++s) {
-      const float2 pa = herm_product<E>(wa + lane, fa + lane, wa + N - lane, fa + N - lane, s, lane);
-      const float2 pb = herm_product<E>(wb + lane, fb + lane, wb + N - lane, fb + N - lane, s, lane);
+      const float2 pa =
+          herm_product<E>(wa + lane, fa + lane, wa + N - lane, fa + N - lane, s, lane, kc);
+      const float2 pb =
+          herm_product<E>(wb + lane, fb + lane, wb + N - lane, fb + N - lane, s, lane, kc);
       v[s] = make_float2(pa.x - pb.y, pa.y + pb.x);
     }
   } else {
 #pragma unroll
     for (int s = 0; s < E; ++s)
-      v[s] = herm_product<E>(wa + lane, fa + lane, wa + N - lane, fa + N - lane, s, lane);
+      v[s] = herm_product<E>(wa + lane, fa + lane, wa + N - lane, fa + N - lane, s, lane, kc);
   }
   warp_ifft<E>(v, s_tw2, s_tw32, buf, lane);
 }
@@ -336,7 +385,7 @@ template <int E>
 __global__ void __launch_bounds__(kRowWarps * 32, 2)
 rowpass_s_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
                  const float2* __restrict__ F1f, const float2* __restrict__ tab,
-                 float* __restrict__ S) {
+                 const int* __restrict__ kcut1, float* __restrict__ S) {
   constexpr int N = 32 * E;
   constexpr int SW = warp_buf_stride(E);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -354,7 +403,8 @@ rowpass_s_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
   const RowJob jb = ra.jobs[j];
   const bool pair = jb.slot_b >= 0;
   float2 v[E];
-  row_fft<E>(ra, jb, r, hz, h, nslots_w, W, F1f, s_tw2, s_tw32, bufs + warp * SW, lane, v);
+  row_fft<E>(ra, jb, r, hz, h, nslots_w, W, F1f, s_tw2, s_tw32, bufs + warp * SW, lane, kcut1[h],
+             v);
   float* da = S + ((size_t)jb.out_a * H + h) * M + (size_t)r * ra.G1;
   float* db = S + ((size_t)(pair ? jb.out_b : jb.out_a) * H + h) * M + (size_t)r * ra.G1;
 #pragma unroll
@@ -392,9 +442,10 @@ inline int t_warps(int njobs) {
 template <int E, int NT>
 __global__ void __launch_bounds__(kMaxTWarps * 32, 2)
 rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
-                       const float2* __restrict__ F1f, const float2* __restrict__ tab, int C,
-                       int ny, const double* __restrict__ zg, const double* __restrict__ Q,
-                       double* __restrict__ my, double* __restrict__ dpart) {
+                       const float2* __restrict__ F1f, const float2* __restrict__ tab,
+                       const int* __restrict__ kcut1, int C, int ny, const double* __restrict__ zg,
+                       const double* __restrict__ Q, double* __restrict__ my,
+                       double* __restrict__ dpart) {
   constexpr int N = 32 * E;
   constexpr int SW = warp_buf_stride(E);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -412,11 +463,12 @@ rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict
   const int G1 = ra.G1, njobs = ra.njobs;
   const int last0 = njobs - nwarps;  // jobs >= last0 are the last of their warp
   float* buf = bufs + warp * SW;
+  const int kc = kcut1[h];
   for (int j = warp; j < njobs; j += nwarps) {
     const RowJob jb = ra.jobs[j];
     const bool pair = jb.slot_b >= 0;
     float2 v[E];
-    row_fft<E>(ra, jb, r, hz, h, nslots_w, W, F1f, s_tw2, s_tw32, buf, lane, v);
+    row_fft<E>(ra, jb, r, hz, h, nslots_w, W, F1f, s_tw2, s_tw32, buf, lane, kc, v);
     float* dst = j >= last0 ? buf : regions + (size_t)j * 2 * G1;
 #pragma unroll
     for (int s = 0; s < E; ++s) {
@@ -494,47 +546,51 @@ static size_t warp_pass_smem(int E, int nwarps) {
 
 template <int E>
 static int launch_col(const ColArgs& ca, int ncolblk, int nslots, int Hc, const float2* Yt,
-                      const float2* F0f, const float2* tab, float2* W, cudaStream_t s) {
+                      const float2* F0f, const float2* tab, const int* kcut1, float2* W,
+                      cudaStream_t s) {
   const size_t smem = warp_pass_smem(E, kColWarps);
   FLPR_TRY(set_smem(colpass_kernel<E>, smem));
-  colpass_kernel<E><<<dim3(ncolblk, nslots, Hc), kColWarps * 32, smem, s>>>(ca, Yt, F0f, tab, W);
+  colpass_kernel<E><<<dim3(ncolblk, nslots, Hc), kColWarps * 32, smem, s>>>(ca, Yt, F0f, tab,
+                                                                          kcut1, W);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
 
 template <int E>
 static int launch_row_s(const RowArgs& ra, int Hc, int H, int nslots_w, const float2* W,
-                        const float2* F1f, const float2* tab, float* S, cudaStream_t s) {
+                        const float2* F1f, const float2* tab, const int* kcut1, float* S,
+                        cudaStream_t s) {
   const size_t smem = warp_pass_smem(E, kRowWarps);
   FLPR_TRY(set_smem(rowpass_s_kernel<E>, smem));
   const int items = ra.G0 * ra.njobs;
   rowpass_s_kernel<E><<<dim3((items + kRowWarps - 1) / kRowWarps, Hc), kRowWarps * 32, smem, s>>>(
-      ra, H, nslots_w, W, F1f, tab, S);
+      ra, H, nslots_w, W, F1f, tab, kcut1, S);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
 
 template <int E, int NT>
 static int launch_row_t_nt(const RowArgs& ra, int Hc, int H, int nslots_w, const float2* W,
-                           const float2* F1f, const float2* tab, int C, int ny, const double* z,
-                           const double* Q, double* my, double* dpart, cudaStream_t s) {
+                           const float2* F1f, const float2* tab, const int* kcut1, int C, int ny,
+                           const double* z, const double* Q, double* my, double* dpart,
+                           cudaStream_t s) {
   const int nwarps = t_warps(ra.njobs);
   const size_t smem = t_smem_bytes(E, nwarps, ra.njobs, ra.G1);
   FLPR_TRY(set_smem(rowpass_t_solve_kernel<E, NT>, smem));
   rowpass_t_solve_kernel<E, NT><<<dim3(ra.G0, Hc), nwarps * 32, smem, s>>>(
-      ra, H, nslots_w, W, F1f, tab, C, ny, z, Q, my, dpart);
+      ra, H, nslots_w, W, F1f, tab, kcut1, C, ny, z, Q, my, dpart);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
 
 template <int E>
 static int launch_row_t(int nt, const RowArgs& ra, int Hc, int H, int nslots_w, const float2* W,
-                        const float2* F1f, const float2* tab, int C, int ny, const double* z,
-                        const double* Q, double* my, double* dpart, cudaStream_t s) {
+                        const float2* F1f, const float2* tab, const int* kc, int C, int ny,
+                        const double* z, const double* Q, double* my, double* dp, cudaStream_t s) {
   switch (nt) {
-    case 1: return launch_row_t_nt<E, 1>(ra, Hc, H, nslots_w, W, F1f, tab, C, ny, z, Q, my, dpart, s);
-    case 3: return launch_row_t_nt<E, 3>(ra, Hc, H, nslots_w, W, F1f, tab, C, ny, z, Q, my, dpart, s);
-    case 6: return launch_row_t_nt<E, 6>(ra, Hc, H, nslots_w, W, F1f, tab, C, ny, z, Q, my, dpart, s);
+    case 1: return launch_row_t_nt<E, 1>(ra, Hc, H, nslots_w, W, F1f, tab, kc, C, ny, z, Q, my, dp, s);
+    case 3: return launch_row_t_nt<E, 3>(ra, Hc, H, nslots_w, W, F1f, tab, kc, C, ny, z, Q, my, dp, s);
+    case 6: return launch_row_t_nt<E, 6>(ra, Hc, H, nslots_w, W, F1f, tab, kc, C, ny, z, Q, my, dp, s);
     default: set_error("fused2d: nt=%d", nt); return FLPR_ERR_ARG;
   }
 }
@@ -672,9 +728,14 @@ static int fused_geom(const int* G, const int* L, const int* qout, int H, const 
   fg->q1 = qout[1];
   fg->M = (int64_t)G[0] * G[1];
   const size_t slab = (size_t)fg->G0 * fg->L1h;  // float2 per (slot, h)
-  // chunks of a few bandwidths: enough row-pass CTAs to fill the GPU while
-  // the column-pass output stays near the L2 size
-  const size_t budget_s = (size_t)256 << 20, budget_t = (size_t)192 << 20;
+  // chunks of a few bandwidths: enough row-pass CTAs to fill the GPU with a
+  // bounded column-pass output (override: FLPR_FUSED_CHUNK_MB)
+  size_t budget = (size_t)192 << 20;
+  if (const char* env = getenv("FLPR_FUSED_CHUNK_MB")) {
+    const long mb = atol(env);
+    if (mb >= 1 && mb <= 65536) budget = (size_t)mb << 20;
+  }
+  const size_t budget_s = budget, budget_t = budget;
   int hs = (int)(budget_s / (sizeof(float2) * slab * t.s_nslots));
   int ht = (int)(budget_t / (sizeof(float2) * slab * t.t_nslots));
   fg->Hc_s = hs < 1 ? 1 : (hs > H ? H : hs);
@@ -689,6 +750,7 @@ static int fused_geom(const int* G, const int* L, const int* qout, int H, const 
 struct FusedBuffers {
   float2 *Yt, *W, *tab0, *tab1, *Ff;
   double *z, *dpart;
+  int* kcut;
 };
 
 template <typename A>
@@ -701,6 +763,7 @@ static void carve(A& ar, const FusedTables& tb, const FusedGeom& fg, int H, int 
   b->Ff = ar.template take<float2>((size_t)H * npow * (fg.L0 + fg.L1));
   b->z = ar.template take<double>((size_t)H * fg.M * tb.nt);
   b->dpart = ar.template take<double>((size_t)C * H * fg.G0);
+  b->kcut = ar.template take<int>(2 * (size_t)H);
 }
 
 template <int E0, int E1>
@@ -720,6 +783,9 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
     factor_f32_kernel<<<nb, 256, 0, s>>>(n0, ntot, scale, F, b.Ff);
     FLPR_LAUNCH_CHECK();
   }
+  band_limit_kernel<<<dim3(H, 2), 256, 0, s>>>(H, npow, fg.L0, fg.L1, F, kBandEps, b.kcut);
+  FLPR_LAUNCH_CHECK();
+  const int* kcut1 = b.kcut + H;
   const float2* F0f = b.Ff;
   const float2* F1f = b.Ff + (size_t)H * npow * fg.L0;
   transpose_spec_kernel<<<dim3((fg.L1h + 31) / 32, (fg.L0 + 31) / 32, 1 + C), dim3(32, 8), 0, s>>>(
@@ -745,8 +811,8 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
     const int hc = H - h0 < fg.Hc_s ? H - h0 : fg.Hc_s;
     ca.hbase = h0;
     ra.hbase = h0;
-    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.s_nslots, hc, b.Yt, F0f, b.tab0, b.W, s));
-    FLPR_TRY(launch_row_s<E1>(ra, hc, H, hc, b.W, F1f, b.tab1, S, s));
+    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.s_nslots, hc, b.Yt, F0f, b.tab0, kcut1, b.W, s));
+    FLPR_TRY(launch_row_s<E1>(ra, hc, H, hc, b.W, F1f, b.tab1, kcut1, S, s));
   }
   FLPR_TRY(global_scalar(order, nt, H, fg.M, S, scalar, FLPR_PREC_F32, s));
   {
@@ -780,9 +846,9 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
     const int hc = H - h0 < fg.Hc_t ? H - h0 : fg.Hc_t;
     ca.hbase = h0;
     ra.hbase = h0;
-    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.t_nslots, hc, b.Yt, F0f, b.tab0, b.W, s));
-    FLPR_TRY(launch_row_t<E1>(nt, ra, hc, H, hc, b.W, F1f, b.tab1, C, ny, b.z, Q, my, b.dpart,
-                              s));
+    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.t_nslots, hc, b.Yt, F0f, b.tab0, kcut1, b.W, s));
+    FLPR_TRY(launch_row_t<E1>(nt, ra, hc, H, hc, b.W, F1f, b.tab1, kcut1, C, ny, b.z, Q, my,
+                              b.dpart, s));
   }
   dots_reduce_kernel<<<C * H, 256, 0, s>>>(C * H, fg.G0, b.dpart, dots);
   FLPR_LAUNCH_CHECK();
