@@ -57,6 +57,17 @@ SIGNATURES = [
     ("flpr_kde_lcv", _I, [_I, _I64, _VP, _PD, _PI, _I, _VP, _D, _PD, _VP, _VP, _VP, _SZ, _VP]),
     ("flpr_log_shift", _I, [_I64, _VP, _D, _VP, _VP]),
     ("flpr_exp_weighted_sum", _I, [_I64, _VP, _VP, _VP, _VP]),
+    ("flpr_bin_moments", _I, [_I, _I64, _VP, _VP, _VP, _VP, _VP]),
+    ("flpr_mlp_gemm", _I, [_I, _I, _I, _VP, _I, _I, _VP, _I, _I, _VP, _I, _VP, _I, _VP, _VP, _I,
+                           _VP]),
+    ("flpr_mlp_param_count", _I64, [_I, _PI]),
+    ("flpr_mlp_ws", _SZ, [_I, _PI, _I]),
+    ("flpr_mlp_fwd", _I, [_I, _PI, _VP, _VP, _I, _VP, _VP, _VP, _SZ, _VP]),
+    ("flpr_mlp_bwd", _I, [_I, _PI, _VP, _I, _VP, _VP, _VP, _VP, _SZ, _VP]),
+    ("flpr_mlp_step", _I, [_I64, _VP, _VP, _VP, _VP, _VP, C.c_float, C.c_float, C.c_float,
+                           C.c_float, C.c_float, _I, _VP]),
+    ("flpr_mlp_mse", _I, [_I, _VP, _VP, _VP, _VP, _VP]),
+    ("flpr_to_bf16", _I, [_I64, _VP, _VP, _VP]),
 ]
 
 

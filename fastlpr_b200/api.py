@@ -214,13 +214,16 @@ class _PhaseEvents:
         self.events = []
 
 
-# probe matrices are a deterministic function of (n, R, seed): cache on device
-_PROBE_CACHE: Dict[Tuple[int, int, int, int, int], torch.Tensor] = {}
+# Probe matrices: MT19937(seed).standard_normal((n, R)) fills the matrix in
+# row-major order, so the probes for n points are the first n rows of any
+# larger draw.  One (R, n_max) device matrix per (device, R, seed) serves
+# every n <= n_max.
+_PROBE_CACHE: Dict[Tuple[int, int, int], torch.Tensor] = {}
 
 
 def _probes(ctx: _Ctx, n: int, R: int, seed, random_matrix) -> Tuple[torch.Tensor, int]:
     """Hutchinson probes p = MT19937(seed).standard_normal((n, R)) as an
-    (R, n) float64 device tensor (regression.py:1182-1194)."""
+    (R, n) float64 device tensor, rows contiguous (regression.py:1182-1194)."""
     if random_matrix is not None:
         p = np.asarray(random_matrix, dtype=float)
         if p.ndim == 1:
@@ -228,15 +231,15 @@ def _probes(ctx: _Ctx, n: int, R: int, seed, random_matrix) -> Tuple[torch.Tenso
         if p.shape[0] != n:
             raise ValueError(f"random_matrix has wrong shape: expected ({n}, *), got {p.shape}")
         return ctx.upload(np.ascontiguousarray(p.T)), p.shape[1]
-    key = (ctx.index, n, R, int(seed), 0)
+    key = (ctx.index, R, int(seed))
     t = _PROBE_CACHE.get(key)
-    if t is None:
+    if t is None or t.shape[1] < n:
         p = np.random.Generator(np.random.MT19937(seed)).standard_normal((n, R))
         t = ctx.upload(np.ascontiguousarray(p.T))
         if len(_PROBE_CACHE) > 8:
             _PROBE_CACHE.clear()
         _PROBE_CACHE[key] = t
-    return t, R
+    return t[:, :n], R
 
 
 def clear_fastlpr_caches() -> None:
@@ -547,7 +550,14 @@ def cv_fastlpr(x, y, h=None, options: Optional[dict] = None) -> RegressionOutput
     kernel_type, y_type_out, calc_dof, gcv_selection, accuracy, N, xrange, dh,
     flag_power2, dstd, random_matrix, dof_seed, interp methods) plus
     ``precision`` ('fp32' | 'fp64'; default follows the reference's dtype
-    rule: FP32 grids below accuracy 5) and ``device``.
+    rule: FP32 grids below accuracy 5), ``device`` and ``bandwidth_search``:
+    'full' (default, the reference's sweep of every bandwidth) or 'learned'
+    (the trained proposal network picks five neighbouring bandwidths of the
+    list; while their GCV minimum sits on an edge of that window the window
+    moves that way, at most three times, and otherwise the full sweep runs;
+    needs a list of isotropic, increasing bandwidths, a real single response
+    and d <= 2, else the full sweep runs).  ``metadata['bandwidth_search']``
+    records what happened.
     """
     x_arr = _as_column_matrix(x)
     y_arr = np.asarray(y)
@@ -596,9 +606,16 @@ def cv_fastlpr(x, y, h=None, options: Optional[dict] = None) -> RegressionOutput
     _check_interp_methods(opts, dims, n)
     prec = _precision(opts)
     ctx = _Ctx(_device(opts))
+    search = str(opts.get("bandwidth_search", "full"))
+    if search not in ("full", "learned"):
+        raise ValueError(f"bandwidth_search must be 'full' or 'learned', got {search!r}")
     with torch.cuda.device(ctx.device):
+        model = None
+        if search == "learned":
+            from . import learned as _learned
+            model = _learned.default_model(ctx.device)
         return _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance,
-                        y_is_complex, timings=opts.get("_timings"))
+                        y_is_complex, timings=opts.get("_timings"), learned=model)
 
 
 def cv_fastlpr_device(x: torch.Tensor, y: torch.Tensor, h=None,
@@ -636,17 +653,29 @@ def cv_fastlpr_device(x: torch.Tensor, y: torch.Tensor, h=None,
         raise NotImplementedError("variance mode: use cv_fastlpr")
     prec = _precision(opts)
     ctx = _Ctx(x.device)
+    search = str(opts.get("bandwidth_search", "full"))
+    if search not in ("full", "learned"):
+        raise ValueError(f"bandwidth_search must be 'full' or 'learned', got {search!r}")
     with torch.cuda.device(ctx.device):
+        model = None
+        if search == "learned":
+            from . import learned as _learned
+            model = _learned.default_model(ctx.device)
         ycols = [y[:, c].contiguous() for c in range(y.shape[1])]
         return _fit_lpr(ctx, None, None, y.shape[1], bandwidths, opts, order, prec, False, False,
-                        dev_inputs=(x, ycols), timings=opts.get("_timings"))
+                        dev_inputs=(x, ycols), timings=opts.get("_timings"), learned=model)
 
 
-def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_is_complex,
-             dev_inputs=None, timings=None):
+class _LprState:
+    """Bandwidth-independent part of one LPR fit: the data on the device, the
+    grid geometry, the probes, the spectra of every channel and (dual form)
+    the adjoint deposits."""
+
+
+def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_complex,
+                 dev_inputs, ev) -> _LprState:
     lib = ctx.lib
-    ev = _PhaseEvents(timings)
-    ev.mark("start")
+    st = _LprState()
     if dev_inputs is not None:
         dx, ycols = dev_inputs
         n, d = dx.shape
@@ -676,16 +705,11 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
                                      ctx.stream), "flpr_log_shift")
         ycols = [ylog]
     ny = len(ycols)
-
     G = _grid_shape(opts, n, d)
     stats = _point_stats(ctx, dx, n, d)
     if flags_h is not None:
         _raise_nonfinite(flags_h.numpy(), [("Input x", 0), ("Response y", 1)], "cv_fastlpr")
     geom = _make_geom(stats, n, d, G, int(opts["accuracy"]), bool(opts.get("flag_power2", True)))
-    npow = 2 * order + 1
-    F, bw, keep, _ = _filter_bandwidths(ctx, geom, bandwidths, npow)
-    H = len(keep)
-    Hf = bw.shape[0]
     calc_dof = bool(opts.get("calc_dof", True))
     if calc_dof:
         probes, R = _probes(ctx, n, int(opts.get("num_dof_sample", 10)),
@@ -696,7 +720,39 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
         pcols = []
     ev.mark("setup")
     spec = _spread_fft(ctx, geom, dx, ycols + pcols, prec, ev)
+    axes_raw = _raw_axes(geom, opts)
+    st.__dict__.update(dict(
+        n=n, d=d, dx=dx, ycols=ycols, pcols=pcols, R=R, ny=ny, y_raw_dev=y_raw_dev,
+        stats=stats, geom=geom, spec=spec, calc_dof=calc_dof, order=order, prec=prec,
+        dy=dy, variance=variance, y_is_complex=y_is_complex, opts=opts,
+        axes_raw=axes_raw, ax_arg=_lib.dvec(_axes_arg(axes_raw)), G_arg=_lib.ivec(geom.G),
+        dual=calc_dof and ny <= 4 and not opts.get("_direct_reduce", False), Q=None))
+    if st.dual:
+        # dual form: grid-domain dot products with the adjoint deposits
+        M = geom.M
+        Cv = ny + R
+        npair = (2 ** d) * (2 ** d + 1) // 2
+        st.Q = ctx.empty((M, Cv))
+        st.Bst = ctx.empty((M, npair))
+        st.sq = ctx.empty(Cv)
+        ctx.check(lib.flpr_deposit(d, n, dx.data_ptr(), st.ax_arg, st.G_arg, Cv,
+                                   _lib.pvec([c.data_ptr() for c in ycols + pcols]),
+                                   st.Q.data_ptr(), st.Bst.data_ptr(), st.sq.data_ptr(),
+                                   ctx.stream), "flpr_deposit")
+        ev.mark("deposit")
+    return st
 
+
+def _evaluate_lpr(ctx, st: _LprState, bandwidths: np.ndarray, ev) -> dict:
+    """Kernel spectra, convolutions, solves and GCV for one bandwidth list."""
+    lib = ctx.lib
+    d, n, ny, R, order, prec = st.d, st.n, st.ny, st.R, st.order, st.prec
+    geom, spec, opts, calc_dof = st.geom, st.spec, st.opts, st.calc_dof
+    ycols, pcols = st.ycols, st.pcols
+    npow = 2 * order + 1
+    F, bw, keep, _ = _filter_bandwidths(ctx, geom, bandwidths, npow)
+    H = len(keep)
+    Hf = bw.shape[0]
     epw = _element_powers(d, order)
     ns = len(epw)
     nt = 1 if order == 0 else len(_design_powers(d, order))
@@ -716,26 +772,12 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
                   [(1 + c, int(hk), epw[i]) for i in range(nt) for c in range(Cv) for hk in h_t],
                   prec, False)
         ev.mark("conv_T")
-    M = geom.M
-    axes_raw = _raw_axes(geom, opts)
-    ax_arg = _lib.dvec(_axes_arg(axes_raw))
-    G_arg = _lib.ivec(geom.G)
     bw_k = bw[keep]
     scalar = ctx.empty(1)
     reg = float(opts["regularization"])
     # lambda (order >= 1) / max(s) (order 0) is taken over every kept bandwidth;
     # without DoF only the first bandwidth's T is needed.
-    if calc_dof and ny <= 4 and not opts.get("_direct_reduce", False):
-        # dual form: grid-domain dot products with the adjoint deposits
-        npair = (2 ** d) * (2 ** d + 1) // 2
-        Q = ctx.empty((M, Cv))
-        Bst = ctx.empty((M, npair))
-        sq = ctx.empty(Cv)
-        ctx.check(lib.flpr_deposit(d, n, dx.data_ptr(), ax_arg, G_arg, Cv,
-                                   _lib.pvec([c.data_ptr() for c in ycols + pcols]),
-                                   Q.data_ptr(), Bst.data_ptr(), sq.data_ptr(), ctx.stream),
-                  "flpr_deposit")
-        ev.mark("deposit")
+    if st.dual:
         m = ctx.empty((H, M, ny))
         dots = ctx.empty((Cv, H))
         if use_fused:
@@ -743,23 +785,23 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
             scale = 1.0 / (SQRT_2PI * float(np.prod(geom.L.astype(float))))
             ws = ctx.ws(lib.flpr_lpr2d_fused_ws(*Lq, H, order, Cv))
             ctx.check(lib.flpr_lpr2d_fused(*Lq, H, npow, order, Cv, ny, spec.data_ptr(),
-                                           F.data_ptr(), scale, Q.data_ptr(), reg, S.data_ptr(),
-                                           m.data_ptr(), dots.data_ptr(), scalar.data_ptr(),
-                                           ws.data_ptr(), ws.numel(), ctx.stream),
-                      "flpr_lpr2d_fused")
+                                           F.data_ptr(), scale, st.Q.data_ptr(), reg,
+                                           S.data_ptr(), m.data_ptr(), dots.data_ptr(),
+                                           scalar.data_ptr(), ws.data_ptr(), ws.numel(),
+                                           ctx.stream), "flpr_lpr2d_fused")
             del ws
             ev.mark("conv_solve")
         else:
             ctx.check(lib.flpr_solve_reduce(order, nt, H, H, M, Cv, S.data_ptr(), T.data_ptr(),
-                                            reg, ny, m.data_ptr(), Q.data_ptr(), dots.data_ptr(),
-                                            scalar.data_ptr(), prec, ctx.stream),
-                      "flpr_solve_reduce")
+                                            reg, ny, m.data_ptr(), st.Q.data_ptr(),
+                                            dots.data_ptr(), scalar.data_ptr(), prec,
+                                            ctx.stream), "flpr_solve_reduce")
             ev.mark("solve")
         quad = ctx.empty((H, ny))
-        ctx.check(lib.flpr_stencil_quad(d, G_arg, H, ny, m.data_ptr(), Bst.data_ptr(),
+        ctx.check(lib.flpr_stencil_quad(d, st.G_arg, H, ny, m.data_ptr(), st.Bst.data_ptr(),
                                         quad.data_ptr(), ctx.stream), "flpr_stencil_quad")
         ev.mark("interp_reduce")
-        sq_h = sq.cpu().numpy()
+        sq_h = st.sq.cpu().numpy()
         dots_h = dots.cpu().numpy()
         quad_h = quad.cpu().numpy()
         rss_h = sq_h[None, :ny] - 2.0 * dots_h[:ny].T + quad_h
@@ -776,8 +818,8 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
             rss = ctx.empty((H, ny))
             pdot = ctx.empty((max(R, 1), H))
             pp = ctx.empty(max(R, 1))
-            ctx.check(lib.flpr_interp_reduce(d, n, dx.data_ptr(), ax_arg, G_arg, H, ny, R,
-                                             m.data_ptr(),
+            ctx.check(lib.flpr_interp_reduce(d, n, st.dx.data_ptr(), st.ax_arg, st.G_arg, H, ny,
+                                             R, m.data_ptr(),
                                              _lib.pvec([c.data_ptr() for c in ycols]),
                                              _lib.pvec([c.data_ptr() for c in pcols]),
                                              rss.data_ptr(), pdot.data_ptr(), pp.data_ptr(),
@@ -787,24 +829,32 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
             pdot_h = pdot.cpu().numpy()[:R]
             pp_h = pp.cpu().numpy()[:R]
     if calc_dof:
-        gcv = _gcv_from_sums(n, rss_h, pdot_h, pp_h, dy, y_is_complex, opts)
+        gcv = _gcv_from_sums(n, rss_h, pdot_h, pp_h, st.dy, st.y_is_complex, opts)
         dstd = float(opts.get("dstd", 0.0))
         sel = _one_se_rule(gcv["gcv_m"], gcv["gcv_sd"], bw_k, prefer_smaller=True, dstd=dstd)
-        msel = sel
     else:
         gcv = None
         sel = 0
-        msel = 0
-    # selected grid values and fitted values
-    mv = m[msel]                                     # (M, mstride)
+    return dict(keep=keep, bw_k=bw_k, H=H, m=m, S=S, ns=ns, mstride=mstride, gcv=gcv, sel=sel)
+
+
+def _finalize_lpr(ctx, st: _LprState, r: dict, ev, search) -> RegressionOutput:
+    """Fitted values at the selected bandwidth and the result structure."""
+    lib = ctx.lib
+    d, n, ny, dy = st.d, st.n, st.ny, st.dy
+    geom, opts = st.geom, st.opts
+    bw_k, sel, gcv, m, S = r["bw_k"], r["sel"], r["gcv"], r["m"], r["S"]
+    H, ns, M = r["H"], r["ns"], geom.M
+    mv = m[sel if st.calc_dof else 0]                # (M, mstride)
     gv_dev = mv[:, :ny].t().contiguous()             # (ny, M)
     yhat_dev = ctx.empty((ny, n))
-    ctx.check(lib.flpr_interp_eval(d, n, dx.data_ptr(), ax_arg, G_arg, ny, gv_dev.data_ptr(),
-                                   yhat_dev.data_ptr(), ctx.stream), "flpr_interp_eval")
+    ctx.check(lib.flpr_interp_eval(d, n, st.dx.data_ptr(), st.ax_arg, st.G_arg, ny,
+                                   gv_dev.data_ptr(), yhat_dev.data_ptr(), ctx.stream),
+              "flpr_interp_eval")
     d_norm = None
-    if variance:
+    if st.variance:
         acc = ctx.empty(1)
-        ctx.check(lib.flpr_exp_weighted_sum(n, y_raw_dev.data_ptr(), yhat_dev.data_ptr(),
+        ctx.check(lib.flpr_exp_weighted_sum(n, st.y_raw_dev.data_ptr(), yhat_dev.data_ptr(),
                                             acc.data_ptr(), ctx.stream), "flpr_exp_weighted_sum")
         d_norm = 1.0 / ((1.0 / n) * float(acc.item()))
         yhat_dev = torch.exp(yhat_dev) / d_norm
@@ -812,10 +862,10 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
     ev.mark("final_interp")
     # residuals on the device; every result is copied into pinned host memory
     # with one synchronisation (the caching host allocator recycles the pages)
-    if variance:
-        res_dev = y_raw_dev[None, :] - yhat_dev
+    if st.variance:
+        res_dev = st.y_raw_dev[None, :] - yhat_dev
     else:
-        res_dev = torch.stack(ycols[:ny], dim=0) - yhat_dev
+        res_dev = torch.stack(st.ycols[:ny], dim=0) - yhat_dev
     yh = _to_host(yhat_dev)
     rh = _to_host(res_dev)
     gvh = _to_host(gv_dev)
@@ -823,7 +873,7 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
     torch.cuda.current_stream(ctx.device).synchronize()
     yh, rh, gvh = yh.numpy(), rh.numpy(), gvh.numpy()
     gshape = tuple(int(g) for g in geom.G)
-    if y_is_complex:
+    if st.y_is_complex:
         yh = yh[0::2] + 1j * yh[1::2]
         rh = rh[0::2] + 1j * rh[1::2]
         gvh = gvh[0::2] + 1j * gvh[1::2]
@@ -838,9 +888,9 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
     s0 = s0h.numpy().reshape(gshape)
     ev.mark("download")
     ev.finish()
-    interp = GridInterpolant(axes_raw, grid_values, ctx.device)
+    interp = GridInterpolant(st.axes_raw, grid_values, ctx.device)
     selected = bw_k[sel]
-    if calc_dof:
+    if st.calc_dof:
         idmin = int(np.argmin(gcv["gcv_m"]))
         gcv_result = {
             "bandwidths": bw_k,
@@ -864,7 +914,7 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
         dof = dof_se = np.nan
     metadata = {
         "options": opts,
-        "order": order,
+        "order": st.order,
         "bandwidths_tested": bw_k,
         "fitted_at_samples": yhat,
         "residuals": residuals,
@@ -872,11 +922,74 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
         "std": geom.std,
         "dof": dof,
         "dof_stderr": dof_se,
-        "precision": "fp32" if prec == _lib.FLPR_PREC_F32 else "fp64",
+        "precision": "fp32" if st.prec == _lib.FLPR_PREC_F32 else "fp64",
+        "bandwidth_search": search if search is not None else {"mode": "full"},
     }
-    return RegressionOutput(yhat=yhat, grid=tuple(axes_raw), h=selected, gcv_yhat=gcv_result,
+    return RegressionOutput(yhat=yhat, grid=tuple(st.axes_raw), h=selected, gcv_yhat=gcv_result,
                             fpp_yhat=interp, metadata=metadata, dof=dof, dof_stderr=dof_se,
                             d=d_norm, s0=s0)
+
+
+# windows a learned search may walk before it falls back to the full sweep
+_MAX_WALKS = 3
+
+
+def _learned_search(ctx, st: _LprState, bandwidths: np.ndarray, model, ev):
+    """Proposal + five-bandwidth window, walked toward an edge minimum (the
+    next window shares the edge bandwidth) at most _MAX_WALKS times; returns
+    (evaluation, search record) or None when the full sweep must run."""
+    from . import learned as _learned
+    if not (st.calc_dof and st.ny == 1 and not st.y_is_complex and st.d <= 2):
+        return None
+    lh = _learned.isotropic_log_h(bandwidths)
+    if lh is None:
+        return None
+    d_stats = ctx.upload(np.ascontiguousarray(st.stats[:2].ravel()))
+    feats = _learned.dataset_features(st.dx, st.ycols[0], d_stats, st.n, st.d, st.order,
+                                      ctx.stream)
+    t = float(model.predict(feats)[0])
+    ev.mark("proposal")
+    nlist = int(bandwidths.shape[0])
+    window = _learned.refine_window(t, lh)
+    record = {"mode": "learned", "proposal_index": t, "windows": [], "nlist": nlist,
+              "accepted": False}
+    for _ in range(_MAX_WALKS + 1):
+        record["windows"].append([int(i) for i in window])
+        r = _evaluate_lpr(ctx, st, bandwidths[window], ev)
+        if r["H"] != len(window):
+            return None                     # a bandwidth of the window was filtered out
+        pos = int(np.argmin(r["gcv"]["gcv_m"]))
+        if _learned.accept_window(window, pos, nlist):
+            record["accepted"] = True
+            record["evaluated"] = len({i for w in record["windows"] for i in w})
+            return r, record
+        step = _learned.REFINE - 1
+        lo = int(window[0]) + (step if pos == len(window) - 1 else -step)
+        lo = int(np.clip(lo, 0, nlist - _learned.REFINE))
+        nxt = np.arange(lo, lo + _learned.REFINE)
+        if np.array_equal(nxt, window):
+            return None
+        window = nxt
+    return None
+
+
+def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_is_complex,
+             dev_inputs=None, timings=None, learned=None):
+    """One LPR fit.  With a proposal network (`learned`) a walked window of
+    five bandwidths replaces the sweep when its GCV minimum is trusted; the
+    full sweep over `bandwidths` runs otherwise (sharing the spectra)."""
+    ev = _PhaseEvents(timings)
+    ev.mark("start")
+    st = _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_complex,
+                      dev_inputs, ev)
+    found = _learned_search(ctx, st, bandwidths, learned, ev) if learned is not None else None
+    if found is not None:
+        r, search = found
+    else:
+        r = _evaluate_lpr(ctx, st, bandwidths, ev)
+        search = None if learned is None else {"mode": "learned", "accepted": False,
+                                               "fallback": "full sweep"}
+    return _finalize_lpr(ctx, st, r, ev, search)
 
 
 def _gcv_from_sums(n, rss, pdot, pp, dy, y_is_complex, opts):

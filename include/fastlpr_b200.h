@@ -264,6 +264,60 @@ int flpr_log_shift(int64_t n, const double* d_in, double shift, double* d_out, v
 int flpr_exp_weighted_sum(int64_t n, const double* d_yraw, const double* d_yhat,
                           double* d_acc, void* stream);
 
+/* ---------------------------------------------------------------------
+ * (11) Learned bandwidth proposal.  No counterpart in the reference: the
+ * reference always sweeps every bandwidth.  A small MLP reads binned moment
+ * summaries of a data set and proposes where the GCV minimum lies; a short
+ * sweep around the proposal is accepted only when its minimum is interior,
+ * otherwise the full sweep runs.
+ *
+ * flpr_bin_moments: d in {1, 2}; d_stats from flpr_point_stats (min, max
+ * per axis).  d_out (3, 4096) float64 receives, per cell of a grid over
+ * [min, max] (4096 bins in 1-D, 64 x 64 row-major in 2-D), the count,
+ * sum y and sum y^2 (zeroed by the call).
+ * --------------------------------------------------------------------- */
+int flpr_bin_moments(int d, int64_t n, const double* d_x, const double* d_y,
+                     const double* d_stats, double* d_out, void* stream);
+
+/* Dense ReLU network h_{l+1} = relu(h_l W_l^T + b_l) (no ReLU on the last
+ * layer) with dims[0..nlayers].  Parameters are packed per layer as
+ * W_l (dims[l+1] x dims[l], row-major) then b_l; d_params32 is the FP32
+ * master copy, d_params16 the BF16 copy the products read.  Products are
+ * BF16 x BF16 with FP32 accumulation on the tensor cores.
+ *
+ * flpr_mlp_gemm: C = op(A) op(B) (+ bias[n]) (relu) (* (mask > 0)), with
+ * A (M x K) stored row-major (a_trans = 0, A[m*lda+k]) or transposed
+ * (a_trans = 1, A[k*lda+m]), B (K x N) stored row-major (b_nk = 0,
+ * B[k*ldb+n]) or as N x K (b_nk = 1, B[n*ldb+k]); BF16 operands and mask,
+ * FP32 and/or BF16 outputs with leading dimension ldc. */
+int flpr_mlp_gemm(int M, int N, int K, const void* d_A, int lda, int a_trans,
+                  const void* d_B, int ldb, int b_nk, const float* d_bias, int relu,
+                  const void* d_mask, int ldm, float* d_C32, void* d_C16, int ldc,
+                  void* stream);
+int64_t flpr_mlp_param_count(int nlayers, const int* h_dims);
+/* Workspace of flpr_mlp_fwd/flpr_mlp_bwd for `batch` rows: the hidden
+ * activations kept for the backward pass and two gradient buffers. */
+size_t flpr_mlp_ws(int nlayers, const int* h_dims, int batch);
+/* d_x16: (batch, dims[0]) BF16 inputs; d_out: (batch, dims[nlayers]) FP32. */
+int flpr_mlp_fwd(int nlayers, const int* h_dims, const void* d_params16,
+                 const float* d_params32, int batch, const void* d_x16, float* d_out,
+                 void* d_ws, size_t ws_bytes, void* stream);
+/* Gradients of sum(d_dout * out) with respect to every parameter, written
+ * to d_grad32 (same packing as the parameters).  Uses the activations the
+ * preceding flpr_mlp_fwd left in the same workspace. */
+int flpr_mlp_bwd(int nlayers, const int* h_dims, const void* d_params16, int batch,
+                 const void* d_x16, const float* d_dout, float* d_grad32, void* d_ws,
+                 size_t ws_bytes, void* stream);
+/* Adam on the FP32 master parameters (an L2 term weight_decay * p is added
+ * to the gradient); refreshes the BF16 copy. */
+int flpr_mlp_step(int64_t nparams, float* d_params32, void* d_params16, const float* d_grad32,
+                  float* d_m, float* d_v, float lr, float beta1, float beta2, float eps,
+                  float weight_decay, int step, void* stream);
+/* d_loss[0] = mean (y - t)^2; d_dy = 2 (y - t) / batch. */
+int flpr_mlp_mse(int batch, const float* d_y, const float* d_t, float* d_dy, float* d_loss,
+                 void* stream);
+int flpr_to_bf16(int64_t n, const float* d_x, void* d_y, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
