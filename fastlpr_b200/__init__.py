@@ -12,15 +12,22 @@ The hot path runs in the in-tree CUDA library ``libfastlpr_b200.so``
 from .bandwidth import get_hlist
 from .structures import KDEOutput, RegressionOutput
 from .api import cv_fastkde, cv_fastlpr, cv_fastlpr_device, clear_fastlpr_caches
+from .confidence import fastlpr_interval
+
+import numpy as np
 
 __version__ = "0.1.0"
 
 
 def fastlpr_predict(regression: RegressionOutput, x_new):
-    """Evaluate a fitted regression at new points (reference predict.py:15-131)."""
+    """Evaluate a fitted regression at new points (reference predict.py:15-131):
+    the fitted grid's interpolant, evaluated on the GPU."""
     if regression.fpp_yhat is None:
-        raise ValueError("regression has no interpolant")
-    return regression.fpp_yhat(x_new)
+        raise ValueError("Regression output does not contain an interpolant (fpp).")
+    points = np.asarray(x_new, dtype=float)
+    if points.ndim == 1:
+        points = points[:, None]
+    return np.asarray(regression.fpp_yhat(points))
 
 
 __all__ = [
@@ -30,6 +37,7 @@ __all__ = [
     "cv_fastlpr_device",
     "get_hlist",
     "fastlpr_predict",
+    "fastlpr_interval",
     "RegressionOutput",
     "KDEOutput",
     "clear_fastlpr_caches",

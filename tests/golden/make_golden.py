@@ -233,7 +233,39 @@ def main():
     _kde_case(fastlpr, "kde3d", xk3, np.column_stack([hk3, hk3, hk3]), {"N": [16, 16, 16]})
 
     _intermediates_case(fastlpr, "inter2d_o1")
+    interval_case(fastlpr)
+
+
+def interval_case(fastlpr):
+    """Mean fit, variance fit of the squared residuals and the reference's
+    fastlpr_interval (confidence and prediction) on the mean's grid."""
+    from fastlpr import cv_fastlpr, get_hlist
+    from fastlpr.confidence import fastlpr_interval
+
+    rng = np.random.default_rng(77)
+    n = 4000
+    x = rng.random((n, 1))
+    sig = 0.05 + 0.2 * x[:, 0]
+    y = np.sin(2 * np.pi * x[:, 0]) + sig * rng.standard_normal(n)
+    h = get_hlist(10, [0.02, 0.6])
+    fastlpr.clear_fastlpr_caches()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        mu = cv_fastlpr(x, y, h, {"order": 1, "N": 256})
+        res = (y - mu.yhat) ** 2
+        var = cv_fastlpr(x, res, h, {"order": 1, "N": 256, "y_type_out": "variance", "dstd": 10})
+    ci = fastlpr_interval(mu, var, 0.05, type="confidence")
+    pi = fastlpr_interval(mu, var, 0.1, type="prediction")
+    np.savez_compressed(os.path.join(HERE, "interval1d.npz"), kind="interval", x=x, y=y,
+                        h=np.asarray(h),
+                        ci=np.asarray(ci), pi=np.asarray(pi), mu_h=np.asarray(mu.h),
+                        var_h=np.asarray(var.h), mu_values=np.asarray(mu.fpp_yhat.values),
+                        var_values=np.asarray(var.fpp_yhat.values), s0=np.asarray(mu.s0))
+    print(f"interval1d: N={n} h_mu={np.asarray(mu.h).ravel()} h_var={np.asarray(var.h).ravel()}")
 
 
 if __name__ == "__main__":
-    main()
+    if "--only-interval" in sys.argv:
+        interval_case(_import_reference())
+    else:
+        main()
