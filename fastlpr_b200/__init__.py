@@ -13,6 +13,8 @@ from .bandwidth import get_hlist
 from .structures import KDEOutput, RegressionOutput
 from .api import cv_fastkde, cv_fastlpr, cv_fastlpr_device, clear_fastlpr_caches
 from .confidence import fastlpr_interval
+from .batch import (SharedData, batch_evaluate_at_points, compute_gcv_scores_batch,
+                    cv_fastlpr_batch, precompute_shared)
 
 import numpy as np
 
@@ -38,6 +40,11 @@ __all__ = [
     "get_hlist",
     "fastlpr_predict",
     "fastlpr_interval",
+    "SharedData",
+    "precompute_shared",
+    "cv_fastlpr_batch",
+    "batch_evaluate_at_points",
+    "compute_gcv_scores_batch",
     "RegressionOutput",
     "KDEOutput",
     "clear_fastlpr_caches",
