@@ -68,9 +68,10 @@ def b_fit(n=N_POINTS, d=2, G=512, H=N_H, R=R_PROBES, order=1, cy=1, parts=False)
 
 
 # DRAM traffic of the fused convolution stage of one metric fit
-# (dram__bytes_read.sum + dram__bytes_write.sum over its kernels), from the
-# ncu capture summarised in profiles/; None until measured.
-CONV_STAGE_TRAFFIC = None
+# (dram__bytes_read.sum + dram__bytes_write.sum over its kernels, bytes), from
+# the ncu capture in profiles/dram_lpr2d_n1e5_g512_h32_single_fit.md (the
+# stage works on grid-sized arrays only, so the N=1e5 capture holds for N=1e6).
+CONV_STAGE_TRAFFIC = 3.438e9
 
 
 # ---------------------------------------------------------------------------
@@ -231,6 +232,16 @@ def run_ours(args):
     xh, yh = xp.numpy(), yp.numpy()
 
     lib = _lib.load()
+    if args.single_fit:
+        # one plain fit and nothing else: the command profiles are captured with
+        l0 = lib.flpr_launch_count()
+        t0 = time.perf_counter()
+        r = fastlpr_b200.cv_fastlpr_device(xd, yd, h, opts)
+        torch.cuda.synchronize()
+        print(json.dumps({"single_fit_ms": 1000.0 * (time.perf_counter() - t0),
+                          "launches": int(lib.flpr_launch_count() - l0),
+                          "h": [float(v) for v in np.atleast_1d(r.h)]}), flush=True)
+        return 0
     for _ in range(max(args.warmup, 3)):
         fastlpr_b200.cv_fastlpr_device(xd, yd, h, opts)
     torch.cuda.synchronize()
@@ -387,6 +398,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--single-fit", action="store_true",
+                    help="run one plain fit of the workload and exit (for profilers)")
     ap.add_argument("--points", type=int, default=N_POINTS,
                     help="points per fit (profiling of smaller cases only)")
     ap.add_argument("--grid", type=int, default=0, help="grid per axis (default 512)")

@@ -387,10 +387,23 @@ def _kernel_factors(ctx: _Ctx, geom: _Geom, bw: np.ndarray, npow: int):
     return F, sum0
 
 
+def _kernel_sums_host(geom: _Geom, bw: np.ndarray) -> np.ndarray:
+    """(d, H) grid sums of the order-0 kernel factor exp(-u^2/2)/h on
+    linspace(lo, hi, G) per axis: the same values flpr_kernel_factors returns
+    in d_sum0, formed on the host so the filter needs no device round trip."""
+    out = np.empty((geom.d, bw.shape[0]))
+    for a in range(geom.d):
+        G = int(geom.G[a])
+        g = np.linspace(geom.lo[a], geom.hi[a], G)
+        u = g[None, :] / bw[:, a:a + 1]
+        out[a] = np.sum(np.exp(-0.5 * (u * u)) / bw[:, a:a + 1], axis=1)
+    return out
+
+
 def _filter_bandwidths(ctx, geom, bw, npow):
     """Kernel factors with the "too small bandwidth" filter of convolution.py:542-605."""
-    F, sum0 = _kernel_factors(ctx, geom, bw, npow)
-    s = sum0.cpu().numpy()
+    F, _ = _kernel_factors(ctx, geom, bw, npow)
+    s = _kernel_sums_host(geom, bw)
     ksum = np.abs(np.prod(s, axis=0) / SQRT_2PI)
     ihbad = ksum < EPS * 10
     keep = np.where(~ihbad)[0]
@@ -801,9 +814,11 @@ def _evaluate_lpr(ctx, st: _LprState, bandwidths: np.ndarray, ev) -> dict:
         ctx.check(lib.flpr_stencil_quad(d, st.G_arg, H, ny, m.data_ptr(), st.Bst.data_ptr(),
                                         quad.data_ptr(), ctx.stream), "flpr_stencil_quad")
         ev.mark("interp_reduce")
-        sq_h = st.sq.cpu().numpy()
-        dots_h = dots.cpu().numpy()
-        quad_h = quad.cpu().numpy()
+        # one device -> host read for the three reductions
+        packed = torch.cat([st.sq.reshape(-1), dots.reshape(-1), quad.reshape(-1)]).cpu().numpy()
+        sq_h = packed[:Cv]
+        dots_h = packed[Cv:Cv + Cv * H].reshape(Cv, H)
+        quad_h = packed[Cv + Cv * H:].reshape(H, ny)
         rss_h = sq_h[None, :ny] - 2.0 * dots_h[:ny].T + quad_h
         pdot_h = dots_h[ny:]
         pp_h = sq_h[ny:]

@@ -455,12 +455,31 @@ rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict
   float* bufs = reinterpret_cast<float*>(s_tw2 + twiddle_entries(N));
   const int nwarps = blockDim.x >> 5;
   float* regions = bufs + (size_t)nwarps * SW;
-  load_twiddles<E>(s_tw2, tab);
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int r = blockIdx.x, hz = blockIdx.y, h = ra.hbase + hz;
   const int64_t M = (int64_t)ra.G0 * ra.G1;
   const int G1 = ra.G1, njobs = ra.njobs;
+  {
+    // start every W row this row's jobs read (up to the band limit) and the
+    // row's solve vectors on their way into L2 before the first transform
+    const int lines = ((kcut1[h] + 1) * (int)sizeof(float2) + 127) / 128;
+    const int per_job = 2 * lines;
+    for (int t = threadIdx.x; t < njobs * per_job; t += blockDim.x) {
+      const int j = t / per_job, rem = t - j * per_job;
+      const int side = rem / lines, l = rem - side * lines;
+      const int slot = side == 0 ? ra.jobs[j].slot_a : ra.jobs[j].slot_b;
+      if (slot < 0) continue;
+      const char* row = reinterpret_cast<const char*>(
+          W + (((size_t)slot * nslots_w + hz) * ra.G0 + r) * (size_t)ra.L1h);
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(row + 128 * l));
+    }
+    const char* zr = reinterpret_cast<const char*>(zg + ((int64_t)h * M + (int64_t)r * G1) * NT);
+    const int zl = (G1 * NT * (int)sizeof(double) + 127) / 128;
+    for (int l = threadIdx.x; l < zl; l += blockDim.x)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(zr + 128 * l));
+  }
+  load_twiddles<E>(s_tw2, tab);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int last0 = njobs - nwarps;  // jobs >= last0 are the last of their warp
   float* buf = bufs + warp * SW;
   const int kc = kcut1[h];

@@ -29,10 +29,7 @@ class GridInterpolant:
         self._M = int(np.prod(self._G))
         extra = self.values.shape[self.ndim:]
         self._extra = extra
-        flat = self.values.reshape(self._M, -1)  # (M, nval)
-        parts = [flat.real, flat.imag] if self.is_complex else [flat]
-        stacked = np.concatenate([p.T for p in parts], axis=0).astype(np.float64)
-        self._dvals = torch.from_numpy(np.ascontiguousarray(stacked)).to(device)
+        self._dvals = None  # device copy, made at the first evaluation
         ax = []
         for a in self.grid_axes:
             ax += [float(a[0]), float(a[1] - a[0]) if len(a) > 1 else 1.0]
@@ -46,6 +43,11 @@ class GridInterpolant:
         n = pts.shape[0]
         lib = _lib.load()
         with torch.cuda.device(self.device):
+            if self._dvals is None:
+                flat = self.values.reshape(self._M, -1)  # (M, nval)
+                parts = [flat.real, flat.imag] if self.is_complex else [flat]
+                stacked = np.concatenate([p.T for p in parts], axis=0).astype(np.float64)
+                self._dvals = torch.from_numpy(np.ascontiguousarray(stacked)).to(self.device)
             dx = torch.from_numpy(np.ascontiguousarray(pts)).to(self.device)
             nval = self._dvals.shape[0]
             out = torch.empty((nval, n), dtype=torch.float64, device=self.device)
