@@ -686,7 +686,10 @@ class _LprState:
 
 
 def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_complex,
-                 dev_inputs, ev) -> _LprState:
+                 dev_inputs, ev, hook=None) -> _LprState:
+    """Bandwidth-independent stage.  `hook(dx, ycols, stats, n, d)` runs after
+    the point statistics, before the spread is enqueued (the learned search
+    starts its data summary there, on a side stream)."""
     lib = ctx.lib
     st = _LprState()
     if dev_inputs is not None:
@@ -732,6 +735,8 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
         R = 0
         pcols = []
     ev.mark("setup")
+    if hook is not None:
+        hook(dx, ycols, stats, n, d)
     spec = _spread_fft(ctx, geom, dx, ycols + pcols, prec, ev)
     axes_raw = _raw_axes(geom, opts)
     st.__dict__.update(dict(
@@ -949,20 +954,54 @@ def _finalize_lpr(ctx, st: _LprState, r: dict, ev, search) -> RegressionOutput:
 _MAX_WALKS = 3
 
 
-def _learned_search(ctx, st: _LprState, bandwidths: np.ndarray, model, ev):
+_SIDE_STREAMS: Dict[int, torch.cuda.Stream] = {}
+
+
+def _side_stream(device: torch.device) -> torch.cuda.Stream:
+    idx = device.index if device.index is not None else torch.cuda.current_device()
+    if idx not in _SIDE_STREAMS:
+        _SIDE_STREAMS[idx] = torch.cuda.Stream(device=device)
+    return _SIDE_STREAMS[idx]
+
+
+def _start_summary(ctx, pending: dict, dx, ycols, stats, n, d) -> None:
+    """Binned moment sums of the data on a side stream, copied to pinned
+    host memory, overlapping the spread that the main stream runs next."""
+    from . import learned as _learned
+    if len(ycols) != 1 or d > 2:
+        return
+    side = _side_stream(ctx.device)
+    ready = torch.cuda.Event()
+    ready.record()                                  # x, y and the statistics are on the device
+    with torch.cuda.stream(side):
+        side.wait_event(ready)
+        dx.record_stream(side)
+        ycols[0].record_stream(side)
+        d_stats = ctx.upload(np.ascontiguousarray(stats[:2].ravel()))
+        bins = _learned.bin_moments(dx, ycols[0], d_stats, n, d, side.cuda_stream)
+        host = torch.empty(bins.shape, dtype=bins.dtype, pin_memory=True)
+        host.copy_(bins, non_blocking=True)
+        done = torch.cuda.Event()
+        done.record(side)
+    pending.update(side=side, host=host, done=done, keep=(bins, d_stats))
+
+
+def _learned_search(ctx, st: _LprState, bandwidths: np.ndarray, model, ev, pending: dict):
     """Proposal + five-bandwidth window, walked toward an edge minimum (the
     next window shares the edge bandwidth) at most _MAX_WALKS times; returns
     (evaluation, search record) or None when the full sweep must run."""
     from . import learned as _learned
-    if not (st.calc_dof and st.ny == 1 and not st.y_is_complex and st.d <= 2):
+    if not (st.calc_dof and st.ny == 1 and not st.y_is_complex and st.d <= 2) or not pending:
         return None
     lh = _learned.isotropic_log_h(bandwidths)
     if lh is None:
         return None
-    d_stats = ctx.upload(np.ascontiguousarray(st.stats[:2].ravel()))
-    feats = _learned.dataset_features(st.dx, st.ycols[0], d_stats, st.n, st.d, st.order,
-                                      ctx.stream)
-    t = float(model.predict(feats)[0])
+    # the summary was enqueued on the side stream before the spread: waiting
+    # for it does not wait for the main stream
+    pending["done"].synchronize()
+    feats = _learned.summarize(pending["host"].numpy(), st.d, st.n, st.order)
+    with torch.cuda.stream(pending["side"]):
+        t = float(model.predict(feats)[0])
     ev.mark("proposal")
     nlist = int(bandwidths.shape[0])
     window = _learned.refine_window(t, lh)
@@ -995,9 +1034,15 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
     full sweep over `bandwidths` runs otherwise (sharing the spectra)."""
     ev = _PhaseEvents(timings)
     ev.mark("start")
+    pending = {}
+    hook = None
+    if learned is not None:
+        def hook(dx, ycols, stats, n, d):
+            _start_summary(ctx, pending, dx, ycols, stats, n, d)
     st = _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_complex,
-                      dev_inputs, ev)
-    found = _learned_search(ctx, st, bandwidths, learned, ev) if learned is not None else None
+                      dev_inputs, ev, hook=hook)
+    found = (_learned_search(ctx, st, bandwidths, learned, ev, pending)
+             if learned is not None else None)
     if found is not None:
         r, search = found
     else:

@@ -433,7 +433,7 @@ inline int t_warps(int njobs) {
   return (njobs + rounds - 1) / rounds;
 }
 
-// T pass fused with the solve and the dual-form reductions: grid (G0, Hc),
+// T pass fused with the solve and the dual-form reductions: grid (Hc, G0),
 // t_warps(njobs) warps.  Warp w computes jobs w, w + nwarps, ...; product
 // p = c * NT + i (job p / 2, half p % 2) stays in shared memory until every
 // job of the row is done; then m_c(x1) = sum_i z_i(x1) T(p, x1) with z the
@@ -455,7 +455,8 @@ rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict
   float* bufs = reinterpret_cast<float*>(s_tw2 + twiddle_entries(N));
   const int nwarps = blockDim.x >> 5;
   float* regions = bufs + (size_t)nwarps * SW;
-  const int r = blockIdx.x, hz = blockIdx.y, h = ra.hbase + hz;
+  // bandwidth fastest: the CTAs of one row (sharing its deposits Q) run together
+  const int hz = blockIdx.x, r = blockIdx.y, h = ra.hbase + hz;
   const int64_t M = (int64_t)ra.G0 * ra.G1;
   const int G1 = ra.G1, njobs = ra.njobs;
   {
@@ -596,7 +597,7 @@ static int launch_row_t_nt(const RowArgs& ra, int Hc, int H, int nslots_w, const
   const int nwarps = t_warps(ra.njobs);
   const size_t smem = t_smem_bytes(E, nwarps, ra.njobs, ra.G1);
   FLPR_TRY(set_smem(rowpass_t_solve_kernel<E, NT>, smem));
-  rowpass_t_solve_kernel<E, NT><<<dim3(ra.G0, Hc), nwarps * 32, smem, s>>>(
+  rowpass_t_solve_kernel<E, NT><<<dim3(Hc, ra.G0), nwarps * 32, smem, s>>>(
       ra, H, nslots_w, W, F1f, tab, kcut1, C, ny, z, Q, my, dpart);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
@@ -759,6 +760,9 @@ static int fused_geom(const int* G, const int* L, const int* qout, int H, const 
   int ht = (int)(budget_t / (sizeof(float2) * slab * t.t_nslots));
   fg->Hc_s = hs < 1 ? 1 : (hs > H ? H : hs);
   fg->Hc_t = ht < 1 ? 1 : (ht > H ? H : ht);
+  // the same number of chunks, filled evenly (5 bandwidths: 3 + 2, not 4 + 1)
+  fg->Hc_s = (H + (H + fg->Hc_s - 1) / fg->Hc_s - 1) / ((H + fg->Hc_s - 1) / fg->Hc_s);
+  fg->Hc_t = (H + (H + fg->Hc_t - 1) / fg->Hc_t - 1) / ((H + fg->Hc_t - 1) / fg->Hc_t);
   size_t ws = slab * t.s_nslots * fg->Hc_s;
   size_t wt = slab * t.t_nslots * fg->Hc_t;
   fg->w_elems = ws > wt ? ws : wt;

@@ -244,41 +244,49 @@ __global__ void deposit_kernel(InterpGeom g, int64_t n, const double* __restrict
 }
 
 // quad[h][c] = sum_b sum_pairs B[b][pair] m(b+c_k) m(b+c_k2); m: (H, M, ny).
+// D fixed at compile time: the 2^D corners and their pairs live in registers.
+template <int D>
 __global__ void stencil_quad_kernel(InterpGeom g, int ny, const double* __restrict__ m,
                                     const double* __restrict__ B, double* __restrict__ quad) {
+  constexpr int NC = 1 << D;
+  constexpr int NP = NC * (NC + 1) / 2;
   __shared__ double sh[32];
   const int h = blockIdx.y;
-  const int npair = corner_pairs(g.d);
-  const int nc = 1 << g.d;
   const double* mh = m + (int64_t)h * g.M * ny;
-  int64_t coff[8];
-  for (int k = 0; k < nc; ++k) {
-    int64_t o = 0;
-    for (int a = 0; a < g.d; ++a) o = o * g.G[a] + ((k >> (g.d - 1 - a)) & 1);
+  int coff[NC];
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
+    int o = 0;
+#pragma unroll
+    for (int a = 0; a < D; ++a) o = o * g.G[a] + ((k >> (D - 1 - a)) & 1);
     coff[k] = o;
   }
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < g.M;
-       b += (int64_t)gridDim.x * blockDim.x) {
+  const int M = (int)g.M;  // grids here hold fewer than 2^31 cells
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < M; b += gridDim.x * blockDim.x) {
     // only base cells with every corner inside the grid carry weight
     bool inside = true;
-    {
-      int64_t r = b;
-      for (int a = g.d - 1; a >= 0; --a) {
-        int ia = (int)(r % g.G[a]);
-        r /= g.G[a];
-        if (ia >= g.G[a] - 1) inside = false;
-      }
+    int r = b;
+#pragma unroll
+    for (int a = D - 1; a >= 0; --a) {
+      const int ia = r % g.G[a];
+      r /= g.G[a];
+      inside = inside && ia < g.G[a] - 1;
     }
     if (!inside) continue;
-    const double* Bb = B + b * npair;
+    double Bv[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) Bv[p] = B[(int64_t)b * NP + p];
     for (int c = 0; c < ny && c < 4; ++c) {
-      double mv[8];
-      for (int k = 0; k < nc; ++k) mv[k] = mh[(b + coff[k]) * ny + c];
+      double mv[NC];
+#pragma unroll
+      for (int k = 0; k < NC; ++k) mv[k] = mh[(int64_t)(b + coff[k]) * ny + c];
       double s = 0.0;
       int p = 0;
-      for (int k = 0; k < nc; ++k)
-        for (int k2 = k; k2 < nc; ++k2, ++p) s += Bb[p] * mv[k] * mv[k2];
+#pragma unroll
+      for (int k = 0; k < NC; ++k)
+#pragma unroll
+        for (int k2 = k; k2 < NC; ++k2, ++p) s += Bv[p] * mv[k] * mv[k2];
       acc[c] += s;
     }
   }
@@ -399,7 +407,12 @@ int flpr_stencil_quad(int d, const int* h_G, int H, int ny, const double* d_m, c
   FLPR_CUDA(cudaMemsetAsync(d_quad, 0, sizeof(double) * H * ny, s));
   int per_h = (pt_blocks(g.M, 4) + H - 1) / H;
   if (per_h < 4) per_h = 4;
-  stencil_quad_kernel<<<dim3(per_h, H), 256, 0, s>>>(g, ny, d_m, d_B, d_quad);
+  FLPR_CHECK_ARG(g.M < ((int64_t)1 << 31), "stencil_quad: grid too large");
+  switch (d) {
+    case 1: stencil_quad_kernel<1><<<dim3(per_h, H), 256, 0, s>>>(g, ny, d_m, d_B, d_quad); break;
+    case 2: stencil_quad_kernel<2><<<dim3(per_h, H), 256, 0, s>>>(g, ny, d_m, d_B, d_quad); break;
+    default: stencil_quad_kernel<3><<<dim3(per_h, H), 256, 0, s>>>(g, ny, d_m, d_B, d_quad); break;
+  }
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
