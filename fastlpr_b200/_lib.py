@@ -35,6 +35,7 @@ SIGNATURES = [
     ("flpr_spread", _I, [_I, _I64, _VP, _PD, _PI, _I, _PD, _I, _I, _PVP, _VP, _I, _VP, _SZ, _VP]),
     ("flpr_forward_fft_ws", _SZ, [_VP, _I, _PI, _I, _I]),
     ("flpr_forward_fft", _I, [_VP, _I, _PI, _I, _VP, _VP, _I, _VP, _SZ, _VP]),
+    ("flpr_oversample_crop", _I, [_I, _PI, _PI, _I, _PD, _I, _VP, _VP, _I, _VP]),
     ("flpr_kernel_factors_ws", _SZ, [_VP, _I, _PI, _I, _I]),
     ("flpr_kernel_factors", _I, [_VP, _I, _PI, _PI, _PD, _PD, _I, _VP, _I, _VP, _VP, _VP, _SZ, _VP]),
     ("flpr_conv_ws", _SZ, [_VP, _I, _PI, _I, _I]),

@@ -260,7 +260,7 @@ class _Geom:
     qout: np.ndarray
     msp: int
     tau: np.ndarray
-    kmap: np.ndarray          # (d, 9)
+    kmap: np.ndarray          # (d, 9), knot spacing 2 pi / L (no oversampling)
     lo: np.ndarray            # scaled kernel grid min (= centred data min)
     hi: np.ndarray
     mean: np.ndarray
@@ -268,6 +268,7 @@ class _Geom:
     center: np.ndarray
     xmin: np.ndarray
     xmax: np.ndarray
+    accuracy: int = 4
 
     @property
     def M(self) -> int:
@@ -308,14 +309,6 @@ def _make_geom(stats: np.ndarray, n: int, d: int, G: np.ndarray, accuracy: int,
     lo = xs_min - center
     hi = xs_max - center
     L, qin, qout = _grid_params(G, flag_power2)
-    if accuracy <= 6:
-        ratio = 1
-    elif accuracy <= 11:
-        ratio = 2
-    else:
-        ratio = 3
-    msp = int(accuracy)
-    tau = (np.pi * msp) / (L * L * ratio * (ratio - 0.5))   # kernel.py:136-156 with N = L
     kmap = np.zeros((d, 9))
     for a in range(d):
         scale = hi[a] - lo[a]
@@ -339,8 +332,10 @@ def _make_geom(stats: np.ndarray, n: int, d: int, G: np.ndarray, accuracy: int,
         shift = -0.5 - kmin
         hx = 2 * np.pi / L[a]
         kmap[a] = [mean[a], std[a], center[a], lo[a], scale, ks, r0, shift, hx]
+    msp, tau, _, _ = _spread_params(L, kmap, accuracy)
     return _Geom(n=n, d=d, G=G, L=L, qin=qin, qout=qout, msp=msp, tau=tau, kmap=kmap, lo=lo,
-                 hi=hi, mean=mean, std=std, center=center, xmin=xmin, xmax=xmax)
+                 hi=hi, mean=mean, std=std, center=center, xmin=xmin, xmax=xmax,
+                 accuracy=int(accuracy))
 
 
 def _design_powers(d: int, order: int) -> List[Tuple[int, ...]]:
@@ -425,28 +420,61 @@ def _filter_bandwidths(ctx, geom, bw, npow):
     return F, bw, keep, ihbad
 
 
+def _spread_params(L: np.ndarray, kmap: np.ndarray, accuracy: int):
+    """(msp, tau (d,), ratio, kmap) of the spreading at one accuracy
+    (kernel.py:97-156): ratio 1/2/3 for accuracy <= 6 / <= 11 / above, Msp =
+    accuracy taps, tau = pi Msp / (L^2 ratio (ratio - 1/2)); accuracy 0 is
+    nearest-bin binning (nufftn_type1.py:442-516): one tap of weight 1, given
+    to the kernel as Msp = 0 with an infinite tau.  The knot grid spacing is
+    2 pi / (ratio L)."""
+    ratio = 1 if accuracy <= 6 else (2 if accuracy <= 11 else 3)
+    msp = int(accuracy)
+    if accuracy == 0:
+        tau = np.full(len(L), np.inf)
+    else:
+        tau = (np.pi * msp) / (L * L * ratio * (ratio - 0.5))
+    kmap = kmap.copy()
+    kmap[:, 8] = 2 * np.pi / (ratio * np.asarray(L, dtype=float))
+    return msp, tau, ratio, kmap
+
+
 def _spread_fft(ctx: _Ctx, geom: _Geom, dx: torch.Tensor, cols: List[torch.Tensor], prec: int,
-                ev=None):
-    """Spread {1, cols...} and transform: returns the (C, L.., L_last/2+1) spectra."""
+                ev=None, accuracy: Optional[int] = None, ones: bool = True):
+    """Spread {1 (if ones), cols...} at `accuracy` and transform: returns the
+    (C, L.., L_last/2+1) spectra.  Oversampled accuracies spread on the
+    ratio*L grid and keep its central deconvolved L frequencies."""
     d, n = geom.d, geom.n
-    C = 1 + len(cols)
-    cells = int(np.prod(geom.L))
+    acc = geom.accuracy if accuracy is None else int(accuracy)
+    msp, tau, ratio, kmap = _spread_params(geom.L, geom.kmap, acc)
+    Lsp = (geom.L * ratio).astype(int)
+    C = (1 if ones else 0) + len(cols)
+    cells = int(np.prod(Lsp))
     real_dt = torch.float32 if prec == _lib.FLPR_PREC_F32 else torch.float64
     grid = ctx.empty((C, cells), dtype=real_dt)
-    ws = ctx.ws(ctx.lib.flpr_spread_ws(d, n, _lib.ivec(geom.L), geom.msp, C, prec))
-    ctx.check(ctx.lib.flpr_spread(d, n, dx.data_ptr(), _lib.dvec(geom.kmap.ravel()),
-                                  _lib.ivec(geom.L), geom.msp, _lib.dvec(geom.tau), C, 1,
+    ws = ctx.ws(ctx.lib.flpr_spread_ws(d, n, _lib.ivec(Lsp), msp, C, prec))
+    ctx.check(ctx.lib.flpr_spread(d, n, dx.data_ptr(), _lib.dvec(kmap.ravel()),
+                                  _lib.ivec(Lsp), msp, _lib.dvec(tau), C, 1 if ones else 0,
                                   _lib.pvec([c.data_ptr() for c in cols]), grid.data_ptr(), prec,
                                   ws.data_ptr(), ws.numel(), ctx.stream), "flpr_spread")
     del ws
     if ev is not None:
         ev.mark("spread")
-    half = cells // int(geom.L[-1]) * (int(geom.L[-1]) // 2 + 1)
+    half = cells // int(Lsp[-1]) * (int(Lsp[-1]) // 2 + 1)
     spec = ctx.empty((C, half, 2), dtype=real_dt)
-    ws = ctx.ws(ctx.lib.flpr_forward_fft_ws(ctx.handle, d, _lib.ivec(geom.L), C, prec))
-    ctx.check(ctx.lib.flpr_forward_fft(ctx.handle, d, _lib.ivec(geom.L), C, grid.data_ptr(),
+    ws = ctx.ws(ctx.lib.flpr_forward_fft_ws(ctx.handle, d, _lib.ivec(Lsp), C, prec))
+    ctx.check(ctx.lib.flpr_forward_fft(ctx.handle, d, _lib.ivec(Lsp), C, grid.data_ptr(),
                                        spec.data_ptr(), prec, ws.data_ptr(), ws.numel(),
                                        ctx.stream), "flpr_forward_fft")
+    if ratio > 1:
+        del grid, ws
+        Lc = int(np.prod(geom.L))
+        half_o = Lc // int(geom.L[-1]) * (int(geom.L[-1]) // 2 + 1)
+        out = ctx.empty((C, half_o, 2), dtype=real_dt)
+        ctx.check(ctx.lib.flpr_oversample_crop(d, _lib.ivec(geom.L), _lib.ivec(Lsp), C,
+                                               _lib.dvec(tau), ratio, spec.data_ptr(),
+                                               out.data_ptr(), prec, ctx.stream),
+                  "flpr_oversample_crop")
+        spec = out
     if ev is not None:
         ev.mark("fft")
     return spec
@@ -495,9 +523,10 @@ def _check_supported(dims: int, opts) -> None:
         raise NotImplementedError(
             f"fastlpr_b200 supports 1-3 predictor dimensions on the GPU; got dx={dims}")
     acc = int(opts["accuracy"])
-    if acc < 1 or acc > 6:
+    if acc < 0 or acc > 12 or (dims == 3 and acc > 6):
         raise NotImplementedError(
-            f"accuracy={acc} is not supported on the GPU (supported: 1-6, no oversampling)")
+            f"accuracy={acc} is not supported on the GPU (supported: 0-12 in 1-D/2-D, "
+            "0-6 in 3-D)")
     kt = str(opts.get("kernel_type", "gaussian")).lower()
     if kt not in ("gaussian", "gauss", "normal"):
         raise NotImplementedError(f"kernel_type={kt!r}: only the Gaussian kernel is supported")
@@ -737,7 +766,18 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
     ev.mark("setup")
     if hook is not None:
         hook(dx, ycols, stats, n, d)
-    spec = _spread_fft(ctx, geom, dx, ycols + pcols, prec, ev)
+    # The user's accuracy applies to the response channels only (their
+    # transform in nufft_regression_with_precomputed_kdf, api.py:640); the
+    # design planes (compute_design_matrix, api.py:571) and the probes
+    # (estimate_dof_nufft_vectorized, regression.py:756) use the default.
+    acc_default = max(6 - int(np.ceil(np.log10(n))), 4)
+    if geom.accuracy == acc_default:
+        spec = _spread_fft(ctx, geom, dx, ycols + pcols, prec, ev)
+    else:
+        spec_s = _spread_fft(ctx, geom, dx, pcols, prec, ev, accuracy=acc_default, ones=True)
+        spec_y = _spread_fft(ctx, geom, dx, ycols, prec, ev, accuracy=geom.accuracy, ones=False)
+        spec = torch.cat([spec_s[:1], spec_y, spec_s[1:]], dim=0)
+        del spec_s, spec_y
     axes_raw = _raw_axes(geom, opts)
     st.__dict__.update(dict(
         n=n, d=d, dx=dx, ycols=ycols, pcols=pcols, R=R, ny=ny, y_raw_dev=y_raw_dev,

@@ -1,5 +1,7 @@
 // Forward FFT of the spread grids, separable kernel-moment spectra and the
 // batched spectral multiply + inverse FFT + crop.
+#include <cfloat>
+
 #include "common.cuh"
 #include "plans.cuh"
 
@@ -181,6 +183,92 @@ static int grid_blocks(int64_t total) {
 
 using namespace flpr;
 
+// Oversampled spreading (accuracy >= 7; nufftn_type1.py:693-770 followed by
+// the ifftshift of convolution.py:235-236): from the R2C spectrum of the
+// ratio*L grid keep the L frequencies f in [-floor(L/2), L - floor(L/2) - 1]
+// per axis, divide by ratio^d and by
+// Kn = sqrt(prod tau / pi^d) exp(-sum_a tau_a f_a^2), and store them in the
+// R2C layout of an L grid (index k <-> f = k for k < (L+1)/2, else k - L).
+// The last axis keeps k in [0, L/2]; a negative f there (the Nyquist entry of
+// an even L) comes from the Hermitian mirror of the input.
+struct OverArgs {
+  int d, C;
+  int Lo[3], Li[3];
+  int64_t half_o, half_i;   // entries per channel
+  double tau[3];
+  double kn0, inv_rd;
+};
+
+// Big-grid spectrum value at frequency g (|g_a| <= Li_a / 2) from its half
+// spectrum: negative last-axis frequencies are read at -g, conjugated.
+template <typename T2>
+__device__ __forceinline__ double2 big_at(const OverArgs& a, const T2* __restrict__ in_c, const int* g) {
+  const int d = a.d;
+  const bool mirror = g[d - 1] < 0;
+  int64_t ii = 0;
+  for (int ax = 0; ax < d - 1; ++ax) {
+    int fi = mirror ? -g[ax] : g[ax];
+    fi %= a.Li[ax];
+    if (fi < 0) fi += a.Li[ax];
+    ii = ii * a.Li[ax] + fi;
+  }
+  ii = ii * (a.Li[d - 1] / 2 + 1) + (mirror ? -g[d - 1] : g[d - 1]);
+  const T2 v = in_c[ii];
+  return make_double2((double)v.x, mirror ? -(double)v.y : (double)v.y);
+}
+
+// Output bin f of the L grid (standard order).  The reference keeps the
+// cropped full spectrum X and takes the real part after its inverse
+// transform, which equals transforming the Hermitian part
+// (X[f] + conj(X[-f])) / 2.  That differs from X only where some f_a is the
+// even-size Nyquist frequency -L_a/2, whose partner -f_a aliases to the same
+// bin; there the Hermitian part is the mean of the big-grid values at -L_a/2
+// and +L_a/2, which is what is stored so that the half spectrum is exact.
+template <typename T2>
+__global__ void oversample_crop_kernel(OverArgs a, const T2* __restrict__ in, T2* __restrict__ out) {
+  const int64_t total = (int64_t)a.C * a.half_o;
+  const int d = a.d;
+  const int Lol = a.Lo[d - 1];
+  const int ho = Lol / 2 + 1;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = t / a.half_o;
+    int64_t r = t - c * a.half_o;
+    int f[3], fp[3];
+    bool nyq = false;
+    // last axis (half spectrum), then the others, row-major
+    const int kl = (int)(r % ho);
+    r /= ho;
+    f[d - 1] = kl < (Lol + 1) / 2 ? kl : kl - Lol;
+    for (int ax = d - 2; ax >= 0; --ax) {
+      const int k = (int)(r % a.Lo[ax]);
+      r /= a.Lo[ax];
+      f[ax] = k < (a.Lo[ax] + 1) / 2 ? k : k - a.Lo[ax];
+    }
+    double ex = 0.0;
+    for (int ax = 0; ax < d; ++ax) {
+      ex += a.tau[ax] * (double)f[ax] * (double)f[ax];
+      const bool nq = (a.Lo[ax] % 2 == 0) && f[ax] == -a.Lo[ax] / 2;
+      fp[ax] = nq ? -f[ax] : f[ax];
+      nyq |= nq;
+    }
+    double kn = a.kn0 * exp(-ex);
+    kn = kn > DBL_MIN ? kn : DBL_MIN;
+    const double scale = a.inv_rd / kn;
+    const T2* in_c = in + c * a.half_i;
+    double2 v = big_at(a, in_c, f);
+    if (nyq) {
+      const double2 w = big_at(a, in_c, fp);
+      v.x = 0.5 * (v.x + w.x);
+      v.y = 0.5 * (v.y + w.y);
+    }
+    T2 o;
+    o.x = (decltype(o.x))(v.x * scale);
+    o.y = (decltype(o.y))(v.y * scale);
+    out[t] = o;
+  }
+}
+
 extern "C" {
 
 size_t flpr_forward_fft_ws(flpr_handle_t handle, int d, const int* h_L, int nchan, int prec) {
@@ -339,6 +427,45 @@ int flpr_conv(flpr_handle_t handle, int d, const int* h_G, const int* h_L, const
     }
     FLPR_LAUNCH_CHECK();
   }
+  return FLPR_OK;
+}
+
+
+int flpr_oversample_crop(int d, const int* h_Lout, const int* h_Lin, int nchan,
+                         const double* h_tau, int ratio, const void* d_in, void* d_out, int prec,
+                         void* stream) {
+  FLPR_CHECK_ARG(d >= 1 && d <= 3, "oversample_crop: d=%d", d);
+  FLPR_CHECK_ARG(nchan >= 1 && ratio >= 1, "oversample_crop: nchan=%d ratio=%d", nchan, ratio);
+  FLPR_CHECK_ARG(prec == FLPR_PREC_F32 || prec == FLPR_PREC_F64, "oversample_crop: precision");
+  OverArgs a;
+  memset(&a, 0, sizeof(a));
+  a.d = d;
+  a.C = nchan;
+  double tprod = 1.0;
+  a.half_o = 1;
+  a.half_i = 1;
+  for (int ax = 0; ax < d; ++ax) {
+    FLPR_CHECK_ARG(h_Lout[ax] >= 1 && h_Lin[ax] >= h_Lout[ax], "oversample_crop: sizes");
+    a.Lo[ax] = h_Lout[ax];
+    a.Li[ax] = h_Lin[ax];
+    a.tau[ax] = h_tau[ax];
+    tprod *= h_tau[ax];
+    a.half_o *= ax == d - 1 ? h_Lout[ax] / 2 + 1 : h_Lout[ax];
+    a.half_i *= ax == d - 1 ? h_Lin[ax] / 2 + 1 : h_Lin[ax];
+  }
+  a.kn0 = sqrt(tprod / pow(M_PI, (double)d));
+  a.inv_rd = 1.0 / pow((double)ratio, (double)d);
+  const int64_t total = (int64_t)nchan * a.half_o;
+  int nb = (int)((total + 255) / 256);
+  if (nb > 16 * sm_count()) nb = 16 * sm_count();
+  cudaStream_t s = as_stream(stream);
+  if (prec == FLPR_PREC_F32)
+    oversample_crop_kernel<float2><<<nb, 256, 0, s>>>(a, static_cast<const float2*>(d_in),
+                                                      static_cast<float2*>(d_out));
+  else
+    oversample_crop_kernel<double2><<<nb, 256, 0, s>>>(a, static_cast<const double2*>(d_in),
+                                                       static_cast<double2*>(d_out));
+  FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
 

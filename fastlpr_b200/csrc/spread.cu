@@ -24,7 +24,7 @@ namespace flpr {
 
 constexpr int kItemPoints = 4096;
 constexpr int kSpreadThreads = 256;
-constexpr int kMaxTaps1 = 13;  // 2*msp+1 for msp <= 6
+constexpr int kMaxTaps1 = 25;  // 2*msp+1 for msp <= 12 (msp = 0: binning with weight 1)
 
 struct SpreadGeom {
   int d;
@@ -538,12 +538,14 @@ __global__ void finalize_kernel(int nchan, int64_t cells, const Acc* __restrict_
 }
 
 // 2-D grids of at least 8 x 8 cells take the per-cell register path.
-static bool use_2d_path(int d, const int* L) { return d == 2 && L[0] >= kT2 && L[1] >= kT2; }
+static bool use_2d_path(int d, const int* L, int msp) {
+  return d == 2 && L[0] >= kT2 && L[1] >= kT2 && 2 * msp + 1 <= 13;
+}
 
 static void make_geom(SpreadGeom& g, int d, const int* L, int msp, const double* tau,
                       const double* kmap) {
   memset(&g, 0, sizeof(g));
-  const bool path2 = use_2d_path(d, L);
+  const bool path2 = use_2d_path(d, L, msp);
   g.d = d;
   g.msp = msp;
   g.ntaps1 = 2 * msp + 1;
@@ -725,7 +727,7 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
                 size_t ws_bytes, void* stream) {
   FLPR_CHECK_ARG(d >= 1 && d <= 3, "spread: d=%d not in [1,3]", d);
   FLPR_CHECK_ARG(n >= 1 && n < (int64_t)1 << 31, "spread: n=%lld out of range", (long long)n);
-  FLPR_CHECK_ARG(msp >= 0 && 2 * msp + 1 <= kMaxTaps1, "spread: msp=%d not in [0,6]", msp);
+  FLPR_CHECK_ARG(msp >= 0 && 2 * msp + 1 <= kMaxTaps1, "spread: msp=%d not in [0,12]", msp);
   FLPR_CHECK_ARG(nchan >= 1 && nchan <= FLPR_MAX_CHANNELS, "spread: nchan=%d", nchan);
   FLPR_CHECK_ARG(ones_channel == 0 || ones_channel == 1, "spread: ones_channel must be 0/1");
   FLPR_CHECK_ARG(prec == FLPR_PREC_F32 || prec == FLPR_PREC_F64, "spread: bad precision");
@@ -766,19 +768,20 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
   FLPR_LAUNCH_CHECK();
 
   int64_t max_items = (int64_t)g.ntiles + (n + kItemPoints - 1) / kItemPoints;
-  if (use_2d_path(d, h_L)) {
+  if (use_2d_path(d, h_L, msp)) {
     const int cg2 = channel_group_2d(g, nchan);
     FLPR_CHECK_ARG(cg2 >= 1, "spread: tile does not fit shared memory");
     dim3 grid2((unsigned)max_items, (unsigned)((nchan + cg2 - 1) / cg2));
     int st = FLPR_OK;
     switch (g.ntaps1) {
+      case 1: st = launch_accumulate_2d<1>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
       case 3: st = launch_accumulate_2d<3>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
       case 5: st = launch_accumulate_2d<5>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
       case 7: st = launch_accumulate_2d<7>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
       case 9: st = launch_accumulate_2d<9>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
       case 11: st = launch_accumulate_2d<11>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
       case 13: st = launch_accumulate_2d<13>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
-      default: set_error("spread: msp=%d not supported (1..6)", g.msp); return FLPR_ERR_ARG;
+      default: set_error("spread: msp=%d not supported (0..12)", g.msp); return FLPR_ERR_ARG;
     }
     if (st != FLPR_OK) return st;
     return finalize(g, n, nchan, fixed, margin, w, d_grid_out, s);
@@ -791,13 +794,20 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
   dim3 grid((unsigned)max_items, (unsigned)ngroups);
   int status = FLPR_OK;
   switch (g.ntaps1) {
+    case 1: status = launch_accumulate<1>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
     case 3: status = launch_accumulate<3>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
     case 5: status = launch_accumulate<5>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
     case 7: status = launch_accumulate<7>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
     case 9: status = launch_accumulate<9>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
     case 11: status = launch_accumulate<11>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
     case 13: status = launch_accumulate<13>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
-    default: set_error("spread: msp=%d not supported (1..6)", g.msp); return FLPR_ERR_ARG;
+    case 15: status = launch_accumulate<15>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
+    case 17: status = launch_accumulate<17>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
+    case 19: status = launch_accumulate<19>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
+    case 21: status = launch_accumulate<21>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
+    case 23: status = launch_accumulate<23>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
+    case 25: status = launch_accumulate<25>(g, n, nchan, ones_channel, cg, w, fixed, margin, smem, grid, s); break;
+    default: set_error("spread: msp=%d not supported (0..12)", g.msp); return FLPR_ERR_ARG;
   }
   if (status != FLPR_OK) return status;
   return finalize(g, n, nchan, fixed, margin, w, d_grid_out, s);

@@ -115,6 +115,16 @@ int flpr_forward_fft(flpr_handle_t handle, int d, const int* h_L, int nchan,
                      void* d_grid, void* d_spec, int prec,
                      void* d_ws, size_t ws_bytes, void* stream);
 
+/* (3b) Oversampled spreading (accuracy >= 7): nufftn_type1.py:693-770 and
+ * the ifftshift of convolution.py:235-236.  d_in: (nchan, Lin.., Lin_last/2+1)
+ * R2C spectra of the ratio*L grids from flpr_forward_fft; d_out receives
+ * (nchan, Lout.., Lout_last/2+1): the central Lout frequencies of each axis,
+ * divided by ratio^d and by the Gaussian spreading transform
+ * sqrt(prod tau / pi^d) exp(-sum tau_a f_a^2), in standard frequency order. */
+int flpr_oversample_crop(int d, const int* h_Lout, const int* h_Lin, int nchan,
+                         const double* h_tau, int ratio, const void* d_in, void* d_out,
+                         int prec, void* stream);
+
 /* ---------------------------------------------------------------------
  * (4) Per-axis kernel-moment spectra.  The Gaussian kernel of
  * kernel.py:330-357 is separable, so the spectrum of K(u)*u^a on the padded

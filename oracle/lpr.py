@@ -85,7 +85,9 @@ def grid_params(G: Sequence[int], flag_power2: bool = True):
 
 
 def spread_params(L: Sequence[int], accuracy: int):
-    """compute_grid_params for the knot grid (kernel.py:136-156): Msp, tau, ratio."""
+    """compute_grid_params for the knot grid (kernel.py:136-156): Msp, tau, ratio.
+    accuracy 0 is nearest-bin binning (nufftn_type1.py:442-516): one tap of
+    weight 1, i.e. Msp = 0 with an infinite tau."""
     L = np.atleast_1d(np.asarray(L, dtype=int))
     if accuracy <= 6:
         ratio = 1
@@ -95,6 +97,8 @@ def spread_params(L: Sequence[int], accuracy: int):
         ratio = 3
     msp = accuracy
     tau = (np.pi * msp) / (L * L * ratio * (ratio - 0.5))
+    if accuracy == 0:
+        tau = np.full(np.shape(L), np.inf)
     return msp, tau, ratio
 
 
@@ -182,6 +186,46 @@ def spread_grid(xmod: np.ndarray, chans: np.ndarray, L, msp: int, tau) -> np.nda
         for c in range(C):
             out[c] += np.bincount(idx, weights=chans[:, c] * w, minlength=total)
     return out.reshape((C,) + tuple(L))
+
+
+def nufft_spectra_oversampled(grid: np.ndarray, n_points: int, L, ratio: int, tau,
+                              workers: int = 1) -> np.ndarray:
+    """Oversampled path (accuracy >= 7), nufftn_type1.py:693-770 then the
+    ifftshift of convolution.py:235-236: FFT of the ratio*L grid, fftshift,
+    the central L frequencies, / (M ratio^d), times 1/Kn with
+    Kn = sqrt(prod tau / pi^d) exp(-sum tau_d f_d^2) over the centred
+    frequencies f of nufftfreqs(L), back to standard order."""
+    dims = grid.ndim - 1
+    L = np.atleast_1d(L).astype(int)
+    tau = np.atleast_1d(tau).astype(float)
+    spec = grid.astype(np.complex128)
+    for ax in range(dims, 0, -1):
+        spec = sfft.fft(spec, axis=ax, workers=workers)
+    spec = np.fft.fftshift(spec, axes=tuple(range(1, dims + 1)))
+    Mr = np.array(spec.shape[1:])
+    start = np.ceil((Mr - L) / 2).astype(int)
+    spec = spec[(slice(None),) + tuple(slice(start[a], start[a] + L[a]) for a in range(dims))]
+    spec = spec / (n_points * ratio ** dims)
+    freqs = [np.arange(int(np.fix(-La / 2)), La - int(np.fix(La / 2))) for La in L]
+    ex = np.zeros(tuple(L))
+    for a in range(dims):
+        shape = [1] * dims
+        shape[a] = L[a]
+        ex = ex + tau[a] * (freqs[a].astype(float) ** 2).reshape(shape)
+    kn = np.sqrt(np.prod(tau) / np.pi ** dims) * np.exp(-ex)
+    kn = np.maximum(kn, np.finfo(float).tiny)
+    spec = spec * (1.0 / kn)[None]
+    return np.fft.ifftshift(spec, axes=tuple(range(1, dims + 1)))
+
+
+def channel_spectra(xmod: np.ndarray, chans: np.ndarray, L, accuracy: int, n_points: int,
+                    workers: int = 1) -> np.ndarray:
+    """(C, *L) spectra of the channels at one accuracy (spreading + FFT)."""
+    msp, tau, ratio = spread_params(L, accuracy)
+    grid = spread_grid(xmod, chans, np.asarray(L) * ratio, msp, tau)
+    if ratio > 1:
+        return nufft_spectra_oversampled(grid, n_points, L, ratio, tau, workers)
+    return nufft_spectra(grid, n_points, workers)
 
 
 def nufft_spectra(grid: np.ndarray, n_points: int, workers: int = 1) -> np.ndarray:
@@ -564,7 +608,6 @@ def cv_fastlpr(x, y, h=None, options: Optional[Dict] = None, workers: int = 1,
     bw = prm["h"]
     H = bw.shape[0]
     L, qin, qout = prm["L"], prm["qin"], prm["qout"]
-    msp, tau, _ = spread_params(L, acc)
     xmod = knot_coordinates(xs, L, G, qin)
 
     y_complex = np.iscomplexobj(y)
@@ -588,11 +631,25 @@ def cv_fastlpr(x, y, h=None, options: Optional[Dict] = None, workers: int = 1,
     else:
         p = np.zeros((n, 0))
         R = 0
-    chans = np.column_stack([np.ones(n), ycols, p])
     _mark("prep")
-    grid = spread_grid(xmod, chans, L, msp, tau)
+    # The user's accuracy applies to the response channels only (their
+    # transform in nufft_regression_with_precomputed_kdf, api.py:640); the
+    # design planes (compute_design_matrix, api.py:571) and the probes
+    # (estimate_dof_nufft_vectorized, regression.py:756) use the default one.
+    acc_default = max(6 - int(np.ceil(np.log10(n))), 4)
+    grid = None
+    if acc == acc_default:
+        msp, tau, ratio = spread_params(L, acc)
+        grid = spread_grid(xmod, np.column_stack([np.ones(n), ycols, p]),
+                           np.asarray(L) * ratio, msp, tau)
+        spec = (nufft_spectra_oversampled(grid, n, L, ratio, tau, workers) if ratio > 1
+                else nufft_spectra(grid, n, workers))
+    else:
+        s_ones_p = channel_spectra(xmod, np.column_stack([np.ones(n), p]), L, acc_default, n,
+                                   workers)
+        s_y = channel_spectra(xmod, ycols, L, acc, n, workers)
+        spec = np.concatenate([s_ones_p[:1], s_y, s_ones_p[1:]], axis=0)
     _mark("spread")
-    spec = nufft_spectra(grid, n, workers)
     spec = np.moveaxis(spec, 0, -1)  # (*L, C)
     _mark("fft")
 
@@ -600,7 +657,7 @@ def cv_fastlpr(x, y, h=None, options: Optional[Dict] = None, workers: int = 1,
     ns = len(kdf)
     Gt = tuple(G)
     S = [np.empty(Gt + (H,)) for _ in range(ns)]
-    Tall = [np.empty(Gt + (H, chans.shape[1] - 1)) for _ in range(nt)]
+    Tall = [np.empty(Gt + (H, spec.shape[-1] - 1)) for _ in range(nt)]
     for h0 in range(0, H, h_chunk):
         sl = slice(h0, min(H, h0 + h_chunk))
         for k in range(ns):
@@ -738,10 +795,13 @@ def cv_fastkde(x, h=None, options: Optional[Dict] = None, workers: int = 1,
     bw = prm["h"]
     H = bw.shape[0]
     L, qin, qout = prm["L"], prm["qin"], prm["qout"]
-    msp, tau, _ = spread_params(L, acc)
+    msp, tau, ratio = spread_params(L, acc)
     xmod = knot_coordinates(xs, L, G, qin)
-    grid = spread_grid(xmod, np.ones((n, 1)), L, msp, tau)
-    spec = np.moveaxis(nufft_spectra(grid, n, workers), 0, -1)
+    grid = spread_grid(xmod, np.ones((n, 1)), np.asarray(L) * ratio, msp, tau)
+    if ratio > 1:
+        spec = np.moveaxis(nufft_spectra_oversampled(grid, n, L, ratio, tau, workers), 0, -1)
+    else:
+        spec = np.moveaxis(nufft_spectra(grid, n, workers), 0, -1)
     s = np.empty(tuple(G) + (H,))
     for h0 in range(0, H, h_chunk):
         sl = slice(h0, min(H, h0 + h_chunk))

@@ -234,6 +234,7 @@ def main():
 
     _intermediates_case(fastlpr, "inter2d_o1")
     interval_case(fastlpr)
+    accuracy_cases(fastlpr)
 
 
 def interval_case(fastlpr):
@@ -264,8 +265,33 @@ def interval_case(fastlpr):
     print(f"interval1d: N={n} h_mu={np.asarray(mu.h).ravel()} h_var={np.asarray(var.h).ravel()}")
 
 
+def accuracy_cases(fastlpr):
+    """Non-default accuracies: 0 (nearest-bin binning, nufftn_type1.py:442-516)
+    and >= 7 (oversampling ratio 2 / 3 with Gaussian deconvolution,
+    nufftn_type1.py:693-770)."""
+    from fastlpr import get_hlist
+
+    rng = np.random.default_rng(99)
+    n = 3000
+    x1 = rng.random((n, 1))
+    y1 = np.sin(2 * np.pi * x1[:, 0]) + 0.1 * rng.standard_normal(n)
+    h1 = get_hlist(6, [0.03, 0.6])
+    _lpr_case(fastlpr, "lpr1d_o1_acc0", x1, y1, h1, {"order": 1, "N": 256, "accuracy": 0})
+    _lpr_case(fastlpr, "lpr1d_o1_acc12", x1, y1, h1, {"order": 1, "N": 128, "accuracy": 12})
+    n2 = 6000  # 2-D with n >= 5000: the reference interpolates GCV/DoF linearly
+    x2 = rng.random((n2, 2))
+    y2 = np.sin(2 * np.pi * x2[:, 0]) * np.cos(2 * np.pi * x2[:, 1]) + 0.1 * rng.standard_normal(n2)
+    hv = np.logspace(np.log10(0.05), np.log10(0.5), 4)
+    h2 = np.column_stack([hv, hv])
+    _lpr_case(fastlpr, "lpr2d_o1_acc7", x2, y2, h2, {"order": 1, "N": [32, 32], "accuracy": 7})
+    xk = rng.standard_normal((3000, 2))
+    _kde_case(fastlpr, "kde2d_acc7", xk, h2, {"N": [32, 32], "accuracy": 7})
+
+
 if __name__ == "__main__":
     if "--only-interval" in sys.argv:
         interval_case(_import_reference())
+    elif "--only-accuracy" in sys.argv:
+        accuracy_cases(_import_reference())
     else:
         main()

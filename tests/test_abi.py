@@ -41,9 +41,10 @@ def test_argument_errors_need_no_gpu():
     st = lib.flpr_solve(3, 2, 1, 1, 10, 1, None, None, 0.0, None, None, 0, None)
     assert st == -1
     assert b"order" in lib.flpr_last_error()
-    st = lib.flpr_spread(1, 10, None, _lib.dvec([0] * 9), L, 9, _lib.dvec([1.0]), 1, 1,
+    st = lib.flpr_spread(1, 10, None, _lib.dvec([0] * 9), L, 13, _lib.dvec([1.0]), 1, 1,
                          _lib.pvec([]), None, 0, None, 0, None)
     assert st == -1
+    assert b"[0,12]" in lib.flpr_last_error()
 
 
 def test_workspace_queries_are_consistent():

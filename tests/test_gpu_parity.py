@@ -292,3 +292,37 @@ def test_validation_rejects_nonfinite(cuda_ok, bad):
         fl.cv_fastlpr(x, yb, [[0.2]], {"order": 1})
     with pytest.raises(ValueError, match=f"Input x contains {word}"):
         fl.cv_fastkde(xb, [[0.2]])
+
+
+@pytest.mark.parametrize("L,ratio", [([64], 2), ([48], 3), ([16, 12], 2), ([9, 8, 6], 3)])
+def test_oversample_crop_matches_oracle(cuda_ok, L, ratio):
+    """flpr_oversample_crop on the FFT of a random ratio*L grid against the
+    oracle's crop + deconvolution; the oracle's full spectrum X enters the
+    reference through real(ifft(K X)), so the device half spectrum must hold
+    the Hermitian part (X[f] + conj(X[-f])) / 2."""
+    import torch
+    from fastlpr_b200 import _lib
+    rng = np.random.default_rng(sum(L) + ratio)
+    L = np.array(L)
+    Li = L * ratio
+    d = len(L)
+    C, n = 2, 1000
+    tau = np.pi * 7 / (L * L * ratio * (ratio - 0.5))
+    big = rng.standard_normal((C,) + tuple(Li))
+    X = oracle.lpr.nufft_spectra_oversampled(big, n, L, ratio, tau)
+    conjneg = np.conj(X)
+    for ax in range(1, d + 1):
+        conjneg = np.roll(np.flip(conjneg, axis=ax), 1, axis=ax)
+    herm = 0.5 * (X + conjneg)
+    want = herm[..., :L[-1] // 2 + 1]
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    spec_in = torch.from_numpy(np.fft.rfftn(big, axes=tuple(range(1, d + 1))) / n).to(dev)
+    spec_in = torch.view_as_real(spec_in.contiguous()).contiguous()
+    out = torch.empty((C,) + want.shape[1:] + (2,), dtype=torch.float64, device=dev)
+    _lib.check(lib.flpr_oversample_crop(d, _lib.ivec(L), _lib.ivec(Li), C, _lib.dvec(tau), ratio,
+                                        spec_in.data_ptr(), out.data_ptr(), _lib.FLPR_PREC_F64,
+                                        None), "oversample_crop")
+    torch.cuda.synchronize()
+    got = torch.view_as_complex(out).cpu().numpy()
+    assert rel_err(got, want) < 1e-13

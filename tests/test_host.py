@@ -66,7 +66,10 @@ def test_unsupported_paths_raise_not_implemented():
         api.cv_fastlpr(x, rng.random(50), [[0.3] * 4], {"calc_dof": False})
     x1 = rng.random((50, 1))
     with pytest.raises(NotImplementedError):
-        api.cv_fastlpr(x1, rng.random(50), [[0.3]], {"accuracy": 8})
+        api.cv_fastlpr(x1, rng.random(50), [[0.3]], {"accuracy": 13})
+    x3 = rng.random((50, 3))
+    with pytest.raises(NotImplementedError):
+        api.cv_fastlpr(x3, rng.random(50), [[0.3] * 3], {"accuracy": 7})
     with pytest.raises(NotImplementedError):
         api.cv_fastlpr(x1, rng.random(50), [[0.3]], {"kernel_type": "epanechnikov"})
 
