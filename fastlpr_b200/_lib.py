@@ -54,6 +54,10 @@ SIGNATURES = [
     ("flpr_interp_reduce", _I, [_I, _I64, _VP, _PD, _PI, _I, _I, _I, _VP, _PVP, _PVP, _VP, _VP,
                                 _VP, _VP, _SZ, _VP]),
     ("flpr_interp_eval", _I, [_I, _I64, _VP, _PD, _PI, _I, _VP, _VP, _VP]),
+    ("flpr_spline_prefilter", _I, [_I, _PI, _I64, _I, _VP, _VP, _VP]),
+    ("flpr_spline_reduce", _I, [_I, _I64, _VP, _VP, _PI, _I, _I, _I, _VP, _PVP, _PVP, _VP, _VP,
+                                _VP, _VP]),
+    ("flpr_spline_eval", _I, [_I, _I64, _VP, _VP, _PI, _I, _VP, _VP, _VP]),
     ("flpr_kde_ws", _SZ, [_I64, _I, _I64]),
     ("flpr_kde_lcv", _I, [_I, _I64, _VP, _PD, _PI, _I, _VP, _D, _PD, _VP, _VP, _VP, _SZ, _VP]),
     ("flpr_log_shift", _I, [_I64, _VP, _D, _VP, _VP]),

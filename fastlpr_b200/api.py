@@ -21,7 +21,7 @@ from typing import Dict, List, Optional, Sequence, Tuple
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, spline
 from .bandwidth import get_hlist
 from .interpolant import GridInterpolant
 from .structures import KDEOutput, RegressionOutput
@@ -532,18 +532,19 @@ def _check_supported(dims: int, opts) -> None:
         raise NotImplementedError(f"kernel_type={kt!r}: only the Gaussian kernel is supported")
 
 
-def _check_interp_methods(opts, dims: int, n: int) -> None:
-    """The GPU path interpolates linearly.  The reference defaults to cubic
-    GCV/DoF interpolation for 2-D+ data with n < 5000 (api.py:594-600,
-    api.py:651-657); that case warns, an explicit 'cubic' raises."""
-    for key in ("gcv_interp_method", "dof_interp_method", "interp_method"):
-        m = opts.get(key, None)
-        if m is not None and str(m) != "linear":
-            raise NotImplementedError(f"{key}={m!r}: only linear interpolation is implemented")
-    if dims >= 2 and n < 5000 and bool(opts.get("calc_dof", True)) and \
-            opts.get("gcv_interp_method") is None:
-        warnings.warn("n < 5000 in 2-D+: the reference interpolates GCV/DoF cubically here; "
-                      "fastlpr_b200 uses linear interpolation", UserWarning, stacklevel=3)
+def _check_interp_methods(opts, dims: int, n: int) -> Dict[str, str]:
+    """Interpolation methods of the fit: GCV and DoF default to linear in 1-D
+    or with n >= 5000 and to the not-a-knot cubic spline otherwise
+    (api.py:594-600, api.py:651-657); the final interpolant defaults to
+    linear (api.py:488).  Only 'linear' and 'cubic' are implemented."""
+    default = "linear" if (dims == 1 or n >= 5000) else "cubic"
+    out = {"gcv": spline.check_method("gcv_interp_method", opts.get("gcv_interp_method", default)),
+           "dof": spline.check_method("dof_interp_method", opts.get("dof_interp_method", default)),
+           "output": spline.check_method("interp_method", opts.get("interp_method", "linear"))}
+    G = _grid_shape(opts, n, dims)
+    if "cubic" in out.values() and np.any(G < 4):
+        raise ValueError(f"cubic interpolation needs at least 4 grid points per axis, got N={G}")
+    return out
 
 
 def _grid_shape(opts, n, dims) -> np.ndarray:
@@ -779,12 +780,17 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
         spec = torch.cat([spec_s[:1], spec_y, spec_s[1:]], dim=0)
         del spec_s, spec_y
     axes_raw = _raw_axes(geom, opts)
+    methods = _check_interp_methods(opts, d, n)
     st.__dict__.update(dict(
         n=n, d=d, dx=dx, ycols=ycols, pcols=pcols, R=R, ny=ny, y_raw_dev=y_raw_dev,
         stats=stats, geom=geom, spec=spec, calc_dof=calc_dof, order=order, prec=prec,
         dy=dy, variance=variance, y_is_complex=y_is_complex, opts=opts,
         axes_raw=axes_raw, ax_arg=_lib.dvec(_axes_arg(axes_raw)), G_arg=_lib.ivec(geom.G),
-        dual=calc_dof and ny <= 4 and not opts.get("_direct_reduce", False), Q=None))
+        methods=methods, spl=None,
+        dual=(calc_dof and ny <= 4 and not opts.get("_direct_reduce", False)
+              and methods["gcv"] == "linear" and methods["dof"] == "linear"), Q=None))
+    if "cubic" in methods.values():
+        st.spl = spline.tables(axes_raw, ctx.device)
     if st.dual:
         # dual form: grid-domain dot products with the adjoint deposits
         M = geom.M
@@ -819,8 +825,8 @@ def _evaluate_lpr(ctx, st: _LprState, bandwidths: np.ndarray, ev) -> dict:
     Cv = ny + R
     M = geom.M
     Lq = (_lib.ivec(geom.G), _lib.ivec(geom.L), _lib.ivec(geom.qout[0]))
-    use_fused = (prec == _lib.FLPR_PREC_F32 and d == 2 and calc_dof and ny <= 4
-                 and not opts.get("_no_fused", False) and not opts.get("_direct_reduce", False)
+    use_fused = (prec == _lib.FLPR_PREC_F32 and d == 2 and st.dual
+                 and not opts.get("_no_fused", False)
                  and lib.flpr_lpr2d_fused_supported(*Lq, H, order, Cv) == 1)
     if not use_fused:
         S = _conv(ctx, geom, spec, F, Hf, npow,
@@ -875,19 +881,36 @@ def _evaluate_lpr(ctx, st: _LprState, bandwidths: np.ndarray, ev) -> dict:
         ev.mark("solve")
         mstride = Cv
         if calc_dof:
-            rss = ctx.empty((H, ny))
-            pdot = ctx.empty((max(R, 1), H))
-            pp = ctx.empty(max(R, 1))
-            ctx.check(lib.flpr_interp_reduce(d, n, st.dx.data_ptr(), st.ax_arg, st.G_arg, H, ny,
-                                             R, m.data_ptr(),
-                                             _lib.pvec([c.data_ptr() for c in ycols]),
-                                             _lib.pvec([c.data_ptr() for c in pcols]),
-                                             rss.data_ptr(), pdot.data_ptr(), pp.data_ptr(),
-                                             None, 0, ctx.stream), "flpr_interp_reduce")
+            yptr = _lib.pvec([c.data_ptr() for c in ycols])
+            pptr = _lib.pvec([c.data_ptr() for c in pcols])
+            red = {}
+            for method in sorted(set((st.methods["gcv"], st.methods["dof"]))):
+                rss = ctx.empty((H, ny))
+                pdot = ctx.empty((max(R, 1), H))
+                pp = ctx.empty(max(R, 1))
+                if method == "linear":
+                    ctx.check(lib.flpr_interp_reduce(d, n, st.dx.data_ptr(), st.ax_arg, st.G_arg,
+                                                     H, ny, R, m.data_ptr(), yptr, pptr,
+                                                     rss.data_ptr(), pdot.data_ptr(),
+                                                     pp.data_ptr(), None, 0, ctx.stream),
+                              "flpr_interp_reduce")
+                else:
+                    # spline coefficients of every fitted grid (H, M, Cv), then
+                    # the same reductions through the cubic spline
+                    coef = m.clone()
+                    ctx.check(lib.flpr_spline_prefilter(d, st.G_arg, Ht, Cv, st.spl.lu.data_ptr(),
+                                                        coef.data_ptr(), ctx.stream),
+                              "flpr_spline_prefilter")
+                    ctx.check(lib.flpr_spline_reduce(d, n, st.dx.data_ptr(),
+                                                     st.spl.axes.data_ptr(), st.G_arg, H, ny, R,
+                                                     coef.data_ptr(), yptr, pptr, rss.data_ptr(),
+                                                     pdot.data_ptr(), pp.data_ptr(), ctx.stream),
+                              "flpr_spline_reduce")
+                red[method] = (rss, pdot, pp)
             ev.mark("interp_reduce")
-            rss_h = rss.cpu().numpy()
-            pdot_h = pdot.cpu().numpy()[:R]
-            pp_h = pp.cpu().numpy()[:R]
+            rss_h = red[st.methods["gcv"]][0].cpu().numpy()
+            pdot_h = red[st.methods["dof"]][1].cpu().numpy()[:R]
+            pp_h = red[st.methods["dof"]][2].cpu().numpy()[:R]
     if calc_dof:
         gcv = _gcv_from_sums(n, rss_h, pdot_h, pp_h, st.dy, st.y_is_complex, opts)
         dstd = float(opts.get("dstd", 0.0))
@@ -908,9 +931,17 @@ def _finalize_lpr(ctx, st: _LprState, r: dict, ev, search) -> RegressionOutput:
     mv = m[sel if st.calc_dof else 0]                # (M, mstride)
     gv_dev = mv[:, :ny].t().contiguous()             # (ny, M)
     yhat_dev = ctx.empty((ny, n))
-    ctx.check(lib.flpr_interp_eval(d, n, st.dx.data_ptr(), st.ax_arg, st.G_arg, ny,
-                                   gv_dev.data_ptr(), yhat_dev.data_ptr(), ctx.stream),
-              "flpr_interp_eval")
+    if st.methods["output"] == "cubic":
+        coef = gv_dev.clone()
+        ctx.check(lib.flpr_spline_prefilter(d, st.G_arg, ny, 1, st.spl.lu.data_ptr(),
+                                            coef.data_ptr(), ctx.stream), "flpr_spline_prefilter")
+        ctx.check(lib.flpr_spline_eval(d, n, st.dx.data_ptr(), st.spl.axes.data_ptr(), st.G_arg,
+                                       ny, coef.data_ptr(), yhat_dev.data_ptr(), ctx.stream),
+                  "flpr_spline_eval")
+    else:
+        ctx.check(lib.flpr_interp_eval(d, n, st.dx.data_ptr(), st.ax_arg, st.G_arg, ny,
+                                       gv_dev.data_ptr(), yhat_dev.data_ptr(), ctx.stream),
+                  "flpr_interp_eval")
     d_norm = None
     if st.variance:
         acc = ctx.empty(1)
@@ -948,7 +979,7 @@ def _finalize_lpr(ctx, st: _LprState, r: dict, ev, search) -> RegressionOutput:
     s0 = s0h.numpy().reshape(gshape)
     ev.mark("download")
     ev.finish()
-    interp = GridInterpolant(st.axes_raw, grid_values, ctx.device)
+    interp = GridInterpolant(st.axes_raw, grid_values, ctx.device, method=st.methods["output"])
     selected = bw_k[sel]
     if st.calc_dof:
         idmin = int(np.argmin(gcv["gcv_m"]))

@@ -1,10 +1,13 @@
 """Grid interpolant returned as ``fpp_yhat`` / ``fpp``.
 
-Clamped multilinear interpolation on the raw evaluation grid, evaluated on
-the GPU (``flpr_interp_eval``).  Mirrors the reference OptimizedInterpolator
-(interp_optimized.py:271-436) for the linear method: same clamping at the
-grid edges and the same call convention (points are ``np.atleast_2d``'d, so
-1-D data is passed as an (n, 1) array).
+Mirrors the reference OptimizedInterpolator (interp_optimized.py:271-436),
+evaluated on the GPU: method 'cubic' is the not-a-knot cubic spline of
+scipy's RegularGridInterpolator (``flpr_spline_prefilter`` once, then
+``flpr_spline_eval``; end pieces extended beyond the grid), every other
+method the clamped multilinear interpolation (``flpr_interp_eval``), as in
+the reference, where only 'cubic' leaves the linear path.  Same call
+convention: points are ``np.atleast_2d``'d, so 1-D data is passed as an
+(n, 1) array.
 """
 from __future__ import annotations
 
@@ -13,7 +16,7 @@ from typing import Sequence
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, spline
 
 
 class GridInterpolant:
@@ -29,7 +32,9 @@ class GridInterpolant:
         self._M = int(np.prod(self._G))
         extra = self.values.shape[self.ndim:]
         self._extra = extra
-        self._dvals = None  # device copy, made at the first evaluation
+        self._dvals = None  # device copy (spline coefficients if cubic), made at first use
+        self._cubic = str(method) == "cubic"
+        self._spl = None
         ax = []
         for a in self.grid_axes:
             ax += [float(a[0]), float(a[1] - a[0]) if len(a) > 1 else 1.0]
@@ -48,13 +53,27 @@ class GridInterpolant:
                 parts = [flat.real, flat.imag] if self.is_complex else [flat]
                 stacked = np.concatenate([p.T for p in parts], axis=0).astype(np.float64)
                 self._dvals = torch.from_numpy(np.ascontiguousarray(stacked)).to(self.device)
+                if self._cubic:
+                    self._spl = spline.tables(self.grid_axes, self.device)
+                    stream = torch.cuda.current_stream(self.device).cuda_stream
+                    _lib.check(lib.flpr_spline_prefilter(self.ndim, _lib.ivec(self._G),
+                                                         self._dvals.shape[0], 1,
+                                                         self._spl.lu.data_ptr(),
+                                                         self._dvals.data_ptr(), stream),
+                               "flpr_spline_prefilter")
             dx = torch.from_numpy(np.ascontiguousarray(pts)).to(self.device)
             nval = self._dvals.shape[0]
             out = torch.empty((nval, n), dtype=torch.float64, device=self.device)
             stream = torch.cuda.current_stream(self.device).cuda_stream
-            _lib.check(lib.flpr_interp_eval(self.ndim, n, dx.data_ptr(), _lib.dvec(self._ax),
-                                            _lib.ivec(self._G), nval, self._dvals.data_ptr(),
-                                            out.data_ptr(), stream), "flpr_interp_eval")
+            if self._cubic:
+                _lib.check(lib.flpr_spline_eval(self.ndim, n, dx.data_ptr(),
+                                                self._spl.axes.data_ptr(), _lib.ivec(self._G),
+                                                nval, self._dvals.data_ptr(), out.data_ptr(),
+                                                stream), "flpr_spline_eval")
+            else:
+                _lib.check(lib.flpr_interp_eval(self.ndim, n, dx.data_ptr(), _lib.dvec(self._ax),
+                                                _lib.ivec(self._G), nval, self._dvals.data_ptr(),
+                                                out.data_ptr(), stream), "flpr_interp_eval")
             res = out.cpu().numpy()
         k = nval // 2 if self.is_complex else nval
         vals = res[:k] + 1j * res[k:] if self.is_complex else res

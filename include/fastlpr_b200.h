@@ -254,6 +254,34 @@ int flpr_stencil_quad(int d, const int* h_G, int H, int ny, const double* d_m, c
 int flpr_interp_eval(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G,
                      int nval, const double* d_vals, double* d_out, void* stream);
 
+/* (8b) Not-a-knot cubic spline interpolation: the 'cubic' GCV / DoF
+ * interpolation of api.py:594-600 / api.py:651-657 (regression.py:1015-1020;
+ * scipy RegularGridInterpolator(method='cubic', fill_value=None), i.e.
+ * make_ndbspl with knots [x0]*4 + x[2:-2] + [x_end]*4 per axis).
+ *
+ * flpr_spline_prefilter turns grid values into spline coefficients in
+ * place.  d_vals: (outer, G_0..G_{d-1}, inner) float64.  d_lu: for each axis
+ * in turn, G_a rows of 7 doubles (l3 l2 l1 1/u0 u1 u2 u3): the banded LU
+ * factors (no pivoting) of that axis' collocation matrix, zero where a band
+ * entry falls outside the matrix.  G >= 4 per axis.
+ *
+ * flpr_spline_reduce: flpr_interp_reduce with the spline of coefficients
+ * d_coef (H, M, ny + R) in place of the multilinear stencil.  d_axes: the
+ * raw grid axes concatenated (sum G doubles, strictly increasing, device).
+ * Points outside the grid use the end polynomial pieces (fill_value=None).
+ *
+ * flpr_spline_eval: d_out (nval, n) = spline of d_coef (nval, M) at the
+ * points; the cubic final interpolant (interp_method='cubic',
+ * api.py:488-503, output_interp_method, api.py:1145-1147). */
+int flpr_spline_prefilter(int d, const int* h_G, int64_t outer, int inner, const double* d_lu,
+                          double* d_vals, void* stream);
+int flpr_spline_reduce(int d, int64_t n, const double* d_x, const double* d_axes, const int* h_G,
+                       int H, int ny, int R, const double* d_coef,
+                       const double* const* h_ycols, const double* const* h_pcols,
+                       double* d_rss, double* d_pdot, double* d_pp, void* stream);
+int flpr_spline_eval(int d, int64_t n, const double* d_x, const double* d_axes, const int* h_G,
+                     int nval, const double* d_coef, double* d_out, void* stream);
+
 /* ---------------------------------------------------------------------
  * (9) KDE normalisation and LCV.  Replaces api.py:1059-1133.
  * d_s: (H, M) density sums (float64, epsilon already added).  For each

@@ -19,6 +19,8 @@ from typing import Dict, List, Optional, Sequence, Tuple
 import numpy as np
 import scipy.fft as sfft
 
+from .spline import cubic_interp
+
 SQRT_2PI = math.sqrt(2.0 * math.pi)
 
 _NATIVE = None
@@ -445,11 +447,13 @@ def linear_interp(axes: Sequence[np.ndarray], values: np.ndarray, pts: np.ndarra
 
 
 def _interp(axes, values, pts, method):
+    """GCV/DoF interpolation (api.py:594-600, api.py:651-657): linear, or the
+    exact not-a-knot cubic spline that scipy's 'cubic' method builds."""
     if method == "linear":
         return linear_interp(axes, values, pts)
-    from scipy.interpolate import RegularGridInterpolator
-    return RegularGridInterpolator(tuple(axes), values, method=method,
-                                   bounds_error=False, fill_value=None)(pts)
+    if method == "cubic":
+        return cubic_interp(axes, values, pts)
+    raise ValueError(f"interpolation method {method!r} is not restated")
 
 
 # --------------------------------------------------------------------------

@@ -235,6 +235,7 @@ def main():
     _intermediates_case(fastlpr, "inter2d_o1")
     interval_case(fastlpr)
     accuracy_cases(fastlpr)
+    cubic_cases(fastlpr)
 
 
 def interval_case(fastlpr):
@@ -288,8 +289,37 @@ def accuracy_cases(fastlpr):
     _kde_case(fastlpr, "kde2d_acc7", xk, h2, {"N": [32, 32], "accuracy": 7})
 
 
+def cubic_cases(fastlpr):
+    """2-D+ data with n < 5000, where the reference interpolates GCV and DoF
+    with scipy's not-a-knot cubic spline (api.py:594-600, api.py:651-657).
+    Kind 'lpr_cubic': scipy solves the spline system iteratively (gcrotmk,
+    atol 1e-6), so GCV/DoF carry that solver's residual."""
+    rng = np.random.default_rng(123)
+    n = 2000
+    x = rng.random((n, 2))
+    y = np.sin(2 * np.pi * x[:, 0]) * np.cos(np.pi * x[:, 1]) + 0.2 * rng.standard_normal(n)
+    hv = np.logspace(np.log10(0.04), np.log10(0.5), 6)
+    _lpr_case(fastlpr, "lpr2d_o1_cubic", x, y, np.column_stack([hv, hv]), {"order": 1},
+              extra={"kind": "lpr_cubic"})
+    n3 = 3000
+    x3 = rng.random((n3, 3))
+    y3 = np.sin(2 * np.pi * x3[:, 0]) + x3[:, 1] * x3[:, 2] + 0.2 * rng.standard_normal(n3)
+    h3 = np.logspace(np.log10(0.1), np.log10(0.6), 4)
+    _lpr_case(fastlpr, "lpr3d_o1_cubic", x3, y3, np.column_stack([h3, h3, h3]),
+              {"order": 1, "N": [16, 16, 16]}, extra={"kind": "lpr_cubic"})
+    n0 = 1500
+    x0 = rng.random((n0, 2))
+    y0 = np.exp(-4 * ((x0[:, 0] - 0.5) ** 2 + (x0[:, 1] - 0.4) ** 2)) + 0.1 * rng.standard_normal(n0)
+    h0 = np.logspace(np.log10(0.05), np.log10(0.4), 5)
+    _lpr_case(fastlpr, "lpr2d_o0_cubic_gcv", x0, y0, np.column_stack([h0, h0]),
+              {"order": 0, "N": [30, 24], "dof_interp_method": "linear"},
+              extra={"kind": "lpr_cubic"})
+
+
 if __name__ == "__main__":
-    if "--only-interval" in sys.argv:
+    if "--only-cubic" in sys.argv:
+        cubic_cases(_import_reference())
+    elif "--only-interval" in sys.argv:
         interval_case(_import_reference())
     elif "--only-accuracy" in sys.argv:
         accuracy_cases(_import_reference())

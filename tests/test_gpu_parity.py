@@ -326,3 +326,87 @@ def test_oversample_crop_matches_oracle(cuda_ok, L, ratio):
     torch.cuda.synchronize()
     got = torch.view_as_complex(out).cpu().numpy()
     assert rel_err(got, want) < 1e-13
+
+
+# scipy's cubic RegularGridInterpolator (the reference) solves the spline
+# system iteratively (gcrotmk, atol 1e-6, rtol 1e-5); the GPU and the oracle
+# solve it exactly.  Against the reference, GCV/DoF therefore hold to that
+# solver's residual; against the oracle, to the usual precision bounds.
+CUBIC_SOLVER_TOL = 2e-5
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("path", golden_files("lpr_cubic"), ids=os.path.basename)
+def test_cubic_lpr_matches_reference_and_oracle(cuda_ok, path, prec):
+    z = load_golden(path)
+    opts = dict(z["opts"], precision=prec)
+    r = _fastlpr().cv_fastlpr(z["x"], z["y"], z["h"], opts)
+    tol = TOL[prec]
+    g = r.gcv_yhat
+    assert g["id1se"] == z["id1se"]
+    assert g["idmin"] == z["idmin"]
+    assert rel_err(r.yhat, z["yhat"]) < tol
+    assert rel_err(r.fpp_yhat.values, z["grid_values"]) < tol
+    assert rel_err(r.s0, z["s0"]) < tol
+    assert elem_rel_err(g["gcv_m"], z["gcv_m"]) < max(tol, CUBIC_SOLVER_TOL)
+    assert rel_err(g["dof"], z["dof"]) < max(tol, CUBIC_SOLVER_TOL)
+    o = oracle.cv_fastlpr(z["x"], z["y"], z["h"], z["opts"])
+    assert elem_rel_err(g["gcv_m"], o["gcv_m"]) < tol
+    assert rel_err(g["gcv_sd"], o["gcv_sd"]) < tol * 10
+    assert rel_err(g["dof"], o["dof_all"]) < tol
+
+
+@pytest.mark.parametrize("shape", [(11,), (9, 14), (6, 7, 5)])
+def test_spline_kernels_match_oracle(cuda_ok, shape):
+    """flpr_spline_prefilter + flpr_spline_eval against the oracle's exact
+    not-a-knot spline, points inside and beyond the grid."""
+    import torch
+    from fastlpr_b200 import _lib, spline
+    from oracle import spline as ospl
+    rng = np.random.default_rng(len(shape))
+    d = len(shape)
+    axes = [np.linspace(-1.0 + a, 2.0 + 0.5 * a, g) for a, g in enumerate(shape)]
+    nval = 3
+    vals = rng.standard_normal(shape + (nval,))
+    pts = np.column_stack([rng.uniform(a[0] - 0.3, a[-1] + 0.3, 500) for a in axes])
+    want = ospl.cubic_interp(axes, vals, pts)            # (n, nval)
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    tabs = spline.tables(axes, dev)
+    M = int(np.prod(shape))
+    coef = torch.from_numpy(np.ascontiguousarray(np.moveaxis(vals, -1, 0).reshape(nval, M))).to(dev)
+    _lib.check(lib.flpr_spline_prefilter(d, _lib.ivec(shape), nval, 1, tabs.lu.data_ptr(),
+                                         coef.data_ptr(), None), "spline_prefilter")
+    dx = torch.from_numpy(np.ascontiguousarray(pts)).to(dev)
+    out = torch.empty((nval, pts.shape[0]), dtype=torch.float64, device=dev)
+    _lib.check(lib.flpr_spline_eval(d, pts.shape[0], dx.data_ptr(), tabs.axes.data_ptr(),
+                                    _lib.ivec(shape), nval, coef.data_ptr(), out.data_ptr(),
+                                    None), "spline_eval")
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().T
+    assert rel_err(got, want) < 1e-12
+    # coefficients themselves, prefiltered with the channels innermost
+    c2 = torch.from_numpy(np.ascontiguousarray(vals.reshape(M, nval))).to(dev)
+    _lib.check(lib.flpr_spline_prefilter(d, _lib.ivec(shape), 1, nval, tabs.lu.data_ptr(),
+                                         c2.data_ptr(), None), "spline_prefilter")
+    torch.cuda.synchronize()
+    assert rel_err(c2.cpu().numpy().reshape(vals.shape), ospl.coefficients(axes, vals)) < 1e-12
+
+
+def test_cubic_output_interpolant_matches_oracle(cuda_ok):
+    """interp_method='cubic': the final yhat and fpp_yhat use the spline."""
+    from oracle import spline as ospl
+    rng = np.random.default_rng(77)
+    n = 6000
+    x = rng.random((n, 2))
+    y = np.cos(3 * x[:, 0]) + x[:, 1] ** 2 + 0.1 * rng.standard_normal(n)
+    hv = np.array([0.08, 0.15, 0.3])
+    r = _fastlpr().cv_fastlpr(x, y, np.column_stack([hv, hv]),
+                              {"order": 1, "N": [40, 36], "interp_method": "cubic"})
+    gv = r.fpp_yhat.values
+    assert rel_err(r.yhat, ospl.cubic_interp(r.grid, gv, x)) < 1e-12
+    newp = np.column_stack([rng.uniform(-0.1, 1.1, 200), rng.uniform(0, 1, 200)])
+    assert rel_err(r.fpp_yhat(newp), ospl.cubic_interp(r.grid, gv, newp)) < 1e-12
+    lin = _fastlpr().cv_fastlpr(x, y, np.column_stack([hv, hv]), {"order": 1, "N": [40, 36]})
+    assert lin.gcv_yhat["id1se"] == r.gcv_yhat["id1se"]
+    np.testing.assert_allclose(lin.fpp_yhat.values, gv, rtol=1e-12)

@@ -149,3 +149,43 @@ def test_gcv_from_sums_matches_oracle_formulas():
     np.testing.assert_allclose(out["dof"], tr.mean(0))
     np.testing.assert_allclose(out["gcv_m"], rss[:, 0] / n * pen.mean(0))
     np.testing.assert_allclose(out["gcv_sd"], rss[:, 0] / n * pen.std(0, ddof=1))
+
+
+@pytest.mark.parametrize("G", [4, 5, 6, 9, 33, 200])
+def test_spline_band_lu_solves_collocation(G):
+    """The 7-column LU rows that flpr_spline_prefilter consumes solve the
+    not-a-knot collocation system (forward / back substitution as the
+    device does it)."""
+    from oracle import spline as ospl
+    from fastlpr_b200 import spline
+    ax = np.linspace(-0.4, 2.2, G)
+    T = spline.band_lu(ax)
+    A = ospl.collocation(ax)
+    b = np.random.default_rng(G).standard_normal(G)
+    y = np.zeros(G)
+    for i in range(G):
+        y[i] = b[i] - sum(T[i, 3 - k] * y[i - k] for k in (1, 2, 3) if i - k >= 0)
+    x = np.zeros(G)
+    for i in range(G - 1, -1, -1):
+        x[i] = (y[i] - sum(T[i, 3 + k] * x[i + k] for k in (1, 2, 3) if i + k < G)) * T[i, 3]
+    np.testing.assert_allclose(x, np.linalg.solve(A, b), rtol=0, atol=1e-13)
+    for i in range(G):
+        for c in range(7):
+            if not 0 <= i + c - 3 < G:
+                assert T[i, c] == 0.0
+
+
+def test_interp_method_resolution():
+    m = api._check_interp_methods({}, 2, 1000)
+    assert m == {"gcv": "cubic", "dof": "cubic", "output": "linear"}
+    assert api._check_interp_methods({}, 2, 5000)["gcv"] == "linear"
+    assert api._check_interp_methods({}, 1, 100)["dof"] == "linear"
+    m = api._check_interp_methods({"dof_interp_method": "linear", "interp_method": "cubic"}, 3, 100)
+    assert m == {"gcv": "cubic", "dof": "linear", "output": "cubic"}
+    with pytest.raises(NotImplementedError):
+        api._check_interp_methods({"gcv_interp_method": "quintic"}, 2, 100)
+    with pytest.raises(ValueError):
+        api._check_interp_methods({"N": [3, 10]}, 2, 100)
+    from fastlpr_b200 import spline
+    with pytest.raises(ValueError):
+        spline.band_lu(np.array([0.0, 1.0, 1.0, 2.0]))

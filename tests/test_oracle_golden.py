@@ -54,3 +54,41 @@ def test_oracle_intermediates_match_reference():
     assert rel_err(spec[1], z["spec_y"]) < 1e-13
     S = [oracle.lpr.convolve(np.moveaxis(spec[:1], 0, -1), k, prm["qout"], G)[..., 0] for k in spectra]
     assert rel_err(np.stack(S), z["S"][..., 0]) < 1e-12
+
+
+# scipy's 'cubic' RegularGridInterpolator solves the spline system with
+# gcrotmk (atol 1e-6, rtol 1e-5); the oracle solves it exactly, so GCV and
+# DoF agree with the reference to that solver's residual, everything else
+# to rounding.
+CUBIC_SOLVER_TOL = 2e-5
+
+
+@pytest.mark.parametrize("path", golden_files("lpr_cubic"), ids=os.path.basename)
+def test_oracle_cubic_lpr_matches_reference(path):
+    z = load_golden(path)
+    o = oracle.cv_fastlpr(z["x"], z["y"], z["h"], z["opts"])
+    assert o["id1se"] == z["id1se"]
+    assert o["idmin"] == z["idmin"]
+    assert rel_err(o["yhat"], z["yhat"]) < 1e-12
+    assert rel_err(o["grid_values"], z["grid_values"]) < 1e-12
+    assert rel_err(o["s0"], z["s0"]) < 1e-12
+    assert elem_rel_err(o["gcv_m"], z["gcv_m"]) < CUBIC_SOLVER_TOL
+    assert rel_err(o["gcv_sd"], z["gcv_sd"]) < CUBIC_SOLVER_TOL
+    assert rel_err(o["dof_all"], z["dof"]) < CUBIC_SOLVER_TOL
+
+
+def test_oracle_spline_is_scipys_exact_spline():
+    """The oracle's cubic interpolation equals scipy's make_ndbspl solved
+    directly (spsolve) on the same grid: the restatement is exact."""
+    import scipy.sparse.linalg as ssl
+    from scipy.interpolate._ndbspline import make_ndbspl
+
+    from oracle import spline
+    rng = np.random.default_rng(5)
+    for shape in ((9,), (7, 12), (5, 6, 8)):
+        axes = [np.sort(rng.uniform(-2, 3, g)) for g in shape]
+        vals = rng.standard_normal(shape + (3,))
+        pts = np.column_stack([rng.uniform(a[0] - 0.2, a[-1] + 0.2, 300) for a in axes])
+        want = make_ndbspl(tuple(axes), vals, 3, solver=ssl.spsolve)(pts)
+        got = spline.cubic_interp(axes, vals, pts)
+        assert np.abs(got - want).max() < 1e-11 * max(1.0, np.abs(want).max())
