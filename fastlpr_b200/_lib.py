@@ -38,6 +38,11 @@ SIGNATURES = [
     ("flpr_oversample_crop", _I, [_I, _PI, _PI, _I, _PD, _I, _VP, _VP, _I, _VP]),
     ("flpr_kernel_factors_ws", _SZ, [_VP, _I, _PI, _I, _I]),
     ("flpr_kernel_factors", _I, [_VP, _I, _PI, _PI, _PD, _PD, _I, _VP, _I, _VP, _VP, _VP, _SZ, _VP]),
+    ("flpr_kernel_spectra_ws", _SZ, [_VP, _I, _PI, _I]),
+    ("flpr_kernel_spectra", _I, [_VP, _I, _PI, _PI, _PD, _PD, _I, _I, _VP, _I, _PI, _VP, _VP,
+                                 _SZ, _VP]),
+    ("flpr_conv_full", _I, [_VP, _I, _PI, _PI, _PI, _I, _VP, _VP, _I, _PI, _PI, _D, _I, _VP, _I,
+                            _VP, _SZ, _VP]),
     ("flpr_conv_ws", _SZ, [_VP, _I, _PI, _I, _I]),
     ("flpr_conv", _I, [_VP, _I, _PI, _PI, _PI, _I, _I, _VP, _VP, _I, _PI, _PI, _PI, _D, _I, _VP,
                        _I, _VP, _SZ, _VP]),

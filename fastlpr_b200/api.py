@@ -27,6 +27,25 @@ from .interpolant import GridInterpolant
 from .structures import KDEOutput, RegressionOutput
 
 SQRT_2PI = math.sqrt(2.0 * math.pi)
+
+# kernel_type names (kernel.py:159-431) -> flpr_kernel_spectra ids; the two
+# Gaussians factor over the axes and use the per-axis path
+_KERNEL_IDS = {"gaussian": 0, "gauss": 0, "normal": 0, "gaussian_ft": 1, "normal_ft": 1,
+               "epan": 2, "epanechnikov": 2, "tricube": 3, "quartic": 4, "biweight": 4,
+               "triweight": 5, "uniform": 6, "rectangular": 6}
+_SUPPORTED_KERNEL_NAMES = ("gaussian, gauss, normal, gaussian_ft, normal_ft, epanechnikov, epan, "
+                           "tricube, quartic, biweight, triweight, uniform, rectangular")
+
+
+def _kernel_id(opts) -> int:
+    kt = str(opts.get("kernel_type", "gaussian")).lower()
+    if kt in ("poly", "polynomial"):
+        # compute_kernel_fourier passes no options to kernel_function
+        raise ValueError('Polynomial kernel requires opt["order"] to be specified')
+    if kt not in _KERNEL_IDS:
+        raise ValueError(f"Unknown kernel type: {opts.get('kernel_type')}. "
+                         f"Supported types: {_SUPPORTED_KERNEL_NAMES}")
+    return _KERNEL_IDS[kt]
 EPS = float(np.finfo(float).eps)
 
 
@@ -395,18 +414,72 @@ def _kernel_sums_host(geom: _Geom, bw: np.ndarray) -> np.ndarray:
     return out
 
 
-def _filter_bandwidths(ctx, geom, bw, npow):
-    """Kernel factors with the "too small bandwidth" filter of convolution.py:542-605."""
-    F, _ = _kernel_factors(ctx, geom, bw, npow)
-    s = _kernel_sums_host(geom, bw)
-    ksum = np.abs(np.prod(s, axis=0) / SQRT_2PI)
-    ihbad = ksum < EPS * 10
+class _Kernel:
+    """Kernel spectra of one bandwidth list: per-axis factors F (Gaussian
+    kernels, flpr_kernel_factors) or full-plane spectra K of every moment
+    element (radial kernels, flpr_kernel_spectra), with the inverse-FFT scale
+    of the convolutions that use them."""
+
+    def __init__(self, kid: int, data: torch.Tensor, H: int, npow: int, scale: float,
+                 elems: Optional[Dict[Tuple[int, ...], int]] = None):
+        self.kid, self.data, self.H, self.npow, self.scale = kid, data, H, npow, scale
+        self.elems = elems
+
+    @property
+    def separable(self) -> bool:
+        return self.elems is None
+
+    def data_ptr(self) -> int:
+        return self.data.data_ptr()
+
+
+def _kernel_spectra_full(ctx, geom, bw, powers, kid):
+    """(len(powers), H, half) complex128 spectra of the radial kernel's
+    moment planes (convolution.py:318-652 with kernel.py:159-431)."""
+    H, d = bw.shape[0], geom.d
+    L = geom.L
+    half = int(np.prod(L[:-1])) * (int(L[-1]) // 2 + 1)
+    dh = ctx.upload(np.ascontiguousarray(bw))
+    K = ctx.empty((len(powers), H, half, 2))
+    nitems = len(powers) * H
+    ws = ctx.ws(ctx.lib.flpr_kernel_spectra_ws(ctx.handle, d, _lib.ivec(L), nitems))
+    ctx.check(ctx.lib.flpr_kernel_spectra(ctx.handle, d, _lib.ivec(geom.G), _lib.ivec(L),
+                                          _lib.dvec(geom.lo), _lib.dvec(geom.hi), kid, H,
+                                          dh.data_ptr(), len(powers),
+                                          _lib.ivec([v for p in powers for v in p]),
+                                          K.data_ptr(), ws.data_ptr(), ws.numel(), ctx.stream),
+              "flpr_kernel_spectra")
+    return K
+
+
+def _make_kernel(ctx, geom, bw, npow, kid) -> Tuple[_Kernel, Optional[np.ndarray]]:
+    """Kernel spectra for bw; for radial kernels also the order-0 plane sums
+    (the DC terms of their spectra), else None."""
+    Lprod = float(np.prod(geom.L.astype(float)))
+    if kid in (0, 1):
+        F, _ = _kernel_factors(ctx, geom, bw, npow)
+        scale = (1.0 / SQRT_2PI if kid == 0 else 1.0) / Lprod
+        return _Kernel(kid, F, bw.shape[0], npow, scale), None
+    powers = _element_powers(geom.d, (npow - 1) // 2)
+    uniq = sorted(set(powers), key=powers.index)
+    K = _kernel_spectra_full(ctx, geom, bw, uniq, kid)
+    sums = K[uniq.index((0,) * geom.d), :, 0, 0].cpu().numpy()
+    return _Kernel(kid, K, bw.shape[0], npow, 1.0 / Lprod, {p: i for i, p in enumerate(uniq)}), sums
+
+
+def _filter_bandwidths(ctx, geom, bw, npow, kid: int = 0):
+    """Kernel spectra with the "too small bandwidth" filter of convolution.py:542-605."""
+    kern, sums = _make_kernel(ctx, geom, bw, npow, kid)
+    if sums is None:
+        s = _kernel_sums_host(geom, bw)
+        sums = np.prod(s, axis=0) / (SQRT_2PI if kid == 0 else 1.0)
+    ihbad = np.abs(sums) < EPS * 10
     keep = np.where(~ihbad)[0]
     if np.any(ihbad) and not np.all(ihbad):
         warnings.warn(f"{int(np.sum(ihbad))} bandwidth(s) are too small for this grid and "
                       "will be removed", stacklevel=3)
         bw = bw[keep]
-        F, _ = _kernel_factors(ctx, geom, bw, npow)
+        kern, _ = _make_kernel(ctx, geom, bw, npow, kid)
         keep = np.arange(bw.shape[0])
     elif np.all(ihbad):
         d = geom.d
@@ -414,10 +487,10 @@ def _filter_bandwidths(ctx, geom, bw, npow):
         warnings.warn(f"All bandwidths too small. Using Silverman's rule: h = {hs:.4f}",
                       stacklevel=3)
         bw = np.array([[hs] * d])
-        F, sum0 = _kernel_factors(ctx, geom, bw, npow)
+        kern, _ = _make_kernel(ctx, geom, bw, npow, kid)
         keep = np.array([0])
         ihbad = np.array([False])
-    return F, bw, keep, ihbad
+    return kern, bw, keep, ihbad
 
 
 def _spread_params(L: np.ndarray, kmap: np.ndarray, accuracy: int):
@@ -480,23 +553,31 @@ def _spread_fft(ctx: _Ctx, geom: _Geom, dx: torch.Tensor, cols: List[torch.Tenso
     return spec
 
 
-def _conv(ctx: _Ctx, geom: _Geom, spec, F, Hf: int, npow: int, prods, prec: int,
-          add_eps: bool):
+def _conv(ctx: _Ctx, geom: _Geom, spec, kern: _Kernel, prods, prec: int, add_eps: bool):
     """Planes for a product list [(chan, hidx, pow tuple)] -> (nprod, M)."""
     d = geom.d
     nprod = len(prods)
     real_dt = torch.float32 if prec == _lib.FLPR_PREC_F32 else torch.float64
     out = ctx.empty((nprod, geom.M), dtype=real_dt)
     chan = [p[0] for p in prods]
-    hidx = [p[1] for p in prods]
-    pw = [v for p in prods for v in p[2]]
-    scale = 1.0 / (SQRT_2PI * float(np.prod(geom.L.astype(float))))
     ws = ctx.ws(ctx.lib.flpr_conv_ws(ctx.handle, d, _lib.ivec(geom.L), nprod, prec))
-    ctx.check(ctx.lib.flpr_conv(ctx.handle, d, _lib.ivec(geom.G), _lib.ivec(geom.L),
-                                _lib.ivec(geom.qout[0]), Hf, npow, spec.data_ptr(),
-                                F.data_ptr(), nprod, _lib.ivec(chan), _lib.ivec(hidx),
-                                _lib.ivec(pw), scale, 1 if add_eps else 0, out.data_ptr(), prec,
-                                ws.data_ptr(), ws.numel(), ctx.stream), "flpr_conv")
+    if kern.separable:
+        hidx = [p[1] for p in prods]
+        pw = [v for p in prods for v in p[2]]
+        ctx.check(ctx.lib.flpr_conv(ctx.handle, d, _lib.ivec(geom.G), _lib.ivec(geom.L),
+                                    _lib.ivec(geom.qout[0]), kern.H, kern.npow, spec.data_ptr(),
+                                    kern.data_ptr(), nprod, _lib.ivec(chan), _lib.ivec(hidx),
+                                    _lib.ivec(pw), kern.scale, 1 if add_eps else 0,
+                                    out.data_ptr(), prec, ws.data_ptr(), ws.numel(), ctx.stream),
+                  "flpr_conv")
+    else:
+        kidx = [kern.elems[tuple(p[2])] * kern.H + int(p[1]) for p in prods]
+        ctx.check(ctx.lib.flpr_conv_full(ctx.handle, d, _lib.ivec(geom.G), _lib.ivec(geom.L),
+                                         _lib.ivec(geom.qout[0]), len(kern.elems) * kern.H,
+                                         spec.data_ptr(), kern.data_ptr(), nprod,
+                                         _lib.ivec(chan), _lib.ivec(kidx), kern.scale,
+                                         1 if add_eps else 0, out.data_ptr(), prec,
+                                         ws.data_ptr(), ws.numel(), ctx.stream), "flpr_conv_full")
     return out
 
 
@@ -527,9 +608,7 @@ def _check_supported(dims: int, opts) -> None:
         raise NotImplementedError(
             f"accuracy={acc} is not supported on the GPU (supported: 0-12 in 1-D/2-D, "
             "0-6 in 3-D)")
-    kt = str(opts.get("kernel_type", "gaussian")).lower()
-    if kt not in ("gaussian", "gauss", "normal"):
-        raise NotImplementedError(f"kernel_type={kt!r}: only the Gaussian kernel is supported")
+    _kernel_id(opts)
 
 
 def _check_interp_methods(opts, dims: int, n: int) -> Dict[str, str]:
@@ -598,8 +677,8 @@ def cv_fastlpr(x, y, h=None, options: Optional[dict] = None) -> RegressionOutput
     (the trained proposal network picks five neighbouring bandwidths of the
     list; while their GCV minimum sits on an edge of that window the window
     moves that way, at most three times, and otherwise the full sweep runs;
-    needs a list of isotropic, increasing bandwidths, a real single response
-    and d <= 2, else the full sweep runs).  ``metadata['bandwidth_search']``
+    needs a list of isotropic, increasing bandwidths, a real single response,
+    the Gaussian kernel and d <= 2, else the full sweep runs).  ``metadata['bandwidth_search']``
     records what happened.
     """
     x_arr = _as_column_matrix(x)
@@ -786,7 +865,7 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
         stats=stats, geom=geom, spec=spec, calc_dof=calc_dof, order=order, prec=prec,
         dy=dy, variance=variance, y_is_complex=y_is_complex, opts=opts,
         axes_raw=axes_raw, ax_arg=_lib.dvec(_axes_arg(axes_raw)), G_arg=_lib.ivec(geom.G),
-        methods=methods, spl=None,
+        methods=methods, spl=None, kid=_kernel_id(opts),
         dual=(calc_dof and ny <= 4 and not opts.get("_direct_reduce", False)
               and methods["gcv"] == "linear" and methods["dof"] == "linear"), Q=None))
     if "cubic" in methods.values():
@@ -814,9 +893,8 @@ def _evaluate_lpr(ctx, st: _LprState, bandwidths: np.ndarray, ev) -> dict:
     geom, spec, opts, calc_dof = st.geom, st.spec, st.opts, st.calc_dof
     ycols, pcols = st.ycols, st.pcols
     npow = 2 * order + 1
-    F, bw, keep, _ = _filter_bandwidths(ctx, geom, bandwidths, npow)
+    kern, bw, keep, _ = _filter_bandwidths(ctx, geom, bandwidths, npow, st.kid)
     H = len(keep)
-    Hf = bw.shape[0]
     epw = _element_powers(d, order)
     ns = len(epw)
     nt = 1 if order == 0 else len(_design_powers(d, order))
@@ -825,14 +903,14 @@ def _evaluate_lpr(ctx, st: _LprState, bandwidths: np.ndarray, ev) -> dict:
     Cv = ny + R
     M = geom.M
     Lq = (_lib.ivec(geom.G), _lib.ivec(geom.L), _lib.ivec(geom.qout[0]))
-    use_fused = (prec == _lib.FLPR_PREC_F32 and d == 2 and st.dual
+    use_fused = (prec == _lib.FLPR_PREC_F32 and d == 2 and st.dual and kern.separable
                  and not opts.get("_no_fused", False)
                  and lib.flpr_lpr2d_fused_supported(*Lq, H, order, Cv) == 1)
     if not use_fused:
-        S = _conv(ctx, geom, spec, F, Hf, npow,
+        S = _conv(ctx, geom, spec, kern,
                   [(0, int(hk), epw[k]) for k in range(ns) for hk in keep], prec, order == 0)
         ev.mark("conv_S")
-        T = _conv(ctx, geom, spec, F, Hf, npow,
+        T = _conv(ctx, geom, spec, kern,
                   [(1 + c, int(hk), epw[i]) for i in range(nt) for c in range(Cv) for hk in h_t],
                   prec, False)
         ev.mark("conv_T")
@@ -846,10 +924,9 @@ def _evaluate_lpr(ctx, st: _LprState, bandwidths: np.ndarray, ev) -> dict:
         dots = ctx.empty((Cv, H))
         if use_fused:
             S = ctx.empty((ns, H, M), dtype=torch.float32)
-            scale = 1.0 / (SQRT_2PI * float(np.prod(geom.L.astype(float))))
             ws = ctx.ws(lib.flpr_lpr2d_fused_ws(*Lq, H, order, Cv))
             ctx.check(lib.flpr_lpr2d_fused(*Lq, H, npow, order, Cv, ny, spec.data_ptr(),
-                                           F.data_ptr(), scale, st.Q.data_ptr(), reg,
+                                           kern.data_ptr(), kern.scale, st.Q.data_ptr(), reg,
                                            S.data_ptr(), m.data_ptr(), dots.data_ptr(),
                                            scalar.data_ptr(), ws.data_ptr(), ws.numel(),
                                            ctx.stream), "flpr_lpr2d_fused")
@@ -1062,7 +1139,8 @@ def _learned_search(ctx, st: _LprState, bandwidths: np.ndarray, model, ev, pendi
     next window shares the edge bandwidth) at most _MAX_WALKS times; returns
     (evaluation, search record) or None when the full sweep must run."""
     from . import learned as _learned
-    if not (st.calc_dof and st.ny == 1 and not st.y_is_complex and st.d <= 2) or not pending:
+    if not (st.calc_dof and st.ny == 1 and not st.y_is_complex and st.d <= 2
+            and st.kid == 0) or not pending:
         return None
     lh = _learned.isotropic_log_h(bandwidths)
     if lh is None:
@@ -1215,13 +1293,13 @@ def _fit_kde(ctx, x_arr, bandwidths, opts, G, prec):
     stats = _point_stats(ctx, dx, n, d)
     _raise_nonfinite(flags_h.numpy(), [("Input x", 0)], "cv_fastkde")
     geom = _make_geom(stats, n, d, G, int(opts["accuracy"]), bool(opts.get("flag_power2", True)))
-    F, bw, keep, ihbad = _filter_bandwidths(ctx, geom, bandwidths, 1)
+    kern, bw, keep, ihbad = _filter_bandwidths(ctx, geom, bandwidths, 1, _kernel_id(opts))
     if len(keep) != bandwidths.shape[0] or bw.shape[0] != bandwidths.shape[0]:
         # the reference indexes its density columns by the unfiltered list here
         raise ValueError("a bandwidth is too small for the KDE grid")
     H = len(keep)
     spec = _spread_fft(ctx, geom, dx, [], prec)
-    S = _conv(ctx, geom, spec, F, H, 1, [(0, int(k), (0,) * d) for k in keep], prec, True)
+    S = _conv(ctx, geom, spec, kern, [(0, int(k), (0,) * d) for k in keep], prec, True)
     S64 = S if S.dtype == torch.float64 else S.to(torch.float64)
     # raw grid axes by inverting centring and z-scoring (api.py:1038-1057)
     axes_raw = []
@@ -1242,8 +1320,7 @@ def _fit_kde(ctx, x_arr, bandwidths, opts, G, prec):
                                ctx.stream), "flpr_kde_lcv")
     lc = lcv.cpu().numpy()
     lcv_m = lc[:, 0].copy()
-    mean_l = lc[:, 0] / n
-    var_l = np.maximum(lc[:, 1] / n - mean_l ** 2, 0.0)
+    var_l = lc[:, 1] / n
     lcv_sd = np.sqrt(var_l) * np.sqrt(n)
     sel = _one_se_rule(lcv_m, lcv_sd, bandwidths, prefer_smaller=False)
     gshape = tuple(int(g) for g in G)

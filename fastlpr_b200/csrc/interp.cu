@@ -174,31 +174,55 @@ struct K0s {
   double k0[256];
 };
 
+// log of the leave-one-out density at point i: log(max(n/(n-1) (f(x_i) - K0/n), 1e-10))
+__device__ __forceinline__ double loo_log(const InterpGeom& g, const double* __restrict__ x,
+                                          int64_t i, const double* __restrict__ fh, double k0n,
+                                          double ratio) {
+  Stencil st;
+  make_stencil(g, x, i, st);
+  double v = 0.0;
+  for (int k = 0; k < st.ncorner; ++k) v += st.w[k] * fh[st.base[k]];
+  double fl = ratio * (v - k0n);
+  if (!(fl > 1e-10)) fl = 1e-10;
+  return log(fl);
+}
+
+// Sums of (l - c) and (l - c)^2 with c = l at point 0: the shift keeps the
+// variance free of cancellation (exactly zero when every l is clamped).
 __global__ void kde_lcv_kernel(InterpGeom g, int64_t n, const double* __restrict__ x,
                                const double* __restrict__ f, int h0, K0s k0,
-                               double* __restrict__ lcv) {
+                               double* __restrict__ part) {
   __shared__ double sh[32];
   const int h = h0 + blockIdx.y;
   const double* fh = f + (int64_t)h * g.M;
   const double k0n = k0.k0[blockIdx.y] / (double)n;
   const double ratio = (double)n / (double)(n - 1);
+  const double c = loo_log(g, x, 0, fh, k0n, ratio);
   double s1 = 0.0, s2 = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    Stencil st;
-    make_stencil(g, x, i, st);
-    double v = 0.0;
-    for (int k = 0; k < st.ncorner; ++k) v += st.w[k] * fh[st.base[k]];
-    double fl = ratio * (v - k0n);
-    if (!(fl > 1e-10)) fl = 1e-10;
-    double l = log(fl);
+    const double l = loo_log(g, x, i, fh, k0n, ratio) - c;
     s1 += l;
     s2 += l * l;
   }
   double a = block_sum(s1, sh);
-  if (threadIdx.x == 0) atomicAdd(&lcv[2 * h], a);
+  if (threadIdx.x == 0) atomicAdd(&part[3 * h], a);
   double b = block_sum(s2, sh);
-  if (threadIdx.x == 0) atomicAdd(&lcv[2 * h + 1], b);
+  if (threadIdx.x == 0) {
+    atomicAdd(&part[3 * h + 1], b);
+    if (blockIdx.x == 0) part[3 * h + 2] = c;
+  }
+}
+
+// lcv[h] = {sum l, sum (l - mean)^2} from the shifted sums
+__global__ void kde_lcv_finish_kernel(int H, int64_t n, const double* __restrict__ part,
+                                      double* __restrict__ lcv) {
+  const int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= H) return;
+  const double s1 = part[3 * h], s2 = part[3 * h + 1], c = part[3 * h + 2];
+  lcv[2 * h] = (double)n * c + s1;
+  const double m2 = s2 - s1 * s1 / (double)n;
+  lcv[2 * h + 1] = m2 > 0.0 ? m2 : 0.0;
 }
 
 // ---- adjoint of the interpolation (dual form of the GCV/Hutchinson sums) --
@@ -420,7 +444,8 @@ int flpr_stencil_quad(int d, const int* h_G, int H, int ny, const double* d_m, c
 size_t flpr_kde_ws(int64_t n, int H, int64_t M) {
   (void)n;
   (void)M;
-  return align_up(sizeof(double) * (size_t)(H > 0 ? H : 1));
+  return align_up(sizeof(double) * (size_t)(H > 0 ? H : 1)) +
+         align_up(sizeof(double) * 3 * (size_t)(H > 0 ? H : 1));
 }
 
 int flpr_kde_lcv(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G, int H,
@@ -435,8 +460,10 @@ int flpr_kde_lcv(int d, int64_t n, const double* d_x, const double* h_ax, const 
   }
   cudaStream_t s = as_stream(stream);
   double* sums = static_cast<double*>(d_ws);
+  double* part = reinterpret_cast<double*>(static_cast<char*>(d_ws) +
+                                           align_up(sizeof(double) * (size_t)H));
   FLPR_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * H, s));
-  FLPR_CUDA(cudaMemsetAsync(d_lcv, 0, sizeof(double) * 2 * H, s));
+  FLPR_CUDA(cudaMemsetAsync(part, 0, sizeof(double) * 3 * H, s));
   int gb = pt_blocks(g.M, 2);
   gb = (gb + H - 1) / H;
   if (gb < 4) gb = 4;
@@ -450,9 +477,11 @@ int flpr_kde_lcv(int d, int64_t n, const double* d_x, const double* h_ax, const 
     int hn = H - h0 < 256 ? H - h0 : 256;
     K0s k0;
     for (int j = 0; j < hn; ++j) k0.k0[j] = h_k0[h0 + j];
-    kde_lcv_kernel<<<dim3(per_h, hn), 256, 0, s>>>(g, n, d_x, d_f, h0, k0, d_lcv);
+    kde_lcv_kernel<<<dim3(per_h, hn), 256, 0, s>>>(g, n, d_x, d_f, h0, k0, part);
     FLPR_LAUNCH_CHECK();
   }
+  kde_lcv_finish_kernel<<<(H + 127) / 128, 128, 0, s>>>(H, n, part, d_lcv);
+  FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
 

@@ -158,6 +158,104 @@ __global__ void crop_kernel(ConvArgs ca, int nb, int p0, const Real* __restrict_
   }
 }
 
+// ---- radial (non-separable) kernels: full-plane spectra ---------------------
+// Kernel ids (kernel.py:159-431): 0 gaussian, 1 gaussian_ft, 2 epanechnikov,
+// 3 tricube, 4 quartic/biweight, 5 triweight, 6 uniform; all of ||u||^2.
+constexpr int kMaxElems = 64;
+
+struct PlaneArgs {
+  int d, kid, H, nelem;
+  int G[3], L[3], before[3];
+  double lo[3], hi[3], step[3];
+  int64_t cells;
+  int pw[kMaxElems][3];
+};
+
+__device__ __forceinline__ double radial_kernel(int kid, double s) {
+  const double eps = 2.220446049250313e-16;
+  switch (kid) {
+    case 0: return ddiv(exp(dmul(-0.5, s)), 2.5066282746310002);   // / sqrt(2 pi)
+    case 1: return exp(dmul(-0.5, s));
+    case 2: { const double v = dmul(dsub(1.0, s), 0.75); return v > eps ? v : eps; }
+    case 3: {
+      const double r = sqrt(s);
+      const double c = dsub(1.0, pow(r, 3.0));
+      const double v = r <= 1.0 ? dmul(70.0 / 81.0, pow(c, 3.0)) : 0.0;
+      return v > eps ? v : eps;
+    }
+    case 4: {
+      const double c = dsub(1.0, s);
+      const double v = s <= 1.0 ? dmul(15.0 / 16.0, dmul(c, c)) : 0.0;
+      return v > eps ? v : eps;
+    }
+    case 5: {
+      const double v = s <= 1.0 ? dmul(35.0 / 32.0, pow(dsub(1.0, s), 3.0)) : 0.0;
+      return v > eps ? v : eps;
+    }
+    default: return sqrt(s) <= 1.0 ? 0.5 : 0.0;
+  }
+}
+
+// Real planes of items [i0, i0 + nb) (item = elem * H + h): on the
+// zero-padded L grid, K(u) prod_a u_a^pw_a / prod_a h_a at the grid point
+// (linspace(lo, hi, G) per axis, u = x / h), zero in the padding.
+__global__ void kernel_plane_kernel(PlaneArgs pa, int i0, int nb, const double* __restrict__ h,
+                                    double* __restrict__ out) {
+  const int64_t total = (int64_t)nb * pa.cells;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int b = (int)(t / pa.cells);
+    int64_t r = t - (int64_t)b * pa.cells;
+    const int item = i0 + b;
+    const int e = item / pa.H, hidx = item - e * pa.H;
+    int k[3] = {0, 0, 0};
+    bool inside = true;
+    for (int a = pa.d - 1; a >= 0; --a) {
+      k[a] = (int)(r % pa.L[a]) - pa.before[a];
+      r /= pa.L[a];
+      inside = inside && k[a] >= 0 && k[a] < pa.G[a];
+    }
+    double v = 0.0;
+    if (inside) {
+      double u[3], ssq = 0.0, deth = 1.0;
+      for (int a = 0; a < pa.d; ++a) {
+        const double g = (k[a] == pa.G[a] - 1 && pa.G[a] > 1) ? pa.hi[a]
+                                                              : dadd(dmul((double)k[a], pa.step[a]), pa.lo[a]);
+        const double hv = h[hidx * pa.d + a];
+        u[a] = ddiv(g, hv);
+        ssq = a == 0 ? dmul(u[a], u[a]) : dadd(ssq, dmul(u[a], u[a]));
+        deth = dmul(deth, hv);
+      }
+      v = ddiv(radial_kernel(pa.kid, ssq), deth);
+      for (int a = 0; a < pa.d; ++a)
+        for (int q = 0; q < pa.pw[e][a]; ++q) v = dmul(v, u[a]);
+    }
+    out[t] = v;
+  }
+}
+
+template <typename Real>
+__global__ void product_full_kernel(ConvArgs ca, int nb, ProdBatch desc,
+                                    const typename Cplx<Real>::type* __restrict__ spec,
+                                    const double2* __restrict__ K,
+                                    typename Cplx<Real>::type* __restrict__ out) {
+  using C = typename Cplx<Real>::type;
+  const int64_t total = (int64_t)nb * ca.half;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int b = (int)(t / ca.half);
+    const int64_t w = t - (int64_t)b * ca.half;
+    const ProdDesc pd = desc.p[b];
+    const double2 k = K[(int64_t)pd.hidx * ca.half + w];  // hidx = elem * H + h here
+    const double kr = k.x * ca.scale, ki = k.y * ca.scale;
+    const C sv = spec[(int64_t)pd.chan * ca.half + w];
+    C o;
+    o.x = (Real)((double)sv.x * kr - (double)sv.y * ki);
+    o.y = (Real)((double)sv.x * ki + (double)sv.y * kr);
+    out[t] = o;
+  }
+}
+
 static int conv_batch(int d, const int* L, int nprod, int prec) {
   int64_t cells = prod(L, d);
   int64_t half = cells / L[d - 1] * (L[d - 1] / 2 + 1);
@@ -430,6 +528,146 @@ int flpr_conv(flpr_handle_t handle, int d, const int* h_G, const int* h_L, const
   return FLPR_OK;
 }
 
+
+static int plane_batch(int d, const int* L, int nitems) {
+  int64_t cells = prod(L, d);
+  size_t per = (size_t)cells * 8;
+  int64_t b = (int64_t)(((size_t)1024 << 20) / per);
+  if (b < 1) b = 1;
+  if (b > nitems) b = nitems;
+  return (int)b;
+}
+
+size_t flpr_kernel_spectra_ws(flpr_handle_t handle, int d, const int* h_L, int nitems) {
+  if (d < 1 || d > 3 || nitems < 1) return 0;
+  const int B = plane_batch(d, h_L, nitems);
+  ArenaSize ar;
+  ar.take<char>((size_t)B * prod(h_L, d) * 8);
+  size_t w1 = 0, w2 = 0;
+  if (plans_of(handle).work_size(grid_plan(d, h_L, CUFFT_D2Z, B), &w1) != FLPR_OK) return 0;
+  const int tail = nitems % B;
+  if (tail && plans_of(handle).work_size(grid_plan(d, h_L, CUFFT_D2Z, tail), &w2) != FLPR_OK)
+    return 0;
+  ar.take<char>(w1 > w2 ? w1 : w2);
+  return ar.used;
+}
+
+int flpr_kernel_spectra(flpr_handle_t handle, int d, const int* h_G, const int* h_L,
+                        const double* h_lo, const double* h_hi, int kernel_id, int H,
+                        const double* d_h, int nelem, const int* h_pow, void* d_K, void* d_ws,
+                        size_t ws_bytes, void* stream) {
+  FLPR_CHECK_ARG(d >= 1 && d <= 3, "kernel_spectra: d=%d", d);
+  FLPR_CHECK_ARG(kernel_id >= 0 && kernel_id <= 6, "kernel_spectra: kernel_id=%d", kernel_id);
+  FLPR_CHECK_ARG(H >= 1 && nelem >= 1 && nelem <= kMaxElems, "kernel_spectra: H=%d nelem=%d", H,
+                 nelem);
+  PlaneArgs pa{};
+  pa.d = d;
+  pa.kid = kernel_id;
+  pa.H = H;
+  pa.nelem = nelem;
+  for (int a = 0; a < d; ++a) {
+    FLPR_CHECK_ARG(h_G[a] >= 1 && h_L[a] >= h_G[a] + 1, "kernel_spectra: G=%d L=%d", h_G[a],
+                   h_L[a]);
+    pa.G[a] = h_G[a];
+    pa.L[a] = h_L[a];
+    pa.before[a] = (h_L[a] - h_G[a]) / 2 + 1;
+    pa.lo[a] = h_lo[a];
+    pa.hi[a] = h_hi[a];
+    pa.step[a] = h_G[a] > 1 ? (h_hi[a] - h_lo[a]) / (double)(h_G[a] - 1) : 0.0;
+  }
+  for (int e = 0; e < nelem; ++e)
+    for (int a = 0; a < 3; ++a) {
+      pa.pw[e][a] = a < d ? h_pow[e * d + a] : 0;
+      FLPR_CHECK_ARG(pa.pw[e][a] >= 0 && pa.pw[e][a] <= 8, "kernel_spectra: power out of range");
+    }
+  pa.cells = prod(h_L, d);
+  const int nitems = nelem * H;
+  if (ws_bytes < flpr_kernel_spectra_ws(handle, d, h_L, nitems)) {
+    set_error("kernel_spectra: workspace too small");
+    return FLPR_ERR_WORKSPACE;
+  }
+  const int B = plane_batch(d, h_L, nitems);
+  const int64_t half = pa.cells / h_L[d - 1] * (h_L[d - 1] / 2 + 1);
+  Arena ar(d_ws, ws_bytes);
+  double* planes = ar.take<double>((size_t)B * pa.cells);
+  size_t work_bytes = ar.size - align_up(ar.used);
+  char* work = ar.take<char>(1);
+  cudaStream_t s = as_stream(stream);
+  for (int i0 = 0; i0 < nitems; i0 += B) {
+    const int nb = nitems - i0 < B ? nitems - i0 : B;
+    kernel_plane_kernel<<<grid_blocks((int64_t)nb * pa.cells), 256, 0, s>>>(pa, i0, nb, d_h,
+                                                                            planes);
+    FLPR_LAUNCH_CHECK();
+    FLPR_TRY(plans_of(handle).exec(grid_plan(d, h_L, CUFFT_D2Z, nb), planes,
+                                   (double2*)d_K + (int64_t)i0 * half, work, work_bytes, s));
+  }
+  return FLPR_OK;
+}
+
+int flpr_conv_full(flpr_handle_t handle, int d, const int* h_G, const int* h_L, const int* h_qout,
+                   int nkern, const void* d_spec, const void* d_K, int nprod, const int* h_chan,
+                   const int* h_kidx, double scale, int add_eps, void* d_out, int prec,
+                   void* d_ws, size_t ws_bytes, void* stream) {
+  FLPR_CHECK_ARG(d >= 1 && d <= 3, "conv_full: d=%d", d);
+  FLPR_CHECK_ARG(nprod >= 1 && nkern >= 1, "conv_full: nprod=%d nkern=%d", nprod, nkern);
+  ConvArgs ca{};
+  ca.d = d;
+  ca.scale = scale;
+  for (int a = 0; a < d; ++a) {
+    FLPR_CHECK_ARG(h_qout[a] >= 0 && h_qout[a] + h_G[a] <= h_L[a], "conv_full: crop window");
+    ca.L[a] = h_L[a];
+    ca.G[a] = h_G[a];
+    ca.qout[a] = h_qout[a];
+  }
+  ca.cells = prod(h_L, d);
+  ca.M = prod(h_G, d);
+  ca.half = ca.cells / h_L[d - 1] * (h_L[d - 1] / 2 + 1);
+  for (int p = 0; p < nprod; ++p)
+    FLPR_CHECK_ARG(h_kidx[p] >= 0 && h_kidx[p] < nkern, "conv_full: kidx[%d]=%d", p, h_kidx[p]);
+  if (ws_bytes < flpr_conv_ws(handle, d, h_L, nprod, prec)) {
+    set_error("conv_full: workspace too small");
+    return FLPR_ERR_WORKSPACE;
+  }
+  const int B = conv_batch(d, h_L, nprod, prec);
+  const size_t es = prec == FLPR_PREC_F32 ? 4 : 8;
+  Arena ar(d_ws, ws_bytes);
+  char* pbuf = ar.take<char>((size_t)B * ca.half * 2 * es);
+  char* rbuf = ar.take<char>((size_t)B * ca.cells * es);
+  size_t work_bytes = ar.size - align_up(ar.used);
+  char* work = ar.take<char>(1);
+  cudaStream_t s = as_stream(stream);
+  ProdBatch batch;
+  const int ctype = prec == FLPR_PREC_F32 ? CUFFT_C2R : CUFFT_Z2D;
+  for (int p0 = 0; p0 < nprod; p0 += B) {
+    int nb = nprod - p0 < B ? nprod - p0 : B;
+    for (int b = 0; b < nb; ++b) {
+      ProdDesc pd{};
+      pd.chan = h_chan[p0 + b];
+      pd.hidx = h_kidx[p0 + b];
+      batch.p[b] = pd;
+    }
+    int blocks = grid_blocks((int64_t)nb * ca.half);
+    if (prec == FLPR_PREC_F32) {
+      product_full_kernel<float><<<blocks, 256, 0, s>>>(ca, nb, batch, (const float2*)d_spec,
+                                                        (const double2*)d_K, (float2*)pbuf);
+    } else {
+      product_full_kernel<double><<<blocks, 256, 0, s>>>(ca, nb, batch, (const double2*)d_spec,
+                                                         (const double2*)d_K, (double2*)pbuf);
+    }
+    FLPR_LAUNCH_CHECK();
+    FLPR_TRY(plans_of(handle).exec(grid_plan(d, h_L, ctype, nb), pbuf, rbuf, work, work_bytes, s));
+    int cb = grid_blocks((int64_t)nb * ca.M);
+    if (prec == FLPR_PREC_F32) {
+      crop_kernel<float><<<cb, 256, 0, s>>>(ca, nb, p0, (const float*)rbuf, add_eps,
+                                            (float*)d_out);
+    } else {
+      crop_kernel<double><<<cb, 256, 0, s>>>(ca, nb, p0, (const double*)rbuf, add_eps,
+                                             (double*)d_out);
+    }
+    FLPR_LAUNCH_CHECK();
+  }
+  return FLPR_OK;
+}
 
 int flpr_oversample_crop(int d, const int* h_Lout, const int* h_Lin, int nchan,
                          const double* h_tau, int ratio, const void* d_in, void* d_out, int prec,

@@ -159,6 +159,29 @@ int flpr_conv(flpr_handle_t handle, int d, const int* h_G, const int* h_L, const
               double scale, int add_eps, void* d_out, int prec,
               void* d_ws, size_t ws_bytes, void* stream);
 
+/* (5b) Non-separable (radial) kernels: kernel.py:310-431 (epanechnikov,
+ * tricube, quartic/biweight, triweight, uniform; also gaussian and
+ * gaussian_ft) for compute_kernel_fourier (convolution.py:318-652) and
+ * nufft_convolve (convolution.py:797-953).  A radial kernel of ||u|| does not
+ * factor over the axes, so its moment planes K(u) prod_a u_a^p_a / prod_a h_a
+ * (u = x / h on linspace(lo, hi, G) per axis, padded with floor((L-G)/2)+1
+ * leading zeros) are sampled on the full L grid and transformed (D2Z).
+ * kernel_id: 0 gaussian, 1 gaussian_ft, 2 epanechnikov, 3 tricube,
+ * 4 quartic, 5 triweight, 6 uniform.  h_pow: (nelem, d) exponents.
+ * d_K: (nelem, H, L0.., L_last/2+1) complex128, item e*H + h.
+ * flpr_conv_full: flpr_conv with d_K in place of the per-axis factors;
+ * product p multiplies channel h_chan[p] by kernel spectrum h_kidx[p]
+ * (< nkern); same output, scale, eps and workspace (flpr_conv_ws). */
+size_t flpr_kernel_spectra_ws(flpr_handle_t handle, int d, const int* h_L, int nitems);
+int flpr_kernel_spectra(flpr_handle_t handle, int d, const int* h_G, const int* h_L,
+                        const double* h_lo, const double* h_hi, int kernel_id, int H,
+                        const double* d_h, int nelem, const int* h_pow, void* d_K, void* d_ws,
+                        size_t ws_bytes, void* stream);
+int flpr_conv_full(flpr_handle_t handle, int d, const int* h_G, const int* h_L, const int* h_qout,
+                   int nkern, const void* d_spec, const void* d_K, int nprod, const int* h_chan,
+                   const int* h_kidx, double scale, int add_eps, void* d_out, int prec,
+                   void* d_ws, size_t ws_bytes, void* stream);
+
 /* ---------------------------------------------------------------------
  * (6) Local polynomial solve at every grid point and bandwidth.
  * Replaces solve_regression_system (regression.py:162-277) and the
@@ -288,7 +311,9 @@ int flpr_spline_eval(int d, int64_t n, const double* d_x, const double* d_axes, 
  * bandwidth: f = max(s / (sum(s) * dxprod), 0) (no division if the sum is
  * not positive), written to d_f (H, M) float64; then f is interpolated at
  * the raw points and the LCV terms log(max(n/(n-1) (f - K0_h/n), 1e-10))
- * are summed: d_lcv (H, 2) = {sum log, sum log^2}.  h_k0: (H) K0_h values.
+ * are reduced: d_lcv (H, 2) = {sum of the logs, sum of their squared
+ * deviations from their mean} (shifted sums, so a constant set of logs
+ * gives exactly zero).  h_k0: (H) K0_h values.
  * --------------------------------------------------------------------- */
 size_t flpr_kde_ws(int64_t n, int H, int64_t M);
 int flpr_kde_lcv(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G,

@@ -287,12 +287,35 @@ def kernel_grid_axes(x_scaled: np.ndarray, G) -> List[np.ndarray]:
     return [np.linspace(x[:, d].min(), x[:, d].max(), int(G[d])) for d in range(x.shape[1])]
 
 
-def kernel_spectra(x_scaled, h, G, order: int, flag_power2: bool = True, workers: int = 1):
+def radial_kernel(kernel_type: str, ssq: np.ndarray) -> np.ndarray:
+    """K as a function of ||u||^2 (kernel.py:159-431), before the 1/det(h)."""
+    kt = kernel_type.lower()
+    eps = np.finfo(float).eps
+    if kt in ("gauss", "gaussian", "normal"):
+        return np.exp(-0.5 * ssq) * (1.0 / SQRT_2PI)
+    if kt in ("gaussian_ft", "normal_ft"):
+        return np.exp(-0.5 * ssq)
+    if kt in ("epan", "epanechnikov"):
+        return np.maximum(0.75 * (1.0 - ssq), eps)
+    if kt == "tricube":
+        r = np.sqrt(ssq)
+        return np.maximum(eps, (70.0 / 81.0) * (1 - r ** 3) ** 3 * (r <= 1))
+    if kt in ("quartic", "biweight"):
+        return np.maximum(eps, (15.0 / 16.0) * (1 - ssq) ** 2 * (ssq <= 1))
+    if kt == "triweight":
+        return np.maximum(eps, (35.0 / 32.0) * (1 - ssq) ** 3 * (ssq <= 1))
+    if kt in ("uniform", "rectangular"):
+        return 0.5 * (np.sqrt(ssq) <= 1).astype(float)
+    raise ValueError(f"Unknown kernel type: {kernel_type}")
+
+
+def kernel_spectra(x_scaled, h, G, order: int, flag_power2: bool = True, workers: int = 1,
+                   kernel_type: str = "gaussian"):
     """FFT of K(u) * u^a on the padded grid for every packed element and bandwidth.
 
     Returns (spectra list[ns] of (*L, H) complex128, params dict with L, qin,
     qout, h (filtered), ihbad).  Follows compute_kernel_fourier
-    (convolution.py:318-652) with the Gaussian kernel (kernel.py:330-357).
+    (convolution.py:318-652) with the kernels of kernel.py:159-431.
     """
     x = np.atleast_2d(np.asarray(x_scaled, dtype=float))
     h = np.atleast_2d(np.asarray(h, dtype=float))
@@ -310,7 +333,7 @@ def kernel_spectra(x_scaled, h, G, order: int, flag_power2: bool = True, workers
         ssq = np.zeros(tuple(G) + (H,))
         for d in range(dims):
             ssq = ssq + u[d] ** 2
-        kd = np.exp(-0.5 * ssq) * (1.0 / SQRT_2PI) / np.prod(hh, axis=1)
+        kd = radial_kernel(kernel_type, ssq) / np.prod(hh, axis=1)
         elems = []
         for pw in element_powers(dims, order):
             e = kd
@@ -607,7 +630,8 @@ def cv_fastlpr(x, y, h=None, options: Optional[Dict] = None, workers: int = 1,
     axes_raw = _raw_axes(x, G, opts)
     flag_power2 = bool(opts.get("flag_power2", True))
     _mark("prep")
-    kdf, prm = kernel_spectra(xs, bw, G, order, flag_power2, workers)
+    kdf, prm = kernel_spectra(xs, bw, G, order, flag_power2, workers,
+                              kernel_type=str(opts.get("kernel_type", "gaussian")))
     _mark("kernel")
     bw = prm["h"]
     H = bw.shape[0]
@@ -795,7 +819,8 @@ def cv_fastkde(x, h=None, options: Optional[Dict] = None, workers: int = 1,
     if G.size == 1:
         G = np.repeat(G, dims)
     flag_power2 = bool(opts.get("flag_power2", True))
-    kdf, prm = kernel_spectra(xs, bw, G, 0, flag_power2, workers)
+    kdf, prm = kernel_spectra(xs, bw, G, 0, flag_power2, workers,
+                              kernel_type=str(opts.get("kernel_type", "gaussian")))
     bw = prm["h"]
     H = bw.shape[0]
     L, qin, qout = prm["L"], prm["qin"], prm["qout"]

@@ -236,6 +236,7 @@ def main():
     interval_case(fastlpr)
     accuracy_cases(fastlpr)
     cubic_cases(fastlpr)
+    kernel_cases(fastlpr)
 
 
 def interval_case(fastlpr):
@@ -316,8 +317,39 @@ def cubic_cases(fastlpr):
               extra={"kind": "lpr_cubic"})
 
 
+def kernel_cases(fastlpr):
+    """Non-Gaussian kernel_type values (kernel.py:159-431): radial kernels
+    of ||u||, not separable over the axes in 2-D."""
+    rng = np.random.default_rng(321)
+    n = 3000
+    x1 = rng.random((n, 1))
+    y1 = np.sin(2 * np.pi * x1[:, 0]) + 0.1 * rng.standard_normal(n)
+    h1 = np.logspace(np.log10(0.03), np.log10(0.5), 6)[:, None]
+    _lpr_case(fastlpr, "lpr1d_o1_epan", x1, y1, h1,
+              {"order": 1, "N": 256, "kernel_type": "epanechnikov"})
+    _lpr_case(fastlpr, "lpr1d_o2_quartic", x1, y1, h1,
+              {"order": 2, "N": 200, "kernel_type": "quartic"})
+    n2 = 6000
+    x2 = rng.random((n2, 2))
+    y2 = np.sin(2 * np.pi * x2[:, 0]) * np.cos(np.pi * x2[:, 1]) + 0.1 * rng.standard_normal(n2)
+    hv = np.logspace(np.log10(0.06), np.log10(0.5), 5)
+    h2 = np.column_stack([hv, hv])
+    _lpr_case(fastlpr, "lpr2d_o1_tricube", x2, y2, h2,
+              {"order": 1, "N": [48, 40], "kernel_type": "tricube"})
+    _lpr_case(fastlpr, "lpr2d_o0_uniform", x2, y2, h2,
+              {"order": 0, "N": [40, 40], "kernel_type": "uniform"})
+    _lpr_case(fastlpr, "lpr2d_o1_triweight", x2, y2, h2,
+              {"order": 1, "N": [32, 36], "kernel_type": "triweight"})
+    _lpr_case(fastlpr, "lpr2d_o1_gaussft", x2, y2, h2,
+              {"order": 1, "N": [40, 40], "kernel_type": "gaussian_ft"})
+    xk = rng.standard_normal((3000, 2))
+    _kde_case(fastlpr, "kde2d_epan", xk, h2, {"N": [40, 40], "kernel_type": "epanechnikov"})
+
+
 if __name__ == "__main__":
-    if "--only-cubic" in sys.argv:
+    if "--only-kernels" in sys.argv:
+        kernel_cases(_import_reference())
+    elif "--only-cubic" in sys.argv:
         cubic_cases(_import_reference())
     elif "--only-interval" in sys.argv:
         interval_case(_import_reference())

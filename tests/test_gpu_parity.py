@@ -410,3 +410,33 @@ def test_cubic_output_interpolant_matches_oracle(cuda_ok):
     lin = _fastlpr().cv_fastlpr(x, y, np.column_stack([hv, hv]), {"order": 1, "N": [40, 36]})
     assert lin.gcv_yhat["id1se"] == r.gcv_yhat["id1se"]
     np.testing.assert_allclose(lin.fpp_yhat.values, gv, rtol=1e-12)
+
+
+@pytest.mark.parametrize("kernel,d", [("tricube", 2), ("uniform", 1), ("epanechnikov", 3),
+                                      ("gaussian", 2)])
+def test_radial_kernel_spectra_match_oracle(cuda_ok, kernel, d):
+    """flpr_kernel_spectra (full-plane moment spectra of a radial kernel)
+    against the oracle's compute_kernel_fourier restatement."""
+    import torch
+    from fastlpr_b200 import api
+    rng = np.random.default_rng(d)
+    n = 500
+    x = rng.random((n, d)) * 3 - 1
+    G = np.array([20, 14, 9][:d])
+    bw = np.column_stack([np.array([0.15, 0.4, 0.9])] * d)
+    order = 1
+    ctx = api._Ctx(torch.device("cuda", 0))
+    stats = api._point_stats(ctx, ctx.upload(x), n, d)
+    geom = api._make_geom(stats, n, d, G, 4, True)
+    powers = oracle.lpr.element_powers(d, order)
+    K = api._kernel_spectra_full(ctx, geom, bw, powers, api._KERNEL_IDS[kernel])
+    xs = (x - geom.mean) / geom.std - geom.center
+    spectra, prm = oracle.kernel_spectra(xs, bw, G, order, kernel_type=kernel)
+    np.testing.assert_array_equal(prm["L"], geom.L)
+    half = int(geom.L[-1]) // 2 + 1
+    K = K.cpu().numpy()
+    K = K[..., 0] + 1j * K[..., 1]
+    for e, pw in enumerate(powers):
+        got = K[e].reshape((bw.shape[0],) + tuple(geom.L[:-1]) + (half,))
+        want = np.moveaxis(spectra[e], -1, 0)[..., :half]
+        assert rel_err(got, want) < 1e-12, (kernel, pw)

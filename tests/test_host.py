@@ -70,8 +70,11 @@ def test_unsupported_paths_raise_not_implemented():
     x3 = rng.random((50, 3))
     with pytest.raises(NotImplementedError):
         api.cv_fastlpr(x3, rng.random(50), [[0.3] * 3], {"accuracy": 7})
-    with pytest.raises(NotImplementedError):
-        api.cv_fastlpr(x1, rng.random(50), [[0.3]], {"kernel_type": "epanechnikov"})
+    # the reference calls kernel_function without options: polynomial fails there
+    with pytest.raises(ValueError, match="Polynomial"):
+        api.cv_fastlpr(x1, rng.random(50), [[0.3]], {"kernel_type": "polynomial"})
+    with pytest.raises(ValueError, match="Unknown kernel type"):
+        api.cv_fastlpr(x1, rng.random(50), [[0.3]], {"kernel_type": "cauchy"})
 
 
 @pytest.mark.parametrize("G,p2", [(np.array([64]), True), (np.array([512, 512]), True),
