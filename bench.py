@@ -49,6 +49,39 @@ def workload(seed: int, n: int = N_POINTS):
     return x, y, h, opts
 
 
+def batched_workload(seed: int = 7, count: int = 512, y_seed: int = 0):
+    """The batched uneven workload: `count` independent problems, half 1-D
+    (grid 1024) and half 2-D (grid 256^2), N lognormal (median 5e4, sigma 1)
+    clipped to [1e3, 1e6], orders drawn from {0, 1, 2}, 25% complex
+    responses y = exp(i 2 pi x1) + complex Gaussian noise (sigma 0.1), the
+    rest sums of 1-4 random sinusoids plus N(0, 0.1^2) noise, 24 isotropic
+    bandwidths in [0.005, 0.5].  The designs x depend on `seed` only; the
+    noise of the responses also on `y_seed`."""
+    rng = np.random.default_rng(seed)
+    hv = np.logspace(np.log10(0.005), np.log10(0.5), 24)
+    probs = []
+    for k in range(count):
+        d = 1 if k % 2 == 0 else 2
+        n = int(np.clip(np.round(5e4 * np.exp(rng.standard_normal())), 1e3, 1e6))
+        order = int(rng.integers(0, 3))
+        cplx = rng.random() < 0.25
+        x = rng.random((n, d))
+        nsin = int(rng.integers(1, 5))
+        freqs = rng.uniform(0.5, 6.0, (nsin, d))
+        phases = rng.uniform(0, 2 * np.pi, nsin)
+        amps = rng.uniform(0.5, 1.5, nsin)
+        ry = np.random.default_rng([seed, k, y_seed])
+        if cplx:
+            y = np.exp(2j * np.pi * x[:, 0]) + 0.1 * (ry.standard_normal(n)
+                                                       + 1j * ry.standard_normal(n))
+        else:
+            y = sum(a * np.sin(2 * np.pi * (x @ f) + ph) for a, f, ph in zip(amps, freqs, phases))
+            y = y + 0.1 * ry.standard_normal(n)
+        opts = {"order": order, "N": 1024 if d == 1 else [256, 256]}
+        probs.append((x, y, np.column_stack([hv] * d), opts))
+    return probs
+
+
 def b_fit(n=N_POINTS, d=2, G=512, H=N_H, R=R_PROBES, order=1, cy=1, parts=False):
     """Compulsory HBM bytes of one FFT-convolution fit (per-unit figure of the
     roofline): point passes, grid spread/FFT, inverse-pass intermediates and

@@ -15,6 +15,7 @@ from .api import cv_fastkde, cv_fastlpr, cv_fastlpr_device, clear_fastlpr_caches
 from .confidence import fastlpr_interval
 from .batch import (SharedData, batch_evaluate_at_points, compute_gcv_scores_batch,
                     cv_fastlpr_batch, precompute_shared)
+from .plan import LprPlan, cv_fastlpr_many
 
 import numpy as np
 
@@ -45,6 +46,8 @@ __all__ = [
     "cv_fastlpr_batch",
     "batch_evaluate_at_points",
     "compute_gcv_scores_batch",
+    "LprPlan",
+    "cv_fastlpr_many",
     "RegressionOutput",
     "KDEOutput",
     "clear_fastlpr_caches",

@@ -26,6 +26,8 @@ SIGNATURES = [
     ("flpr_last_error", C.c_char_p, []),
     ("flpr_version", _I, []),
     ("flpr_launch_count", _I64, []),
+    ("flpr_set_tuning", _I, [_I, _I]),
+    ("flpr_get_tuning", _I, [_I]),
     ("flpr_create", _I, [C.POINTER(_VP), _I]),
     ("flpr_destroy", _I, [_VP]),
     ("flpr_point_stats_ws", _SZ, [_I, _I64]),
@@ -44,6 +46,9 @@ SIGNATURES = [
     ("flpr_conv_full", _I, [_VP, _I, _PI, _PI, _PI, _I, _VP, _VP, _I, _PI, _PI, _D, _I, _VP, _I,
                             _VP, _SZ, _VP]),
     ("flpr_conv_ws", _SZ, [_VP, _I, _PI, _I, _I]),
+    ("flpr_conv2d_sep_ws", _SZ, [_VP, _PI, _PI, _I, _I]),
+    ("flpr_conv2d_sep", _I, [_VP, _PI, _PI, _PI, _I, _I, _VP, _VP, _I, _PI, _PI, _PI, _D, _I, _VP,
+                             _I, _VP, _SZ, _VP]),
     ("flpr_conv", _I, [_VP, _I, _PI, _PI, _PI, _I, _I, _VP, _VP, _I, _PI, _PI, _PI, _D, _I, _VP,
                        _I, _VP, _SZ, _VP]),
     ("flpr_solve", _I, [_I, _I, _I, _I, _I64, _I, _VP, _VP, _D, _VP, _VP, _I, _VP]),

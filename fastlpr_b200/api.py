@@ -553,6 +553,11 @@ def _spread_fft(ctx: _Ctx, geom: _Geom, dx: torch.Tensor, cols: List[torch.Tenso
     return spec
 
 
+# 2-D separable kernels take the two-pass convolution unless this is set
+# (the full 2-D inverse per product, kept for comparison)
+_CONV_FULL_2D = False
+
+
 def _conv(ctx: _Ctx, geom: _Geom, spec, kern: _Kernel, prods, prec: int, add_eps: bool):
     """Planes for a product list [(chan, hidx, pow tuple)] -> (nprod, M)."""
     d = geom.d
@@ -560,6 +565,19 @@ def _conv(ctx: _Ctx, geom: _Geom, spec, kern: _Kernel, prods, prec: int, add_eps
     real_dt = torch.float32 if prec == _lib.FLPR_PREC_F32 else torch.float64
     out = ctx.empty((nprod, geom.M), dtype=real_dt)
     chan = [p[0] for p in prods]
+    if kern.separable and d == 2 and not _CONV_FULL_2D:
+        hidx = [p[1] for p in prods]
+        pw = [v for p in prods for v in p[2]]
+        ws = ctx.ws(ctx.lib.flpr_conv2d_sep_ws(ctx.handle, _lib.ivec(geom.G), _lib.ivec(geom.L),
+                                               nprod, prec))
+        ctx.check(ctx.lib.flpr_conv2d_sep(ctx.handle, _lib.ivec(geom.G), _lib.ivec(geom.L),
+                                          _lib.ivec(geom.qout[0]), kern.H, kern.npow,
+                                          spec.data_ptr(), kern.data_ptr(), nprod,
+                                          _lib.ivec(chan), _lib.ivec(hidx), _lib.ivec(pw),
+                                          kern.scale, 1 if add_eps else 0, out.data_ptr(), prec,
+                                          ws.data_ptr(), ws.numel(), ctx.stream),
+                  "flpr_conv2d_sep")
+        return out
     ws = ctx.ws(ctx.lib.flpr_conv_ws(ctx.handle, d, _lib.ivec(geom.L), nprod, prec))
     if kern.separable:
         hidx = [p[1] for p in prods]
@@ -664,23 +682,15 @@ def _axes_arg(axes: Sequence[np.ndarray]) -> List[float]:
 # ---------------------------------------------------------------------------
 # cv_fastlpr
 # ---------------------------------------------------------------------------
-def cv_fastlpr(x, y, h=None, options: Optional[dict] = None) -> RegressionOutput:
-    """Local polynomial regression with GCV bandwidth selection (drop-in for the
-    reference ``cv_fastlpr``, api.py:167-832).
+class _LprSetup:
+    """Validated inputs and options of one cv_fastlpr call."""
 
-    Options are the reference's (order, regularization, num_dof_sample,
-    kernel_type, y_type_out, calc_dof, gcv_selection, accuracy, N, xrange, dh,
-    flag_power2, dstd, random_matrix, dof_seed, interp methods) plus
-    ``precision`` ('fp32' | 'fp64'; default follows the reference's dtype
-    rule: FP32 grids below accuracy 5), ``device`` and ``bandwidth_search``:
-    'full' (default, the reference's sweep of every bandwidth) or 'learned'
-    (the trained proposal network picks five neighbouring bandwidths of the
-    list; while their GCV minimum sits on an edge of that window the window
-    moves that way, at most three times, and otherwise the full sweep runs;
-    needs a list of isotropic, increasing bandwidths, a real single response,
-    the Gaussian kernel and d <= 2, else the full sweep runs).  ``metadata['bandwidth_search']``
-    records what happened.
-    """
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+def _lpr_setup(x, y, h, options) -> _LprSetup:
+    """Input checks and option defaults of cv_fastlpr (api.py:167-420)."""
     x_arr = _as_column_matrix(x)
     y_arr = np.asarray(y)
     if y_arr.ndim == 1:
@@ -727,8 +737,31 @@ def cv_fastlpr(x, y, h=None, options: Optional[dict] = None) -> RegressionOutput
         raise NotImplementedError("variance mode needs a real response")
     _check_interp_methods(opts, dims, n)
     prec = _precision(opts)
-    ctx = _Ctx(_device(opts))
-    search = str(opts.get("bandwidth_search", "full"))
+    return _LprSetup(x_arr=x_arr, y_arr=y_arr, dy=dy, bandwidths=bandwidths, opts=opts,
+                     order=order, prec=prec, variance=variance, y_is_complex=y_is_complex,
+                     n=n, d=dims)
+
+
+def cv_fastlpr(x, y, h=None, options: Optional[dict] = None) -> RegressionOutput:
+    """Local polynomial regression with GCV bandwidth selection (drop-in for the
+    reference ``cv_fastlpr``, api.py:167-832).
+
+    Options are the reference's (order, regularization, num_dof_sample,
+    kernel_type, y_type_out, calc_dof, gcv_selection, accuracy, N, xrange, dh,
+    flag_power2, dstd, random_matrix, dof_seed, interp methods) plus
+    ``precision`` ('fp32' | 'fp64'; default follows the reference's dtype
+    rule: FP32 grids below accuracy 5), ``device`` and ``bandwidth_search``:
+    'full' (default, the reference's sweep of every bandwidth) or 'learned'
+    (the trained proposal network picks five neighbouring bandwidths of the
+    list; while their GCV minimum sits on an edge of that window the window
+    moves that way, at most three times, and otherwise the full sweep runs;
+    needs a list of isotropic, increasing bandwidths, a real single response,
+    the Gaussian kernel and d <= 2, else the full sweep runs).  ``metadata['bandwidth_search']``
+    records what happened.
+    """
+    su = _lpr_setup(x, y, h, options)
+    ctx = _Ctx(_device(su.opts))
+    search = str(su.opts.get("bandwidth_search", "full"))
     if search not in ("full", "learned"):
         raise ValueError(f"bandwidth_search must be 'full' or 'learned', got {search!r}")
     with torch.cuda.device(ctx.device):
@@ -736,8 +769,9 @@ def cv_fastlpr(x, y, h=None, options: Optional[dict] = None) -> RegressionOutput
         if search == "learned":
             from . import learned as _learned
             model = _learned.default_model(ctx.device)
-        return _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance,
-                        y_is_complex, timings=opts.get("_timings"), learned=model)
+        return _fit_lpr(ctx, su.x_arr, su.y_arr, su.dy, su.bandwidths, su.opts, su.order,
+                        su.prec, su.variance, su.y_is_complex, timings=su.opts.get("_timings"),
+                        learned=model)
 
 
 def cv_fastlpr_device(x: torch.Tensor, y: torch.Tensor, h=None,
@@ -795,10 +829,13 @@ class _LprState:
 
 
 def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_complex,
-                 dev_inputs, ev, hook=None) -> _LprState:
+                 dev_inputs, ev, hook=None, stats=None, probes=None) -> _LprState:
     """Bandwidth-independent stage.  `hook(dx, ycols, stats, n, d)` runs after
     the point statistics, before the spread is enqueued (the learned search
-    starts its data summary there, on a side stream)."""
+    starts its data summary there, on a side stream).  With `stats` (the
+    point statistics of these device inputs, already checked) nothing here
+    waits for the device, so the stage can be captured in a CUDA graph
+    (`probes`: the (tensor, R) of _probes for these points, formed earlier)."""
     lib = ctx.lib
     st = _LprState()
     if dev_inputs is not None:
@@ -818,7 +855,7 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
                 ycols.append(ctx.upload(np.ascontiguousarray(col, dtype=float)))
     y_raw_dev = None
     flags_h = None
-    if dev_inputs is None:
+    if dev_inputs is None and stats is None:
         # NaN/Inf checks of the inputs (api.py:310-323) run on the device; the
         # flags come back with the point statistics' synchronisation
         flags_h = _to_host(_finite_flags([dx, torch.stack(ycols)]))
@@ -831,15 +868,18 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
         ycols = [ylog]
     ny = len(ycols)
     G = _grid_shape(opts, n, d)
-    stats = _point_stats(ctx, dx, n, d)
+    if stats is None:
+        stats = _point_stats(ctx, dx, n, d)
     if flags_h is not None:
         _raise_nonfinite(flags_h.numpy(), [("Input x", 0), ("Response y", 1)], "cv_fastlpr")
     geom = _make_geom(stats, n, d, G, int(opts["accuracy"]), bool(opts.get("flag_power2", True)))
     calc_dof = bool(opts.get("calc_dof", True))
     if calc_dof:
-        probes, R = _probes(ctx, n, int(opts.get("num_dof_sample", 10)),
-                            opts.get("dof_seed", 42), opts.get("random_matrix", None))
-        pcols = [probes[r] for r in range(R)]
+        if probes is None:
+            probes = _probes(ctx, n, int(opts.get("num_dof_sample", 10)),
+                             opts.get("dof_seed", 42), opts.get("random_matrix", None))
+        ptens, R = probes
+        pcols = [ptens[r] for r in range(R)]
     else:
         R = 0
         pcols = []
@@ -888,12 +928,21 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
 
 def _evaluate_lpr(ctx, st: _LprState, bandwidths: np.ndarray, ev) -> dict:
     """Kernel spectra, convolutions, solves and GCV for one bandwidth list."""
+    filt = _filter_bandwidths(ctx, st.geom, bandwidths, 2 * st.order + 1, st.kid)
+    r = _evaluate_device(ctx, st, filt, ev)
+    return _evaluate_host(st, r, r["packed"].cpu().numpy() if r["packed"] is not None else None)
+
+
+def _evaluate_device(ctx, st: _LprState, filt, ev) -> dict:
+    """Device part of the evaluation: convolutions, solves and the GCV/DoF
+    reductions, packed into one device vector (``packed``).  `filt` is the
+    result of _filter_bandwidths.  Nothing here waits for the device."""
     lib = ctx.lib
     d, n, ny, R, order, prec = st.d, st.n, st.ny, st.R, st.order, st.prec
     geom, spec, opts, calc_dof = st.geom, st.spec, st.opts, st.calc_dof
     ycols, pcols = st.ycols, st.pcols
     npow = 2 * order + 1
-    kern, bw, keep, _ = _filter_bandwidths(ctx, geom, bandwidths, npow, st.kid)
+    kern, bw, keep, _ = filt
     H = len(keep)
     epw = _element_powers(d, order)
     ns = len(epw)
@@ -943,15 +992,10 @@ def _evaluate_lpr(ctx, st: _LprState, bandwidths: np.ndarray, ev) -> dict:
                                         quad.data_ptr(), ctx.stream), "flpr_stencil_quad")
         ev.mark("interp_reduce")
         # one device -> host read for the three reductions
-        packed = torch.cat([st.sq.reshape(-1), dots.reshape(-1), quad.reshape(-1)]).cpu().numpy()
-        sq_h = packed[:Cv]
-        dots_h = packed[Cv:Cv + Cv * H].reshape(Cv, H)
-        quad_h = packed[Cv + Cv * H:].reshape(H, ny)
-        rss_h = sq_h[None, :ny] - 2.0 * dots_h[:ny].T + quad_h
-        pdot_h = dots_h[ny:]
-        pp_h = sq_h[ny:]
+        packed = torch.cat([st.sq.reshape(-1), dots.reshape(-1), quad.reshape(-1)])
         mstride = ny
     else:
+        packed = None
         m = ctx.empty((Ht, M, Cv))
         ctx.check(lib.flpr_solve(order, nt, H, Ht, M, Cv, S.data_ptr(), T.data_ptr(), reg,
                                  m.data_ptr(), scalar.data_ptr(), prec, ctx.stream), "flpr_solve")
@@ -985,25 +1029,55 @@ def _evaluate_lpr(ctx, st: _LprState, bandwidths: np.ndarray, ev) -> dict:
                               "flpr_spline_reduce")
                 red[method] = (rss, pdot, pp)
             ev.mark("interp_reduce")
-            rss_h = red[st.methods["gcv"]][0].cpu().numpy()
-            pdot_h = red[st.methods["dof"]][1].cpu().numpy()[:R]
-            pp_h = red[st.methods["dof"]][2].cpu().numpy()[:R]
-    if calc_dof:
-        gcv = _gcv_from_sums(n, rss_h, pdot_h, pp_h, st.dy, st.y_is_complex, opts)
-        dstd = float(opts.get("dstd", 0.0))
-        sel = _one_se_rule(gcv["gcv_m"], gcv["gcv_sd"], bw_k, prefer_smaller=True, dstd=dstd)
+            packed = torch.cat([red[st.methods["gcv"]][0].reshape(-1),
+                                red[st.methods["dof"]][1].reshape(-1),
+                                red[st.methods["dof"]][2].reshape(-1)])
+    return dict(keep=keep, bw_k=bw_k, H=H, m=m, S=S, ns=ns, mstride=mstride, packed=packed,
+                dual=st.dual)
+
+
+def _evaluate_host(st: _LprState, r: dict, packed: Optional[np.ndarray]) -> dict:
+    """GCV, DoF and the 1-SE choice from the downloaded reductions."""
+    n, ny, R, H = st.n, st.ny, st.R, r["H"]
+    Cv = ny + R
+    if st.calc_dof:
+        if r["dual"]:
+            sq_h = packed[:Cv]
+            dots_h = packed[Cv:Cv + Cv * H].reshape(Cv, H)
+            quad_h = packed[Cv + Cv * H:].reshape(H, ny)
+            rss_h = sq_h[None, :ny] - 2.0 * dots_h[:ny].T + quad_h
+            pdot_h = dots_h[ny:]
+            pp_h = sq_h[ny:]
+        else:
+            Rm = max(R, 1)
+            rss_h = packed[:H * ny].reshape(H, ny)
+            pdot_h = packed[H * ny:H * ny + Rm * H].reshape(Rm, H)[:R]
+            pp_h = packed[H * ny + Rm * H:][:R]
+        gcv = _gcv_from_sums(n, rss_h, pdot_h, pp_h, st.dy, st.y_is_complex, st.opts)
+        dstd = float(st.opts.get("dstd", 0.0))
+        sel = _one_se_rule(gcv["gcv_m"], gcv["gcv_sd"], r["bw_k"], prefer_smaller=True,
+                           dstd=dstd)
     else:
         gcv = None
         sel = 0
-    return dict(keep=keep, bw_k=bw_k, H=H, m=m, S=S, ns=ns, mstride=mstride, gcv=gcv, sel=sel)
+    return dict(r, gcv=gcv, sel=sel)
 
 
 def _finalize_lpr(ctx, st: _LprState, r: dict, ev, search) -> RegressionOutput:
     """Fitted values at the selected bandwidth and the result structure."""
+    pend = _finalize_enqueue(ctx, st, r, ev)
+    torch.cuda.current_stream(ctx.device).synchronize()
+    return _finalize_build(ctx, st, r, pend, ev, search)
+
+
+def _finalize_enqueue(ctx, st: _LprState, r: dict, ev) -> dict:
+    """Device part of the output stage: fitted values at the selected
+    bandwidth, residuals, grid and s0 copied into pinned host memory
+    (asynchronously; valid after the stream synchronises)."""
     lib = ctx.lib
-    d, n, ny, dy = st.d, st.n, st.ny, st.dy
-    geom, opts = st.geom, st.opts
-    bw_k, sel, gcv, m, S = r["bw_k"], r["sel"], r["gcv"], r["m"], r["S"]
+    d, n, ny = st.d, st.n, st.ny
+    geom = st.geom
+    sel, m, S = r["sel"], r["m"], r["S"]
     H, ns, M = r["H"], r["ns"], geom.M
     mv = m[sel if st.calc_dof else 0]                # (M, mstride)
     gv_dev = mv[:, :ny].t().contiguous()             # (ny, M)
@@ -1019,14 +1093,15 @@ def _finalize_lpr(ctx, st: _LprState, r: dict, ev, search) -> RegressionOutput:
         ctx.check(lib.flpr_interp_eval(d, n, st.dx.data_ptr(), st.ax_arg, st.G_arg, ny,
                                        gv_dev.data_ptr(), yhat_dev.data_ptr(), ctx.stream),
                   "flpr_interp_eval")
-    d_norm = None
+    dn = None
     if st.variance:
         acc = ctx.empty(1)
         ctx.check(lib.flpr_exp_weighted_sum(n, st.y_raw_dev.data_ptr(), yhat_dev.data_ptr(),
                                             acc.data_ptr(), ctx.stream), "flpr_exp_weighted_sum")
-        d_norm = 1.0 / ((1.0 / n) * float(acc.item()))
-        yhat_dev = torch.exp(yhat_dev) / d_norm
-        gv_dev = torch.exp(gv_dev) / d_norm
+        # d = 1 / mean(y exp(-yhat)) (api.py:777-786), kept on the device
+        dn = 1.0 / ((1.0 / n) * acc)
+        yhat_dev = torch.exp(yhat_dev) / dn
+        gv_dev = torch.exp(gv_dev) / dn
     ev.mark("final_interp")
     # residuals on the device; every result is copied into pinned host memory
     # with one synchronisation (the caching host allocator recycles the pages)
@@ -1034,12 +1109,19 @@ def _finalize_lpr(ctx, st: _LprState, r: dict, ev, search) -> RegressionOutput:
         res_dev = st.y_raw_dev[None, :] - yhat_dev
     else:
         res_dev = torch.stack(st.ycols[:ny], dim=0) - yhat_dev
-    yh = _to_host(yhat_dev)
-    rh = _to_host(res_dev)
-    gvh = _to_host(gv_dev)
-    s0h = _to_host(S.view(ns, H, M)[0, sel])
-    torch.cuda.current_stream(ctx.device).synchronize()
-    yh, rh, gvh = yh.numpy(), rh.numpy(), gvh.numpy()
+    return {"yh": _to_host(yhat_dev), "rh": _to_host(res_dev), "gvh": _to_host(gv_dev),
+            "s0h": _to_host(S.view(ns, H, M)[0, sel]),
+            "dn": _to_host(dn) if dn is not None else None}
+
+
+def _finalize_build(ctx, st: _LprState, r: dict, pend: dict, ev, search) -> RegressionOutput:
+    """Result structure from the downloaded outputs of _finalize_enqueue."""
+    d, dy = st.d, st.dy
+    geom, opts = st.geom, st.opts
+    bw_k, sel, gcv = r["bw_k"], r["sel"], r["gcv"]
+    yh, rh, gvh = pend["yh"].numpy(), pend["rh"].numpy(), pend["gvh"].numpy()
+    s0h = pend["s0h"]
+    d_norm = float(pend["dn"].numpy()[0]) if pend["dn"] is not None else None
     gshape = tuple(int(g) for g in geom.G)
     if st.y_is_complex:
         yh = yh[0::2] + 1j * yh[1::2]

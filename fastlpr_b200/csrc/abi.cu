@@ -13,6 +13,13 @@ static std::atomic<long long> g_launches{0};
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+// defaults and ranges of the FLPR_TUNE_* parameters
+static std::atomic<int> g_tune[FLPR_TUNE_COUNT] = {{4096}, {192}};
+static const int kTuneMin[FLPR_TUNE_COUNT] = {256, 8};
+static const int kTuneMax[FLPR_TUNE_COUNT] = {65536, 16384};
+
+int tuning(int param) { return g_tune[param].load(std::memory_order_relaxed); }
+
 void set_error(const char* fmt, ...) {
   va_list ap;
   va_start(ap, fmt);
@@ -37,7 +44,10 @@ int PlanCache::get(const PlanKey& key, Plan** out) {
   int rank = key.rank;
   int n[3] = {key.n[0], key.n[1], key.n[2]};
   size_t ws = 0;
-  cufftResult r = cufftMakePlanMany(p.plan, rank, n, nullptr, 1, key.idist, nullptr, 1, key.odist,
+  const int stride = key.stride > 1 ? key.stride : 1;
+  int emb[3] = {n[0], n[1], n[2]};
+  cufftResult r = cufftMakePlanMany(p.plan, rank, n, stride > 1 ? emb : nullptr, stride, key.idist,
+                                    stride > 1 ? emb : nullptr, stride, key.odist,
                                     static_cast<cufftType>(key.type), key.batch, &ws);
   if (r != CUFFT_SUCCESS) {
     cufftDestroy(p.plan);
@@ -76,7 +86,11 @@ int PlanCache::exec(const PlanKey& key, void* in, void* out, void* work, size_t 
       break;
     case CUFFT_Z2Z:
       FLPR_CUFFT(cufftExecZ2Z(p->plan, (cufftDoubleComplex*)in, (cufftDoubleComplex*)out,
-                              CUFFT_FORWARD));
+                              key.inverse ? CUFFT_INVERSE : CUFFT_FORWARD));
+      break;
+    case CUFFT_C2C:
+      FLPR_CUFFT(cufftExecC2C(p->plan, (cufftComplex*)in, (cufftComplex*)out,
+                              key.inverse ? CUFFT_INVERSE : CUFFT_FORWARD));
       break;
     default:
       set_error("unsupported FFT type %d", key.type);
@@ -110,6 +124,20 @@ const char* flpr_last_error(void) { return flpr::g_err; }
 int flpr_version(void) { return 100; }
 
 int64_t flpr_launch_count(void) { return (int64_t)flpr::g_launches.load(); }
+
+int flpr_set_tuning(int param, int value) {
+  FLPR_CHECK_ARG(param >= 0 && param < FLPR_TUNE_COUNT, "set_tuning: param=%d", param);
+  FLPR_CHECK_ARG(value >= flpr::kTuneMin[param] && value <= flpr::kTuneMax[param],
+                 "set_tuning: value %d of param %d outside [%d, %d]", value, param,
+                 flpr::kTuneMin[param], flpr::kTuneMax[param]);
+  flpr::g_tune[param].store(value, std::memory_order_relaxed);
+  return FLPR_OK;
+}
+
+int flpr_get_tuning(int param) {
+  if (param < 0 || param >= FLPR_TUNE_COUNT) return -1;
+  return flpr::tuning(param);
+}
 
 int flpr_create(flpr_handle_t* out, int device) {
   FLPR_CHECK_ARG(out != nullptr, "flpr_create: null output pointer");

@@ -22,6 +22,8 @@ void set_error(const char* fmt, ...);
 
 // Number of kernels this library has launched (flpr_launch_count()).
 void count_launch();
+// process-wide tuning parameters (flpr_set_tuning)
+int tuning(int param);
 
 #define FLPR_CHECK_ARG(cond, ...)            \
   do {                                       \

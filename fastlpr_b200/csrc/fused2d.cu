@@ -749,12 +749,8 @@ static int fused_geom(const int* G, const int* L, const int* qout, int H, const 
   fg->M = (int64_t)G[0] * G[1];
   const size_t slab = (size_t)fg->G0 * fg->L1h;  // float2 per (slot, h)
   // chunks of a few bandwidths: enough row-pass CTAs to fill the GPU with a
-  // bounded column-pass output (override: FLPR_FUSED_CHUNK_MB)
-  size_t budget = (size_t)192 << 20;
-  if (const char* env = getenv("FLPR_FUSED_CHUNK_MB")) {
-    const long mb = atol(env);
-    if (mb >= 1 && mb <= 65536) budget = (size_t)mb << 20;
-  }
+  // bounded column-pass output (FLPR_TUNE_FUSED_CHUNK_MB)
+  size_t budget = (size_t)tuning(FLPR_TUNE_FUSED_CHUNK_MB) << 20;
   const size_t budget_s = budget, budget_t = budget;
   int hs = (int)(budget_s / (sizeof(float2) * slab * t.s_nslots));
   int ht = (int)(budget_t / (sizeof(float2) * slab * t.t_nslots));

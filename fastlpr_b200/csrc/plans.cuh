@@ -13,9 +13,12 @@ struct PlanKey {
   int batch;
   int idist;
   int odist;
+  int stride;   // element stride of input and output (0 or 1: contiguous)
+  int inverse;  // C2C / Z2Z direction
   bool operator<(const PlanKey& o) const {
-    return std::tie(rank, n[0], n[1], n[2], type, batch, idist, odist) <
-           std::tie(o.rank, o.n[0], o.n[1], o.n[2], o.type, o.batch, o.idist, o.odist);
+    return std::tie(rank, n[0], n[1], n[2], type, batch, idist, odist, stride, inverse) <
+           std::tie(o.rank, o.n[0], o.n[1], o.n[2], o.type, o.batch, o.idist, o.odist, o.stride,
+                    o.inverse);
   }
 };
 

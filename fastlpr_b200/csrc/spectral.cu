@@ -1,6 +1,10 @@
 // Forward FFT of the spread grids, separable kernel-moment spectra and the
 // batched spectral multiply + inverse FFT + crop.
 #include <cfloat>
+#include <algorithm>
+#include <map>
+#include <tuple>
+#include <vector>
 
 #include "common.cuh"
 #include "plans.cuh"
@@ -253,6 +257,103 @@ __global__ void product_full_kernel(ConvArgs ca, int nb, ProdBatch desc,
     o.x = (Real)((double)sv.x * kr - (double)sv.y * ki);
     o.y = (Real)((double)sv.x * ki + (double)sv.y * kr);
     out[t] = o;
+  }
+}
+
+// ---- 2-D separable convolution -----------------------------------------------
+// The kernel spectrum factors as A0(w0) A1(w1): a column pass (times A0,
+// inverse FFT along axis 0, rows q0..q0+G0-1 kept) shared by every product
+// with the same (channel, bandwidth, axis-0 exponent), then a row pass per
+// product (times A1 and the scale, C2R along axis 1, columns q1..q1+G1-1).
+constexpr int kSepMax = 256;  // jobs per column chunk / products per row batch
+
+struct SepJobs {
+  int chan[kSepMax], hidx[kSepMax], p0[kSepMax];
+};
+
+struct SepProds {
+  int job[kSepMax], hidx[kSepMax], p1[kSepMax], out[kSepMax];
+};
+
+struct SepArgs {
+  int L0, L1, L1h, G0, G1, q0, q1, npow;
+  int64_t f1off;  // start of the axis-1 factors in F
+  double scale;
+};
+
+// colbuf (L0, Jc, L1h) = spec[chan_j](w0, w1) * A0_{h_j, p0_j}(w0)
+template <typename Real>
+__global__ void sep_colprod_kernel(SepArgs sa, int jc, int nj, SepJobs jobs,
+                                   const typename Cplx<Real>::type* __restrict__ spec,
+                                   const double2* __restrict__ F,
+                                   typename Cplx<Real>::type* __restrict__ col) {
+  using C = typename Cplx<Real>::type;
+  const int64_t total = (int64_t)sa.L0 * jc * sa.L1h;
+  const int64_t half = (int64_t)sa.L0 * sa.L1h;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int w1 = (int)(t % sa.L1h);
+    const int64_t r = t / sa.L1h;
+    const int j = (int)(r % jc);
+    const int w0 = (int)(r / jc);
+    C o;
+    if (j < nj) {
+      const double2 f = F[((int64_t)jobs.hidx[j] * sa.npow + jobs.p0[j]) * sa.L0 + w0];
+      const C v = spec[(int64_t)jobs.chan[j] * half + (int64_t)w0 * sa.L1h + w1];
+      o.x = (Real)((double)v.x * f.x - (double)v.y * f.y);
+      o.y = (Real)((double)v.x * f.y + (double)v.y * f.x);
+    } else {
+      o.x = (Real)0;
+      o.y = (Real)0;
+    }
+    col[t] = o;
+  }
+}
+
+// rowbuf (P, G0, L1h) = col(q0 + x0, job_p, w1) * A1_{h_p, p1_p}(w1) * scale
+template <typename Real>
+__global__ void sep_rowprod_kernel(SepArgs sa, int jc, int np, int pc, SepProds prods,
+                                   const typename Cplx<Real>::type* __restrict__ col,
+                                   const double2* __restrict__ F,
+                                   typename Cplx<Real>::type* __restrict__ row) {
+  using C = typename Cplx<Real>::type;
+  const int64_t total = (int64_t)pc * sa.G0 * sa.L1h;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int w1 = (int)(t % sa.L1h);
+    const int64_t r = t / sa.L1h;
+    const int x0 = (int)(r % sa.G0);
+    const int p = (int)(r / sa.G0);
+    C o;
+    if (p < np) {
+      const double2 f = F[sa.f1off + ((int64_t)prods.hidx[p] * sa.npow + prods.p1[p]) * sa.L1 + w1];
+      const double fr = f.x * sa.scale, fi = f.y * sa.scale;
+      const C v = col[((int64_t)(sa.q0 + x0) * jc + prods.job[p]) * sa.L1h + w1];
+      o.x = (Real)((double)v.x * fr - (double)v.y * fi);
+      o.y = (Real)((double)v.x * fi + (double)v.y * fr);
+    } else {
+      o.x = (Real)0;
+      o.y = (Real)0;
+    }
+    row[t] = o;
+  }
+}
+
+// out[prod.out][x0 * G1 + x1] = real(q1 + x1) of row (p, x0)
+template <typename Real>
+__global__ void sep_crop_kernel(SepArgs sa, int np, SepProds prods, const Real* __restrict__ real,
+                                int add_eps, Real* __restrict__ out) {
+  const int64_t M = (int64_t)sa.G0 * sa.G1;
+  const int64_t total = (int64_t)np * M;
+  const double eps = 2.220446049250313e-16;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int p = (int)(t / M);
+    const int64_t g = t - (int64_t)p * M;
+    const int x0 = (int)(g / sa.G1), x1 = (int)(g - (int64_t)x0 * sa.G1);
+    Real v = real[((int64_t)p * sa.G0 + x0) * sa.L1 + sa.q1 + x1];
+    if (add_eps) v = (Real)((double)v + eps);
+    out[(int64_t)prods.out[p] * M + g] = v;
   }
 }
 
@@ -524,6 +625,175 @@ int flpr_conv(flpr_handle_t handle, int d, const int* h_G, const int* h_L, const
                                              (double*)d_out);
     }
     FLPR_LAUNCH_CHECK();
+  }
+  return FLPR_OK;
+}
+
+
+struct SepSizes {
+  int jc, pc;
+  size_t col_bytes, row_bytes, real_bytes;
+};
+
+static SepSizes sep_sizes(const int* G, const int* L, int nprod, int prec) {
+  SepSizes z{};
+  const size_t es = prec == FLPR_PREC_F32 ? 4 : 8;
+  const int L1h = L[1] / 2 + 1;
+  const size_t budget = (size_t)256 << 20;
+  const size_t per_job = (size_t)L[0] * L1h * 2 * es;
+  const size_t per_prod = (size_t)G[0] * (L1h * 2 + L[1]) * es;
+  int64_t jc = (int64_t)(budget / per_job), pc = (int64_t)(budget / per_prod);
+  z.jc = (int)std::max<int64_t>(1, std::min<int64_t>({jc, (int64_t)kSepMax, (int64_t)nprod}));
+  z.pc = (int)std::max<int64_t>(1, std::min<int64_t>({pc, (int64_t)kSepMax, (int64_t)nprod}));
+  z.col_bytes = per_job * z.jc;
+  z.row_bytes = (size_t)z.pc * G[0] * L1h * 2 * es;
+  z.real_bytes = (size_t)z.pc * G[0] * L[1] * es;
+  return z;
+}
+
+static PlanKey sep_col_plan(const int* L, int jc, int prec) {
+  PlanKey k{};
+  k.rank = 1;
+  k.n[0] = L[0];
+  k.type = prec == FLPR_PREC_F32 ? CUFFT_C2C : CUFFT_Z2Z;
+  k.batch = jc * (L[1] / 2 + 1);
+  k.stride = jc * (L[1] / 2 + 1);
+  k.idist = 1;
+  k.odist = 1;
+  k.inverse = 1;
+  return k;
+}
+
+static PlanKey sep_row_plan(const int* G, const int* L, int pc, int prec) {
+  PlanKey k{};
+  k.rank = 1;
+  k.n[0] = L[1];
+  k.type = prec == FLPR_PREC_F32 ? CUFFT_C2R : CUFFT_Z2D;
+  k.batch = pc * G[0];
+  k.idist = L[1] / 2 + 1;
+  k.odist = L[1];
+  return k;
+}
+
+size_t flpr_conv2d_sep_ws(flpr_handle_t handle, const int* h_G, const int* h_L, int nprod,
+                          int prec) {
+  if (nprod < 1) return 0;
+  const SepSizes z = sep_sizes(h_G, h_L, nprod, prec);
+  size_t w1 = 0, w2 = 0;
+  if (plans_of(handle).work_size(sep_col_plan(h_L, z.jc, prec), &w1) != FLPR_OK) return 0;
+  if (plans_of(handle).work_size(sep_row_plan(h_G, h_L, z.pc, prec), &w2) != FLPR_OK) return 0;
+  ArenaSize ar;
+  ar.take<char>(z.col_bytes);
+  ar.take<char>(z.row_bytes);
+  ar.take<char>(z.real_bytes);
+  ar.take<char>(w1 > w2 ? w1 : w2);
+  return ar.used;
+}
+
+int flpr_conv2d_sep(flpr_handle_t handle, const int* h_G, const int* h_L, const int* h_qout,
+                    int H, int npow, const void* d_spec, const void* d_F, int nprod,
+                    const int* h_chan, const int* h_hidx, const int* h_pow, double scale,
+                    int add_eps, void* d_out, int prec, void* d_ws, size_t ws_bytes,
+                    void* stream) {
+  FLPR_CHECK_ARG(nprod >= 1 && H >= 1 && npow >= 1, "conv2d_sep: nprod=%d H=%d npow=%d", nprod,
+                 H, npow);
+  for (int a = 0; a < 2; ++a)
+    FLPR_CHECK_ARG(h_qout[a] >= 0 && h_qout[a] + h_G[a] <= h_L[a] && h_G[a] >= 1,
+                   "conv2d_sep: crop window");
+  for (int p = 0; p < nprod; ++p) {
+    FLPR_CHECK_ARG(h_hidx[p] >= 0 && h_hidx[p] < H, "conv2d_sep: hidx[%d]=%d", p, h_hidx[p]);
+    FLPR_CHECK_ARG(h_pow[2 * p] >= 0 && h_pow[2 * p] < npow && h_pow[2 * p + 1] >= 0 &&
+                       h_pow[2 * p + 1] < npow,
+                   "conv2d_sep: pow out of range");
+    FLPR_CHECK_ARG(h_chan[p] >= 0, "conv2d_sep: chan[%d]=%d", p, h_chan[p]);
+  }
+  if (ws_bytes < flpr_conv2d_sep_ws(handle, h_G, h_L, nprod, prec)) {
+    set_error("conv2d_sep: workspace too small");
+    return FLPR_ERR_WORKSPACE;
+  }
+  const SepSizes z = sep_sizes(h_G, h_L, nprod, prec);
+  SepArgs sa{};
+  sa.L0 = h_L[0];
+  sa.L1 = h_L[1];
+  sa.L1h = h_L[1] / 2 + 1;
+  sa.G0 = h_G[0];
+  sa.G1 = h_G[1];
+  sa.q0 = h_qout[0];
+  sa.q1 = h_qout[1];
+  sa.npow = npow;
+  sa.f1off = (int64_t)H * npow * h_L[0];
+  sa.scale = scale;
+  Arena ar(d_ws, ws_bytes);
+  char* col = ar.take<char>(z.col_bytes);
+  char* row = ar.take<char>(z.row_bytes);
+  char* real = ar.take<char>(z.real_bytes);
+  size_t work_bytes = ar.size - align_up(ar.used);
+  char* work = ar.take<char>(1);
+  cudaStream_t s = as_stream(stream);
+  // column jobs: distinct (channel, bandwidth, axis-0 exponent), first-seen order
+  std::vector<int> job_of(nprod);
+  std::map<std::tuple<int, int, int>, int> ids;
+  std::vector<std::tuple<int, int, int>> jobs;
+  for (int p = 0; p < nprod; ++p) {
+    auto key = std::make_tuple(h_chan[p], h_hidx[p], h_pow[2 * p]);
+    auto it = ids.find(key);
+    if (it == ids.end()) {
+      it = ids.emplace(key, (int)jobs.size()).first;
+      jobs.push_back(key);
+    }
+    job_of[p] = it->second;
+  }
+  const int njobs = (int)jobs.size();
+  const PlanKey colk = sep_col_plan(h_L, z.jc, prec), rowk = sep_row_plan(h_G, h_L, z.pc, prec);
+  std::vector<int> members;
+  for (int j0 = 0; j0 < njobs; j0 += z.jc) {
+    const int nj = std::min(z.jc, njobs - j0);
+    SepJobs sj{};
+    for (int j = 0; j < nj; ++j) {
+      sj.chan[j] = std::get<0>(jobs[j0 + j]);
+      sj.hidx[j] = std::get<1>(jobs[j0 + j]);
+      sj.p0[j] = std::get<2>(jobs[j0 + j]);
+    }
+    const int cb = grid_blocks((int64_t)sa.L0 * z.jc * sa.L1h);
+    if (prec == FLPR_PREC_F32)
+      sep_colprod_kernel<float><<<cb, 256, 0, s>>>(sa, z.jc, nj, sj, (const float2*)d_spec,
+                                                   (const double2*)d_F, (float2*)col);
+    else
+      sep_colprod_kernel<double><<<cb, 256, 0, s>>>(sa, z.jc, nj, sj, (const double2*)d_spec,
+                                                    (const double2*)d_F, (double2*)col);
+    FLPR_LAUNCH_CHECK();
+    FLPR_TRY(plans_of(handle).exec(colk, col, col, work, work_bytes, s));
+    members.clear();
+    for (int p = 0; p < nprod; ++p)
+      if (job_of[p] >= j0 && job_of[p] < j0 + nj) members.push_back(p);
+    for (size_t m0 = 0; m0 < members.size(); m0 += z.pc) {
+      const int np = (int)std::min<size_t>(z.pc, members.size() - m0);
+      SepProds sp{};
+      for (int q = 0; q < np; ++q) {
+        const int p = members[m0 + q];
+        sp.job[q] = job_of[p] - j0;
+        sp.hidx[q] = h_hidx[p];
+        sp.p1[q] = h_pow[2 * p + 1];
+        sp.out[q] = p;
+      }
+      const int rb = grid_blocks((int64_t)z.pc * sa.G0 * sa.L1h);
+      if (prec == FLPR_PREC_F32)
+        sep_rowprod_kernel<float><<<rb, 256, 0, s>>>(sa, z.jc, np, z.pc, sp, (const float2*)col,
+                                                     (const double2*)d_F, (float2*)row);
+      else
+        sep_rowprod_kernel<double><<<rb, 256, 0, s>>>(sa, z.jc, np, z.pc, sp, (const double2*)col,
+                                                      (const double2*)d_F, (double2*)row);
+      FLPR_LAUNCH_CHECK();
+      FLPR_TRY(plans_of(handle).exec(rowk, row, real, work, work_bytes, s));
+      const int ob = grid_blocks((int64_t)np * sa.G0 * sa.G1);
+      if (prec == FLPR_PREC_F32)
+        sep_crop_kernel<float><<<ob, 256, 0, s>>>(sa, np, sp, (const float*)real, add_eps,
+                                                  (float*)d_out);
+      else
+        sep_crop_kernel<double><<<ob, 256, 0, s>>>(sa, np, sp, (const double*)real, add_eps,
+                                                   (double*)d_out);
+      FLPR_LAUNCH_CHECK();
+    }
   }
   return FLPR_OK;
 }

@@ -6,7 +6,7 @@
 //                    scale of the FP32 path).
 //   2. tile_scan   : exclusive scans of the histogram and of the number of
 //                    work items per tile (a tile is split into chunks of at
-//                    most kItemPoints points).
+//                    most FLPR_TUNE_SPREAD_ITEM_POINTS points).
 //   3. bin_scatter : point indices sorted by tile.
 //   4. tile_accumulate : one CTA per work item; every point of the chunk is
 //                    spread into a shared-memory copy of its tile plus a
@@ -22,7 +22,7 @@
 
 namespace flpr {
 
-constexpr int kItemPoints = 4096;
+// points per work item: tuning(FLPR_TUNE_SPREAD_ITEM_POINTS), carried in SpreadGeom
 constexpr int kSpreadThreads = 256;
 constexpr int kMaxTaps1 = 25;  // 2*msp+1 for msp <= 12 (msp = 0: binning with weight 1)
 
@@ -37,6 +37,7 @@ struct SpreadGeom {
   int64_t cells;   // prod(L)
   int tile_cells;  // prod(W)
   int ntiles;
+  int item_points;  // points per work item (one CTA)
   double four_tau[3];
   KnotAxis ax[3];
 };
@@ -101,43 +102,66 @@ __global__ void bin_count_kernel(SpreadGeom g, int64_t n, const double* __restri
   }
 }
 
-// Single-block exclusive scans over the tile histogram.
-__global__ void tile_scan_kernel(int ntiles, const int* __restrict__ counts,
+// Single-block exclusive scans over the tile histogram (points and work
+// items per tile): per 1024-tile chunk a warp-shuffle scan, the warp totals
+// scanned by warp 0, and a running carry.  Launched with 1024 threads.
+__global__ void tile_scan_kernel(int ntiles, int item_points, const int* __restrict__ counts,
                                  int* __restrict__ offsets, int* __restrict__ items,
                                  int* __restrict__ cursor) {
-  __shared__ int sh_a[1024];
-  __shared__ int sh_b[1024];
+  __shared__ int wa[32], wb[32];
   __shared__ int carry_a, carry_b;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) {
     carry_a = 0;
     carry_b = 0;
   }
   __syncthreads();
   for (int base = 0; base < ntiles; base += blockDim.x) {
-    int t = base + threadIdx.x;
-    int c = t < ntiles ? counts[t] : 0;
-    int a = c;
-    int b = (c + kItemPoints - 1) / kItemPoints;
-    sh_a[threadIdx.x] = a;
-    sh_b[threadIdx.x] = b;
-    __syncthreads();
-    for (int s = 1; s < blockDim.x; s <<= 1) {
-      int va = threadIdx.x >= s ? sh_a[threadIdx.x - s] : 0;
-      int vb = threadIdx.x >= s ? sh_b[threadIdx.x - s] : 0;
-      __syncthreads();
-      sh_a[threadIdx.x] += va;
-      sh_b[threadIdx.x] += vb;
-      __syncthreads();
+    const int t = base + threadIdx.x;
+    const int c = t < ntiles ? counts[t] : 0;
+    const int a = c;
+    const int b = (c + item_points - 1) / item_points;
+    int ia = a, ib = b;  // inclusive warp scans
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int va = __shfl_up_sync(0xffffffffu, ia, o);
+      const int vb = __shfl_up_sync(0xffffffffu, ib, o);
+      if (lane >= o) {
+        ia += va;
+        ib += vb;
+      }
     }
+    if (lane == 31) {
+      wa[warp] = ia;
+      wb[warp] = ib;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      int xa = wa[lane], xb = wb[lane];  // 32 warps of 32 threads
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int va = __shfl_up_sync(0xffffffffu, xa, o);
+        const int vb = __shfl_up_sync(0xffffffffu, xb, o);
+        if (lane >= o) {
+          xa += va;
+          xb += vb;
+        }
+      }
+      wa[lane] = xa;  // inclusive warp totals
+      wb[lane] = xb;
+    }
+    __syncthreads();
+    const int pa = carry_a + (warp ? wa[warp - 1] : 0) + ia - a;
+    const int pb = carry_b + (warp ? wb[warp - 1] : 0) + ib - b;
     if (t < ntiles) {
-      offsets[t] = carry_a + sh_a[threadIdx.x] - a;
-      items[t] = carry_b + sh_b[threadIdx.x] - b;
+      offsets[t] = pa;
+      items[t] = pb;
       cursor[t] = 0;
     }
     __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) {
-      carry_a += sh_a[threadIdx.x];
-      carry_b += sh_b[threadIdx.x];
+    if (threadIdx.x == 0) {
+      carry_a += wa[31];
+      carry_b += wb[31];
     }
     __syncthreads();
   }
@@ -211,7 +235,7 @@ __device__ __forceinline__ double fixed_scale(double absum, int margin_bits) {
 __device__ __forceinline__ float fexp(float v) { return expf(v); }
 __device__ __forceinline__ double fexp(double v) { return exp(v); }
 
-// One CTA per work item (a tile, or a chunk of at most kItemPoints points of
+// One CTA per work item (a tile, or a chunk of at most g.item_points points of
 // a tile).  Threads take (point, tap row) pairs: a tap row fixes the tap
 // offsets of all axes but the last, and the thread walks the NT1 taps of the
 // last axis, adding every channel of the point into the shared-memory copy of
@@ -238,8 +262,8 @@ tile_accumulate_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, int
     if (items[mid] <= item) lo = mid; else hi = mid;
   }
   const int tile = lo;
-  const int p_begin = offsets[tile] + (item - items[tile]) * kItemPoints;
-  const int p_end = min(offsets[tile + 1], p_begin + kItemPoints);
+  const int p_begin = offsets[tile] + (item - items[tile]) * g.item_points;
+  const int p_end = min(offsets[tile + 1], p_begin + g.item_points);
   int tcoord[3] = {0, 0, 0};
   {
     int r = tile;
@@ -393,8 +417,8 @@ tile_accumulate_2d_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, 
     if (items[mid] <= item) lo = mid; else hi = mid;
   }
   const int tile = lo;
-  const int p_begin = offsets[tile] + (item - items[tile]) * kItemPoints;
-  const int p_end = min(offsets[tile + 1], p_begin + kItemPoints);
+  const int p_begin = offsets[tile] + (item - items[tile]) * g.item_points;
+  const int p_end = min(offsets[tile + 1], p_begin + g.item_points);
   const int tc0 = tile / g.ntile[1], tc1 = tile - tc0 * g.ntile[1];
 
   for (int i = threadIdx.x; i < nc * CS; i += blockDim.x) acc[i] = Acc(0);
@@ -549,6 +573,7 @@ static void make_geom(SpreadGeom& g, int d, const int* L, int msp, const double*
   g.d = d;
   g.msp = msp;
   g.ntaps1 = 2 * msp + 1;
+  g.item_points = tuning(FLPR_TUNE_SPREAD_ITEM_POINTS);
   static const int tile2[3] = {16, 16, 1};
   static const int tile3[3] = {8, 8, 8};
   g.cells = 1;
@@ -739,6 +764,16 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
   cudaStream_t s = as_stream(stream);
   SpreadGeom g;
   make_geom(g, d, h_L, msp, h_tau, h_kmap);
+  {
+    // few tiles (small 1-D grids): smaller work items, about four per SM
+    const int64_t target = 4LL * sm_count();
+    if (g.ntiles < target) {
+      const int64_t per = (n + target - 1) / target;
+      int ip = 256;
+      while (ip < per && ip < g.item_points) ip <<= 1;
+      if (ip < g.item_points) g.item_points = ip;
+    }
+  }
   ChanPtrs cp;
   memset(&cp, 0, sizeof(cp));
   for (int c = 0; c < nchan - ones_channel; ++c) cp.col[c] = h_cols[c];
@@ -757,7 +792,8 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
   bin_count_kernel<<<nb, 256, 0, s>>>(g, n, d_x, w.point_tile, w.counts, nchan, ones_channel, cp,
                                       fixed ? w.absum : nullptr);
   FLPR_LAUNCH_CHECK();
-  tile_scan_kernel<<<1, 1024, 0, s>>>(g.ntiles, w.counts, w.offsets, w.items, w.cursor);
+  tile_scan_kernel<<<1, 1024, 0, s>>>(g.ntiles, g.item_points, w.counts, w.offsets, w.items,
+                                      w.cursor);
   FLPR_LAUNCH_CHECK();
   // records and tap weights are float64 in both precisions: FP32 weights
   // lose ~1e-6 on the far taps (exponents near 8), which ill-conditioned
@@ -767,7 +803,7 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
                                                 (double*)w.rec_val);
   FLPR_LAUNCH_CHECK();
 
-  int64_t max_items = (int64_t)g.ntiles + (n + kItemPoints - 1) / kItemPoints;
+  int64_t max_items = (int64_t)g.ntiles + (n + g.item_points - 1) / g.item_points;
   if (use_2d_path(d, h_L, msp)) {
     const int cg2 = channel_group_2d(g, nchan);
     FLPR_CHECK_ARG(cg2 >= 1, "spread: tile does not fit shared memory");

@@ -1,0 +1,279 @@
+"""Many LPR fits in one captured CUDA graph.
+
+    plan = LprPlan([(x1, y1, h1, opts1), (x2, y2, h2, opts2), ...])
+    regs = plan.run()                  # the responses given above
+    regs = plan.run([y1b, y2b, ...])   # new responses on the same designs
+
+No reference counterpart: the reference fits one data set per call
+(api.py:167-832).  Every problem is validated like ``cv_fastlpr`` and gives
+the same result (full GCV sweep).  What depends on x only -- point
+statistics, grid geometry, kernel spectra, the bandwidth filter, probes --
+is formed when the plan is built; everything that reads y -- spread and
+transform of every channel, deposits, convolutions, solves, GCV/DoF
+reductions -- is captured once into a CUDA graph and replayed by ``run``.
+The problems are spread over several streams inside the graph (largest
+first, each to the least loaded stream), so small and large data sets of
+uneven size run concurrently.  After the replay one device-to-host copy
+brings every problem's reductions back; the 1-SE choice runs on the host and
+the fitted values at the chosen bandwidths are produced with one more
+synchronisation for all problems.
+
+``cv_fastlpr_many`` runs a list of problems once (eagerly, on the same
+streams, no capture).
+"""
+from __future__ import annotations
+
+from typing import List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib, api
+from .structures import RegressionOutput
+
+
+class _Problem:
+    pass
+
+
+def _cost(p) -> float:
+    """Relative device time of one fit: per-point spreading plus the
+    per-bandwidth convolutions on the padded grid."""
+    L = float(np.prod(p.geom.L.astype(float)))
+    nprod = (len(api._element_powers(p.d, p.su.order)) + (p.su.dy + 10) *
+             (1 if p.su.order == 0 else len(api._design_powers(p.d, p.su.order))))
+    return p.su.n * (p.su.dy + 11) * (3 ** p.d) + len(p.filt[2]) * nprod * L
+
+
+class LprPlan:
+    """A set of LPR fits captured as one CUDA graph (see the module docstring).
+
+    problems: sequence of (x, y, h, options) exactly as for cv_fastlpr
+    (h explicit; 'bandwidth_search' other than 'full' is not allowed).
+    streams: concurrent streams inside the graph (default: up to 8).
+    graph: capture a CUDA graph (True) or issue eagerly on every run.
+    autotune: pick the number of streams and the spread work-item size by
+    timing graph replays of this plan (cached per workload signature, see
+    fastlpr_b200.autotune); the spread setting stays applied afterwards.
+    """
+
+    def __init__(self, problems: Sequence, device=None, streams: Optional[int] = None,
+                 graph: bool = True, autotune: bool = False):
+        if len(problems) == 0:
+            raise ValueError("LprPlan needs at least one problem")
+        self.device = torch.device(device) if device is not None else api._device({})
+        self.probs: List[_Problem] = []
+        with torch.cuda.device(self.device):
+            ctx = api._Ctx(self.device)
+            self._ctx = ctx
+            setups = []
+            for (x, y, h, options) in problems:
+                opts = dict(options or {})
+                if str(opts.get("bandwidth_search", "full")) != "full":
+                    raise ValueError("LprPlan runs the full GCV sweep ('bandwidth_search' must "
+                                     "be 'full')")
+                opts["device"] = str(self.device)
+                if h is None:
+                    raise ValueError("LprPlan needs explicit bandwidths for every problem")
+                setups.append(api._lpr_setup(x, y, h, opts))
+            # probes: one cached matrix per (R, seed) covering the largest n
+            nmax = max(s.n for s in setups)
+            for su in setups:
+                if bool(su.opts.get("calc_dof", True)) and su.opts.get("random_matrix") is None:
+                    api._probes(ctx, nmax, int(su.opts.get("num_dof_sample", 10)),
+                                su.opts.get("dof_seed", 42), None)
+            for su in setups:
+                self.probs.append(self._build(ctx, su))
+            self._write_y([p.su.y_arr for p in self.probs])
+            self.graph = None
+            self.outs = None
+            self.sums = None
+            self.tuning = None
+            if autotune and graph:
+                self.tuning = self._autotune()
+                streams = self.tuning["best"]["streams"]
+            self._set_streams(streams if streams is not None else min(8, len(self.probs)))
+            if graph:
+                self._capture()
+
+    def _set_streams(self, nstreams: int) -> None:
+        self.streams = [torch.cuda.Stream(self.device) for _ in range(max(1, int(nstreams)))]
+        # largest first, each to the least loaded stream
+        order = sorted(range(len(self.probs)), key=lambda i: -_cost(self.probs[i]))
+        load = [0.0] * len(self.streams)
+        self.assign = {}
+        for i in order:
+            k = int(np.argmin(load))
+            self.assign[i] = k
+            load[k] += _cost(self.probs[i])
+        self.order = order
+
+    def _capture(self) -> None:
+        # eager pass: cuFFT plans, kernel attributes, reduction sizes
+        outs = self._issue()
+        torch.cuda.synchronize(self.device)
+        self._size_sums(outs)
+        del outs
+        self.graph = torch.cuda.CUDAGraph()
+        cap = torch.cuda.Stream(self.device)
+        cap.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.graph(self.graph, stream=cap):
+            self.outs = self._issue()
+        torch.cuda.synchronize(self.device)
+
+    def _autotune(self) -> dict:
+        """Streams x spread work-item size, timed as graph replays."""
+        from . import autotune as at
+        sig = sorted((p.d, tuple(int(v) for v in p.geom.L), p.su.order, p.su.dy,
+                      p.su.y_is_complex, int(np.round(np.log2(p.su.n))), len(p.filt[2]))
+                     for p in self.probs)
+        key = "plan|" + at.device_key(self.device) + "|" + str(hash(tuple(sig)) & 0xFFFFFFFF)
+        saved = at.get_params()
+        cands = [{"streams": s, "spread_item_points": a}
+                 for s in (2, 4, 8, 16) if s <= max(2, len(self.probs))
+                 for a in at.ITEM_POINTS]
+
+        def measure(c):
+            at.set_params({"spread_item_points": c["spread_item_points"]})
+            self._set_streams(c["streams"])
+            self._capture()
+            ms = at.time_ms(self.graph.replay, device=self.device)
+            self.graph = None
+            self.outs = None
+            return ms
+
+        try:
+            rec = at.tune(key, cands, measure)
+        finally:
+            at.set_params(saved)
+        at.set_params({"spread_item_points": rec["best"]["spread_item_points"]})
+        return rec
+
+    # -- construction -------------------------------------------------------
+    def _build(self, ctx, su) -> _Problem:
+        p = _Problem()
+        p.su = su
+        p.d = su.d
+        x = su.x_arr
+        if not np.all(np.isfinite(x)):
+            raise ValueError("Input x contains NaN or Inf values")
+        p.dx = ctx.upload(x)
+        p.stats = api._point_stats(ctx, p.dx, su.n, su.d)
+        G = api._grid_shape(su.opts, su.n, su.d)
+        p.geom = api._make_geom(p.stats, su.n, su.d, G, int(su.opts["accuracy"]),
+                                bool(su.opts.get("flag_power2", True)))
+        p.filt = api._filter_bandwidths(ctx, p.geom, su.bandwidths, 2 * su.order + 1,
+                                        api._kernel_id(su.opts))
+        p.probes = None
+        if bool(su.opts.get("calc_dof", True)):
+            p.probes = api._probes(ctx, su.n, int(su.opts.get("num_dof_sample", 10)),
+                                   su.opts.get("dof_seed", 42), su.opts.get("random_matrix"))
+        methods = api._check_interp_methods(su.opts, su.d, su.n)
+        if "cubic" in methods.values():
+            from . import spline
+            spline.tables(api._raw_axes(p.geom, su.opts), ctx.device)
+        nch = su.dy * (2 if su.y_is_complex else 1)
+        p.ycols = [torch.zeros(su.n, dtype=torch.float64, device=self.device) for _ in range(nch)]
+        p.staging = torch.empty((nch, su.n), dtype=torch.float64, pin_memory=True)
+        return p
+
+    def _write_y(self, ys) -> None:
+        stream = torch.cuda.current_stream(self.device)
+        for p, y in zip(self.probs, ys):
+            y_arr = np.asarray(y)
+            if y_arr.ndim == 1:
+                y_arr = y_arr[:, None]
+            elif y_arr.ndim == 2 and y_arr.shape[0] == 1 and y_arr.shape[1] > 1:
+                y_arr = y_arr.T
+            if y_arr.shape != p.su.y_arr.shape:
+                raise ValueError(f"response shape {y_arr.shape} differs from the planned "
+                                 f"{p.su.y_arr.shape}")
+            if bool(np.iscomplexobj(y_arr)) != p.su.y_is_complex:
+                raise ValueError("a response changed between real and complex")
+            if not np.all(np.isfinite(y_arr)):
+                raise ValueError("Response y contains NaN or Inf values")
+            st = p.staging.numpy()
+            for c in range(p.su.dy):
+                if p.su.y_is_complex:
+                    st[2 * c] = y_arr[:, c].real
+                    st[2 * c + 1] = y_arr[:, c].imag
+                else:
+                    st[c] = y_arr[:, c]
+            for c, col in enumerate(p.ycols):
+                col.copy_(p.staging[c], non_blocking=True)
+            # the staging rows are reused by the next run
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            p.staged = ev
+
+    def _size_sums(self, outs) -> None:
+        sizes = [0 if r["packed"] is None else int(r["packed"].numel()) for _, r in outs]
+        self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(int)
+        self.sums = torch.zeros(max(1, int(self.offsets[-1])), dtype=torch.float64,
+                                device=self.device)
+
+    def _issue(self):
+        """Enqueue the y-dependent stages of every problem on its stream; the
+        reductions are copied into `self.sums` when it exists."""
+        main = torch.cuda.current_stream(self.device)
+        for s in self.streams:
+            s.wait_stream(main)
+        outs = [None] * len(self.probs)
+        for i in self.order:
+            p = self.probs[i]
+            su = p.su
+            with torch.cuda.stream(self.streams[self.assign[i]]):
+                ctx = api._Ctx(self.device)
+                st = api._prepare_lpr(ctx, None, None, su.dy, su.opts, su.order, su.prec,
+                                      su.variance, su.y_is_complex, (p.dx, list(p.ycols)),
+                                      api._PhaseEvents(None), stats=p.stats, probes=p.probes)
+                r = api._evaluate_device(ctx, st, p.filt, api._PhaseEvents(None))
+                if self.sums is not None and r["packed"] is not None:
+                    self.sums[self.offsets[i]:self.offsets[i + 1]].copy_(r["packed"])
+                outs[i] = (st, r)
+        for s in self.streams:
+            main.wait_stream(s)
+        return outs
+
+    # -- execution ----------------------------------------------------------
+    def run(self, ys: Optional[Sequence] = None) -> List[RegressionOutput]:
+        """Fit every problem (with new responses `ys` if given)."""
+        with torch.cuda.device(self.device):
+            if ys is not None:
+                if len(ys) != len(self.probs):
+                    raise ValueError(f"expected {len(self.probs)} responses, got {len(ys)}")
+                for p in self.probs:
+                    p.staged.synchronize()
+                self._write_y(ys)
+            if self.graph is not None:
+                self.graph.replay()
+                outs = self.outs
+            else:
+                outs = self._issue()
+                if self.sums is None:
+                    self._size_sums(outs)
+                for i, (_, r) in enumerate(outs):
+                    if r["packed"] is not None:
+                        self.sums[self.offsets[i]:self.offsets[i + 1]].copy_(r["packed"])
+            sums = self.sums.cpu().numpy()
+            ctx = self._ctx
+            ctx.stream = torch.cuda.current_stream(self.device).cuda_stream
+            ev = api._PhaseEvents(None)
+            res, pend = [], []
+            for i, p in enumerate(self.probs):
+                st, r = outs[i]
+                packed = sums[self.offsets[i]:self.offsets[i + 1]]
+                r = api._evaluate_host(st, r, packed if len(packed) else None)
+                res.append(r)
+                pend.append(api._finalize_enqueue(ctx, st, r, ev))
+            torch.cuda.current_stream(self.device).synchronize()
+            return [api._finalize_build(ctx, outs[i][0], res[i], pend[i], ev, None)
+                    for i in range(len(self.probs))]
+
+
+def cv_fastlpr_many(problems: Sequence, device=None,
+                    streams: Optional[int] = None) -> List[RegressionOutput]:
+    """cv_fastlpr for every (x, y, h, options) of `problems`, issued on
+    concurrent streams with one synchronisation for the reductions and one
+    for the outputs.  Same results as separate cv_fastlpr calls."""
+    return LprPlan(problems, device=device, streams=streams, graph=False).run()

@@ -44,6 +44,19 @@ int flpr_version(void);
  * (cuFFT's own kernels are not counted). */
 int64_t flpr_launch_count(void);
 
+/* Tuning parameters, process-wide (they hold for every later call on every
+ * device; calls already enqueued keep the values they were launched with).
+ * Set by the autotuner of the Python host (fastlpr_b200/autotune.py).
+ *   FLPR_TUNE_SPREAD_ITEM_POINTS: points per spread work item (one CTA),
+ *     256..65536, default 4096;
+ *   FLPR_TUNE_FUSED_CHUNK_MB: column-pass output budget of the fused 2-D
+ *     convolution (bandwidths per chunk), 8..16384 MB, default 192. */
+#define FLPR_TUNE_SPREAD_ITEM_POINTS 0
+#define FLPR_TUNE_FUSED_CHUNK_MB 1
+#define FLPR_TUNE_COUNT 2
+int flpr_set_tuning(int param, int value);
+int flpr_get_tuning(int param);
+
 /* Handle: owns cuFFT plans (without work areas) for one device. */
 int flpr_create(flpr_handle_t* out, int device);
 int flpr_destroy(flpr_handle_t handle);
@@ -158,6 +171,22 @@ int flpr_conv(flpr_handle_t handle, int d, const int* h_G, const int* h_L, const
               int nprod, const int* h_chan, const int* h_hidx, const int* h_pow,
               double scale, int add_eps, void* d_out, int prec,
               void* d_ws, size_t ws_bytes, void* stream);
+
+/* (5a) flpr_conv for d = 2 as two passes of 1-D transforms: per distinct
+ * (channel, bandwidth, axis-0 exponent) the channel spectrum times the
+ * axis-0 factor, inverse FFT along axis 0 and rows qout[0]..+G0-1 kept
+ * (shared by every product with that triple); per product those rows times
+ * the axis-1 factor and `scale`, C2R along axis 1 and columns
+ * qout[1]..+G1-1 kept.  Same arguments (d = 2) and output as flpr_conv;
+ * about half the transform work and a quarter of the traffic of the full
+ * 2-D inverse per product. */
+size_t flpr_conv2d_sep_ws(flpr_handle_t handle, const int* h_G, const int* h_L, int nprod,
+                          int prec);
+int flpr_conv2d_sep(flpr_handle_t handle, const int* h_G, const int* h_L, const int* h_qout,
+                    int H, int npow, const void* d_spec, const void* d_F, int nprod,
+                    const int* h_chan, const int* h_hidx, const int* h_pow, double scale,
+                    int add_eps, void* d_out, int prec, void* d_ws, size_t ws_bytes,
+                    void* stream);
 
 /* (5b) Non-separable (radial) kernels: kernel.py:310-431 (epanechnikov,
  * tricube, quartic/biweight, triweight, uniform; also gaussian and

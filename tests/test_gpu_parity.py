@@ -440,3 +440,54 @@ def test_radial_kernel_spectra_match_oracle(cuda_ok, kernel, d):
         got = K[e].reshape((bw.shape[0],) + tuple(geom.L[:-1]) + (half,))
         want = np.moveaxis(spectra[e], -1, 0)[..., :half]
         assert rel_err(got, want) < 1e-12, (kernel, pw)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_conv2d_sep_matches_full_inverse(cuda_ok, prec):
+    """flpr_conv2d_sep (column pass shared per (channel, h, axis-0 power),
+    then row passes) equals flpr_conv (full 2-D inverse per product) on the
+    same spectra, factors and product list; more jobs and products than one
+    chunk holds."""
+    import torch
+    from fastlpr_b200 import _lib, api
+    rng = np.random.default_rng(31 + prec)
+    G = np.array([40, 36])
+    L, qin, qout = api._grid_params(G, True)
+    C, H, npow = 6, 10, 5
+    L1h = int(L[1]) // 2 + 1
+    dev = torch.device("cuda", 0)
+    cdt = torch.complex64 if prec == _lib.FLPR_PREC_F32 else torch.complex128
+    # spectra of real grids and factors of real sequences, as in a fit (the
+    # half-spectrum inverses assume Hermitian symmetry)
+    spec = torch.from_numpy(np.fft.rfft2(rng.standard_normal((C, int(L[0]), int(L[1])))))
+    spec = spec.to(cdt).to(dev)
+    F = torch.from_numpy(np.concatenate(
+        [np.fft.fft(rng.standard_normal((H * npow, int(La))), axis=1).ravel() for La in L])).to(dev)
+    prods = [(c, h, (a, b)) for c in range(C) for h in range(H)
+             for a in range(npow) for b in range(npow) if a + b < npow]
+    rng.shuffle(prods)
+    lib = _lib.load()
+    ctx = api._Ctx(dev)
+    args = (_lib.ivec([p[0] for p in prods]), _lib.ivec([p[1] for p in prods]),
+            _lib.ivec([v for p in prods for v in p[2]]))
+    rdt = torch.float32 if prec == _lib.FLPR_PREC_F32 else torch.float64
+    outs = []
+    for sep in (True, False):
+        out = torch.empty((len(prods), int(np.prod(G))), dtype=rdt, device=dev)
+        if sep:
+            ws = ctx.ws(lib.flpr_conv2d_sep_ws(ctx.handle, _lib.ivec(G), _lib.ivec(L),
+                                               len(prods), prec))
+            st = lib.flpr_conv2d_sep(ctx.handle, _lib.ivec(G), _lib.ivec(L), _lib.ivec(qout[0]),
+                                     H, npow, spec.data_ptr(), F.data_ptr(), len(prods), *args,
+                                     0.37, 0, out.data_ptr(), prec, ws.data_ptr(), ws.numel(),
+                                     ctx.stream)
+        else:
+            ws = ctx.ws(lib.flpr_conv_ws(ctx.handle, 2, _lib.ivec(L), len(prods), prec))
+            st = lib.flpr_conv(ctx.handle, 2, _lib.ivec(G), _lib.ivec(L), _lib.ivec(qout[0]), H,
+                               npow, spec.data_ptr(), F.data_ptr(), len(prods), *args, 0.37, 0,
+                               out.data_ptr(), prec, ws.data_ptr(), ws.numel(), ctx.stream)
+        _lib.check(st, "conv")
+        outs.append(out)
+    torch.cuda.synchronize()
+    a, b = outs[0].double().cpu().numpy(), outs[1].double().cpu().numpy()
+    assert rel_err(a, b) < (1e-5 if prec == _lib.FLPR_PREC_F32 else 1e-12)

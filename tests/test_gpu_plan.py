@@ -1,0 +1,108 @@
+"""LprPlan / cv_fastlpr_many: many fits in one captured CUDA graph give the
+same results as separate cv_fastlpr calls (the same kernels run; FP64
+atomics make the last bits order dependent, hence rtol 1e-12 / the FP32
+bound), including replays with new responses."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import elem_rel_err, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _problems(seed=0):
+    """A small mix of the batched workload's kinds: 1-D and 2-D, orders
+    0-2, complex responses, uneven n, a variance fit, a radial kernel and a
+    2-D fit with n < 5000 (cubic GCV/DoF)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    hv = np.logspace(np.log10(0.02), np.log10(0.5), 8)
+    for k, (d, n, order, cplx) in enumerate([(1, 30000, 1, False), (1, 2000, 0, False),
+                                             (1, 12000, 2, True), (2, 20000, 1, False),
+                                             (2, 6000, 0, True), (2, 8000, 2, False),
+                                             (1, 60000, 1, True), (2, 3000, 1, False)]):
+        x = rng.random((n, d))
+        f = np.sin(2 * np.pi * x[:, 0]) * (np.cos(np.pi * x[:, 1]) if d == 2 else 1.0)
+        if cplx:
+            y = np.exp(2j * np.pi * x[:, 0]) + 0.1 * (rng.standard_normal(n)
+                                                       + 1j * rng.standard_normal(n))
+        else:
+            y = f + 0.1 * rng.standard_normal(n)
+        h = np.column_stack([hv] * d)
+        opts = {"order": order, "N": 256 if d == 1 else [48, 40]}
+        out.append((x, y, h, opts))
+    x = rng.random((5000, 1))
+    out.append((x, np.exp(np.sin(4 * x[:, 0])) + 0.2 * rng.random(5000), hv[:, None],
+                {"order": 1, "N": 200, "y_type_out": "variance"}))
+    x = rng.random((7000, 2))
+    out.append((x, np.cos(3 * x[:, 0]) + 0.1 * rng.standard_normal(7000),
+                np.column_stack([hv[2:], hv[2:]]), {"order": 1, "N": [40, 40],
+                                                    "kernel_type": "epanechnikov"}))
+    return out
+
+
+def _same(a, b, tol):
+    np.testing.assert_array_equal(a.gcv_yhat["bandwidths"], b.gcv_yhat["bandwidths"])
+    assert a.gcv_yhat["id1se"] == b.gcv_yhat["id1se"]
+    assert rel_err(a.yhat, b.yhat) < tol
+    assert elem_rel_err(a.gcv_yhat["gcv_m"], b.gcv_yhat["gcv_m"]) < tol
+    assert rel_err(a.gcv_yhat["dof"], b.gcv_yhat["dof"]) < tol
+    assert rel_err(a.fpp_yhat.values, b.fpp_yhat.values) < tol
+    assert rel_err(a.s0, b.s0) < tol
+    if a.d is not None:
+        assert abs(a.d - b.d) <= tol * abs(b.d)
+
+
+def _tol(opts):
+    # order 2 runs in FP64 (bound 1e-9), the rest in FP32 (bound 1e-5); the
+    # same kernels run, so the differences are far smaller than either
+    return 1e-9 if opts.get("order", 0) == 2 else 1e-6
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_plan_matches_single_fits(cuda_ok, graph):
+    import fastlpr_b200
+    probs = _problems()
+    plan = fastlpr_b200.LprPlan(probs, graph=graph, streams=4)
+    got = plan.run()
+    for (x, y, h, o), g in zip(probs, got):
+        ref = fastlpr_b200.cv_fastlpr(x, y, h, o)
+        _same(g, ref, _tol(o))
+    # new responses on the same designs
+    rng = np.random.default_rng(9)
+    ys = []
+    for (x, y, h, o) in probs:
+        if np.iscomplexobj(y):
+            ys.append(y * np.exp(0.3j))
+        elif o.get("y_type_out") == "variance":
+            ys.append(y * (1.0 + 0.2 * rng.random(y.shape)))
+        else:
+            ys.append(y + 0.05 * rng.standard_normal(y.shape))
+    got2 = plan.run(ys)
+    for (x, y, h, o), y2, g in zip(probs, ys, got2):
+        ref = fastlpr_b200.cv_fastlpr(x, y2, h, o)
+        _same(g, ref, _tol(o))
+
+
+def test_plan_replay_is_reproducible(cuda_ok):
+    """Replaying with y unchanged reproduces the first run."""
+    import fastlpr_b200
+    probs = _problems(1)[:4]
+    plan = fastlpr_b200.LprPlan(probs)
+    a = plan.run()
+    b = plan.run([p[1] for p in probs])
+    for ra, rb in zip(a, b):
+        _same(ra, rb, 1e-12)
+
+
+def test_cv_fastlpr_many_matches_oracle(cuda_ok):
+    import fastlpr_b200
+    probs = _problems(2)[:3]
+    got = fastlpr_b200.cv_fastlpr_many([(x, y, h, dict(o, precision="fp64"))
+                                        for (x, y, h, o) in probs])
+    for (x, y, h, o), g in zip(probs, got):
+        z = oracle.cv_fastlpr(x, y, h, o)
+        assert g.gcv_yhat["id1se"] == z["id1se"]
+        assert rel_err(g.yhat, z["yhat"]) < 1e-9
+        assert elem_rel_err(g.gcv_yhat["gcv_m"], z["gcv_m"]) < 1e-9
