@@ -65,6 +65,8 @@ SIGNATURES = [
                                 _VP, _VP, _SZ, _VP]),
     ("flpr_interp_eval", _I, [_I, _I64, _VP, _PD, _PI, _I, _VP, _VP, _VP]),
     ("flpr_spline_prefilter", _I, [_I, _PI, _I64, _I, _VP, _VP, _VP]),
+    ("flpr_gcv_select", _I, [_I, _I, _I, _I, _I, _I, _D, _D, _VP, _VP, _VP, _VP, _VP]),
+    ("flpr_select_grid", _I, [_I64, _I, _I, _I, _VP, _VP, _I, _VP, _VP, _VP, _VP]),
     ("flpr_spline_reduce", _I, [_I, _I64, _VP, _VP, _PI, _I, _I, _I, _VP, _PVP, _PVP, _VP, _VP,
                                 _VP, _VP]),
     ("flpr_spline_eval", _I, [_I, _I64, _VP, _VP, _PI, _I, _VP, _VP, _VP]),

@@ -1070,17 +1070,54 @@ def _finalize_lpr(ctx, st: _LprState, r: dict, ev, search) -> RegressionOutput:
     return _finalize_build(ctx, st, r, pend, ev, search)
 
 
-def _finalize_enqueue(ctx, st: _LprState, r: dict, ev) -> dict:
+def _finalize_enqueue(ctx, st: _LprState, r: dict, ev, device_select: bool = False,
+                      bufs: Optional[dict] = None, hsum_dev: Optional[torch.Tensor] = None) -> dict:
     """Device part of the output stage: fitted values at the selected
     bandwidth, residuals, grid and s0 copied into pinned host memory
-    (asynchronously; valid after the stream synchronises)."""
+    (asynchronously; valid after the stream synchronises).
+
+    device_select: GCV, DoF and the 1-SE choice come from flpr_gcv_select
+    on the packed reductions and the chosen grid is gathered on the device
+    (flpr_select_grid), so nothing here waits for the host; `r` then needs
+    no host evaluation.  bufs: preallocated pinned outputs (see _output_bufs)
+    instead of fresh ones; hsum_dev: per-bandwidth sums of h on the device."""
     lib = ctx.lib
     d, n, ny = st.d, st.n, st.ny
     geom = st.geom
-    sel, m, S = r["sel"], r["m"], r["S"]
+    m, S = r["m"], r["S"]
     H, ns, M = r["H"], r["ns"], geom.M
-    mv = m[sel if st.calc_dof else 0]                # (M, mstride)
-    gv_dev = mv[:, :ny].t().contiguous()             # (ny, M)
+    gcv_dev = sel_dev = None
+    if device_select:
+        sel_dev = ctx.empty(1, dtype=torch.int32)
+        if st.calc_dof:
+            if hsum_dev is None:
+                hs = torch.from_numpy(np.ascontiguousarray(np.sum(r["bw_k"], axis=1))).pin_memory()
+                hsum_dev = hs.to(ctx.device, non_blocking=True)
+            gcv_dev = ctx.empty(4 * H)
+            agg = {"first": 0, "average": 1, "sum": 2}.get(str(st.opts.get("gcv_selection",
+                                                                            "first")))
+            if agg is None:
+                raise ValueError(f"Unknown aggregation method: {st.opts.get('gcv_selection')}. "
+                                 "Use 'first', 'average', or 'sum'.")
+            ctx.check(lib.flpr_gcv_select(H, ny, st.R, 1 if r["dual"] else 0,
+                                          1 if st.y_is_complex else 0, agg, float(n),
+                                          float(st.opts.get("dstd", 0.0)), r["packed"].data_ptr(),
+                                          hsum_dev.data_ptr(), gcv_dev.data_ptr(),
+                                          sel_dev.data_ptr(), ctx.stream), "flpr_gcv_select")
+        else:
+            sel_dev.zero_()
+        gv_dev = ctx.empty((ny, M))
+        s0_dev = ctx.empty(M)
+        s_prec = _lib.FLPR_PREC_F32 if S.dtype == torch.float32 else _lib.FLPR_PREC_F64
+        ctx.check(lib.flpr_select_grid(M, ny, r["mstride"], m.shape[0], m.data_ptr(),
+                                       S.data_ptr(), s_prec, sel_dev.data_ptr(),
+                                       gv_dev.data_ptr(), s0_dev.data_ptr(), ctx.stream),
+                  "flpr_select_grid")
+    else:
+        sel = r["sel"]
+        mv = m[sel if st.calc_dof else 0]                # (M, mstride)
+        gv_dev = mv[:, :ny].t().contiguous()             # (ny, M)
+        s0_dev = S.view(ns, H, M)[0, sel]
     yhat_dev = ctx.empty((ny, n))
     if st.methods["output"] == "cubic":
         coef = gv_dev.clone()
@@ -1109,17 +1146,56 @@ def _finalize_enqueue(ctx, st: _LprState, r: dict, ev) -> dict:
         res_dev = st.y_raw_dev[None, :] - yhat_dev
     else:
         res_dev = torch.stack(st.ycols[:ny], dim=0) - yhat_dev
-    return {"yh": _to_host(yhat_dev), "rh": _to_host(res_dev), "gvh": _to_host(gv_dev),
-            "s0h": _to_host(S.view(ns, H, M)[0, sel]),
-            "dn": _to_host(dn) if dn is not None else None}
+    parts = {"yh": yhat_dev, "rh": res_dev, "gvh": gv_dev, "s0h": s0_dev, "dn": dn,
+             "gcv": gcv_dev, "sel": sel_dev}
+    out = {}
+    for k, t in parts.items():
+        if t is None:
+            out[k] = None
+        elif bufs is not None:
+            bufs[k].copy_(t.reshape(bufs[k].shape), non_blocking=True)
+            out[k] = bufs[k]
+        else:
+            out[k] = _to_host(t)
+    return out
 
 
-def _finalize_build(ctx, st: _LprState, r: dict, pend: dict, ev, search) -> RegressionOutput:
-    """Result structure from the downloaded outputs of _finalize_enqueue."""
+def _output_bufs(st: _LprState, H: int) -> dict:
+    """Pinned host buffers for every output of _finalize_enqueue(device_select=True)."""
+    n, ny, M = st.n, st.ny, st.geom.M
+
+    def pin(shape, dtype=torch.float64):
+        return torch.empty(shape, dtype=dtype, pin_memory=True)
+
+    return {"yh": pin((ny, n)), "rh": pin((ny, n)), "gvh": pin((ny, M)), "s0h": pin(M),
+            "dn": pin(1) if st.variance else None,
+            "gcv": pin(4 * H) if st.calc_dof else None, "sel": pin(1, torch.int32)}
+
+
+def _finalize_build(ctx, st: _LprState, r: dict, pend: dict, ev, search,
+                    copy: bool = False) -> RegressionOutput:
+    """Result structure from the downloaded outputs of _finalize_enqueue
+    (copy: detach the arrays from reused pinned buffers)."""
     d, dy = st.d, st.dy
     geom, opts = st.geom, st.opts
-    bw_k, sel, gcv = r["bw_k"], r["sel"], r["gcv"]
+    bw_k = r["bw_k"]
+    if pend.get("sel") is not None:
+        sel = int(pend["sel"].numpy()[0])
+        if st.calc_dof:
+            if sel < 0:
+                raise ValueError(
+                    "All GCV scores are NaN or Inf. Regression failed for all bandwidths. "
+                    "Try: (1) Use larger bandwidth h, (2) Increase grid points, "
+                    "(3) Check for data quality issues")
+            g4 = pend["gcv"].numpy().reshape(4, r["H"]).copy()
+            gcv = {"gcv_m": g4[0], "gcv_sd": g4[1], "dof": g4[2], "dof_stderr": g4[3]}
+        else:
+            gcv = None
+    else:
+        sel, gcv = r["sel"], r["gcv"]
     yh, rh, gvh = pend["yh"].numpy(), pend["rh"].numpy(), pend["gvh"].numpy()
+    if copy:
+        yh, rh, gvh = yh.copy(), rh.copy(), gvh.copy()
     s0h = pend["s0h"]
     d_norm = float(pend["dn"].numpy()[0]) if pend["dn"] is not None else None
     gshape = tuple(int(g) for g in geom.G)
@@ -1136,6 +1212,8 @@ def _finalize_build(ctx, st: _LprState, r: dict, pend: dict, ev, search) -> Regr
         residuals = rh.T.copy()
         grid_values = np.moveaxis(gvh.reshape((dy,) + gshape), 0, -1)
     s0 = s0h.numpy().reshape(gshape)
+    if copy:
+        s0 = s0.copy()
     ev.mark("download")
     ev.finish()
     interp = GridInterpolant(st.axes_raw, grid_values, ctx.device, method=st.methods["output"])
@@ -1276,11 +1354,16 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
              if learned is not None else None)
     if found is not None:
         r, search = found
-    else:
-        r = _evaluate_lpr(ctx, st, bandwidths, ev)
-        search = None if learned is None else {"mode": "learned", "accepted": False,
-                                               "fallback": "full sweep"}
-    return _finalize_lpr(ctx, st, r, ev, search)
+        return _finalize_lpr(ctx, st, r, ev, search)
+    # full sweep: GCV, the 1-SE choice and the output stage are enqueued on
+    # the device behind the reductions; one synchronisation at the end
+    search = None if learned is None else {"mode": "learned", "accepted": False,
+                                           "fallback": "full sweep"}
+    filt = _filter_bandwidths(ctx, st.geom, bandwidths, 2 * st.order + 1, st.kid)
+    r = _evaluate_device(ctx, st, filt, ev)
+    pend = _finalize_enqueue(ctx, st, r, ev, device_select=True)
+    torch.cuda.current_stream(ctx.device).synchronize()
+    return _finalize_build(ctx, st, r, pend, ev, search)
 
 
 def _gcv_from_sums(n, rss, pdot, pp, dy, y_is_complex, opts):

@@ -10,13 +10,12 @@ the same result (full GCV sweep).  What depends on x only -- point
 statistics, grid geometry, kernel spectra, the bandwidth filter, probes --
 is formed when the plan is built; everything that reads y -- spread and
 transform of every channel, deposits, convolutions, solves, GCV/DoF
-reductions -- is captured once into a CUDA graph and replayed by ``run``.
-The problems are spread over several streams inside the graph (largest
-first, each to the least loaded stream), so small and large data sets of
-uneven size run concurrently.  After the replay one device-to-host copy
-brings every problem's reductions back; the 1-SE choice runs on the host and
-the fitted values at the chosen bandwidths are produced with one more
-synchronisation for all problems.
+reductions, the 1-SE choice, the fitted values at the chosen bandwidth and
+the copies of every output into pinned host buffers -- is captured once into
+a CUDA graph and replayed by ``run``.  The problems are spread over several
+streams inside the graph (largest first, each to the least loaded stream),
+so small and large data sets of uneven size run concurrently.  A run is one
+replay and one synchronisation for all problems.
 
 ``cv_fastlpr_many`` runs a list of problems once (eagerly, on the same
 streams, no capture).
@@ -87,7 +86,6 @@ class LprPlan:
             self._write_y([p.su.y_arr for p in self.probs])
             self.graph = None
             self.outs = None
-            self.sums = None
             self.tuning = None
             if autotune and graph:
                 self.tuning = self._autotune()
@@ -109,10 +107,9 @@ class LprPlan:
         self.order = order
 
     def _capture(self) -> None:
-        # eager pass: cuFFT plans, kernel attributes, reduction sizes
+        # eager pass: cuFFT plans, kernel attributes, output buffers
         outs = self._issue()
         torch.cuda.synchronize(self.device)
-        self._size_sums(outs)
         del outs
         self.graph = torch.cuda.CUDAGraph()
         cap = torch.cuda.Stream(self.device)
@@ -164,6 +161,10 @@ class LprPlan:
                                 bool(su.opts.get("flag_power2", True)))
         p.filt = api._filter_bandwidths(ctx, p.geom, su.bandwidths, 2 * su.order + 1,
                                         api._kernel_id(su.opts))
+        bw_k = p.filt[1][p.filt[2]]
+        hs = torch.from_numpy(np.ascontiguousarray(np.sum(bw_k, axis=1)))
+        p.hsum = hs.to(self.device)
+        p.bufs = None
         p.probes = None
         if bool(su.opts.get("calc_dof", True)):
             p.probes = api._probes(ctx, su.n, int(su.opts.get("num_dof_sample", 10)),
@@ -206,15 +207,9 @@ class LprPlan:
             ev.record(stream)
             p.staged = ev
 
-    def _size_sums(self, outs) -> None:
-        sizes = [0 if r["packed"] is None else int(r["packed"].numel()) for _, r in outs]
-        self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(int)
-        self.sums = torch.zeros(max(1, int(self.offsets[-1])), dtype=torch.float64,
-                                device=self.device)
-
     def _issue(self):
-        """Enqueue the y-dependent stages of every problem on its stream; the
-        reductions are copied into `self.sums` when it exists."""
+        """Enqueue the y-dependent stages of every problem on its stream, up
+        to its outputs in the pinned buffers."""
         main = torch.cuda.current_stream(self.device)
         for s in self.streams:
             s.wait_stream(main)
@@ -224,12 +219,15 @@ class LprPlan:
             su = p.su
             with torch.cuda.stream(self.streams[self.assign[i]]):
                 ctx = api._Ctx(self.device)
+                ev = api._PhaseEvents(None)
                 st = api._prepare_lpr(ctx, None, None, su.dy, su.opts, su.order, su.prec,
                                       su.variance, su.y_is_complex, (p.dx, list(p.ycols)),
-                                      api._PhaseEvents(None), stats=p.stats, probes=p.probes)
-                r = api._evaluate_device(ctx, st, p.filt, api._PhaseEvents(None))
-                if self.sums is not None and r["packed"] is not None:
-                    self.sums[self.offsets[i]:self.offsets[i + 1]].copy_(r["packed"])
+                                      ev, stats=p.stats, probes=p.probes)
+                r = api._evaluate_device(ctx, st, p.filt, ev)
+                if p.bufs is None:
+                    p.bufs = api._output_bufs(st, r["H"])
+                api._finalize_enqueue(ctx, st, r, ev, device_select=True, bufs=p.bufs,
+                                      hsum_dev=p.hsum)
                 outs[i] = (st, r)
         for s in self.streams:
             main.wait_stream(s)
@@ -250,25 +248,11 @@ class LprPlan:
                 outs = self.outs
             else:
                 outs = self._issue()
-                if self.sums is None:
-                    self._size_sums(outs)
-                for i, (_, r) in enumerate(outs):
-                    if r["packed"] is not None:
-                        self.sums[self.offsets[i]:self.offsets[i + 1]].copy_(r["packed"])
-            sums = self.sums.cpu().numpy()
-            ctx = self._ctx
-            ctx.stream = torch.cuda.current_stream(self.device).cuda_stream
-            ev = api._PhaseEvents(None)
-            res, pend = [], []
-            for i, p in enumerate(self.probs):
-                st, r = outs[i]
-                packed = sums[self.offsets[i]:self.offsets[i + 1]]
-                r = api._evaluate_host(st, r, packed if len(packed) else None)
-                res.append(r)
-                pend.append(api._finalize_enqueue(ctx, st, r, ev))
             torch.cuda.current_stream(self.device).synchronize()
-            return [api._finalize_build(ctx, outs[i][0], res[i], pend[i], ev, None)
-                    for i in range(len(self.probs))]
+            ev = api._PhaseEvents(None)
+            return [api._finalize_build(self._ctx, outs[i][0], outs[i][1], p.bufs, ev, None,
+                                        copy=True)
+                    for i, p in enumerate(self.probs)]
 
 
 def cv_fastlpr_many(problems: Sequence, device=None,

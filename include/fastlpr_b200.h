@@ -334,6 +334,24 @@ int flpr_spline_reduce(int d, int64_t n, const double* d_x, const double* d_axes
 int flpr_spline_eval(int d, int64_t n, const double* d_x, const double* d_axes, const int* h_G,
                      int nval, const double* d_coef, double* d_out, void* stream);
 
+/* (8c) GCV, DoF and the 1-SE choice on the device (regression.py:280-471,
+ * regression.py:1276-1354, api.py:73-164), so that the output stage can be
+ * enqueued or captured without a host round trip.  d_packed: the reductions
+ * of one fit, dual form {sq (C), dots (C, H), quad (H, ny)} (dual = 1) or
+ * pointwise form {rss (H, ny), pdot (max(R,1), H), pp (max(R,1))}, C = ny + R;
+ * complex responses: ny = 2 dy (real/imaginary interleaved); agg 0/1/2 =
+ * gcv_selection 'first'/'average'/'sum'; d_hsum (H): sum over axes of each
+ * bandwidth.  d_out (4H) = {gcv_m, gcv_sd, dof, dof_stderr}; d_sel: the
+ * 1-SE index, or -1 when no score is finite.  One block.
+ * flpr_select_grid: d_gv (ny, M) = d_m[sel][:, :ny] transposed (d_m:
+ * (H, M, mstride) float64) and d_s0 (M) = S[0][sel] (S: (ns, H, M), float
+ * when s_prec is FLPR_PREC_F32 else double); NaN when sel is out of range. */
+int flpr_gcv_select(int H, int ny, int R, int dual, int y_complex, int agg, double n, double dstd,
+                    const double* d_packed, const double* d_hsum, double* d_out, int* d_sel,
+                    void* stream);
+int flpr_select_grid(int64_t M, int ny, int mstride, int H, const double* d_m, const void* d_S,
+                     int s_prec, const int* d_sel, double* d_gv, double* d_s0, void* stream);
+
 /* ---------------------------------------------------------------------
  * (9) KDE normalisation and LCV.  Replaces api.py:1059-1133.
  * d_s: (H, M) density sums (float64, epsilon already added).  For each

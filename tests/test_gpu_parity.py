@@ -491,3 +491,58 @@ def test_conv2d_sep_matches_full_inverse(cuda_ok, prec):
     torch.cuda.synchronize()
     a, b = outs[0].double().cpu().numpy(), outs[1].double().cpu().numpy()
     assert rel_err(a, b) < (1e-5 if prec == _lib.FLPR_PREC_F32 else 1e-12)
+
+
+@pytest.mark.parametrize("dual,cplx,R,agg", [(1, 0, 10, "first"), (0, 0, 10, "first"),
+                                             (1, 1, 10, "first"), (0, 0, 1, "first"),
+                                             (1, 0, 10, "average"), (0, 1, 6, "sum")])
+def test_device_gcv_select_matches_host(cuda_ok, dual, cplx, R, agg):
+    """flpr_gcv_select (GCV, DoF and the 1-SE choice on the device) equals
+    the host formulas (_gcv_from_sums, _one_se_rule) on the same reductions."""
+    import torch
+    from fastlpr_b200 import _lib, api
+    rng = np.random.default_rng(dual * 7 + cplx * 3 + R)
+    H, n = 17, 5000
+    dy = 2 if agg != "first" else 1
+    ny = dy * (2 if cplx else 1)
+    C = ny + R
+    bw = np.column_stack([np.logspace(-2, -0.3, H)] * 2)
+    bw[5] = bw[6]  # a tie in the bandwidth sums
+    rss_true = rng.uniform(50, 80, (H, ny))
+    tr = np.clip(rng.uniform(-20, 900, (R, H)), -10, None)
+    pp = rng.uniform(4000, 6000, max(R, 1))
+    pdot = tr * pp[:R, None] / n
+    if R > 1:
+        pdot[0, 3] = np.nan
+    if dual:
+        sq = np.concatenate([rng.uniform(900, 1000, ny), pp[:R]])
+        dots = np.zeros((C, H))
+        dots[ny:] = pdot
+        dots[:ny] = rng.uniform(100, 200, (ny, H))
+        quad = rss_true - sq[None, :ny] + 2.0 * dots[:ny].T
+        packed = np.concatenate([sq, dots.ravel(), quad.ravel()])
+        rss_h = sq[None, :ny] - 2.0 * dots[:ny].T + quad
+        pp_h = sq[ny:]
+    else:
+        Rm = max(R, 1)
+        pd_full = np.zeros((Rm, H))
+        pd_full[:R] = pdot
+        packed = np.concatenate([rss_true.ravel(), pd_full.ravel(), pp[:Rm]])
+        rss_h, pp_h = rss_true, pp[:R]
+    opts = {"gcv_selection": agg, "dstd": 0.5}
+    want = api._gcv_from_sums(n, rss_h, pdot, pp_h, dy, bool(cplx), opts)
+    wsel = api._one_se_rule(want["gcv_m"], want["gcv_sd"], bw, prefer_smaller=True, dstd=0.5)
+    dev = torch.device("cuda", 0)
+    lib = _lib.load()
+    dp = torch.from_numpy(packed).to(dev)
+    hs = torch.from_numpy(np.sum(bw, axis=1)).to(dev)
+    out = torch.empty(4 * H, dtype=torch.float64, device=dev)
+    sel = torch.empty(1, dtype=torch.int32, device=dev)
+    agg_id = {"first": 0, "average": 1, "sum": 2}[agg]
+    _lib.check(lib.flpr_gcv_select(H, ny, R, dual, cplx, agg_id, float(n), 0.5, dp.data_ptr(),
+                                   hs.data_ptr(), out.data_ptr(), sel.data_ptr(), None),
+               "gcv_select")
+    g4 = out.cpu().numpy().reshape(4, H)
+    for k, key in enumerate(("gcv_m", "gcv_sd", "dof", "dof_stderr")):
+        np.testing.assert_allclose(g4[k], want[key], rtol=1e-13, atol=1e-13, err_msg=key)
+    assert int(sel.cpu()[0]) == wsel
