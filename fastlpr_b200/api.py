@@ -1079,8 +1079,10 @@ def _finalize_enqueue(ctx, st: _LprState, r: dict, ev, device_select: bool = Fal
     device_select: GCV, DoF and the 1-SE choice come from flpr_gcv_select
     on the packed reductions and the chosen grid is gathered on the device
     (flpr_select_grid), so nothing here waits for the host; `r` then needs
-    no host evaluation.  bufs: preallocated pinned outputs (see _output_bufs)
-    instead of fresh ones; hsum_dev: per-bandwidth sums of h on the device."""
+    no host evaluation.  bufs: preallocated pinned buffers (see _output_bufs)
+    for the outputs they name; with bufs given, the other outputs are
+    returned as device tensors for the caller to download.  hsum_dev:
+    per-bandwidth sums of h on the device."""
     lib = ctx.lib
     d, n, ny = st.d, st.n, st.ny
     geom = st.geom
@@ -1152,23 +1154,24 @@ def _finalize_enqueue(ctx, st: _LprState, r: dict, ev, device_select: bool = Fal
     for k, t in parts.items():
         if t is None:
             out[k] = None
-        elif bufs is not None:
+        elif bufs is not None and bufs.get(k) is not None:
             bufs[k].copy_(t.reshape(bufs[k].shape), non_blocking=True)
             out[k] = bufs[k]
+        elif bufs is not None:
+            out[k] = t
         else:
             out[k] = _to_host(t)
     return out
 
 
 def _output_bufs(st: _LprState, H: int) -> dict:
-    """Pinned host buffers for every output of _finalize_enqueue(device_select=True)."""
-    n, ny, M = st.n, st.ny, st.geom.M
-
+    """Pinned host buffers for the small outputs of
+    _finalize_enqueue(device_select=True): the bandwidth choice, the GCV
+    arrays and the variance normaliser."""
     def pin(shape, dtype=torch.float64):
         return torch.empty(shape, dtype=dtype, pin_memory=True)
 
-    return {"yh": pin((ny, n)), "rh": pin((ny, n)), "gvh": pin((ny, M)), "s0h": pin(M),
-            "dn": pin(1) if st.variance else None,
+    return {"dn": pin(1) if st.variance else None,
             "gcv": pin(4 * H) if st.calc_dof else None, "sel": pin(1, torch.int32)}
 
 

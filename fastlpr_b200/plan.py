@@ -226,9 +226,9 @@ class LprPlan:
                 r = api._evaluate_device(ctx, st, p.filt, ev)
                 if p.bufs is None:
                     p.bufs = api._output_bufs(st, r["H"])
-                api._finalize_enqueue(ctx, st, r, ev, device_select=True, bufs=p.bufs,
-                                      hsum_dev=p.hsum)
-                outs[i] = (st, r)
+                pend = api._finalize_enqueue(ctx, st, r, ev, device_select=True, bufs=p.bufs,
+                                             hsum_dev=p.hsum)
+                outs[i] = (st, r, pend)
         for s in self.streams:
             main.wait_stream(s)
         return outs
@@ -248,11 +248,16 @@ class LprPlan:
                 outs = self.outs
             else:
                 outs = self._issue()
+            # the large outputs go into fresh pinned memory (no host copies;
+            # the results stay valid after later runs)
+            pends = []
+            for st, r, pend in outs:
+                pends.append({k: (api._to_host(v) if isinstance(v, torch.Tensor) and v.is_cuda
+                                  else v) for k, v in pend.items()})
             torch.cuda.current_stream(self.device).synchronize()
             ev = api._PhaseEvents(None)
-            return [api._finalize_build(self._ctx, outs[i][0], outs[i][1], p.bufs, ev, None,
-                                        copy=True)
-                    for i, p in enumerate(self.probs)]
+            return [api._finalize_build(self._ctx, outs[i][0], outs[i][1], pends[i], ev, None)
+                    for i in range(len(self.probs))]
 
 
 def cv_fastlpr_many(problems: Sequence, device=None,
