@@ -1486,13 +1486,17 @@ def _fit_kde(ctx, x_arr, bandwidths, opts, G, prec):
                                _lib.ivec(geom.G), H, S64.data_ptr(), dxg, _lib.dvec(k0),
                                f.data_ptr(), lcv.data_ptr(), ws.data_ptr(), ws.numel(),
                                ctx.stream), "flpr_kde_lcv")
-    lc = lcv.cpu().numpy()
+    # both results into pinned memory with one synchronisation (a pageable
+    # copy of the (H, M) densities runs at a fraction of the link speed)
+    lc_h, f_h = _to_host(lcv), _to_host(f)
+    torch.cuda.current_stream(ctx.device).synchronize()
+    lc = lc_h.numpy()
     lcv_m = lc[:, 0].copy()
     var_l = lc[:, 1] / n
     lcv_sd = np.sqrt(var_l) * np.sqrt(n)
     sel = _one_se_rule(lcv_m, lcv_sd, bandwidths, prefer_smaller=False)
     gshape = tuple(int(g) for g in G)
-    fall = f.cpu().numpy().reshape((H,) + gshape)
+    fall = f_h.numpy().reshape((H,) + gshape)
     fhat_all = np.moveaxis(fall, 0, -1)
     fhat = fall[sel]
     interp = GridInterpolant(axes_raw, fhat, ctx.device,

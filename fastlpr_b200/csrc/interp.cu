@@ -269,14 +269,21 @@ __global__ void deposit_kernel(InterpGeom g, int64_t n, const double* __restrict
 
 // quad[h][c] = sum_b sum_pairs B[b][pair] m(b+c_k) m(b+c_k2); m: (H, M, ny).
 // D fixed at compile time: the 2^D corners and their pairs live in registers.
+// blockIdx.y = a chunk of QB bandwidths: each base cell's pair weights are
+// read once per chunk and applied to every bandwidth of it.
 template <int D>
-__global__ void stencil_quad_kernel(InterpGeom g, int ny, const double* __restrict__ m,
+struct QuadChunk {
+  static constexpr int value = D == 3 ? 4 : 8;
+};
+
+template <int D>
+__global__ void stencil_quad_kernel(InterpGeom g, int H, int ny, const double* __restrict__ m,
                                     const double* __restrict__ B, double* __restrict__ quad) {
   constexpr int NC = 1 << D;
   constexpr int NP = NC * (NC + 1) / 2;
+  constexpr int QB = QuadChunk<D>::value;
   __shared__ double sh[32];
-  const int h = blockIdx.y;
-  const double* mh = m + (int64_t)h * g.M * ny;
+  const int h0 = blockIdx.y * QB;
   int coff[NC];
 #pragma unroll
   for (int k = 0; k < NC; ++k) {
@@ -285,7 +292,11 @@ __global__ void stencil_quad_kernel(InterpGeom g, int ny, const double* __restri
     for (int a = 0; a < D; ++a) o = o * g.G[a] + ((k >> (D - 1 - a)) & 1);
     coff[k] = o;
   }
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  double acc[QB][4];
+#pragma unroll
+  for (int q = 0; q < QB; ++q)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[q][c] = 0.0;
   const int M = (int)g.M;  // grids here hold fewer than 2^31 cells
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < M; b += gridDim.x * blockDim.x) {
     // only base cells with every corner inside the grid carry weight
@@ -301,22 +312,35 @@ __global__ void stencil_quad_kernel(InterpGeom g, int ny, const double* __restri
     double Bv[NP];
 #pragma unroll
     for (int p = 0; p < NP; ++p) Bv[p] = B[(int64_t)b * NP + p];
-    for (int c = 0; c < ny && c < 4; ++c) {
-      double mv[NC];
 #pragma unroll
-      for (int k = 0; k < NC; ++k) mv[k] = mh[(int64_t)(b + coff[k]) * ny + c];
-      double s = 0.0;
-      int p = 0;
+    for (int q = 0; q < QB; ++q) {
+      if (h0 + q >= H) break;
+      const double* mh = m + (int64_t)(h0 + q) * g.M * ny;
 #pragma unroll
-      for (int k = 0; k < NC; ++k)
+      for (int c = 0; c < 4; ++c) {
+        if (c >= ny) break;
+        double mv[NC];
 #pragma unroll
-        for (int k2 = k; k2 < NC; ++k2, ++p) s += Bv[p] * mv[k] * mv[k2];
-      acc[c] += s;
+        for (int k = 0; k < NC; ++k) mv[k] = mh[(int64_t)(b + coff[k]) * ny + c];
+        double s = 0.0;
+        int p = 0;
+#pragma unroll
+        for (int k = 0; k < NC; ++k)
+#pragma unroll
+          for (int k2 = k; k2 < NC; ++k2, ++p) s += Bv[p] * mv[k] * mv[k2];
+        acc[q][c] += s;
+      }
     }
   }
-  for (int c = 0; c < ny && c < 4; ++c) {
-    double s = block_sum(acc[c], sh);
-    if (threadIdx.x == 0) atomicAdd(&quad[h * ny + c], s);
+#pragma unroll
+  for (int q = 0; q < QB; ++q) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (h0 + q < H && c < ny) {
+        const double s = block_sum(acc[q][c], sh);
+        if (threadIdx.x == 0) atomicAdd(&quad[(h0 + q) * ny + c], s);
+      }
+    }
   }
 }
 
@@ -429,13 +453,15 @@ int flpr_stencil_quad(int d, const int* h_G, int H, int ny, const double* d_m, c
   FLPR_CHECK_ARG(H >= 1 && ny >= 1 && ny <= 4, "stencil_quad: H=%d ny=%d", H, ny);
   cudaStream_t s = as_stream(stream);
   FLPR_CUDA(cudaMemsetAsync(d_quad, 0, sizeof(double) * H * ny, s));
-  int per_h = (pt_blocks(g.M, 4) + H - 1) / H;
-  if (per_h < 4) per_h = 4;
   FLPR_CHECK_ARG(g.M < ((int64_t)1 << 31), "stencil_quad: grid too large");
+  const int qb = d == 3 ? QuadChunk<3>::value : QuadChunk<2>::value;
+  const int nchunk = (H + qb - 1) / qb;
+  int per = (pt_blocks(g.M, 4) + nchunk - 1) / nchunk;
+  if (per < 4) per = 4;
   switch (d) {
-    case 1: stencil_quad_kernel<1><<<dim3(per_h, H), 256, 0, s>>>(g, ny, d_m, d_B, d_quad); break;
-    case 2: stencil_quad_kernel<2><<<dim3(per_h, H), 256, 0, s>>>(g, ny, d_m, d_B, d_quad); break;
-    default: stencil_quad_kernel<3><<<dim3(per_h, H), 256, 0, s>>>(g, ny, d_m, d_B, d_quad); break;
+    case 1: stencil_quad_kernel<1><<<dim3(per, nchunk), 256, 0, s>>>(g, H, ny, d_m, d_B, d_quad); break;
+    case 2: stencil_quad_kernel<2><<<dim3(per, nchunk), 256, 0, s>>>(g, H, ny, d_m, d_B, d_quad); break;
+    default: stencil_quad_kernel<3><<<dim3(per, nchunk), 256, 0, s>>>(g, H, ny, d_m, d_B, d_quad); break;
   }
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;

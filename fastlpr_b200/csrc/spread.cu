@@ -543,21 +543,23 @@ static size_t smem_2d(int W0, int nt1, int cg) {
   return sizeof(double) * ((size_t)cg * chan_stride2(W0, nt1) + (size_t)kBatch2 * (2 * nt1 + cg));
 }
 
+// Grid value = accumulator / fixed-point scale (a power of two, so the
+// product with its inverse is exact) / n.  Thread per cell, all channels.
 template <typename Acc, typename Out, bool kFixed>
 __global__ void finalize_kernel(int nchan, int64_t cells, const Acc* __restrict__ gacc,
                                 const double* __restrict__ absum, int margin_bits, double inv_n,
                                 Out* __restrict__ out) {
-  int64_t total = (int64_t)nchan * cells;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+  __shared__ double inv_scale[FLPR_MAX_CHANNELS];
+  for (int c = threadIdx.x; c < nchan; c += blockDim.x)
+    inv_scale[c] = kFixed ? 1.0 / fixed_scale(absum[c], margin_bits) : 1.0;
+  __syncthreads();
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cells;
        i += (int64_t)gridDim.x * blockDim.x) {
-    int c = (int)(i / cells);
-    double v;
-    if (kFixed) {
-      v = (double)gacc[i] / fixed_scale(absum[c], margin_bits);
-    } else {
-      v = (double)gacc[i];
+    for (int c = 0; c < nchan; ++c) {
+      const int64_t k = (int64_t)c * cells + i;
+      const double v = (double)gacc[k] * inv_scale[c];
+      out[k] = (Out)(v * inv_n);
     }
-    out[i] = (Out)(v * inv_n);
   }
 }
 
@@ -855,9 +857,9 @@ namespace flpr {
 
 static int finalize(const SpreadGeom& g, int64_t n, int nchan, bool fixed, int margin,
                     const SpreadWs& w, void* d_grid_out, cudaStream_t s) {
-  int64_t total = (int64_t)nchan * g.cells;
-  int fb = (int)((total + 255) / 256);
-  if (fb > 16 * sm_count()) fb = 16 * sm_count();
+  int64_t fb64 = (g.cells + 255) / 256;
+  if (fb64 > 16 * sm_count()) fb64 = 16 * sm_count();
+  const int fb = (int)fb64;
   double inv_n = 1.0 / (double)n;
   if (fixed) {
     finalize_kernel<long long, float, true><<<fb, 256, 0, s>>>(nchan, g.cells, (long long*)w.gacc,
