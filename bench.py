@@ -202,6 +202,22 @@ def _dist_env():
     return world, rank, local
 
 
+def replica_seed(rank: int) -> int:
+    """Seed of the data set a rank fits: every replica has its own data."""
+    return 1000 + rank
+
+
+def max_over_ranks(ms: float, world: int, device) -> float:
+    """The slowest rank's elapsed time (the job's time for weak scaling)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args):
     world, rank, _ = _dist_env()
     if rank != 0:
@@ -306,7 +322,7 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    x, y, h, opts = workload(1000 + rank, args.points)
+    x, y, h, opts = workload(replica_seed(rank), args.points)
     if args.grid:
         opts["N"] = [args.grid, args.grid]
     if args.bandwidths:
@@ -349,12 +365,7 @@ def run_ours(args):
         e.record()
         torch.cuda.synchronize()
         barrier()
-        ms = s.elapsed_time(e)
-        if world > 1:
-            t = torch.tensor([ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(s.elapsed_time(e), world, dev)
 
     clocks = ClockSampler(local)
     clocks.start()
