@@ -253,18 +253,24 @@ def run_reference(args):
     return 0
 
 
-def run_batched(args, dev):
+def run_batched(args, dev, world: int = 1, rank: int = 0, barrier=lambda: None):
     """The batched uneven workload through LprPlan: every problem's
     y-dependent work captured in one CUDA graph over concurrent streams and
     replayed; each step replaces all responses (fresh noise, pinned staging,
     host-to-device copies inside the timed region) and returns every
-    RegressionOutput.  Compared with one cv_fastlpr call per problem."""
+    RegressionOutput.  Compared with one cv_fastlpr call per problem.  With
+    several ranks the problems are split between them by estimated cost and
+    the batch time is the slowest rank's (no other collective)."""
     import torch
 
     import fastlpr_b200
+    from fastlpr_b200.plan import estimated_cost, partition_by_cost
     count = args.batched
-    probs = batched_workload(count=count)
-    ys = [[p[1] for p in probs], [p[1] for p in batched_workload(count=count, y_seed=1)]]
+    allp = batched_workload(count=count)
+    ally = batched_workload(count=count, y_seed=1)
+    mine = partition_by_cost([estimated_cost(*p) for p in allp], world)[rank]
+    probs = [allp[i] for i in mine]
+    ys = [[p[1] for p in probs], [ally[i][1] for i in mine]]
     t0 = time.perf_counter()
     plan = fastlpr_b200.LprPlan(probs, device=dev)
     build_s = time.perf_counter() - t0
@@ -272,10 +278,11 @@ def run_batched(args, dev):
         plan.run(ys[k % 2])
     torch.cuda.synchronize(dev)
     steps = max(2, min(args.steps, 5))
+    barrier()
     t0 = time.perf_counter()
     for k in range(steps):
         plan.run(ys[k % 2])
-    ms = 1000.0 * (time.perf_counter() - t0) / steps
+    ms = max_over_ranks(1000.0 * (time.perf_counter() - t0) / steps, world, dev)
     s = torch.cuda.Event(enable_timing=True)
     e = torch.cuda.Event(enable_timing=True)
     s.record()
@@ -283,12 +290,13 @@ def run_batched(args, dev):
     e.record()
     e.synchronize()
     replay_ms = s.elapsed_time(e)
+    barrier()
     t0 = time.perf_counter()
     for (x, y, h, o) in probs:
         fastlpr_b200.cv_fastlpr(x, y, h, o)
     torch.cuda.synchronize(dev)
-    seq_ms = 1000.0 * (time.perf_counter() - t0)
-    npts = int(sum(p[0].shape[0] for p in probs))
+    seq_ms = max_over_ranks(1000.0 * (time.perf_counter() - t0), world, dev)
+    npts = int(sum(p[0].shape[0] for p in allp))
     return {
         "workload": (f"{count} independent problems: half 1-D (grid 1024), half 2-D (grid 256^2), "
                      "N lognormal median 5e4 clipped [1e3,1e6], orders 0-2, 25% complex, 24 h; "
@@ -299,6 +307,7 @@ def run_batched(args, dev):
         "sequential_fits_per_s": count * 1000.0 / seq_ms,
         "speedup_vs_sequential": seq_ms / ms,
         "streams": len(plan.streams), "plan_build_s": build_s,
+        "ranks": world, "problems_per_rank": len(probs),
         "timing": "wall clock per step (host staging, replay, reductions, outputs), after 2 warm-up steps",
     }
 
@@ -425,7 +434,7 @@ def run_ours(args):
 
     batched = None
     if args.batched and not args.bandwidths and args.points == N_POINTS:
-        batched = run_batched(args, dev)
+        batched = run_batched(args, dev, world, rank, barrier)
 
     per_step_ms = ms_dev / args.steps
     value = world * 1000.0 / per_step_ms

@@ -44,6 +44,37 @@ def _cost(p) -> float:
     return p.su.n * (p.su.dy + 11) * (3 ** p.d) + len(p.filt[2]) * nprod * L
 
 
+def estimated_cost(x, y, h, options) -> float:
+    """Relative device time of one problem from its sizes alone (points,
+    dimension, order, response channels, bandwidths, padded grid), for
+    splitting a set of problems between GPUs before any work is done."""
+    x = np.asarray(x)
+    n = x.shape[0]
+    d = 1 if x.ndim == 1 else x.shape[1]
+    opts = dict(options or {})
+    order = int(opts.get("order", 0))
+    dy = (1 if np.asarray(y).ndim == 1 else np.asarray(y).shape[1]) * \
+        (2 if np.iscomplexobj(y) else 1)
+    G = api._grid_shape(opts, n, d)
+    L = 2.0 ** np.ceil(np.log2(2 * G - 1))
+    H = np.atleast_2d(np.asarray(h)).shape[0]
+    nprod = (len(api._element_powers(d, order)) + (dy + 10) *
+             (1 if order == 0 else len(api._design_powers(d, order))))
+    return float(n * (dy + 11) * (3 ** d) + H * nprod * np.prod(L) * (2.0 if order == 2 else 1.0))
+
+
+def partition_by_cost(costs: Sequence[float], parts: int) -> List[List[int]]:
+    """Indices split into `parts` groups of similar total cost (largest
+    first, each to the least loaded group)."""
+    groups: List[List[int]] = [[] for _ in range(max(1, parts))]
+    load = [0.0] * len(groups)
+    for i in sorted(range(len(costs)), key=lambda i: -costs[i]):
+        k = int(np.argmin(load))
+        groups[k].append(i)
+        load[k] += costs[i]
+    return [sorted(g) for g in groups]
+
+
 class LprPlan:
     """A set of LPR fits captured as one CUDA graph (see the module docstring).
 

@@ -61,3 +61,18 @@ def test_reference_arm_runs_on_rank_zero_only():
                        capture_output=True, text=True, env=env, timeout=120)
     assert p.returncode == 0
     assert p.stdout.strip() == ""
+
+
+def test_batched_problems_split_between_ranks_by_cost():
+    """Problem sharding of the batched workload: every problem goes to
+    exactly one rank and the ranks' estimated loads are close."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from fastlpr_b200.plan import estimated_cost, partition_by_cost
+    probs = bench.batched_workload(count=64)
+    costs = [estimated_cost(*p) for p in probs]
+    for world in (1, 2, 4):
+        parts = partition_by_cost(costs, world)
+        assert sorted(i for p in parts for i in p) == list(range(64))
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) <= 1.2 * min(loads)
