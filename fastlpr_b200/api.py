@@ -1300,7 +1300,11 @@ def _start_summary(ctx, pending: dict, dx, ycols, stats, n, d) -> None:
 def _learned_search(ctx, st: _LprState, bandwidths: np.ndarray, model, ev, pending: dict):
     """Proposal + five-bandwidth window, walked toward an edge minimum (the
     next window shares the edge bandwidth) at most _MAX_WALKS times; returns
-    (evaluation, search record) or None when the full sweep must run."""
+    (evaluation, search record, pending outputs or None) or None when the
+    full sweep must run.  The first window is evaluated speculatively: its
+    GCV, 1-SE choice and output stage are enqueued on the device together
+    and one synchronisation brings back the scores that decide acceptance
+    with the outputs (used as they are when the window is accepted)."""
     from . import learned as _learned
     if not (st.calc_dof and st.ny == 1 and not st.y_is_complex and st.d <= 2
             and st.kid == 0) or not pending:
@@ -1319,16 +1323,26 @@ def _learned_search(ctx, st: _LprState, bandwidths: np.ndarray, model, ev, pendi
     window = _learned.refine_window(t, lh)
     record = {"mode": "learned", "proposal_index": t, "windows": [], "nlist": nlist,
               "accepted": False}
-    for _ in range(_MAX_WALKS + 1):
+    for walk in range(_MAX_WALKS + 1):
         record["windows"].append([int(i) for i in window])
-        r = _evaluate_lpr(ctx, st, bandwidths[window], ev)
-        if r["H"] != len(window):
+        filt = _filter_bandwidths(ctx, st.geom, bandwidths[window], 2 * st.order + 1, st.kid)
+        if len(filt[2]) != len(window):
             return None                     # a bandwidth of the window was filtered out
-        pos = int(np.argmin(r["gcv"]["gcv_m"]))
+        pend = None
+        if walk == 0:
+            r = _evaluate_device(ctx, st, filt, ev)
+            pend = _finalize_enqueue(ctx, st, r, ev, device_select=True)
+            torch.cuda.current_stream(ctx.device).synchronize()
+            gcv_m = pend["gcv"].numpy()[:len(window)]
+        else:
+            r = _evaluate_device(ctx, st, filt, ev)
+            r = _evaluate_host(st, r, r["packed"].cpu().numpy())
+            gcv_m = r["gcv"]["gcv_m"]
+        pos = int(np.argmin(gcv_m))
         if _learned.accept_window(window, pos, nlist):
             record["accepted"] = True
             record["evaluated"] = len({i for w in record["windows"] for i in w})
-            return r, record
+            return r, record, pend
         step = _learned.REFINE - 1
         lo = int(window[0]) + (step if pos == len(window) - 1 else -step)
         lo = int(np.clip(lo, 0, nlist - _learned.REFINE))
@@ -1356,7 +1370,9 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
     found = (_learned_search(ctx, st, bandwidths, learned, ev, pending)
              if learned is not None else None)
     if found is not None:
-        r, search = found
+        r, search, pend = found
+        if pend is not None:
+            return _finalize_build(ctx, st, r, pend, ev, search)
         return _finalize_lpr(ctx, st, r, ev, search)
     # full sweep: GCV, the 1-SE choice and the output stage are enqueued on
     # the device behind the reductions; one synchronisation at the end
