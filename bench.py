@@ -357,6 +357,7 @@ def run_ours(args):
                           "h": [float(v) for v in np.atleast_1d(r.h)]}), flush=True)
         return 0
     warm = max(args.warmup, 3)
+    counts = {}
 
     def timed(fn, steps):
         # W untimed steps of this same path right before its timed steps
@@ -366,6 +367,7 @@ def run_ours(args):
             fn()
         barrier()
         torch.cuda.synchronize()
+        counts["l0"] = lib.flpr_launch_count()
         s = torch.cuda.Event(enable_timing=True)
         e = torch.cuda.Event(enable_timing=True)
         s.record()
@@ -373,19 +375,19 @@ def run_ours(args):
             fn()
         e.record()
         torch.cuda.synchronize()
+        counts["launches"] = (lib.flpr_launch_count() - counts["l0"]) // max(1, steps)
         barrier()
         return max_over_ranks(s.elapsed_time(e), world, dev)
 
     clocks = ClockSampler(local)
     clocks.start()
-    l0 = lib.flpr_launch_count()
     res = {}
 
     def step_dev():
         res["r"] = fastlpr_b200.cv_fastlpr_device(xd, yd, h, opts)
 
     ms_dev = timed(step_dev, args.steps)
-    launches = (lib.flpr_launch_count() - l0) // max(1, args.steps)
+    launches = counts["launches"]
 
     def step_e2e():
         res["e"] = fastlpr_b200.cv_fastlpr(xh, yh, h, opts)
