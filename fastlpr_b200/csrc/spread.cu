@@ -223,13 +223,19 @@ struct AccOps<double> {
 };
 
 // Fixed-point scale 2^e per channel so that |sum| over any subset of
-// contributions stays below 2^62 (each point adds at most |v| to a cell when
-// the taps do not wrap onto the same cell).
+// contributions stays below 2^50 (each point adds at most |v| to a cell when
+// the taps do not wrap onto the same cell): every rounded product and every
+// partial sum is then an integer that a double holds exactly, so the 2-D
+// path can round and add in FP64 registers and still be exact and
+// independent of the order of the points.  The quantum, 2^-50 of the
+// channel's absolute sum, is far below the FP32 rounding of the grid.
+constexpr int kFixedBits = 50;
+
 __device__ __forceinline__ double fixed_scale(double absum, int margin_bits) {
   if (!(absum > 0.0)) return 1.0;
   int e = 0;
   frexp(absum, &e);  // absum < 2^e
-  return ldexp(1.0, 62 - e - margin_bits);
+  return ldexp(1.0, kFixedBits - e - margin_bits);
 }
 
 __device__ __forceinline__ float fexp(float v) { return expf(v); }
@@ -365,15 +371,32 @@ constexpr int kT2 = 8;         // tile edge of the 2-D path
 constexpr int kBatch2 = 256;   // points per batch (one per thread while caching)
 constexpr int kUnitCh = 2;     // channels per lane
 
+// Register accumulators hold doubles in both precisions.  Fixed point: each
+// product is rounded to the nearest integer (ties to even, like
+// __double2ll_rn) by adding and subtracting 1.5 * 2^52 (exact for
+// |v| < 2^51), and the integer sums stay below 2^50, so every addition is
+// exact; the flush converts the exact integer sum once.
 template <typename Acc>
-__device__ __forceinline__ void reg_add(Acc& a, double v);
+__device__ __forceinline__ void reg_add(double& a, double v);
 template <>
-__device__ __forceinline__ void reg_add<long long>(long long& a, double v) {
-  a += __double2ll_rn(v);
+__device__ __forceinline__ void reg_add<long long>(double& a, double v) {
+  constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
+  a = __dadd_rn(a, __dsub_rn(__dadd_rn(v, kRound), kRound));
 }
 template <>
 __device__ __forceinline__ void reg_add<double>(double& a, double v) {
   a += v;
+}
+
+template <typename Acc>
+__device__ __forceinline__ Acc reg_value(double a);
+template <>
+__device__ __forceinline__ long long reg_value<long long>(double a) {
+  return __double2ll_rn(a);
+}
+template <>
+__device__ __forceinline__ double reg_value<double>(double a) {
+  return a;
 }
 
 __device__ __forceinline__ void shared_add(long long* p, long long v) {
@@ -486,11 +509,11 @@ tile_accumulate_2d_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, 
       const int grp = gb * GPL + gsub;
       const bool active = lane < NT1 * GPL && grp < ngrp;
       const int c0 = grp * kUnitCh;
-      Acc a[kUnitCh][NACC];
+      double a[kUnitCh][NACC];
 #pragma unroll
       for (int k = 0; k < kUnitCh; ++k)
 #pragma unroll
-        for (int j = 0; j < NACC; ++j) a[k][j] = Acc(0);
+        for (int j = 0; j < NACC; ++j) a[k][j] = 0.0;
       const int rowbase = l0 * kT2;
 #pragma unroll
       for (int cr = 0; cr < kT2; ++cr) {
@@ -516,7 +539,8 @@ tile_accumulate_2d_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, 
           if (c0 + k >= nc) break;
 #pragma unroll
           for (int j = 0; j < NACC; ++j)
-            if (a[k][j] != Acc(0)) shared_add(rowp + (size_t)(c0 + k) * CS + j, a[k][j]);
+            if (a[k][j] != 0.0)
+              shared_add(rowp + (size_t)(c0 + k) * CS + j, reg_value<Acc>(a[k][j]));
         }
       }
     }
