@@ -346,6 +346,10 @@ def run_ours(args):
     xh, yh = xp.numpy(), yp.numpy()
 
     lib = _lib.load()
+    if args.only_batched:
+        # the batched leg alone (profiling): no metric fits before it
+        print(json.dumps(run_batched(args, dev, world, rank, barrier)), flush=True)
+        return 0
     if args.single_fit:
         # one plain fit and nothing else: the command profiles are captured with
         l0 = lib.flpr_launch_count()
@@ -517,6 +521,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched", type=int, default=512,
                     help="problems of the batched workload leg (0: skip)")
+    ap.add_argument("--only-batched", action="store_true",
+                    help="run only the batched workload leg (profiling)")
     ap.add_argument("--single-fit", action="store_true",
                     help="run one plain fit of the workload and exit (for profilers)")
     ap.add_argument("--points", type=int, default=N_POINTS,
