@@ -106,22 +106,27 @@ __global__ void product_kernel(ConvArgs ca, int nb, ProdBatch desc,
                                const double2* __restrict__ F,
                                typename Cplx<Real>::type* __restrict__ out) {
   using C = typename Cplx<Real>::type;
-  const int64_t total = (int64_t)nb * ca.half;
-  const int Llast_half = ca.L[ca.d - 1] / 2 + 1;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int b = (int)(t / ca.half);
-    int64_t w = t - (int64_t)b * ca.half;
+  // a batch holds fewer than 2^31 elements (conv_batch budget): 32-bit indices
+  const unsigned total = (unsigned)nb * (unsigned)ca.half;
+  const unsigned half = (unsigned)ca.half;
+  const unsigned Llast_half = ca.L[ca.d - 1] / 2 + 1;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned bu = t / half;
+    const int b = (int)bu;
+    const unsigned w = t - bu * half;
     const ProdDesc pd = desc.p[b];
     // decode frequency index (row-major, last axis half length)
     int om[3] = {0, 0, 0};
     {
-      int64_t r = w;
-      om[ca.d - 1] = (int)(r % Llast_half);
-      r /= Llast_half;
+      unsigned r = w;
+      unsigned q = r / Llast_half;
+      om[ca.d - 1] = (int)(r - q * Llast_half);
+      r = q;
       for (int a = ca.d - 2; a >= 0; --a) {
-        om[a] = (int)(r % ca.L[a]);
-        r /= ca.L[a];
+        const unsigned La = ca.L[a];
+        q = r / La;
+        om[a] = (int)(r - q * La);
+        r = q;
       }
     }
     double kr = ca.scale, ki = 0.0;
@@ -143,22 +148,26 @@ __global__ void product_kernel(ConvArgs ca, int nb, ProdBatch desc,
 template <typename Real>
 __global__ void crop_kernel(ConvArgs ca, int nb, int p0, const Real* __restrict__ full,
                             int add_eps, Real* __restrict__ out) {
-  const int64_t total = (int64_t)nb * ca.M;
+  const unsigned M = (unsigned)ca.M;
+  const unsigned total = (unsigned)nb * M;
   const double eps = 2.220446049250313e-16;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int b = (int)(t / ca.M);
-    int64_t g = t - (int64_t)b * ca.M;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned bu = t / M;
+    const int b = (int)bu;
+    const unsigned g0 = t - bu * M;
+    unsigned g = g0;
     int gc[3] = {0, 0, 0};
     for (int a = ca.d - 1; a >= 0; --a) {
-      gc[a] = (int)(g % ca.G[a]);
-      g /= ca.G[a];
+      const unsigned Ga = ca.G[a];
+      const unsigned q = g / Ga;
+      gc[a] = (int)(g - q * Ga);
+      g = q;
     }
     int64_t src = 0;
     for (int a = 0; a < ca.d; ++a) src = src * ca.L[a] + (gc[a] + ca.qout[a]);
     Real v = full[(int64_t)b * ca.cells + src];
     if (add_eps) v = (Real)((double)v + eps);
-    out[(int64_t)(p0 + b) * ca.M + (t - (int64_t)b * ca.M)] = v;
+    out[(int64_t)(p0 + b) * ca.M + g0] = v;
   }
 }
 
@@ -288,14 +297,17 @@ __global__ void sep_colprod_kernel(SepArgs sa, int jc, int nj, SepJobs jobs,
                                    const double2* __restrict__ F,
                                    typename Cplx<Real>::type* __restrict__ col) {
   using C = typename Cplx<Real>::type;
-  const int64_t total = (int64_t)sa.L0 * jc * sa.L1h;
+  // sizes here stay below 2^31 (the buffers are bounded by the workspace
+  // budget): 32-bit index arithmetic
+  const unsigned total = (unsigned)sa.L0 * jc * sa.L1h;
   const int64_t half = (int64_t)sa.L0 * sa.L1h;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int w1 = (int)(t % sa.L1h);
-    const int64_t r = t / sa.L1h;
-    const int j = (int)(r % jc);
-    const int w0 = (int)(r / jc);
+  const unsigned L1h = sa.L1h, ujc = jc;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned r = t / L1h;
+    const int w1 = (int)(t - r * L1h);
+    const unsigned w0u = r / ujc;
+    const int j = (int)(r - w0u * ujc);
+    const int w0 = (int)w0u;
     C o;
     if (j < nj) {
       const double2 f = F[((int64_t)jobs.hidx[j] * sa.npow + jobs.p0[j]) * sa.L0 + w0];
@@ -317,13 +329,14 @@ __global__ void sep_rowprod_kernel(SepArgs sa, int jc, int np, int pc, SepProds 
                                    const double2* __restrict__ F,
                                    typename Cplx<Real>::type* __restrict__ row) {
   using C = typename Cplx<Real>::type;
-  const int64_t total = (int64_t)pc * sa.G0 * sa.L1h;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int w1 = (int)(t % sa.L1h);
-    const int64_t r = t / sa.L1h;
-    const int x0 = (int)(r % sa.G0);
-    const int p = (int)(r / sa.G0);
+  const unsigned total = (unsigned)pc * sa.G0 * sa.L1h;
+  const unsigned L1h = sa.L1h, G0 = sa.G0;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned r = t / L1h;
+    const int w1 = (int)(t - r * L1h);
+    const unsigned pu = r / G0;
+    const int x0 = (int)(r - pu * G0);
+    const int p = (int)pu;
     C o;
     if (p < np) {
       const double2 f = F[sa.f1off + ((int64_t)prods.hidx[p] * sa.npow + prods.p1[p]) * sa.L1 + w1];
@@ -343,14 +356,16 @@ __global__ void sep_rowprod_kernel(SepArgs sa, int jc, int np, int pc, SepProds 
 template <typename Real>
 __global__ void sep_crop_kernel(SepArgs sa, int np, SepProds prods, const Real* __restrict__ real,
                                 int add_eps, Real* __restrict__ out) {
-  const int64_t M = (int64_t)sa.G0 * sa.G1;
-  const int64_t total = (int64_t)np * M;
+  const unsigned M = (unsigned)sa.G0 * sa.G1;
+  const unsigned total = (unsigned)np * M;
+  const unsigned G1 = sa.G1;
   const double eps = 2.220446049250313e-16;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int p = (int)(t / M);
-    const int64_t g = t - (int64_t)p * M;
-    const int x0 = (int)(g / sa.G1), x1 = (int)(g - (int64_t)x0 * sa.G1);
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned pu = t / M;
+    const unsigned g = t - pu * M;
+    const unsigned x0u = g / G1;
+    const int p = (int)pu;
+    const int x0 = (int)x0u, x1 = (int)(g - x0u * G1);
     Real v = real[((int64_t)p * sa.G0 + x0) * sa.L1 + sa.q1 + x1];
     if (add_eps) v = (Real)((double)v + eps);
     out[(int64_t)prods.out[p] * M + g] = v;
@@ -588,6 +603,8 @@ int flpr_conv(flpr_handle_t handle, int d, const int* h_G, const int* h_L, const
     return FLPR_ERR_WORKSPACE;
   }
   const int B = conv_batch(d, h_L, nprod, prec);
+  FLPR_CHECK_ARG((int64_t)B * ca.cells < ((int64_t)1 << 31),
+                 "conv: grid too large for 32-bit batch indexing");
   const size_t es = prec == FLPR_PREC_F32 ? 4 : 8;
   Arena ar(d_ws, ws_bytes);
   char* pbuf = ar.take<char>((size_t)B * ca.half * 2 * es);
@@ -712,6 +729,9 @@ int flpr_conv2d_sep(flpr_handle_t handle, const int* h_G, const int* h_L, const 
     return FLPR_ERR_WORKSPACE;
   }
   const SepSizes z = sep_sizes(h_G, h_L, nprod, prec);
+  FLPR_CHECK_ARG((int64_t)h_L[0] * z.jc * (h_L[1] / 2 + 1) < ((int64_t)1 << 31) &&
+                     (int64_t)z.pc * h_G[0] * h_L[1] < ((int64_t)1 << 31),
+                 "conv2d_sep: pass sizes exceed 32-bit indexing");
   SepArgs sa{};
   sa.L0 = h_L[0];
   sa.L1 = h_L[1];
@@ -899,6 +919,8 @@ int flpr_conv_full(flpr_handle_t handle, int d, const int* h_G, const int* h_L, 
     return FLPR_ERR_WORKSPACE;
   }
   const int B = conv_batch(d, h_L, nprod, prec);
+  FLPR_CHECK_ARG((int64_t)B * ca.cells < ((int64_t)1 << 31),
+                 "conv_full: grid too large for 32-bit batch indexing");
   const size_t es = prec == FLPR_PREC_F32 ? 4 : 8;
   Arena ar(d_ws, ws_bytes);
   char* pbuf = ar.take<char>((size_t)B * ca.half * 2 * es);
