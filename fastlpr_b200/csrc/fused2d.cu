@@ -27,7 +27,7 @@ namespace {
 
 constexpr int kColWarps = 8;    // columns per column-pass CTA (one per warp)
 constexpr int kRowWarps = 8;    // (row, job) items per S row-pass CTA (one per warp)
-constexpr int kMaxTWarps = 8;   // warps of a T row-pass CTA
+constexpr int kTWarps = 6;      // warps of a T row-pass CTA (12 products per round)
 constexpr int kMaxSlots = 64;
 constexpr int kMaxJobs = 64;
 constexpr size_t kMaxSmem = 227 * 1024;
@@ -417,30 +417,29 @@ rowpass_s_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
   }
 }
 
-// Shared memory of the T pass: twiddles, one transpose buffer per warp, and
-// 2*G1 floats for each job that is not the last job of its warp (the last
-// job of warp w leaves its results in w's own buffer).
+// Shared memory of the T pass: twiddles and one transpose buffer per warp
+// (a warp's job leaves its two cropped products there for its round).
 inline size_t t_smem_bytes(int E, int nwarps, int njobs, int G1) {
-  const int extra = njobs > nwarps ? njobs - nwarps : 0;
+  (void)njobs;
+  (void)G1;
   return sizeof(float2) * (size_t)twiddle_entries(32 * E) +
-         sizeof(float) * ((size_t)nwarps * warp_buf_stride(E) + (size_t)extra * 2 * G1);
+         sizeof(float) * (size_t)nwarps * warp_buf_stride(E);
 }
 
-// Warps of a T-pass CTA: as few rounds of at most kMaxTWarps jobs as
-// possible, spread evenly.
-inline int t_warps(int njobs) {
-  const int rounds = (njobs + kMaxTWarps - 1) / kMaxTWarps;
-  return (njobs + rounds - 1) / rounds;
-}
+// Warps of a T-pass CTA: rounds of kTWarps jobs (12 products: whole
+// channels for NT = 1, 3 and 6), or one round when there are fewer jobs.
+inline int t_warps(int njobs) { return njobs < kTWarps ? njobs : kTWarps; }
 
 // T pass fused with the solve and the dual-form reductions: grid (Hc, G0),
-// t_warps(njobs) warps.  Warp w computes jobs w, w + nwarps, ...; product
-// p = c * NT + i (job p / 2, half p % 2) stays in shared memory until every
-// job of the row is done; then m_c(x1) = sum_i z_i(x1) T(p, x1) with z the
-// row's solve vectors, the response fits go to `my`, and sum_x1 m_c Q_c goes
-// to one partial per (c, h, row).
+// t_warps(njobs) warps.  Product p = c * NT + i is half p % 2 of job p / 2.
+// In round r the warps compute jobs r * nwarps + w, each leaving its two
+// cropped products in its own buffer; then, for the channels completed in
+// that round, m_c(x1) = sum_i z_i(x1) T(p, x1) with z the row's solve
+// vectors, the response fits go to `my`, and sum_x1 m_c Q_c accumulates into
+// one partial per (c, h, row).  Nothing is staged across rounds, which keeps
+// the CTA's shared memory small.
 template <int E, int NT>
-__global__ void __launch_bounds__(kMaxTWarps * 32, 2)
+__global__ void __maxnreg__(112)
 rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
                        const float2* __restrict__ F1f, const float2* __restrict__ tab,
                        const int* __restrict__ kcut1, int C, int ny, const double* __restrict__ zg,
@@ -449,12 +448,11 @@ rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict
   constexpr int N = 32 * E;
   constexpr int SW = warp_buf_stride(E);
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double red[kMaxTWarps * 32];
+  __shared__ double red[kTWarps * 32];
   float2* s_tw2 = reinterpret_cast<float2*>(smem_raw);
   float2* s_tw32 = s_tw2 + N;
   float* bufs = reinterpret_cast<float*>(s_tw2 + twiddle_entries(N));
   const int nwarps = blockDim.x >> 5;
-  float* regions = bufs + (size_t)nwarps * SW;
   // bandwidth fastest: the CTAs of one row (sharing its deposits Q) run together
   const int hz = blockIdx.x, r = blockIdx.y, h = ra.hbase + hz;
   const int64_t M = (int64_t)ra.G0 * ra.G1;
@@ -481,46 +479,50 @@ rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict
   load_twiddles<E>(s_tw2, tab);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int last0 = njobs - nwarps;  // jobs >= last0 are the last of their warp
   float* buf = bufs + warp * SW;
   const int kc = kcut1[h];
-  for (int j = warp; j < njobs; j += nwarps) {
-    const RowJob jb = ra.jobs[j];
-    const bool pair = jb.slot_b >= 0;
-    float2 v[E];
-    row_fft<E>(ra, jb, r, hz, h, nslots_w, W, F1f, s_tw2, s_tw32, buf, lane, kc, v);
-    float* dst = j >= last0 ? buf : regions + (size_t)j * 2 * G1;
+  const int nprod = C * NT;
+  for (int r0 = 0; r0 < njobs; r0 += nwarps) {
+    const int j = r0 + warp;
+    if (j < njobs) {
+      const RowJob jb = ra.jobs[j];
+      const bool pair = jb.slot_b >= 0;
+      float2 v[E];
+      row_fft<E>(ra, jb, r, hz, h, nslots_w, W, F1f, s_tw2, s_tw32, buf, lane, kc, v);
 #pragma unroll
-    for (int s = 0; s < E; ++s) {
-      const int x = out_index<E>(lane, s) - ra.q1;
-      if (x >= 0 && x < G1) {
-        dst[x] = v[s].x;
-        if (pair) dst[G1 + x] = v[s].y;
+      for (int s = 0; s < E; ++s) {
+        const int x = out_index<E>(lane, s) - ra.q1;
+        if (x >= 0 && x < G1) {
+          buf[x] = v[s].x;
+          if (pair) buf[G1 + x] = v[s].y;
+        }
       }
     }
-    __syncwarp();
-  }
-  __syncthreads();
-  for (int c = 0; c < C; ++c) {
-    const float* src[NT];
+    __syncthreads();
+    // channels whose NT products all came out of this round
+    const int p_end = min(nprod, 2 * (r0 + nwarps));
+    const int c_begin = (2 * r0) / NT, c_end = p_end / NT;
+    for (int c = c_begin; c < c_end; ++c) {
+      const float* src[NT];
 #pragma unroll
-    for (int i = 0; i < NT; ++i) {
-      const int p = c * NT + i, j = p >> 1;
-      src[i] = (j >= last0 ? bufs + (size_t)(j % nwarps) * SW : regions + (size_t)j * 2 * G1) +
-               (p & 1) * G1;
-    }
-    double acc = 0.0;
-    for (int x = threadIdx.x; x < G1; x += blockDim.x) {
-      const int64_t g = (int64_t)r * G1 + x;
-      const double* z = zg + ((int64_t)h * M + g) * NT;
-      double m = 0.0;
+      for (int i = 0; i < NT; ++i) {
+        const int p = c * NT + i, jj = p >> 1;
+        src[i] = bufs + (size_t)(jj - r0) * SW + (p & 1) * G1;
+      }
+      double acc = 0.0;
+      for (int x = threadIdx.x; x < G1; x += blockDim.x) {
+        const int64_t g = (int64_t)r * G1 + x;
+        const double* z = zg + ((int64_t)h * M + g) * NT;
+        double m = 0.0;
 #pragma unroll
-      for (int i = 0; i < NT; ++i) m += z[i] * (double)src[i][x];
-      if (c < ny) my[((int64_t)h * M + g) * ny + c] = m;
-      acc += m * Q[g * C + c];
+        for (int i = 0; i < NT; ++i) m += z[i] * (double)src[i][x];
+        if (c < ny) my[((int64_t)h * M + g) * ny + c] = m;
+        acc += m * Q[g * C + c];
+      }
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) red[c * nwarps + warp] = acc;  // C * nwarps <= 32 * kTWarps
     }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) red[c * nwarps + warp] = acc;  // C * nwarps <= 32 * kMaxTWarps
+    __syncthreads();  // the next round overwrites the buffers
   }
   __syncthreads();
   for (int c = threadIdx.x; c < C; c += blockDim.x) {
@@ -913,6 +915,9 @@ int fused2d_check(const int* G, const int* L, const int* qout, int H, int order,
   const int nwarps = t_warps(tb->t_row.njobs);
   FLPR_CHECK_ARG(t_smem_bytes(L[1] / 32, nwarps, tb->t_row.njobs, G[1]) <= kMaxSmem,
                  "fused2d: T row tile does not fit shared memory");
+  // a round's products must be whole channels
+  FLPR_CHECK_ARG(tb->t_row.njobs <= kTWarps || (2 * kTWarps) % tb->nt == 0,
+                 "fused2d: %d terms per channel do not divide a T round", tb->nt);
   fused_geom(G, L, qout, H, *tb, fg);
   return FLPR_OK;
 }
