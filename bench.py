@@ -312,6 +312,49 @@ def run_batched(args, dev, world: int = 1, rank: int = 0, barrier=lambda: None):
     }
 
 
+def kde3d_workload(n: int, seed: int = 5):
+    """The 3-D KDE case: a mixture of 8 anisotropic Gaussians (means
+    U[0.2,0.8]^3, per-axis std U[0.02,0.1], equal weights) plus 10% uniform
+    background on [0,1]^3; grid 128^3, 16 isotropic h in [0.01, 0.3]."""
+    rng = np.random.default_rng(seed)
+    nb = n // 10
+    means = rng.uniform(0.2, 0.8, (8, 3))
+    sds = rng.uniform(0.02, 0.1, (8, 3))
+    comp = rng.integers(0, 8, n - nb)
+    x = np.vstack([means[comp] + sds[comp] * rng.standard_normal((n - nb, 3)), rng.random((nb, 3))])
+    hv = np.logspace(np.log10(0.01), np.log10(0.3), 16)
+    return x, np.column_stack([hv] * 3), {"N": [128, 128, 128]}
+
+
+def run_profile_case(args, dev):
+    """One small fit of a kind the benchmark leg does not run, for kernel
+    profiles: 'kde3d' (3-D KDE, grid 128^3), 'learned' (learned search on
+    the benchmark data), 'cubic2d' (2-D, n = 3000: cubic GCV/DoF), 'order2'
+    (2-D local quadratic, FP64 separable convolution)."""
+    import torch
+
+    import fastlpr_b200
+    case = args.profile_case
+    t0 = time.perf_counter()
+    if case == "kde3d":
+        x, h, o = kde3d_workload(args.points)
+        r = fastlpr_b200.cv_fastkde(x, h, dict(o, device=str(dev)))
+    else:
+        n = {"learned": args.points, "cubic2d": 3000, "order2": 50000}[case]
+        x, y, h, o = workload(0, n)
+        opts = dict(o, device=str(dev))
+        if case == "learned":
+            opts.update(precision="fp32", bandwidth_search="learned")
+        elif case == "cubic2d":
+            opts.update(N=[64, 64])
+        else:
+            opts.update(order=2, N=[256, 256])
+        r = fastlpr_b200.cv_fastlpr(x, y, h, opts)
+    torch.cuda.synchronize(dev)
+    return {"profile_case": case, "seconds": time.perf_counter() - t0,
+            "h": [float(v) for v in np.atleast_1d(r.h)]}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -346,6 +389,9 @@ def run_ours(args):
     xh, yh = xp.numpy(), yp.numpy()
 
     lib = _lib.load()
+    if args.profile_case:
+        print(json.dumps(run_profile_case(args, dev)), flush=True)
+        return 0
     if args.only_batched:
         # the batched leg alone (profiling): no metric fits before it
         print(json.dumps(run_batched(args, dev, world, rank, barrier)), flush=True)
@@ -523,6 +569,9 @@ def main():
                     help="problems of the batched workload leg (0: skip)")
     ap.add_argument("--only-batched", action="store_true",
                     help="run only the batched workload leg (profiling)")
+    ap.add_argument("--profile-case", default="",
+                    choices=["", "kde3d", "learned", "cubic2d", "order2"],
+                    help="run one small fit of another kind (profiling)")
     ap.add_argument("--single-fit", action="store_true",
                     help="run one plain fit of the workload and exit (for profilers)")
     ap.add_argument("--points", type=int, default=N_POINTS,
