@@ -2,6 +2,8 @@
 same results as separate cv_fastlpr calls (the same kernels run; FP64
 atomics make the last bits order dependent, hence rtol 1e-12 / the FP32
 bound), including replays with new responses."""
+import os
+
 import numpy as np
 import pytest
 
@@ -106,3 +108,44 @@ def test_cv_fastlpr_many_matches_oracle(cuda_ok):
         assert g.gcv_yhat["id1se"] == z["id1se"]
         assert rel_err(g.yhat, z["yhat"]) < 1e-9
         assert elem_rel_err(g.gcv_yhat["gcv_m"], z["gcv_m"]) < 1e-9
+
+
+def test_spread_item_size_does_not_change_results(cuda_ok):
+    """The autotuned spread work-item size only regroups the work: the
+    fixed-point spread is exact and order-independent, so the FP32 fit is
+    bitwise the same for every setting."""
+    import fastlpr_b200
+    from fastlpr_b200 import autotune
+    rng = np.random.default_rng(4)
+    x = rng.random((40000, 2))
+    y = np.sin(4 * x[:, 0]) + 0.1 * rng.standard_normal(40000)
+    hv = np.logspace(-1.7, -0.5, 6)
+    h = np.column_stack([hv, hv])
+    saved = autotune.get_params()
+    outs = []
+    try:
+        for ip in (1024, 8192):
+            autotune.set_params({"spread_item_points": ip})
+            outs.append(fastlpr_b200.cv_fastlpr(x, y, h, {"order": 1, "N": [96, 80],
+                                                          "precision": "fp32",
+                                                          "calc_dof": False}))
+    finally:
+        autotune.set_params(saved)
+    np.testing.assert_array_equal(outs[0].fpp_yhat.values, outs[1].fpp_yhat.values)
+
+
+def test_tune_fit_applies_a_candidate(cuda_ok, tmp_path, monkeypatch):
+    monkeypatch.setenv("FASTLPR_B200_CACHE", str(tmp_path / "c.json"))
+    from fastlpr_b200 import autotune
+    rng = np.random.default_rng(5)
+    x = rng.random((20000, 2))
+    y = np.cos(3 * x[:, 1]) + 0.1 * rng.standard_normal(20000)
+    hv = np.logspace(-1.5, -0.5, 4)
+    saved = autotune.get_params()
+    try:
+        rec = autotune.tune_fit(x, y, np.column_stack([hv, hv]), {"order": 1, "N": [64, 64]})
+        assert rec["best"]["spread_item_points"] in autotune.ITEM_POINTS
+        assert autotune.get_params()["spread_item_points"] == rec["best"]["spread_item_points"]
+        assert os.path.exists(tmp_path / "c.json")
+    finally:
+        autotune.set_params(saved)
