@@ -27,7 +27,7 @@ namespace {
 
 constexpr int kColWarps = 8;    // columns per column-pass CTA (one per warp)
 constexpr int kRowWarps = 8;    // (row, job) items per S row-pass CTA (one per warp)
-constexpr int kTWarps = 6;      // warps of a T row-pass CTA (12 products per round)
+constexpr int kTWarps = 4;      // warps of a T row-pass CTA (8 products per round)
 constexpr int kMaxSlots = 64;
 constexpr int kMaxJobs = 64;
 constexpr size_t kMaxSmem = 227 * 1024;
@@ -417,27 +417,30 @@ rowpass_s_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
   }
 }
 
-// Shared memory of the T pass: twiddles and one transpose buffer per warp
-// (a warp's job leaves its two cropped products there for its round).
+// Shared memory of the T pass: twiddles and two transpose buffers per warp
+// (rounds alternate between them; a warp's job leaves its two cropped
+// products there).
 inline size_t t_smem_bytes(int E, int nwarps, int njobs, int G1) {
   (void)njobs;
   (void)G1;
   return sizeof(float2) * (size_t)twiddle_entries(32 * E) +
-         sizeof(float) * (size_t)nwarps * warp_buf_stride(E);
+         sizeof(float) * (size_t)2 * nwarps * warp_buf_stride(E);
 }
 
-// Warps of a T-pass CTA: rounds of kTWarps jobs (12 products: whole
-// channels for NT = 1, 3 and 6), or one round when there are fewer jobs.
+// Warps of a T-pass CTA: rounds of kTWarps jobs, or one round when there
+// are fewer jobs.  Four warps at the 112-register cap let four CTAs share
+// an SM (16 warps; six-warp CTAs are allocated as eight warps, two CTAs).
 inline int t_warps(int njobs) { return njobs < kTWarps ? njobs : kTWarps; }
 
 // T pass fused with the solve and the dual-form reductions: grid (Hc, G0),
 // t_warps(njobs) warps.  Product p = c * NT + i is half p % 2 of job p / 2.
-// In round r the warps compute jobs r * nwarps + w, each leaving its two
-// cropped products in its own buffer; then, for the channels completed in
-// that round, m_c(x1) = sum_i z_i(x1) T(p, x1) with z the row's solve
-// vectors, the response fits go to `my`, and sum_x1 m_c Q_c accumulates into
-// one partial per (c, h, row).  Nothing is staged across rounds, which keeps
-// the CTA's shared memory small.
+// In round k the warps compute jobs k * nwarps + w, each leaving its two
+// cropped products in its buffer of parity k % 2; then, for the channels
+// completed in that round, m_c(x1) = sum_i z_i(x1) T(p, x1) with z the row's
+// solve vectors, the response fits go to `my`, and sum_x1 m_c Q_c
+// accumulates into one partial per (c, h, row).  A channel's NT products
+// span at most two consecutive rounds (NT <= 2 nwarps + 1), so the buffers
+// of the previous round still hold its earlier products.
 template <int E, int NT>
 __global__ void __maxnreg__(112)
 rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
@@ -479,11 +482,11 @@ rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict
   load_twiddles<E>(s_tw2, tab);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* buf = bufs + warp * SW;
   const int kc = kcut1[h];
   const int nprod = C * NT;
   for (int r0 = 0; r0 < njobs; r0 += nwarps) {
     const int j = r0 + warp;
+    float* buf = bufs + ((size_t)(((r0 / nwarps) & 1) * nwarps) + warp) * SW;
     if (j < njobs) {
       const RowJob jb = ra.jobs[j];
       const bool pair = jb.slot_b >= 0;
@@ -506,8 +509,8 @@ rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict
       const float* src[NT];
 #pragma unroll
       for (int i = 0; i < NT; ++i) {
-        const int p = c * NT + i, jj = p >> 1;
-        src[i] = bufs + (size_t)(jj - r0) * SW + (p & 1) * G1;
+        const int p = c * NT + i, jj = p >> 1, kk = jj / nwarps;
+        src[i] = bufs + ((size_t)((kk & 1) * nwarps) + (jj - kk * nwarps)) * SW + (p & 1) * G1;
       }
       double acc = 0.0;
       for (int x = threadIdx.x; x < G1; x += blockDim.x) {
@@ -915,9 +918,9 @@ int fused2d_check(const int* G, const int* L, const int* qout, int H, int order,
   const int nwarps = t_warps(tb->t_row.njobs);
   FLPR_CHECK_ARG(t_smem_bytes(L[1] / 32, nwarps, tb->t_row.njobs, G[1]) <= kMaxSmem,
                  "fused2d: T row tile does not fit shared memory");
-  // a round's products must be whole channels
-  FLPR_CHECK_ARG(tb->t_row.njobs <= kTWarps || (2 * kTWarps) % tb->nt == 0,
-                 "fused2d: %d terms per channel do not divide a T round", tb->nt);
+  // a channel's products span at most two consecutive T rounds
+  FLPR_CHECK_ARG(tb->t_row.njobs <= kTWarps || tb->nt <= 2 * kTWarps + 1,
+                 "fused2d: %d terms per channel span more than two T rounds", tb->nt);
   fused_geom(G, L, qout, H, *tb, fg);
   return FLPR_OK;
 }
