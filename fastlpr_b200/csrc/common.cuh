@@ -112,6 +112,54 @@ inline int sm_count() {
   return cached;
 }
 
+// Shared-memory carveout of `kernel` sized for as many CTAs per SM as its
+// registers and `dyn_smem` allow at the largest carveout; the rest of the
+// unified L1/shared array stays L1.  Both attributes are set on every call
+// (another size may have been set since); the occupancy query runs once per
+// (device, kernel, size, threads).
+template <typename K>
+inline cudaError_t fit_carveout(K kernel, int threads, size_t dyn_smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void*, size_t, int>, int> pct_of;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)dyn_smem)) != cudaSuccess)
+    return e;
+  const auto key = std::make_tuple(dev, reinterpret_cast<const void*>(kernel), dyn_smem, threads);
+  int pct = -1;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pct_of.find(key);
+    if (it != pct_of.end()) pct = it->second;
+  }
+  if (pct < 0) {
+    if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
+      return e;
+    int blocks = 0, per_sm = 0, reserved = 0;
+    cudaFuncAttributes fa;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, dyn_smem)) !=
+            cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) !=
+            cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev)) !=
+            cudaSuccess ||
+        (e = cudaFuncGetAttributes(&fa, kernel)) != cudaSuccess)
+      return e;
+    pct = 100;
+    if (blocks > 0 && per_sm > 0) {
+      const size_t need = (size_t)blocks * (dyn_smem + fa.sharedSizeBytes + (size_t)reserved);
+      pct = (int)((need * 100 + (size_t)per_sm - 1) / (size_t)per_sm);
+      pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    pct_of[key] = pct;
+  }
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+}
+
 inline int64_t prod(const int* v, int d) {
   int64_t p = 1;
   for (int i = 0; i < d; ++i) p *= v[i];

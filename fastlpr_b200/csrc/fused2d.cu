@@ -556,11 +556,10 @@ __global__ void dots_reduce_kernel(int CH, int G0, const double* __restrict__ dp
 namespace {
 
 template <typename K>
-static int set_smem(K kernel, size_t bytes) {
-  FLPR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  // let several CTAs share an SM: take the whole unified L1/shared array as shared memory
-  FLPR_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 cudaSharedmemCarveoutMaxShared));
+static int set_smem(K kernel, size_t bytes, int threads) {
+  // the FFT passes re-read their kernel factor rows from L1: give shared
+  // memory only what the resident CTAs use
+  FLPR_CUDA(fit_carveout(kernel, threads, bytes));
   return FLPR_OK;
 }
 
@@ -574,7 +573,7 @@ static int launch_col(const ColArgs& ca, int ncolblk, int nslots, int Hc, const 
                       const float2* F0f, const float2* tab, const int* kcut1, float2* W,
                       cudaStream_t s) {
   const size_t smem = warp_pass_smem(E, kColWarps);
-  FLPR_TRY(set_smem(colpass_kernel<E>, smem));
+  FLPR_TRY(set_smem(colpass_kernel<E>, smem, kColWarps * 32));
   colpass_kernel<E><<<dim3(ncolblk, nslots, Hc), kColWarps * 32, smem, s>>>(ca, Yt, F0f, tab,
                                                                           kcut1, W);
   FLPR_LAUNCH_CHECK();
@@ -586,7 +585,7 @@ static int launch_row_s(const RowArgs& ra, int Hc, int H, int nslots_w, const fl
                         const float2* F1f, const float2* tab, const int* kcut1, float* S,
                         cudaStream_t s) {
   const size_t smem = warp_pass_smem(E, kRowWarps);
-  FLPR_TRY(set_smem(rowpass_s_kernel<E>, smem));
+  FLPR_TRY(set_smem(rowpass_s_kernel<E>, smem, kRowWarps * 32));
   const int items = ra.G0 * ra.njobs;
   rowpass_s_kernel<E><<<dim3((items + kRowWarps - 1) / kRowWarps, Hc), kRowWarps * 32, smem, s>>>(
       ra, H, nslots_w, W, F1f, tab, kcut1, S);
@@ -601,7 +600,7 @@ static int launch_row_t_nt(const RowArgs& ra, int Hc, int H, int nslots_w, const
                            cudaStream_t s) {
   const int nwarps = t_warps(ra.njobs);
   const size_t smem = t_smem_bytes(E, nwarps, ra.njobs, ra.G1);
-  FLPR_TRY(set_smem(rowpass_t_solve_kernel<E, NT>, smem));
+  FLPR_TRY(set_smem(rowpass_t_solve_kernel<E, NT>, smem, nwarps * 32));
   rowpass_t_solve_kernel<E, NT><<<dim3(Hc, ra.G0), nwarps * 32, smem, s>>>(
       ra, H, nslots_w, W, F1f, tab, kcut1, C, ny, z, Q, my, dpart);
   FLPR_LAUNCH_CHECK();
