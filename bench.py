@@ -489,9 +489,13 @@ def run_ours(args):
     per_step_ms = ms_dev / args.steps
     value = world * 1000.0 / per_step_ms
     e2e_value = world * 1000.0 / (ms_e2e / args.steps)
-    h2d = x.nbytes + y.nbytes
-    # fitted values, selected grid (float64) and s0 plane (float32)
-    d2h = y.nbytes + int(np.prod(opts["N"])) * (8 + 4)
+    # x, y and the per-bandwidth sums of h for the device-side 1-SE choice
+    h2d = x.nbytes + y.nbytes + len(h) * 8
+    # fitted values and residuals (float64, n each), selected grid and s0
+    # plane (float64, M each), GCV / DoF arrays (4 H float64) and the chosen
+    # index (int32)
+    M_grid = int(np.prod(opts["N"]))
+    d2h = 2 * y.nbytes + 2 * M_grid * 8 + 4 * len(h) * 8 + 4
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
