@@ -326,6 +326,68 @@ def kde3d_workload(n: int, seed: int = 5):
     return x, np.column_stack([hv] * 3), {"N": [128, 128, 128]}
 
 
+def config_workloads():
+    """The other configurations, at full size (seeded synthetic data):
+    'lpr1d'  1-D local linear, N = 1e5, x ~ U[0,1], y = sin 2 pi x + 0.1 N(0,1),
+             grid 1024, 20 h in [0.01, 1];
+    'lpr2d_o2_hetero'  2-D local quadratic, N = 2e6, x ~ U[0,1]^2,
+             y = sin(2 pi x1) cos(2 pi x2) + (0.05 + 0.1 x1) N(0,1), grid 512^2,
+             32 isotropic h in [0.005, 0.5], then the variance fit of the
+             squared residuals (order 2, y_type_out 'variance') on the same h;
+    'kde3d'  3-D KDE, N = 1e7 (kde3d_workload), grid 128^3, 16 h."""
+    rng = np.random.default_rng(11)
+    x1 = rng.random(100_000)
+    y1 = np.sin(2 * np.pi * x1) + 0.1 * rng.standard_normal(x1.size)
+    h1 = np.logspace(-2, 0, 20)[:, None]
+    rng = np.random.default_rng(12)
+    x2 = rng.random((2_000_000, 2))
+    y2 = (np.sin(2 * np.pi * x2[:, 0]) * np.cos(2 * np.pi * x2[:, 1])
+          + (0.05 + 0.1 * x2[:, 0]) * rng.standard_normal(x2.shape[0]))
+    hv = np.logspace(np.log10(0.005), np.log10(0.5), 32)
+    h2 = np.column_stack([hv, hv])
+    x3, h3, o3 = kde3d_workload(10_000_000)
+    return {"lpr1d": (x1, y1, h1, {"order": 1, "N": [1024]}),
+            "lpr2d_o2_hetero": (x2, y2, h2, {"order": 2, "N": [512, 512]}),
+            "kde3d": (x3, None, h3, o3)}
+
+
+def run_configs(args, dev, steps: int = 3):
+    """Each other configuration through the public API with host arrays
+    (cv_fastlpr / cv_fastkde; uploads and downloads included), after one
+    warm-up call: seconds per fit by wall clock around synchronised calls."""
+    import torch
+
+    import fastlpr_b200
+    out = {}
+    for name, (x, y, h, o) in config_workloads().items():
+        opts = dict(o, device=str(dev))
+        try:
+            if name == "kde3d":
+                def step():
+                    return fastlpr_b200.cv_fastkde(x, h, opts)
+            elif name == "lpr2d_o2_hetero":
+                def step():
+                    r = fastlpr_b200.cv_fastlpr(x, y, h, opts)
+                    v = fastlpr_b200.cv_fastlpr(x, (y - r.yhat) ** 2, h,
+                                                dict(opts, y_type_out="variance"))
+                    return r, v
+            else:
+                def step():
+                    return fastlpr_b200.cv_fastlpr(x, y, h, opts)
+            step()
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                step()
+            torch.cuda.synchronize(dev)
+            sec = (time.perf_counter() - t0) / steps
+            out[name] = {"seconds_per_fit": sec, "fits_per_s": 1.0 / sec, "steps": steps,
+                         "points": int(x.shape[0]), "bandwidths": int(len(h))}
+        except Exception as e:  # an out-of-memory or unsupported case is reported, not fatal
+            out[name] = {"error": f"{type(e).__name__}: {e}"[:200]}
+    return out
+
+
 def run_profile_case(args, dev):
     """One small fit of a kind the benchmark leg does not run, for kernel
     profiles: 'kde3d' (3-D KDE, grid 128^3), 'learned' (learned search on
@@ -391,6 +453,9 @@ def run_ours(args):
     lib = _lib.load()
     if args.profile_case:
         print(json.dumps(run_profile_case(args, dev)), flush=True)
+        return 0
+    if args.only_configs:
+        print(json.dumps({"configs": run_configs(args, dev)}), flush=True)
         return 0
     if args.only_batched:
         # the batched leg alone (profiling): no metric fits before it
@@ -485,6 +550,10 @@ def run_ours(args):
     batched = None
     if args.batched and not args.bandwidths and args.points == N_POINTS:
         batched = run_batched(args, dev, world, rank, barrier)
+    # the other configurations, one GPU only (informational, end to end)
+    configs = None
+    if world == 1 and not args.no_configs and not args.bandwidths and args.points == N_POINTS:
+        configs = run_configs(args, dev)
 
     per_step_ms = ms_dev / args.steps
     value = world * 1000.0 / per_step_ms
@@ -545,6 +614,7 @@ def run_ours(args):
                                "algorithmic_bytes": bf},
         "learned": learned,
         "batched": batched,
+        "configs": configs,
         "phase_ms": {k: round(v, 3) for k, v in phases.items()},
         "clocks": clk,
     }
@@ -571,6 +641,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched", type=int, default=512,
                     help="problems of the batched workload leg (0: skip)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the timing of the other configurations")
+    ap.add_argument("--only-configs", action="store_true",
+                    help="time only the other configurations (1-D, 2-D order 2 + variance, "
+                         "3-D KDE) through the public API")
     ap.add_argument("--only-batched", action="store_true",
                     help="run only the batched workload leg (profiling)")
     ap.add_argument("--profile-case", default="",
