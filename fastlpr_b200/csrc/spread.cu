@@ -563,6 +563,135 @@ tile_accumulate_2d_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, 
   }
 }
 
+// ---- 3-D path: column ownership ------------------------------------------
+// Tiles of 8 x 8 x 8 cells, halo width W = 7 + NT1 (16 for 9 taps).  Thread
+// t of a CTA owns the halo column (x0, x1) = (t / W, t % W) and holds its W
+// cells along the last axis in registers.  The points of the work item go in
+// batches of kBatch3: their base cells, the 3 x NT1 per-axis tap weights and
+// the channel value are staged in shared memory, then every thread walks the
+// batch and adds, for each point whose tap footprint covers its column, the
+// NT1 taps along the last axis into its registers.  The lanes of a warp take
+// the same point, so the footprint's offset along the last axis is the same
+// for the whole warp.  Products are the generic kernel's, in its order
+// ((e0 e1) e2, times v, times the fixed-point scale), rounded to integers
+// and summed exactly: the grid is the same, bit for bit, without shared
+// atomics.  One channel at a time (blockIdx.y).
+constexpr int kBatch3 = 128;
+constexpr int kThreads3 = 256;
+
+inline size_t smem_3d(int nt1) {
+  return (size_t)kBatch3 * (3 * nt1 + 1) * sizeof(double) + (size_t)kBatch3 * sizeof(int);
+}
+
+template <typename Acc, int NT1, int BZ>
+__device__ __forceinline__ void column_taps(double (&acc)[7 + NT1], double wxy, double v, double sc,
+                                            const double* __restrict__ e2) {
+#pragma unroll
+  for (int k = 0; k < NT1; ++k) {
+    const double q = __dmul_rn(v, __dmul_rn(wxy, e2[k]));
+    reg_add<Acc>(acc[BZ + k], sc == 1.0 ? q : __dmul_rn(q, sc));
+  }
+}
+
+template <typename Acc, int NT1, int BZ = 0>
+__device__ __forceinline__ void column_dispatch(int bz, double (&acc)[7 + NT1], double wxy,
+                                                double v, double sc, const double* e2) {
+  if constexpr (BZ < 8) {
+    if (bz == BZ)
+      column_taps<Acc, NT1, BZ>(acc, wxy, v, sc, e2);
+    else
+      column_dispatch<Acc, NT1, BZ + 1>(bz, acc, wxy, v, sc, e2);
+  }
+}
+
+template <typename Acc, int NT1>
+__global__ void __launch_bounds__(kThreads3)
+tile_columns_3d_kernel(SpreadGeom g, int64_t n, int ones_channel, const int* __restrict__ offsets,
+                       const int* __restrict__ items, const int* __restrict__ rec_base,
+                       const double* __restrict__ rec_frac, const double* __restrict__ rec_val,
+                       const double* __restrict__ absum, int margin_bits,
+                       Acc* __restrict__ gacc) {
+  constexpr int MSP = (NT1 - 1) / 2;
+  constexpr int W = 7 + NT1;
+  constexpr int PP = 3 * NT1;  // per-axis weights of one point
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* s_w = reinterpret_cast<double*>(smem_raw);  // [kBatch3][PP]
+  double* s_v = s_w + kBatch3 * PP;                   // [kBatch3]
+  int* s_base = reinterpret_cast<int*>(s_v + kBatch3);
+  const int ch = blockIdx.y;
+  const int item = blockIdx.x;
+  if (item >= items[g.ntiles]) return;
+  int lo = 0, hi = g.ntiles;  // tile owning this item: largest t with items[t] <= item
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (items[mid] <= item) lo = mid; else hi = mid;
+  }
+  const int tile = lo;
+  const int p_begin = offsets[tile] + (item - items[tile]) * g.item_points;
+  const int p_end = min(offsets[tile + 1], p_begin + g.item_points);
+  const double sc = absum ? (double)fixed_scale(absum[ch], margin_bits) : 1.0;
+  const bool ones = ones_channel && ch == 0;
+  const double* vals = ones ? nullptr : rec_val + (int64_t)(ch - ones_channel) * n;
+
+  const int t = threadIdx.x;
+  const bool owner = t < W * W;
+  const int c0 = t / W, c1 = t - (t / W) * W;
+  double acc[W];
+#pragma unroll
+  for (int z = 0; z < W; ++z) acc[z] = 0.0;
+
+  for (int b0 = p_begin; b0 < p_end; b0 += kBatch3) {
+    const int nb = min(kBatch3, p_end - b0);
+    for (int i = t; i < nb * PP; i += blockDim.x) {
+      const int pp = i / PP;
+      const int r = i - pp * PP;
+      const int a = r / NT1, j = r - a * NT1;
+      const double fr = rec_frac[(int64_t)a * n + b0 + pp];
+      const double diff = fr - g.ax[a].hx * (double)(j - MSP);
+      s_w[i] = fexp(-(diff * diff) / g.four_tau[a]);
+    }
+    for (int i = t; i < nb; i += blockDim.x) {
+      s_base[i] = rec_base[b0 + i];
+      s_v[i] = ones ? 1.0 : vals[b0 + i];
+    }
+    __syncthreads();
+    if (owner) {
+      for (int pp = 0; pp < nb; ++pp) {
+        const int packed = s_base[pp];
+        const int d0 = c0 - (packed & 1023);
+        const int d1 = c1 - ((packed >> 10) & 1023);
+        if (d0 >= 0 && d0 < NT1 && d1 >= 0 && d1 < NT1) {
+          const double* wp = s_w + pp * PP;
+          const double wxy = wp[d0] * wp[NT1 + d1];
+          column_dispatch<Acc, NT1>((packed >> 20) & 1023, acc, wxy, s_v[pp], sc, wp + 2 * NT1);
+        }
+      }
+    }
+    __syncthreads();  // the next batch overwrites the staged points
+  }
+  if (!owner) return;
+  int tcoord[3];
+  {
+    int r = tile;
+    for (int a = 2; a >= 0; --a) {
+      tcoord[a] = r % g.ntile[a];
+      r /= g.ntile[a];
+    }
+  }
+  int gc0 = (tcoord[0] * g.T[0] + c0 - g.msp) % g.L[0];
+  if (gc0 < 0) gc0 += g.L[0];
+  int gc1 = (tcoord[1] * g.T[1] + c1 - g.msp) % g.L[1];
+  if (gc1 < 0) gc1 += g.L[1];
+  Acc* base = gacc + (int64_t)ch * g.cells + ((int64_t)gc0 * g.L[1] + gc1) * g.L[2];
+#pragma unroll
+  for (int z = 0; z < W; ++z) {
+    if (acc[z] == 0.0) continue;
+    int gc2 = (tcoord[2] * g.T[2] + z - g.msp) % g.L[2];
+    if (gc2 < 0) gc2 += g.L[2];
+    AccOps<Acc>::add_global(base + gc2, reg_value<Acc>(acc[z]));
+  }
+}
+
 static size_t smem_2d(int W0, int nt1, int cg) {
   return sizeof(double) * ((size_t)cg * chan_stride2(W0, nt1) + (size_t)kBatch2 * (2 * nt1 + cg));
 }
@@ -753,6 +882,39 @@ static int launch_accumulate_2d(const SpreadGeom& g, int64_t n, int nchan, int o
   return FLPR_OK;
 }
 
+
+// The column kernel covers 3-D tiles of 8^3 with at most 9 taps per axis
+// (halo columns fit one CTA of 256 threads).
+static bool use_3d_columns(const SpreadGeom& g) {
+  if (g.d != 3 || g.ntaps1 > 9) return false;
+  for (int a = 0; a < 3; ++a)
+    if (g.T[a] != 8 || g.W[a] != 7 + g.ntaps1) return false;
+  return true;
+}
+
+template <int NT1>
+static int launch_columns_3d(const SpreadGeom& g, int64_t n, int nchan, int ones_channel,
+                             const SpreadWs& w, bool fixed, int margin, dim3 grid,
+                             cudaStream_t s) {
+  const size_t smem = smem_3d(NT1);
+  if (fixed) {
+    auto k = tile_columns_3d_kernel<long long, NT1>;
+    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, kThreads3, smem, s>>>(g, n, ones_channel, w.offsets, w.items, w.rec_base,
+                                    (const double*)w.rec_frac, (const double*)w.rec_val, w.absum,
+                                    margin, (long long*)w.gacc);
+  } else {
+    auto k = tile_columns_3d_kernel<double, NT1>;
+    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, kThreads3, smem, s>>>(g, n, ones_channel, w.offsets, w.items, w.rec_base,
+                                    (const double*)w.rec_frac, (const double*)w.rec_val, nullptr,
+                                    margin, (double*)w.gacc);
+  }
+  (void)nchan;
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
 static int finalize(const SpreadGeom& g, int64_t n, int nchan, bool fixed, int margin,
                     const SpreadWs& w, void* d_grid_out, cudaStream_t s);
 
@@ -844,6 +1006,20 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
       case 11: st = launch_accumulate_2d<11>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
       case 13: st = launch_accumulate_2d<13>(g, n, nchan, ones_channel, cg2, w, fixed, margin, grid2, s); break;
       default: set_error("spread: msp=%d not supported (0..12)", g.msp); return FLPR_ERR_ARG;
+    }
+    if (st != FLPR_OK) return st;
+    return finalize(g, n, nchan, fixed, margin, w, d_grid_out, s);
+  }
+  if (use_3d_columns(g)) {
+    dim3 grid3((unsigned)max_items, (unsigned)nchan);
+    int st = FLPR_OK;
+    switch (g.ntaps1) {
+      case 1: st = launch_columns_3d<1>(g, n, nchan, ones_channel, w, fixed, margin, grid3, s); break;
+      case 3: st = launch_columns_3d<3>(g, n, nchan, ones_channel, w, fixed, margin, grid3, s); break;
+      case 5: st = launch_columns_3d<5>(g, n, nchan, ones_channel, w, fixed, margin, grid3, s); break;
+      case 7: st = launch_columns_3d<7>(g, n, nchan, ones_channel, w, fixed, margin, grid3, s); break;
+      case 9: st = launch_columns_3d<9>(g, n, nchan, ones_channel, w, fixed, margin, grid3, s); break;
+      default: set_error("spread: msp=%d not supported by the 3-D path", g.msp); return FLPR_ERR_ARG;
     }
     if (st != FLPR_OK) return st;
     return finalize(g, n, nchan, fixed, margin, w, d_grid_out, s);

@@ -115,13 +115,16 @@ def test_spread_kernel_matches_oracle(cuda_ok, d, G):
             assert rel_err(g[c], ref[c]) < tol, (prec, c)
 
 
-def test_fp32_spread_is_deterministic(cuda_ok):
+@pytest.mark.parametrize("d,G", [(2, [64, 64]), (3, [24, 20, 24])])
+def test_fp32_spread_is_deterministic(cuda_ok, d, G):
+    # the fixed-point accumulators make the grid independent of the order in
+    # which points reach a tile (that order comes from atomics)
     from fastlpr_b200 import _lib
     rng = np.random.default_rng(7)
-    x = rng.random((20000, 2))
+    x = rng.random((20000, d))
     v = rng.standard_normal((20000, 3))
-    a, _ = _spread_via_abi(None, x, v, [64, 64], _lib.FLPR_PREC_F32)
-    b, _ = _spread_via_abi(None, x, v, [64, 64], _lib.FLPR_PREC_F32)
+    a, _ = _spread_via_abi(None, x, v, G, _lib.FLPR_PREC_F32)
+    b, _ = _spread_via_abi(None, x, v, G, _lib.FLPR_PREC_F32)
     np.testing.assert_array_equal(a, b)
 
 
