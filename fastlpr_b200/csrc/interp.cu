@@ -57,6 +57,38 @@ __device__ __forceinline__ void make_stencil(const InterpGeom& g, const double* 
   }
 }
 
+// The same stencil with the dimension fixed at compile time (corners held
+// in registers): identical indices, weights and order.
+template <int D>
+struct StencilD {
+  int64_t base[1 << D];
+  double w[1 << D];
+};
+
+template <int D>
+__device__ __forceinline__ void make_stencil_d(const InterpGeom& g, const double* __restrict__ x,
+                                               int64_t i, StencilD<D>& st) {
+  int ix[D];
+  double fr[D];
+#pragma unroll
+  for (int a = 0; a < D; ++a) axis_cell(x[i * D + a], g.x0[a], g.dx[a], g.G[a], &ix[a], &fr[a]);
+#pragma unroll
+  for (int c = 0; c < (1 << D); ++c) {
+    int64_t idx = 0;
+    double w = 1.0;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      const int bit = (c >> (D - 1 - a)) & 1;
+      int ia = ix[a] + bit;
+      if (ia >= g.G[a]) ia = g.G[a] - 1;  // single-point axis
+      idx = idx * g.G[a] + ia;
+      w *= bit ? fr[a] : (1.0 - fr[a]);
+    }
+    st.base[c] = idx;
+    st.w[c] = w;
+  }
+}
+
 __device__ __forceinline__ double block_sum(double v, double* sh) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -157,60 +189,112 @@ __global__ void plane_sum_kernel(int64_t M, const double* __restrict__ s, double
   if (threadIdx.x == 0) atomicAdd(&sums[h], t);
 }
 
+// f (H, M) and its bandwidth-fastest copy fT (M, H), through a 32 x 32 tile:
+// grid (ceil(M / 32), ceil(H / 32)), block (32, 8).
 __global__ void kde_normalize_kernel(int64_t M, int H, const double* __restrict__ s,
                                      const double* __restrict__ sums, double dxprod,
-                                     double* __restrict__ f) {
-  const int64_t total = (int64_t)H * M;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    int h = (int)(t / M);
-    double tot = sums[h] * dxprod;
-    double v = tot > 0.0 ? s[t] / tot : s[t];
-    f[t] = v > 0.0 ? v : 0.0;
+                                     double* __restrict__ f, double* __restrict__ fT) {
+  __shared__ double tile[32][33];
+  const int64_t m0 = (int64_t)blockIdx.x * 32;
+  const int h0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int hh = ty; hh < 32; hh += blockDim.y) {
+    const int h = h0 + hh;
+    const int64_t m = m0 + tx;
+    if (h < H && m < M) {
+      const int64_t t = (int64_t)h * M + m;
+      const double tot = sums[h] * dxprod;
+      double v = tot > 0.0 ? s[t] / tot : s[t];
+      v = v > 0.0 ? v : 0.0;
+      f[t] = v;
+      tile[hh][tx] = v;
+    }
+  }
+  __syncthreads();
+  for (int mm = ty; mm < 32; mm += blockDim.y) {
+    const int64_t m = m0 + mm;
+    const int h = h0 + tx;
+    if (h < H && m < M) fT[m * H + h] = tile[tx][mm];
   }
 }
 
-struct K0s {
-  double k0[256];
+constexpr int kLcvGroup = 8;  // bandwidths per LCV pass
+
+struct K0g {
+  double k0[kLcvGroup];
 };
 
-// log of the leave-one-out density at point i: log(max(n/(n-1) (f(x_i) - K0/n), 1e-10))
-__device__ __forceinline__ double loo_log(const InterpGeom& g, const double* __restrict__ x,
-                                          int64_t i, const double* __restrict__ fh, double k0n,
-                                          double ratio) {
-  Stencil st;
-  make_stencil(g, x, i, st);
-  double v = 0.0;
-  for (int k = 0; k < st.ncorner; ++k) v += st.w[k] * fh[st.base[k]];
-  double fl = ratio * (v - k0n);
-  if (!(fl > 1e-10)) fl = 1e-10;
-  return log(fl);
-}
-
-// Sums of (l - c) and (l - c)^2 with c = l at point 0: the shift keeps the
-// variance free of cancellation (exactly zero when every l is clamped).
-__global__ void kde_lcv_kernel(InterpGeom g, int64_t n, const double* __restrict__ x,
-                               const double* __restrict__ f, int h0, K0s k0,
-                               double* __restrict__ part) {
+// LCV terms l = log(max(n/(n-1) (f(x_i) - K0/n), 1e-10)) of a group of up to
+// kLcvGroup bandwidths h0.. from the bandwidth-fastest densities fT (M, H):
+// the trilinear stencil of a point is formed once and each corner's
+// densities of the group are contiguous.  Sums of (l - c) and (l - c)^2
+// with c = l at point 0: the shift keeps the variance free of cancellation
+// (exactly zero when every l is clamped).
+template <int D>
+__global__ void kde_lcv_group_kernel(InterpGeom g, int64_t n, const double* __restrict__ x,
+                                     const double* __restrict__ fT, int H, int h0, int hn, K0g k0,
+                                     double* __restrict__ part) {
   __shared__ double sh[32];
-  const int h = h0 + blockIdx.y;
-  const double* fh = f + (int64_t)h * g.M;
-  const double k0n = k0.k0[blockIdx.y] / (double)n;
+  __shared__ double s_c[kLcvGroup], s_k0n[kLcvGroup];
   const double ratio = (double)n / (double)(n - 1);
-  const double c = loo_log(g, x, 0, fh, k0n, ratio);
-  double s1 = 0.0, s2 = 0.0;
+  if (threadIdx.x < kLcvGroup) {
+    const int j = threadIdx.x;
+    const double k0n = j < hn ? k0.k0[j] / (double)n : 0.0;
+    s_k0n[j] = k0n;
+    double c = 0.0;
+    if (j < hn) {
+      StencilD<D> st;
+      make_stencil_d<D>(g, x, 0, st);
+      double v = 0.0;
+#pragma unroll
+      for (int k = 0; k < (1 << D); ++k) v += st.w[k] * fT[st.base[k] * H + h0 + j];
+      double fl = ratio * (v - k0n);
+      if (!(fl > 1e-10)) fl = 1e-10;
+      c = log(fl);
+    }
+    s_c[j] = c;
+  }
+  __syncthreads();
+  double s1[kLcvGroup], s2[kLcvGroup];
+#pragma unroll
+  for (int j = 0; j < kLcvGroup; ++j) s1[j] = s2[j] = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const double l = loo_log(g, x, i, fh, k0n, ratio) - c;
-    s1 += l;
-    s2 += l * l;
+    StencilD<D> st;
+    make_stencil_d<D>(g, x, i, st);
+    double v[kLcvGroup];
+#pragma unroll
+    for (int j = 0; j < kLcvGroup; ++j) v[j] = 0.0;
+#pragma unroll
+    for (int k = 0; k < (1 << D); ++k) {
+      const double* row = fT + st.base[k] * H + h0;
+      const double w = st.w[k];
+#pragma unroll
+      for (int j = 0; j < kLcvGroup; ++j)
+        if (j < hn) v[j] += w * row[j];
+    }
+#pragma unroll
+    for (int j = 0; j < kLcvGroup; ++j) {
+      if (j < hn) {
+        double fl = ratio * (v[j] - s_k0n[j]);
+        if (!(fl > 1e-10)) fl = 1e-10;
+        const double l = log(fl) - s_c[j];
+        s1[j] += l;
+        s2[j] += l * l;
+      }
+    }
   }
-  double a = block_sum(s1, sh);
-  if (threadIdx.x == 0) atomicAdd(&part[3 * h], a);
-  double b = block_sum(s2, sh);
-  if (threadIdx.x == 0) {
-    atomicAdd(&part[3 * h + 1], b);
-    if (blockIdx.x == 0) part[3 * h + 2] = c;
+#pragma unroll
+  for (int j = 0; j < kLcvGroup; ++j) {
+    if (j < hn) {  // hn is the same for the whole block
+      const double a = block_sum(s1[j], sh);
+      if (threadIdx.x == 0) atomicAdd(&part[3 * (h0 + j)], a);
+      const double b = block_sum(s2[j], sh);
+      if (threadIdx.x == 0) {
+        atomicAdd(&part[3 * (h0 + j) + 1], b);
+        if (blockIdx.x == 0) part[3 * (h0 + j) + 2] = s_c[j];
+      }
+    }
   }
 }
 
@@ -469,9 +553,9 @@ int flpr_stencil_quad(int d, const int* h_G, int H, int ny, const double* d_m, c
 
 size_t flpr_kde_ws(int64_t n, int H, int64_t M) {
   (void)n;
-  (void)M;
-  return align_up(sizeof(double) * (size_t)(H > 0 ? H : 1)) +
-         align_up(sizeof(double) * 3 * (size_t)(H > 0 ? H : 1));
+  const size_t h = (size_t)(H > 0 ? H : 1);
+  return align_up(sizeof(double) * h) + align_up(sizeof(double) * 3 * h) +
+         align_up(sizeof(double) * h * (size_t)(M > 0 ? M : 1));
 }
 
 int flpr_kde_lcv(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G, int H,
@@ -495,15 +579,24 @@ int flpr_kde_lcv(int d, int64_t n, const double* d_x, const double* h_ax, const 
   if (gb < 4) gb = 4;
   plane_sum_kernel<<<dim3(gb, H), 256, 0, s>>>(g.M, d_s, sums);
   FLPR_LAUNCH_CHECK();
-  kde_normalize_kernel<<<pt_blocks((int64_t)H * g.M, 8), 256, 0, s>>>(g.M, H, d_s, sums, dxprod,
-                                                                      d_f);
+  double* fT = reinterpret_cast<double*>(static_cast<char*>(d_ws) +
+                                         align_up(sizeof(double) * (size_t)H) +
+                                         align_up(sizeof(double) * 3 * (size_t)H));
+  FLPR_CHECK_ARG((g.M + 31) / 32 < ((int64_t)1 << 31), "kde_lcv: grid too large");
+  kde_normalize_kernel<<<dim3((unsigned)((g.M + 31) / 32), (unsigned)((H + 31) / 32)),
+                         dim3(32, 8), 0, s>>>(g.M, H, d_s, sums, dxprod, d_f, fT);
   FLPR_LAUNCH_CHECK();
-  const int per_h = 2 * sm_count() / (H < 8 ? H : 8) + 1;
-  for (int h0 = 0; h0 < H; h0 += 256) {
-    int hn = H - h0 < 256 ? H - h0 : 256;
-    K0s k0;
-    for (int j = 0; j < hn; ++j) k0.k0[j] = h_k0[h0 + j];
-    kde_lcv_kernel<<<dim3(per_h, hn), 256, 0, s>>>(g, n, d_x, d_f, h0, k0, part);
+  const int ngroups = (H + kLcvGroup - 1) / kLcvGroup;
+  const int per_g = (4 * sm_count() + ngroups - 1) / ngroups;
+  for (int h0 = 0; h0 < H; h0 += kLcvGroup) {
+    const int hn = H - h0 < kLcvGroup ? H - h0 : kLcvGroup;
+    K0g k0;
+    for (int j = 0; j < kLcvGroup; ++j) k0.k0[j] = j < hn ? h_k0[h0 + j] : 0.0;
+    switch (d) {
+      case 1: kde_lcv_group_kernel<1><<<per_g, 256, 0, s>>>(g, n, d_x, fT, H, h0, hn, k0, part); break;
+      case 2: kde_lcv_group_kernel<2><<<per_g, 256, 0, s>>>(g, n, d_x, fT, H, h0, hn, k0, part); break;
+      default: kde_lcv_group_kernel<3><<<per_g, 256, 0, s>>>(g, n, d_x, fT, H, h0, hn, k0, part); break;
+    }
     FLPR_LAUNCH_CHECK();
   }
   kde_lcv_finish_kernel<<<(H + 127) / 128, 128, 0, s>>>(H, n, part, d_lcv);

@@ -360,7 +360,9 @@ int flpr_select_grid(int64_t M, int ny, int mstride, int H, const double* d_m, c
  * the raw points and the LCV terms log(max(n/(n-1) (f - K0_h/n), 1e-10))
  * are reduced: d_lcv (H, 2) = {sum of the logs, sum of their squared
  * deviations from their mean} (shifted sums, so a constant set of logs
- * gives exactly zero).  h_k0: (H) K0_h values.
+ * gives exactly zero).  h_k0: (H) K0_h values.  The workspace
+ * (flpr_kde_ws) also holds a bandwidth-fastest (M, H) copy of the densities
+ * that the point-wise interpolation reads.
  * --------------------------------------------------------------------- */
 size_t flpr_kde_ws(int64_t n, int H, int64_t M);
 int flpr_kde_lcv(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G,
