@@ -567,40 +567,37 @@ tile_accumulate_2d_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, 
 // Tiles of 8 x 8 x 8 cells, halo width W = 7 + NT1 (16 for 9 taps).  Thread
 // t of a CTA owns the halo column (x0, x1) = (t / W, t % W) and holds its W
 // cells along the last axis in registers.  The points of the work item go in
-// batches of kBatch3: their base cells, the 3 x NT1 per-axis tap weights and
-// the channel value are staged in shared memory, then every thread walks the
-// batch and adds, for each point whose tap footprint covers its column, the
-// NT1 taps along the last axis into its registers.  The lanes of a warp take
-// the same point, so the footprint's offset along the last axis is the same
-// for the whole warp.  Products are the generic kernel's, in its order
-// ((e0 e1) e2, times v, times the fixed-point scale), rounded to integers
-// and summed exactly: the grid is the same, bit for bit, without shared
-// atomics.  One channel at a time (blockIdx.y).
+// batches of kBatch3: their base cells and per-axis tap weights are staged
+// in shared memory, the last axis's already times the channel value and the
+// fixed-point scale; then every thread walks the batch and adds, for each
+// point whose tap footprint covers its column, the NT1 taps along the last
+// axis into its registers: (e0 e1) (e2 v scale), rounded to an integer and
+// summed exactly, so the grid does not depend on the order of the points
+// (no shared atomics).  The lanes of a warp take the same point, so the
+// footprint's offset along the last axis is the same for the whole warp.
+// One channel at a time (blockIdx.y).
 constexpr int kBatch3 = 128;
 constexpr int kThreads3 = 256;
 
 inline size_t smem_3d(int nt1) {
-  return (size_t)kBatch3 * (3 * nt1 + 1) * sizeof(double) + (size_t)kBatch3 * sizeof(int);
+  return (size_t)kBatch3 * 3 * nt1 * sizeof(double) + (size_t)kBatch3 * sizeof(int);
 }
 
 template <typename Acc, int NT1, int BZ>
-__device__ __forceinline__ void column_taps(double (&acc)[7 + NT1], double wxy, double v, double sc,
-                                            const double* __restrict__ e2) {
+__device__ __forceinline__ void column_taps(double (&acc)[7 + NT1], double wxy,
+                                            const double* __restrict__ e2v) {
 #pragma unroll
-  for (int k = 0; k < NT1; ++k) {
-    const double q = __dmul_rn(v, __dmul_rn(wxy, e2[k]));
-    reg_add<Acc>(acc[BZ + k], sc == 1.0 ? q : __dmul_rn(q, sc));
-  }
+  for (int k = 0; k < NT1; ++k) reg_add<Acc>(acc[BZ + k], __dmul_rn(wxy, e2v[k]));
 }
 
 template <typename Acc, int NT1, int BZ = 0>
 __device__ __forceinline__ void column_dispatch(int bz, double (&acc)[7 + NT1], double wxy,
-                                                double v, double sc, const double* e2) {
+                                                const double* e2v) {
   if constexpr (BZ < 8) {
     if (bz == BZ)
-      column_taps<Acc, NT1, BZ>(acc, wxy, v, sc, e2);
+      column_taps<Acc, NT1, BZ>(acc, wxy, e2v);
     else
-      column_dispatch<Acc, NT1, BZ + 1>(bz, acc, wxy, v, sc, e2);
+      column_dispatch<Acc, NT1, BZ + 1>(bz, acc, wxy, e2v);
   }
 }
 
@@ -616,8 +613,7 @@ tile_columns_3d_kernel(SpreadGeom g, int64_t n, int ones_channel, const int* __r
   constexpr int PP = 3 * NT1;  // per-axis weights of one point
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* s_w = reinterpret_cast<double*>(smem_raw);  // [kBatch3][PP]
-  double* s_v = s_w + kBatch3 * PP;                   // [kBatch3]
-  int* s_base = reinterpret_cast<int*>(s_v + kBatch3);
+  int* s_base = reinterpret_cast<int*>(s_w + kBatch3 * PP);
   const int ch = blockIdx.y;
   const int item = blockIdx.x;
   if (item >= items[g.ntiles]) return;
@@ -648,12 +644,15 @@ tile_columns_3d_kernel(SpreadGeom g, int64_t n, int ones_channel, const int* __r
       const int a = r / NT1, j = r - a * NT1;
       const double fr = rec_frac[(int64_t)a * n + b0 + pp];
       const double diff = fr - g.ax[a].hx * (double)(j - MSP);
-      s_w[i] = fexp(-(diff * diff) / g.four_tau[a]);
+      double e = fexp(-(diff * diff) / g.four_tau[a]);
+      if (a == 2) {
+        // last axis: times the channel value and the fixed-point scale
+        if (!ones) e = __dmul_rn(e, vals[b0 + pp]);
+        if (sc != 1.0) e = __dmul_rn(e, sc);
+      }
+      s_w[i] = e;
     }
-    for (int i = t; i < nb; i += blockDim.x) {
-      s_base[i] = rec_base[b0 + i];
-      s_v[i] = ones ? 1.0 : vals[b0 + i];
-    }
+    for (int i = t; i < nb; i += blockDim.x) s_base[i] = rec_base[b0 + i];
     __syncthreads();
     if (owner) {
       for (int pp = 0; pp < nb; ++pp) {
@@ -662,8 +661,8 @@ tile_columns_3d_kernel(SpreadGeom g, int64_t n, int ones_channel, const int* __r
         const int d1 = c1 - ((packed >> 10) & 1023);
         if (d0 >= 0 && d0 < NT1 && d1 >= 0 && d1 < NT1) {
           const double* wp = s_w + pp * PP;
-          const double wxy = wp[d0] * wp[NT1 + d1];
-          column_dispatch<Acc, NT1>((packed >> 20) & 1023, acc, wxy, s_v[pp], sc, wp + 2 * NT1);
+          const double wxy = __dmul_rn(wp[d0], wp[NT1 + d1]);
+          column_dispatch<Acc, NT1>((packed >> 20) & 1023, acc, wxy, wp + 2 * NT1);
         }
       }
     }
