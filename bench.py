@@ -392,7 +392,8 @@ def run_profile_case(args, dev):
     """One small fit of a kind the benchmark leg does not run, for kernel
     profiles: 'kde3d' (3-D KDE, grid 128^3), 'learned' (learned search on
     the benchmark data), 'cubic2d' (2-D, n = 3000: cubic GCV/DoF), 'order2'
-    (2-D local quadratic, FP64 separable convolution)."""
+    (2-D local quadratic, FP64 separable convolution), 'hetero2d' (the full
+    2-D local-quadratic mean + variance pair of config_workloads)."""
     import torch
 
     import fastlpr_b200
@@ -401,6 +402,11 @@ def run_profile_case(args, dev):
     if case == "kde3d":
         x, h, o = kde3d_workload(args.points)
         r = fastlpr_b200.cv_fastkde(x, h, dict(o, device=str(dev)))
+    elif case == "hetero2d":
+        x, y, h, o = config_workloads()["lpr2d_o2_hetero"]
+        opts = dict(o, device=str(dev))
+        r = fastlpr_b200.cv_fastlpr(x, y, h, opts)
+        fastlpr_b200.cv_fastlpr(x, (y - r.yhat) ** 2, h, dict(opts, y_type_out="variance"))
     else:
         n = {"learned": args.points, "cubic2d": 3000, "order2": 50000}[case]
         x, y, h, o = workload(0, n)
@@ -649,7 +655,7 @@ def main():
     ap.add_argument("--only-batched", action="store_true",
                     help="run only the batched workload leg (profiling)")
     ap.add_argument("--profile-case", default="",
-                    choices=["", "kde3d", "learned", "cubic2d", "order2"],
+                    choices=["", "kde3d", "learned", "cubic2d", "order2", "hetero2d"],
                     help="run one small fit of another kind (profiling)")
     ap.add_argument("--single-fit", action="store_true",
                     help="run one plain fit of the workload and exit (for profilers)")
