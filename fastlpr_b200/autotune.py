@@ -32,7 +32,7 @@ from . import _lib
 
 PARAMS = {"spread_item_points": 0, "fused_chunk_mb": 1}
 ITEM_POINTS = (1024, 2048, 4096, 8192)
-CHUNK_MB = (96, 192, 384)
+CHUNK_MB = (192, 384, 768, 1536)
 
 
 def set_params(values: Dict[str, int]) -> None:

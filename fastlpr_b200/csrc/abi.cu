@@ -14,7 +14,7 @@ static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 // defaults and ranges of the FLPR_TUNE_* parameters
-static std::atomic<int> g_tune[FLPR_TUNE_COUNT] = {{4096}, {192}};
+static std::atomic<int> g_tune[FLPR_TUNE_COUNT] = {{4096}, {768}};
 static const int kTuneMin[FLPR_TUNE_COUNT] = {256, 8};
 static const int kTuneMax[FLPR_TUNE_COUNT] = {65536, 16384};
 

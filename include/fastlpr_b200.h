@@ -50,7 +50,7 @@ int64_t flpr_launch_count(void);
  *   FLPR_TUNE_SPREAD_ITEM_POINTS: points per spread work item (one CTA),
  *     256..65536, default 4096;
  *   FLPR_TUNE_FUSED_CHUNK_MB: column-pass output budget of the fused 2-D
- *     convolution (bandwidths per chunk), 8..16384 MB, default 192. */
+ *     convolution (bandwidths per chunk), 8..16384 MB, default 768. */
 #define FLPR_TUNE_SPREAD_ITEM_POINTS 0
 #define FLPR_TUNE_FUSED_CHUNK_MB 1
 #define FLPR_TUNE_COUNT 2
