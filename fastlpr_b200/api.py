@@ -1148,6 +1148,11 @@ def _finalize_enqueue(ctx, st: _LprState, r: dict, ev, device_select: bool = Fal
         res_dev = st.y_raw_dev[None, :] - yhat_dev
     else:
         res_dev = torch.stack(st.ycols[:ny], dim=0) - yhat_dev
+    # fitted values, residuals and grid values in the layouts of the result
+    # (formed here so the host only takes views of the downloaded arrays)
+    yhat_dev = _result_layout(yhat_dev, st.dy, st.y_is_complex)
+    res_dev = _result_layout(res_dev, st.dy, st.y_is_complex)
+    gv_dev = _result_layout(gv_dev, st.dy, st.y_is_complex)
     parts = {"yh": yhat_dev, "rh": res_dev, "gvh": gv_dev, "s0h": s0_dev, "dn": dn,
              "gcv": gcv_dev, "sel": sel_dev}
     out = {}
@@ -1162,6 +1167,18 @@ def _finalize_enqueue(ctx, st: _LprState, r: dict, ev, device_select: bool = Fal
         else:
             out[k] = _to_host(t)
     return out
+
+
+def _result_layout(t: torch.Tensor, dy: int, y_is_complex: bool) -> torch.Tensor:
+    """(channels, k) device rows -> (k,) for one response column, (k, dy)
+    otherwise; complex responses (real/imaginary row pairs) as complex128."""
+    if y_is_complex:
+        t = torch.view_as_complex(t.reshape(dy, 2, -1).permute(2, 0, 1).contiguous())
+    elif dy > 1:
+        t = t.t().contiguous()
+    else:
+        return t[0]
+    return t[:, 0] if dy == 1 else t
 
 
 def _output_bufs(st: _LprState, H: int) -> dict:
@@ -1202,18 +1219,9 @@ def _finalize_build(ctx, st: _LprState, r: dict, pend: dict, ev, search,
     s0h = pend["s0h"]
     d_norm = float(pend["dn"].numpy()[0]) if pend["dn"] is not None else None
     gshape = tuple(int(g) for g in geom.G)
-    if st.y_is_complex:
-        yh = yh[0::2] + 1j * yh[1::2]
-        rh = rh[0::2] + 1j * rh[1::2]
-        gvh = gvh[0::2] + 1j * gvh[1::2]
-    if dy == 1:
-        yhat = yh[0]
-        residuals = rh[0]
-        grid_values = gvh[0].reshape(gshape)
-    else:
-        yhat = yh.T.copy()
-        residuals = rh.T.copy()
-        grid_values = np.moveaxis(gvh.reshape((dy,) + gshape), 0, -1)
+    # already (n,) / (n, dy), complex where the response is (_result_layout)
+    yhat, residuals = yh, rh
+    grid_values = gvh.reshape(gshape if dy == 1 else gshape + (dy,))
     s0 = s0h.numpy().reshape(gshape)
     if copy:
         s0 = s0.copy()
