@@ -22,6 +22,8 @@ streams, no capture).
 """
 from __future__ import annotations
 
+import os
+from concurrent.futures import ThreadPoolExecutor
 from typing import List, Optional, Sequence
 
 import numpy as np
@@ -114,7 +116,10 @@ class LprPlan:
                                 su.opts.get("dof_seed", 42), None)
             for su in setups:
                 self.probs.append(self._build(ctx, su))
+            self._pool = None
+            self._finite = None
             self._write_y([p.su.y_arr for p in self.probs])
+            self._check_finite(self._finite)
             self.graph = None
             self.outs = None
             self.tuning = None
@@ -210,7 +215,11 @@ class LprPlan:
         return p
 
     def _write_y(self, ys) -> None:
+        """Copy the responses into the pinned staging rows (a few host threads:
+        numpy's copies release the GIL) and on to the device; their NaN/Inf
+        check runs on the device (self._finite, read with the outputs)."""
         stream = torch.cuda.current_stream(self.device)
+        arrs = []
         for p, y in zip(self.probs, ys):
             y_arr = np.asarray(y)
             if y_arr.ndim == 1:
@@ -222,8 +231,10 @@ class LprPlan:
                                  f"{p.su.y_arr.shape}")
             if bool(np.iscomplexobj(y_arr)) != p.su.y_is_complex:
                 raise ValueError("a response changed between real and complex")
-            if not np.all(np.isfinite(y_arr)):
-                raise ValueError("Response y contains NaN or Inf values")
+            arrs.append(y_arr)
+
+        def stage(i):
+            p, y_arr = self.probs[i], arrs[i]
             st = p.staging.numpy()
             for c in range(p.su.dy):
                 if p.su.y_is_complex:
@@ -231,12 +242,25 @@ class LprPlan:
                     st[2 * c + 1] = y_arr[:, c].imag
                 else:
                     st[c] = y_arr[:, c]
+
+        if self._pool is None:
+            self._pool = ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1)))
+        list(self._pool.map(stage, range(len(self.probs))))
+        flags = []
+        for p in self.probs:
             for c, col in enumerate(p.ycols):
                 col.copy_(p.staging[c], non_blocking=True)
+                flags.append(torch.isfinite(col).all())
             # the staging rows are reused by the next run
             ev = torch.cuda.Event()
             ev.record(stream)
             p.staged = ev
+        self._finite = torch.stack(flags).all()
+
+    @staticmethod
+    def _check_finite(flag) -> None:
+        if flag is not None and not bool(flag):
+            raise ValueError("Response y contains NaN or Inf values")
 
     def _issue(self):
         """Enqueue the y-dependent stages of every problem on its stream, up
@@ -268,12 +292,14 @@ class LprPlan:
     def run(self, ys: Optional[Sequence] = None) -> List[RegressionOutput]:
         """Fit every problem (with new responses `ys` if given)."""
         with torch.cuda.device(self.device):
+            finite = None
             if ys is not None:
                 if len(ys) != len(self.probs):
                     raise ValueError(f"expected {len(self.probs)} responses, got {len(ys)}")
                 for p in self.probs:
                     p.staged.synchronize()
                 self._write_y(ys)
+                finite = api._to_host(self._finite.reshape(1))
             if self.graph is not None:
                 self.graph.replay()
                 outs = self.outs
@@ -286,6 +312,7 @@ class LprPlan:
                 pends.append({k: (api._to_host(v) if isinstance(v, torch.Tensor) and v.is_cuda
                                   else v) for k, v in pend.items()})
             torch.cuda.current_stream(self.device).synchronize()
+            self._check_finite(finite[0] if finite is not None else None)
             ev = api._PhaseEvents(None)
             return [api._finalize_build(self._ctx, outs[i][0], outs[i][1], pends[i], ev, None)
                     for i in range(len(self.probs))]

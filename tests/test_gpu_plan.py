@@ -98,6 +98,26 @@ def test_plan_replay_is_reproducible(cuda_ok):
         _same(ra, rb, 1e-12)
 
 
+def test_plan_rejects_nonfinite_responses_and_recovers(cuda_ok):
+    # the NaN/Inf check of new responses runs on the device and raises after
+    # the replay (api.py:310-323 raises the same error); the next run with
+    # finite responses gives the results of a fresh fit
+    import fastlpr_b200
+    probs = _problems()[:4]
+    plan = fastlpr_b200.LprPlan(probs)
+    bad = [p[1].copy() for p in probs]
+    bad[2][17] = np.nan
+    with pytest.raises(ValueError, match="NaN or Inf"):
+        plan.run(bad)
+    bad[2][17] = 0.0
+    bad[3][5] = np.inf
+    with pytest.raises(ValueError, match="NaN or Inf"):
+        plan.run(bad)
+    out = plan.run([p[1] for p in probs])
+    for (x, y, h, opts), r in zip(probs, out):
+        _same(r, fastlpr_b200.cv_fastlpr(x, y, h, opts), _tol(opts))
+
+
 def test_cv_fastlpr_many_matches_oracle(cuda_ok):
     import fastlpr_b200
     probs = _problems(2)[:3]
