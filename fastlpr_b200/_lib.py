@@ -122,17 +122,25 @@ def check(status: int, what: str = "") -> None:
         raise FastLPRError(f"{what} failed with status {status}: {msg}")
 
 
+def _carray(vals, np_type, c_type):
+    # one conversion pass in numpy and one copy into the ctypes array (a
+    # Python-level loop per element costs more than the calls it feeds)
+    a = np.ascontiguousarray(vals, dtype=np_type).reshape(-1)
+    if a.size == 0:
+        a = np.zeros(1, dtype=np_type)
+    return (c_type * a.size).from_buffer_copy(a)
+
+
 def ivec(vals: Sequence[int]):
-    a = (C.c_int * max(1, len(vals)))(*[int(v) for v in vals])
-    return a
+    return _carray(vals, np.int32, C.c_int)
 
 
 def dvec(vals: Sequence[float]):
-    return (C.c_double * max(1, len(vals)))(*[float(v) for v in vals])
+    return _carray(vals, np.float64, C.c_double)
 
 
 def pvec(ptrs: Sequence[int]):
-    return (C.c_void_p * max(1, len(ptrs)))(*[C.c_void_p(int(p)) for p in ptrs])
+    return _carray([int(p) for p in ptrs], np.uint64, C.c_void_p)
 
 
 _handles: Dict[int, C.c_void_p] = {}
