@@ -102,9 +102,9 @@ def b_fit(n=N_POINTS, d=2, G=512, H=N_H, R=R_PROBES, order=1, cy=1, parts=False)
 
 # DRAM traffic of the fused convolution stage of one metric fit
 # (dram__bytes_read.sum + dram__bytes_write.sum over its kernels, bytes), from
-# the ncu capture in profiles/dram_lpr2d_n1e5_g512_h32_single_fit.md (the
-# stage works on grid-sized arrays only, so the N=1e5 capture holds for N=1e6).
-CONV_STAGE_TRAFFIC = 3.438e9
+# an ncu capture of `bench.py --single-fit --points 100000` (the stage works
+# on grid-sized arrays only, so the N=1e5 capture holds for N=1e6).
+CONV_STAGE_TRAFFIC = 3.388e9
 
 
 # ---------------------------------------------------------------------------
