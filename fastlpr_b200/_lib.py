@@ -35,6 +35,9 @@ SIGNATURES = [
     ("flpr_point_stats_noalloc", _I, [_I, _I64, _VP, _VP, _VP]),
     ("flpr_spread_ws", _SZ, [_I, _I64, _PI, _I, _I, _I]),
     ("flpr_spread", _I, [_I, _I64, _VP, _PD, _PI, _I, _PD, _I, _I, _PVP, _VP, _I, _VP, _SZ, _VP]),
+    ("flpr_spread_dkmap", _I, [_I, _I64, _VP, _VP, _PD, _PI, _I, _PD, _I, _I, _PVP, _VP, _I, _VP,
+                               _SZ, _VP]),
+    ("flpr_knot_map", _I, [_I, _I64, _VP, _PD, _PD, _PD, _VP, _VP]),
     ("flpr_forward_fft_ws", _SZ, [_VP, _I, _PI, _I, _I]),
     ("flpr_forward_fft", _I, [_VP, _I, _PI, _I, _VP, _VP, _I, _VP, _SZ, _VP]),
     ("flpr_oversample_crop", _I, [_I, _PI, _PI, _I, _PD, _I, _VP, _VP, _I, _VP]),

@@ -15,6 +15,7 @@ from __future__ import annotations
 import math
 import time
 import warnings
+from types import SimpleNamespace
 from dataclasses import dataclass
 from typing import Dict, List, Optional, Sequence, Tuple
 
@@ -309,12 +310,35 @@ def _grid_params(G: np.ndarray, flag_power2: bool):
     return L, qin, qout
 
 
-def _point_stats(ctx: _Ctx, dx: torch.Tensor, n: int, d: int) -> np.ndarray:
+def _point_stats_dev(ctx: _Ctx, dx: torch.Tensor, n: int, d: int) -> torch.Tensor:
+    """(4 d) device statistics: minimum, maximum, mean, M2 per axis."""
     out = ctx.empty(4 * d)
     ws = ctx.ws(ctx.lib.flpr_point_stats_ws(d, n))
     ctx.check(ctx.lib.flpr_point_stats(d, n, dx.data_ptr(), out.data_ptr(), ws.data_ptr(),
                                        ws.numel(), ctx.stream), "flpr_point_stats")
-    return out.cpu().numpy().reshape(4, d)
+    return out
+
+
+def _point_stats(ctx: _Ctx, dx: torch.Tensor, n: int, d: int) -> np.ndarray:
+    return _point_stats_dev(ctx, dx, n, d).cpu().numpy().reshape(4, d)
+
+
+def _knot_consts(G: np.ndarray, L: np.ndarray, qin: np.ndarray):
+    """Per-axis constants of the knot mapping that depend on the grid only:
+    the knot range ks and start r0 of convolution.py:190-208 and the knot
+    spacing hx = 2 pi / L."""
+    d = len(G)
+    ks, r0, hx = np.empty(d), np.empty(d), np.empty(d)
+    for a in range(d):
+        idx_range = np.linspace(-0.5, 0.5 - 1 / L[a], L[a])
+        if G[a] != L[a]:
+            ks[a] = idx_range[qin[1, a]] - idx_range[qin[0, a]]
+            r0[a] = idx_range[qin[0, a]]
+        else:
+            ks[a] = idx_range[-1] - idx_range[0]
+            r0[a] = -0.5
+        hx[a] = 2 * np.pi / L[a]
+    return ks, r0, hx
 
 
 def _make_geom(stats: np.ndarray, n: int, d: int, G: np.ndarray, accuracy: int,
@@ -329,17 +353,12 @@ def _make_geom(stats: np.ndarray, n: int, d: int, G: np.ndarray, accuracy: int,
     hi = xs_max - center
     L, qin, qout = _grid_params(G, flag_power2)
     kmap = np.zeros((d, 9))
+    ks_all, r0_all, hx_all = _knot_consts(G, L, qin)       # convolution.py:190-208
     for a in range(d):
         scale = hi[a] - lo[a]
         if scale == 0:
             scale = 1.0
-        idx_range = np.linspace(-0.5, 0.5 - 1 / L[a], L[a])   # convolution.py:190-208
-        if G[a] != L[a]:
-            ks = idx_range[qin[1, a]] - idx_range[qin[0, a]]
-            r0 = idx_range[qin[0, a]]
-        else:
-            ks = idx_range[-1] - idx_range[0]
-            r0 = -0.5
+        ks, r0 = ks_all[a], r0_all[a]
 
         def chain(v):
             xn = (np.float64(v) - lo[a]) / scale * ks + r0
@@ -517,29 +536,45 @@ def _spread_params(L: np.ndarray, kmap: np.ndarray, accuracy: int):
         tau = np.full(len(L), np.inf)
     else:
         tau = (np.pi * msp) / (L * L * ratio * (ratio - 0.5))
-    kmap = kmap.copy()
-    kmap[:, 8] = 2 * np.pi / (ratio * np.asarray(L, dtype=float))
+    if kmap is not None:
+        kmap = kmap.copy()
+        kmap[:, 8] = 2 * np.pi / (ratio * np.asarray(L, dtype=float))
     return msp, tau, ratio, kmap
 
 
 def _spread_fft(ctx: _Ctx, geom: _Geom, dx: torch.Tensor, cols: List[torch.Tensor], prec: int,
-                ev=None, accuracy: Optional[int] = None, ones: bool = True):
+                ev=None, accuracy: Optional[int] = None, ones: bool = True,
+                kmap_dev: Optional[torch.Tensor] = None):
     """Spread {1 (if ones), cols...} at `accuracy` and transform: returns the
     (C, L.., L_last/2+1) spectra.  Oversampled accuracies spread on the
-    ratio*L grid and keep its central deconvolved L frequencies."""
+    ratio*L grid and keep its central deconvolved L frequencies.  kmap_dev:
+    the knot maps on the device (flpr_knot_map; accuracy <= 6 only), in
+    which case `geom` needs only d, n, L and accuracy."""
     d, n = geom.d, geom.n
     acc = geom.accuracy if accuracy is None else int(accuracy)
-    msp, tau, ratio, kmap = _spread_params(geom.L, geom.kmap, acc)
+    msp, tau, ratio, kmap = _spread_params(geom.L, None if kmap_dev is not None else geom.kmap,
+                                           acc)
     Lsp = (geom.L * ratio).astype(int)
     C = (1 if ones else 0) + len(cols)
     cells = int(np.prod(Lsp))
     real_dt = torch.float32 if prec == _lib.FLPR_PREC_F32 else torch.float64
     grid = ctx.empty((C, cells), dtype=real_dt)
     ws = ctx.ws(ctx.lib.flpr_spread_ws(d, n, _lib.ivec(Lsp), msp, C, prec))
-    ctx.check(ctx.lib.flpr_spread(d, n, dx.data_ptr(), _lib.dvec(kmap.ravel()),
-                                  _lib.ivec(Lsp), msp, _lib.dvec(tau), C, 1 if ones else 0,
-                                  _lib.pvec([c.data_ptr() for c in cols]), grid.data_ptr(), prec,
-                                  ws.data_ptr(), ws.numel(), ctx.stream), "flpr_spread")
+    chans = _lib.pvec([c.data_ptr() for c in cols])
+    if kmap_dev is not None:
+        if ratio != 1:
+            raise ValueError("device knot maps serve accuracies up to 6")
+        hx = 2 * np.pi / (ratio * np.asarray(geom.L, dtype=float))
+        ctx.check(ctx.lib.flpr_spread_dkmap(d, n, dx.data_ptr(), kmap_dev.data_ptr(),
+                                            _lib.dvec(hx), _lib.ivec(Lsp), msp, _lib.dvec(tau),
+                                            C, 1 if ones else 0, chans, grid.data_ptr(), prec,
+                                            ws.data_ptr(), ws.numel(), ctx.stream),
+                  "flpr_spread_dkmap")
+    else:
+        ctx.check(ctx.lib.flpr_spread(d, n, dx.data_ptr(), _lib.dvec(kmap.ravel()),
+                                      _lib.ivec(Lsp), msp, _lib.dvec(tau), C, 1 if ones else 0,
+                                      chans, grid.data_ptr(), prec, ws.data_ptr(), ws.numel(),
+                                      ctx.stream), "flpr_spread")
     del ws
     if ev is not None:
         ev.mark("spread")
@@ -841,9 +876,11 @@ class _LprState:
 
 def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_complex,
                  dev_inputs, ev, hook=None, stats=None, probes=None) -> _LprState:
-    """Bandwidth-independent stage.  `hook(dx, ycols, stats, n, d)` runs after
-    the point statistics, before the spread is enqueued (the learned search
-    starts its data summary there, on a side stream).  With `stats` (the
+    """Bandwidth-independent stage.  `hook(dx, ycols, stats, n, d, d_stats=None)`
+    runs once the point statistics exist, before the spread is enqueued (the
+    learned search starts its data summary there, on a side stream); on the
+    path whose knot maps are formed on the device it gets the device
+    statistics (d_stats: minima then maxima) instead of the host ones.  With `stats` (the
     point statistics of these device inputs, already checked) nothing here
     waits for the device, so the stage can be captured in a CUDA graph
     (`probes`: the (tensor, R) of _probes for these points, formed earlier)."""
@@ -879,11 +916,8 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
         ycols = [ylog]
     ny = len(ycols)
     G = _grid_shape(opts, n, d)
-    if stats is None:
-        stats = _point_stats(ctx, dx, n, d)
-    if flags_h is not None:
-        _raise_nonfinite(flags_h.numpy(), [("Input x", 0), ("Response y", 1)], "cv_fastlpr")
-    geom = _make_geom(stats, n, d, G, int(opts["accuracy"]), bool(opts.get("flag_power2", True)))
+    accuracy = int(opts["accuracy"])
+    flag_power2 = bool(opts.get("flag_power2", True))
     calc_dof = bool(opts.get("calc_dof", True))
     if calc_dof:
         if probes is None:
@@ -894,21 +928,50 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
     else:
         R = 0
         pcols = []
-    ev.mark("setup")
-    if hook is not None:
-        hook(dx, ycols, stats, n, d)
     # The user's accuracy applies to the response channels only (their
     # transform in nufft_regression_with_precomputed_kdf, api.py:640); the
     # design planes (compute_design_matrix, api.py:571) and the probes
     # (estimate_dof_nufft_vectorized, regression.py:756) use the default.
     acc_default = max(6 - int(np.ceil(np.log10(n))), 4)
-    if geom.accuracy == acc_default:
-        spec = _spread_fft(ctx, geom, dx, ycols + pcols, prec, ev)
-    else:
-        spec_s = _spread_fft(ctx, geom, dx, pcols, prec, ev, accuracy=acc_default, ones=True)
-        spec_y = _spread_fft(ctx, geom, dx, ycols, prec, ev, accuracy=geom.accuracy, ones=False)
-        spec = torch.cat([spec_s[:1], spec_y, spec_s[1:]], dim=0)
-        del spec_s, spec_y
+    spec = None
+    if stats is None and accuracy == acc_default and accuracy <= 6:
+        # one spread at the default accuracy: its knot maps are formed on the
+        # device from the statistics, so the spread and the transform are
+        # enqueued before the statistics reach the host (the host geometry
+        # below repeats the same arithmetic)
+        st_dev = _point_stats_dev(ctx, dx, n, d)
+        st_host = _to_host(st_dev)
+        st_ready = torch.cuda.Event()
+        st_ready.record()
+        L, qin, _ = _grid_params(G, flag_power2)
+        ks, r0, hx = _knot_consts(G, L, qin)
+        kmap_dev = ctx.empty(9 * d)
+        ctx.check(lib.flpr_knot_map(d, n, st_dev.data_ptr(), _lib.dvec(ks), _lib.dvec(r0),
+                                    _lib.dvec(hx), kmap_dev.data_ptr(), ctx.stream),
+                  "flpr_knot_map")
+        if hook is not None:
+            hook(dx, ycols, None, n, d, d_stats=st_dev[:2 * d])
+        pre = SimpleNamespace(n=n, d=d, L=L, accuracy=accuracy, kmap=None)
+        spec = _spread_fft(ctx, pre, dx, ycols + pcols, prec, ev, kmap_dev=kmap_dev)
+        st_ready.synchronize()
+        stats = st_host.numpy().reshape(4, d)
+    elif stats is None:
+        stats = _point_stats(ctx, dx, n, d)
+    if flags_h is not None:
+        _raise_nonfinite(flags_h.numpy(), [("Input x", 0), ("Response y", 1)], "cv_fastlpr")
+    geom = _make_geom(stats, n, d, G, accuracy, flag_power2)
+    ev.mark("setup")
+    if spec is None:
+        if hook is not None:
+            hook(dx, ycols, stats, n, d)
+        if geom.accuracy == acc_default:
+            spec = _spread_fft(ctx, geom, dx, ycols + pcols, prec, ev)
+        else:
+            spec_s = _spread_fft(ctx, geom, dx, pcols, prec, ev, accuracy=acc_default, ones=True)
+            spec_y = _spread_fft(ctx, geom, dx, ycols, prec, ev, accuracy=geom.accuracy,
+                                 ones=False)
+            spec = torch.cat([spec_s[:1], spec_y, spec_s[1:]], dim=0)
+            del spec_s, spec_y
     axes_raw = _raw_axes(geom, opts)
     methods = _check_interp_methods(opts, d, n)
     st.__dict__.update(dict(
@@ -1294,7 +1357,7 @@ def _side_stream(device: torch.device) -> torch.cuda.Stream:
     return _SIDE_STREAMS[idx]
 
 
-def _start_summary(ctx, pending: dict, dx, ycols, stats, n, d) -> None:
+def _start_summary(ctx, pending: dict, dx, ycols, stats, n, d, d_stats=None) -> None:
     """Binned moment sums of the data on a side stream, copied to pinned
     host memory, overlapping the spread that the main stream runs next."""
     from . import learned as _learned
@@ -1307,7 +1370,8 @@ def _start_summary(ctx, pending: dict, dx, ycols, stats, n, d) -> None:
         side.wait_event(ready)
         dx.record_stream(side)
         ycols[0].record_stream(side)
-        d_stats = ctx.upload(np.ascontiguousarray(stats[:2].ravel()))
+        if d_stats is None:
+            d_stats = ctx.upload(np.ascontiguousarray(stats[:2].ravel()))
         bins = _learned.bin_moments(dx, ycols[0], d_stats, n, d, side.cuda_stream)
         host = torch.empty(bins.shape, dtype=bins.dtype, pin_memory=True)
         host.copy_(bins, non_blocking=True)
@@ -1382,8 +1446,8 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
     pending = {}
     hook = None
     if learned is not None:
-        def hook(dx, ycols, stats, n, d):
-            _start_summary(ctx, pending, dx, ycols, stats, n, d)
+        def hook(dx, ycols, stats, n, d, d_stats=None):
+            _start_summary(ctx, pending, dx, ycols, stats, n, d, d_stats=d_stats)
     st = _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_complex,
                       dev_inputs, ev, hook=hook)
     found = (_learned_search(ctx, st, bandwidths, learned, ev, pending)

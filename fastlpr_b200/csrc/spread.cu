@@ -46,13 +46,15 @@ struct ChanPtrs {
   const double* col[FLPR_MAX_CHANNELS];
 };
 
-// Home cell and tile of a point; also its unwrapped knot index m.
-__device__ __forceinline__ int point_tile(const SpreadGeom& g, const double* __restrict__ x,
-                                          int64_t i, int* m_out, double* k_out) {
+// Home cell and tile of a point; also its unwrapped knot index m.  ax: the
+// knot maps of the axes (the geometry's, or a device-computed copy).
+__device__ __forceinline__ int point_tile(const SpreadGeom& g, const KnotAxis* ax,
+                                          const double* __restrict__ x, int64_t i, int* m_out,
+                                          double* k_out) {
   int tile = 0;
   for (int a = 0; a < g.d; ++a) {
-    double k = knot_of(x[i * g.d + a], g.ax[a]);
-    int m = (int)rint(ddiv(k, g.ax[a].hx));
+    double k = knot_of(x[i * g.d + a], ax[a]);
+    int m = (int)rint(ddiv(k, ax[a].hx));
     int home = m % g.L[a];
     if (home < 0) home += g.L[a];
     tile = tile * g.ntile[a] + home / g.T[a];
@@ -62,18 +64,82 @@ __device__ __forceinline__ int point_tile(const SpreadGeom& g, const double* __r
   return tile;
 }
 
+// Knot maps of the axes into shared memory: from d_kmap (d x 9, the layout
+// of the host geometry's rows) when given, else from the geometry.
+__device__ __forceinline__ void load_axes(const SpreadGeom& g, const double* __restrict__ d_kmap,
+                                          KnotAxis* s_ax) {
+  if (threadIdx.x < g.d) {
+    const int a = threadIdx.x;
+    if (d_kmap) {
+      const double* k = d_kmap + 9 * a;
+      s_ax[a] = KnotAxis{k[0], k[1], k[2], k[3], k[4], k[5], k[6], k[7], k[8]};
+    } else {
+      s_ax[a] = g.ax[a];
+    }
+  }
+}
+
+// Knot maps (d x 9: mean, std, centre, centred minimum, scale, ks, r0, shift,
+// hx) from the point statistics (4 x d: minimum, maximum, mean, M2), with
+// the operations, in the order, of the host geometry: z-score with ddof 1
+// (model.py:58-68), mid-range centring, the knot-range mapping
+// (convolution.py:190-208) and the centring shift (nufftn_type1.py:164-166).
+// One thread per axis.  nm1 = n - 1 (negative for one point: std NaN).
+struct KnotConsts {
+  double ks[3], r0[3], hx[3];
+};
+
+__global__ void knot_map_kernel(int d, double nm1, const double* __restrict__ st, KnotConsts kc,
+                                double* __restrict__ kmap) {
+  const int a = threadIdx.x;
+  if (a >= d) return;
+  const double xmin = st[a], xmax = st[d + a], mean = st[2 * d + a], m2 = st[3 * d + a];
+  double sd = nm1 > 0.0 ? __dsqrt_rn(ddiv(m2, nm1)) : NAN;
+  if (sd == 0.0) sd = 1.0;
+  const double xs_min = ddiv(dsub(xmin, mean), sd);
+  const double xs_max = ddiv(dsub(xmax, mean), sd);
+  const double center = ddiv(dadd(xs_max, xs_min), 2.0);
+  const double lo = dsub(xs_min, center);
+  const double hi = dsub(xs_max, center);
+  double scale = dsub(hi, lo);
+  if (scale == 0.0) scale = 1.0;
+  const double ks = kc.ks[a], r0 = kc.r0[a];
+  double c[2];
+  for (int e = 0; e < 2; ++e) {
+    double xn = dadd(dmul(ddiv(dsub(e == 0 ? lo : hi, lo), scale), ks), r0);
+    xn = dadd(xn, 0.5);
+    xn = np_mod(xn, 1.0);
+    c[e] = dsub(xn, 0.5);
+  }
+  const double kmin = dsub(dmul(dadd(c[0], c[1]), 0.5), 0.5);
+  const double shift = dsub(-0.5, kmin);
+  double* o = kmap + 9 * a;
+  o[0] = mean;
+  o[1] = sd;
+  o[2] = center;
+  o[3] = lo;
+  o[4] = scale;
+  o[5] = ks;
+  o[6] = r0;
+  o[7] = shift;
+  o[8] = kc.hx[a];
+}
+
 __global__ void bin_count_kernel(SpreadGeom g, int64_t n, const double* __restrict__ x,
+                                 const double* __restrict__ d_kmap,
                                  int* __restrict__ point_tile_out, int* __restrict__ counts,
                                  int nchan, int ones_channel, ChanPtrs cp,
                                  double* __restrict__ absum) {
   __shared__ double sh_abs[FLPR_MAX_CHANNELS];
+  __shared__ KnotAxis s_ax[3];
   for (int c = threadIdx.x; c < nchan; c += blockDim.x) sh_abs[c] = 0.0;
+  load_axes(g, d_kmap, s_ax);
   __syncthreads();
   int nv = nchan - ones_channel;
   double local[8];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    int t = point_tile(g, x, i, nullptr, nullptr);
+    int t = point_tile(g, s_ax, x, i, nullptr, nullptr);
     point_tile_out[i] = t;
     atomicAdd(&counts[t], 1);
   }
@@ -178,14 +244,18 @@ __global__ void tile_scan_kernel(int ntiles, int item_points, const int* __restr
 //   rec_val[c * n + pos]   value of channel c (ones channel excluded).
 template <typename Real>
 __global__ void bin_scatter_kernel(SpreadGeom g, int64_t n, const double* __restrict__ x,
+                                   const double* __restrict__ d_kmap,
                                    const int* __restrict__ offsets, int* __restrict__ cursor,
                                    int nv, ChanPtrs cp, int* __restrict__ rec_base,
                                    Real* __restrict__ rec_frac, Real* __restrict__ rec_val) {
+  __shared__ KnotAxis s_ax[3];
+  load_axes(g, d_kmap, s_ax);
+  __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     int m[3];
     double k[3];
-    const int t = point_tile(g, x, i, m, k);
+    const int t = point_tile(g, s_ax, x, i, m, k);
     const int pos = offsets[t] + atomicAdd(&cursor[t], 1);
     int packed = 0;
     for (int a = 0; a < g.d; ++a) {
@@ -933,10 +1003,12 @@ size_t flpr_spread_ws(int d, int64_t n, const int* h_L, int msp, int nchan, int 
   return ar.used;
 }
 
-int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const int* h_L,
-                int msp, const double* h_tau, int nchan, int ones_channel,
-                const double* const* h_cols, void* d_grid_out, int prec, void* d_ws,
-                size_t ws_bytes, void* stream) {
+// d_kmap: when not null, the knot maps (d x 9) are read on the device from
+// there (h_kmap then only supplies the knot spacings, column 8).
+static int spread_impl(int d, int64_t n, const double* d_x, const double* h_kmap,
+                       const double* d_kmap, const int* h_L, int msp, const double* h_tau,
+                       int nchan, int ones_channel, const double* const* h_cols,
+                       void* d_grid_out, int prec, void* d_ws, size_t ws_bytes, void* stream) {
   FLPR_CHECK_ARG(d >= 1 && d <= 3, "spread: d=%d not in [1,3]", d);
   FLPR_CHECK_ARG(n >= 1 && n < (int64_t)1 << 31, "spread: n=%lld out of range", (long long)n);
   FLPR_CHECK_ARG(msp >= 0 && 2 * msp + 1 <= kMaxTaps1, "spread: msp=%d not in [0,12]", msp);
@@ -976,7 +1048,7 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
 
   int nb = (int)((n + 255) / 256);
   if (nb > 8 * sm_count()) nb = 8 * sm_count();
-  bin_count_kernel<<<nb, 256, 0, s>>>(g, n, d_x, w.point_tile, w.counts, nchan, ones_channel, cp,
+  bin_count_kernel<<<nb, 256, 0, s>>>(g, n, d_x, d_kmap, w.point_tile, w.counts, nchan, ones_channel, cp,
                                       fixed ? w.absum : nullptr);
   FLPR_LAUNCH_CHECK();
   tile_scan_kernel<<<1, 1024, 0, s>>>(g.ntiles, g.item_points, w.counts, w.offsets, w.items,
@@ -985,7 +1057,7 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
   // records and tap weights are float64 in both precisions: FP32 weights
   // lose ~1e-6 on the far taps (exponents near 8), which ill-conditioned
   // local systems in sparse corners amplify; only the accumulator differs
-  bin_scatter_kernel<double><<<nb, 256, 0, s>>>(g, n, d_x, w.offsets, w.cursor, nv, cp,
+  bin_scatter_kernel<double><<<nb, 256, 0, s>>>(g, n, d_x, d_kmap, w.offsets, w.cursor, nv, cp,
                                                 w.rec_base, (double*)w.rec_frac,
                                                 (double*)w.rec_val);
   FLPR_LAUNCH_CHECK();
@@ -1048,6 +1120,43 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const
   }
   if (status != FLPR_OK) return status;
   return finalize(g, n, nchan, fixed, margin, w, d_grid_out, s);
+}
+
+int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap, const int* h_L,
+                int msp, const double* h_tau, int nchan, int ones_channel,
+                const double* const* h_cols, void* d_grid_out, int prec, void* d_ws,
+                size_t ws_bytes, void* stream) {
+  FLPR_CHECK_ARG(h_kmap != nullptr, "spread: null knot map");
+  return spread_impl(d, n, d_x, h_kmap, nullptr, h_L, msp, h_tau, nchan, ones_channel, h_cols,
+                     d_grid_out, prec, d_ws, ws_bytes, stream);
+}
+
+int flpr_spread_dkmap(int d, int64_t n, const double* d_x, const double* d_kmap,
+                      const double* h_hx, const int* h_L, int msp, const double* h_tau,
+                      int nchan, int ones_channel, const double* const* h_cols,
+                      void* d_grid_out, int prec, void* d_ws, size_t ws_bytes, void* stream) {
+  FLPR_CHECK_ARG(d >= 1 && d <= 3, "spread: d=%d not in [1,3]", d);
+  FLPR_CHECK_ARG(d_kmap != nullptr && h_hx != nullptr, "spread: null knot map");
+  double hk[27] = {0.0};
+  for (int a = 0; a < d; ++a) hk[9 * a + 8] = h_hx[a];
+  return spread_impl(d, n, d_x, hk, d_kmap, h_L, msp, h_tau, nchan, ones_channel, h_cols,
+                     d_grid_out, prec, d_ws, ws_bytes, stream);
+}
+
+int flpr_knot_map(int d, int64_t n, const double* d_stats, const double* h_ks,
+                  const double* h_r0, const double* h_hx, double* d_kmap, void* stream) {
+  FLPR_CHECK_ARG(d >= 1 && d <= 3, "knot_map: d=%d not in [1,3]", d);
+  FLPR_CHECK_ARG(n >= 1, "knot_map: n=%lld", (long long)n);
+  FLPR_CHECK_ARG(d_stats && h_ks && h_r0 && h_hx && d_kmap, "knot_map: null pointer");
+  KnotConsts kc{};
+  for (int a = 0; a < d; ++a) {
+    kc.ks[a] = h_ks[a];
+    kc.r0[a] = h_r0[a];
+    kc.hx[a] = h_hx[a];
+  }
+  knot_map_kernel<<<1, 32, 0, as_stream(stream)>>>(d, (double)(n - 1), d_stats, kc, d_kmap);
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
 }
 
 }  // extern "C"

@@ -116,6 +116,23 @@ int flpr_spread(int d, int64_t n, const double* d_x, const double* h_kmap,
                 const int* h_L, int msp, const double* h_tau,
                 int nchan, int ones_channel, const double* const* h_cols,
                 void* d_grid_out, int prec, void* d_ws, size_t ws_bytes, void* stream);
+/* The same spread with the knot maps read on the device (d_kmap, d x 9, the
+ * rows of h_kmap above; h_hx: the knot spacings of the axes), so that it can
+ * be enqueued before the point statistics reach the host.  Same workspace
+ * as flpr_spread.  No separate reference counterpart: it is the spread of
+ * nufftn_type1.py:378-772 with the geometry of model.py:58-68 and
+ * convolution.py:190-208 formed on the device. */
+int flpr_spread_dkmap(int d, int64_t n, const double* d_x, const double* d_kmap,
+                      const double* h_hx, const int* h_L, int msp, const double* h_tau,
+                      int nchan, int ones_channel, const double* const* h_cols,
+                      void* d_grid_out, int prec, void* d_ws, size_t ws_bytes, void* stream);
+/* Knot maps d_kmap (d x 9) from the point statistics d_stats (4 x d:
+ * minimum, maximum, mean, M2 as flpr_point_stats writes them) and the
+ * host-known per-axis constants of the grid (ks, r0: the knot range of
+ * convolution.py:190-208; hx = 2 pi / L), in the operations and order of the
+ * host geometry (model.py:58-68, nufftn_type1.py:164-166). */
+int flpr_knot_map(int d, int64_t n, const double* d_stats, const double* h_ks,
+                  const double* h_r0, const double* h_hx, double* d_kmap, void* stream);
 
 /* ---------------------------------------------------------------------
  * (3) Forward FFT of the spread grids: real-to-complex over all axes,

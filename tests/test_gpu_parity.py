@@ -115,6 +115,31 @@ def test_spread_kernel_matches_oracle(cuda_ok, d, G):
             assert rel_err(g[c], ref[c]) < tol, (prec, c)
 
 
+@pytest.mark.parametrize("d,G,flag_power2", [(1, [300], True), (2, [48, 40], True),
+                                              (2, [50, 33], False), (3, [12, 16, 10], True)])
+def test_device_knot_map_equals_host_geometry(cuda_ok, d, G, flag_power2):
+    # flpr_knot_map repeats the host geometry's arithmetic on the device
+    # statistics: the knot maps must be the same bits (the spread that reads
+    # them is enqueued before the host has the statistics)
+    import torch
+    from fastlpr_b200 import _lib, api
+    rng = np.random.default_rng(30 + d)
+    n = 5000
+    x = rng.random((n, d)) * np.arange(1, d + 1) * 3.7 - 1.1
+    ctx = api._Ctx(torch.device("cuda:0"))
+    dx = ctx.upload(x)
+    st_dev = api._point_stats_dev(ctx, dx, n, d)
+    stats = st_dev.cpu().numpy().reshape(4, d)
+    G = np.asarray(G)
+    geom = api._make_geom(stats, n, d, G, 4, flag_power2)
+    L, qin, _ = api._grid_params(G, flag_power2)
+    ks, r0, hx = api._knot_consts(G, L, qin)
+    kmap = ctx.empty(9 * d)
+    ctx.check(ctx.lib.flpr_knot_map(d, n, st_dev.data_ptr(), _lib.dvec(ks), _lib.dvec(r0),
+                                    _lib.dvec(hx), kmap.data_ptr(), ctx.stream), "knot_map")
+    np.testing.assert_array_equal(kmap.cpu().numpy().reshape(d, 9), geom.kmap)
+
+
 @pytest.mark.parametrize("d,G", [(2, [64, 64]), (3, [24, 20, 24])])
 def test_fp32_spread_is_deterministic(cuda_ok, d, G):
     # the fixed-point accumulators make the grid independent of the order in
