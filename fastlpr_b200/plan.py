@@ -130,6 +130,15 @@ class LprPlan:
             if graph:
                 self._capture()
 
+    def close(self) -> None:
+        """Stop the staging threads (also done when the plan is collected)."""
+        pool, self._pool = getattr(self, "_pool", None), None
+        if pool is not None:
+            pool.shutdown(wait=False)
+
+    def __del__(self):
+        self.close()
+
     def _set_streams(self, nstreams: int) -> None:
         self.streams = [torch.cuda.Stream(self.device) for _ in range(max(1, int(nstreams)))]
         # largest first, each to the least loaded stream
