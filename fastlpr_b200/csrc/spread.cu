@@ -1057,7 +1057,11 @@ static int spread_impl(int d, int64_t n, const double* d_x, const double* h_kmap
   // records and tap weights are float64 in both precisions: FP32 weights
   // lose ~1e-6 on the far taps (exponents near 8), which ill-conditioned
   // local systems in sparse corners amplify; only the accumulator differs
-  bin_scatter_kernel<double><<<nb, 256, 0, s>>>(g, n, d_x, d_kmap, w.offsets, w.cursor, nv, cp,
+  // one point per thread up to 32 CTAs per SM: every thread waits for the
+  // slot its cursor atomic returns, so more of them in flight hide it
+  int nbs = (int)((n + 255) / 256);
+  if (nbs > 32 * sm_count()) nbs = 32 * sm_count();
+  bin_scatter_kernel<double><<<nbs, 256, 0, s>>>(g, n, d_x, d_kmap, w.offsets, w.cursor, nv, cp,
                                                 w.rec_base, (double*)w.rec_frac,
                                                 (double*)w.rec_val);
   FLPR_LAUNCH_CHECK();
