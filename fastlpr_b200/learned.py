@@ -6,7 +6,7 @@ the GCV minimum lies on a canonical sweep; ``cv_fastlpr`` with option
 ``bandwidth_search='learned'`` then evaluates only the five bandwidths of
 the list around the proposal and accepts the result when its GCV minimum is
 interior to that window (or at an end of the whole list).  Otherwise it runs
-the full sweep, which stays the fallback and the judge.
+the full sweep, which stays the fallback and the reference score.
 
 Everything runs on the GPU through the C ABI: ``flpr_bin_moments`` for the
 summaries, ``flpr_mlp_fwd/bwd/step`` (BF16 tensor-core products with FP32

@@ -16,7 +16,7 @@ Pipeline (all on one GPU):
    the standardised fractional index of the GCV minimum);
 4. evaluation on held-out problems: proposal + five-bandwidth refine (the
    window moves toward an edge minimum at most three times, else the full
-   sweep runs), judged by the GCV ratio against the full sweep's minimum.
+   sweep runs), scored by the GCV ratio against the full sweep's minimum.
 """
 from __future__ import annotations
 
