@@ -17,18 +17,44 @@ __device__ __forceinline__ double from_ordered(unsigned long long b) {
   return __longlong_as_double((long long)b);
 }
 
-// max over one plane of |S| (use_abs) or S; NaN never wins.
+// Largest value (absolute value with use_abs; NaN ignored) over the nt
+// diagonal planes k of S (offset (k nt - k (k-1)/2) planes), as ordered bits
+// atomically maxed into *out; vec: the planes start on 16-byte boundaries
+// and hold whole vectors, so each load takes 16 bytes.
+__device__ __forceinline__ void max_in(double v, int use_abs, unsigned long long& best) {
+  if (use_abs) v = fabs(v);
+  const unsigned long long b = ordered_bits(v);
+  if (v == v && b > best) best = b;
+}
+
 template <typename Real>
-__global__ void plane_max_kernel(int64_t plane_len, const Real* __restrict__ S, int use_abs,
-                                 unsigned long long* __restrict__ out) {
+__global__ void diag_max_kernel(int64_t plane_len, int nt, const Real* __restrict__ S, int use_abs,
+                                int vec, unsigned long long* __restrict__ out) {
   __shared__ unsigned long long sh[256];
   unsigned long long best = ordered_bits(-INFINITY);
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < plane_len;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    double v = (double)S[i];
-    if (use_abs) v = fabs(v);
-    unsigned long long b = ordered_bits(v);
-    if (v == v && b > best) best = b;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (int k = 0; k < nt; ++k) {
+    const Real* P = S + (int64_t)(k * nt - k * (k - 1) / 2) * plane_len;
+    if (vec && sizeof(Real) == 4) {
+      const float4* P4 = reinterpret_cast<const float4*>(P);
+      for (int64_t i = t0; i < plane_len / 4; i += stride) {
+        const float4 q = P4[i];
+        max_in(q.x, use_abs, best);
+        max_in(q.y, use_abs, best);
+        max_in(q.z, use_abs, best);
+        max_in(q.w, use_abs, best);
+      }
+    } else if (vec) {
+      const double2* P2 = reinterpret_cast<const double2*>(P);
+      for (int64_t i = t0; i < plane_len / 2; i += stride) {
+        const double2 q = P2[i];
+        max_in(q.x, use_abs, best);
+        max_in(q.y, use_abs, best);
+      }
+    } else {
+      for (int64_t i = t0; i < plane_len; i += stride) max_in((double)P[i], use_abs, best);
+    }
   }
   sh[threadIdx.x] = best;
   __syncthreads();
@@ -183,16 +209,18 @@ int global_scalar(int order, int nt, int H, int64_t M, const void* d_S, double* 
   bits_init_kernel<<<1, 1, 0, s>>>(bits);
   FLPR_LAUNCH_CHECK();
   const int64_t plane = (int64_t)H * M;
-  const int nb = blocks_for(plane, 4);
-  for (int k = 0; k < nt; ++k) {
-    const int64_t off = (int64_t)(k * nt - k * (k - 1) / 2) * plane;  // diagonal element k
-    if (prec == FLPR_PREC_F32) {
-      plane_max_kernel<float><<<nb, 256, 0, s>>>(plane, (const float*)d_S + off, order > 0, bits);
-    } else {
-      plane_max_kernel<double><<<nb, 256, 0, s>>>(plane, (const double*)d_S + off, order > 0, bits);
-    }
-    FLPR_LAUNCH_CHECK();
+  // every diagonal element k (k nt - k (k-1)/2) in one launch
+  const int nb = blocks_for(plane / 4 + 1, 16);
+  const bool aligned = (reinterpret_cast<uintptr_t>(d_S) & 15) == 0;
+  if (prec == FLPR_PREC_F32) {
+    const int vec = aligned && plane % 4 == 0;
+    diag_max_kernel<float><<<nb, 256, 0, s>>>(plane, nt, (const float*)d_S, order > 0, vec, bits);
+  } else {
+    const int vec = aligned && plane % 2 == 0;
+    diag_max_kernel<double><<<nb, 256, 0, s>>>(plane, nt, (const double*)d_S, order > 0, vec,
+                                               bits);
   }
+  FLPR_LAUNCH_CHECK();
   scalar_from_bits_kernel<<<1, 1, 0, s>>>(bits, order > 0 ? 1e-6 : 1.0, d_scalar);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
