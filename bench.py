@@ -104,7 +104,7 @@ def b_fit(n=N_POINTS, d=2, G=512, H=N_H, R=R_PROBES, order=1, cy=1, parts=False)
 # (dram__bytes_read.sum + dram__bytes_write.sum over its kernels, bytes), from
 # an ncu capture of `bench.py --single-fit --points 100000` (the stage works
 # on grid-sized arrays only, so the N=1e5 capture holds for N=1e6).
-CONV_STAGE_TRAFFIC = 3.388e9
+CONV_STAGE_TRAFFIC = 3.396e9
 
 
 # ---------------------------------------------------------------------------
