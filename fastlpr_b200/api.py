@@ -433,6 +433,25 @@ def _kernel_sums_host(geom: _Geom, bw: np.ndarray) -> np.ndarray:
     return out
 
 
+def _separable_kernel_sums(geom: _Geom, bw: np.ndarray, norm: float) -> np.ndarray:
+    """Per-bandwidth kernel sums for the "too small bandwidth" test
+    (convolution.py:542-605), exact where the test is close: every term of
+    the positive grid sums is at most their total, so where the product of
+    the largest terms already clears twice the threshold (10 eps) the
+    bandwidth stays and that product stands in for the sum; only the others
+    get the exact sums."""
+    peak = np.ones(bw.shape[0])
+    for a in range(geom.d):
+        g = np.linspace(geom.lo[a], geom.hi[a], int(geom.G[a]))
+        u = np.min(np.abs(g)) / bw[:, a]
+        peak = peak * (np.exp(-0.5 * (u * u)) / bw[:, a])
+    sums = peak / norm
+    low = np.where(sums < EPS * 20)[0]
+    if len(low):
+        sums[low] = np.prod(_kernel_sums_host(geom, bw[low]), axis=0) / norm
+    return sums
+
+
 class _Kernel:
     """Kernel spectra of one bandwidth list: per-axis factors F (Gaussian
     kernels, flpr_kernel_factors) or full-plane spectra K of every moment
@@ -490,19 +509,7 @@ def _filter_bandwidths(ctx, geom, bw, npow, kid: int = 0):
     """Kernel spectra with the "too small bandwidth" filter of convolution.py:542-605."""
     kern, sums = _make_kernel(ctx, geom, bw, npow, kid)
     if sums is None:
-        # every term of the positive grid sums is at most their total: where
-        # the product of the largest terms already clears twice the
-        # threshold the bandwidth stays, and only the others need the sums
-        norm = SQRT_2PI if kid == 0 else 1.0
-        peak = np.ones(bw.shape[0])
-        for a in range(geom.d):
-            g = np.linspace(geom.lo[a], geom.hi[a], int(geom.G[a]))
-            u = np.min(np.abs(g)) / bw[:, a]
-            peak = peak * (np.exp(-0.5 * (u * u)) / bw[:, a])
-        sums = peak / norm
-        low = np.where(sums < EPS * 20)[0]
-        if len(low):
-            sums[low] = np.prod(_kernel_sums_host(geom, bw[low]), axis=0) / norm
+        sums = _separable_kernel_sums(geom, bw, SQRT_2PI if kid == 0 else 1.0)
     ihbad = np.abs(sums) < EPS * 10
     keep = np.where(~ihbad)[0]
     if np.any(ihbad) and not np.all(ihbad):

@@ -192,3 +192,21 @@ def test_interp_method_resolution():
     from fastlpr_b200 import spline
     with pytest.raises(ValueError):
         spline.band_lu(np.array([0.0, 1.0, 1.0, 2.0]))
+
+
+def test_bandwidth_filter_bound_matches_exact_sums():
+    # the "too small bandwidth" test (convolution.py:542-605) decided from
+    # the largest-term bound agrees with the decision from the exact sums
+    from types import SimpleNamespace
+    rng = np.random.default_rng(0)
+    for _ in range(200):
+        d = int(rng.integers(1, 4))
+        G = rng.integers(3, 600, size=d)
+        hi = rng.uniform(0.5, 3.0, size=d)
+        lo = -hi * rng.uniform(0.9, 1.1, size=d)
+        geom = SimpleNamespace(d=d, G=G, lo=lo, hi=hi)
+        bw = np.exp(rng.uniform(np.log(1e-4), np.log(2.0), size=(40, d)))
+        exact = np.prod(api._kernel_sums_host(geom, bw), axis=0) / api.SQRT_2PI
+        fast = api._separable_kernel_sums(geom, bw, api.SQRT_2PI)
+        np.testing.assert_array_equal(fast < api.EPS * 10, exact < api.EPS * 10)
+        assert np.all(fast <= exact * (1 + 1e-12))
