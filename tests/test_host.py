@@ -210,3 +210,19 @@ def test_bandwidth_filter_bound_matches_exact_sums():
         fast = api._separable_kernel_sums(geom, bw, api.SQRT_2PI)
         np.testing.assert_array_equal(fast < api.EPS * 10, exact < api.EPS * 10)
         assert np.all(fast <= exact * (1 + 1e-12))
+
+
+@pytest.mark.parametrize("dy,cplx", [(1, False), (3, False), (1, True), (2, True)])
+def test_result_layout_matches_channel_rows(dy, cplx):
+    # the output stage downloads fitted values / residuals / grid values in
+    # the result's layout: (k,) or (k, dy), complex from real/imaginary row
+    # pairs; the same arrays as assembling them from the channel rows
+    import torch
+    rng = np.random.default_rng(dy)
+    k = 37
+    rows = rng.standard_normal(((2 if cplx else 1) * dy, k))
+    got = api._result_layout(torch.from_numpy(rows), dy, cplx).numpy()
+    ref = rows[0::2] + 1j * rows[1::2] if cplx else rows
+    ref = ref[0] if dy == 1 else ref.T
+    assert got.shape == ref.shape and got.dtype == ref.dtype
+    np.testing.assert_array_equal(got, ref)
