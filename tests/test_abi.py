@@ -54,3 +54,17 @@ def test_workspace_queries_are_consistent():
     assert 0 < small < big
     assert lib.flpr_point_stats_ws(2, 10 ** 6) > 0
     assert lib.flpr_kde_ws(100, 16, 4096) >= 16 * 8
+
+
+def test_device_knot_map_argument_errors_need_no_gpu():
+    lib = _lib.load()
+    v = _lib.dvec([0.0, 0.0, 0.0])
+    assert lib.flpr_knot_map(5, 10, None, v, v, v, None, None) == -1
+    assert b"d=5" in lib.flpr_last_error()
+    assert lib.flpr_knot_map(2, 10, None, v, v, v, None, None) == -1
+    assert b"null" in lib.flpr_last_error()
+    L = _lib.ivec([64, 64])
+    st = lib.flpr_spread_dkmap(2, 10, None, None, v, L, 4, v, 1, 1, _lib.pvec([]), None, 0,
+                               None, 0, None)
+    assert st == -1
+    assert b"null knot map" in lib.flpr_last_error()
