@@ -172,26 +172,151 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # CPU baseline: the oracle restatement of the reference path
 # ---------------------------------------------------------------------------
-def cpu_baseline(h_sample: int = 2, n: int = N_POINTS):
-    """Fits/s of the CPU oracle on the metric workload, on a bounded sample:
-    a fit over `h_sample` of the 32 bandwidths at full N; phases whose cost
-    grows with the number of bandwidths are scaled to 32."""
+def cpu_fit(seed: int, n: int = N_POINTS, workers: int = 0):
+    """One full fit of the metric workload (all 32 bandwidths) by the CPU
+    oracle on the host cores: (seconds, oracle result, phase seconds)."""
     import oracle
-    x, y, h, opts = workload(0, n)
-    sel = np.linspace(0, N_H - 1, h_sample).round().astype(int)
-    workers = os.cpu_count() or 1
+    x, y, h, opts = workload(seed, n)
+    workers = workers or (os.cpu_count() or 1)
     t = {}
     t0 = time.perf_counter()
-    oracle.cv_fastlpr(x, y, h[sel], opts, workers=workers, timings=t)
-    wall = time.perf_counter() - t0
-    per_h = sum(t.get(k, 0.0) for k in ("kernel", "conv", "solve", "interp"))
-    fixed = sum(t.get(k, 0.0) for k in ("prep", "spread", "fft", "final"))
-    full = fixed + per_h * (N_H / h_sample)
-    return {"value": 1.0 / full, "unit": "fits/s", "cores": workers, "kind": "port",
-            "sample": (f"CPU oracle (numpy/scipy restatement of the reference path), N=1e6, "
-                       f"grid 512^2, {h_sample} of 32 bandwidths ({wall:.1f} s); "
-                       f"bandwidth-proportional phases scaled x{N_H / h_sample:g}"),
-            "seconds_per_fit": full, "phase_seconds": {k: round(v, 3) for k, v in t.items()}}
+    o = oracle.cv_fastlpr(x, y, h, opts, workers=workers, timings=t)
+    return time.perf_counter() - t0, o, t
+
+
+def cpu_baseline(seed: int, n: int = N_POINTS):
+    """Fits/s of the CPU oracle on the metric workload: one full fit (all 32
+    bandwidths, the data set the GPU arm fits), timed as a whole."""
+    workers = os.cpu_count() or 1
+    sec, o, t = cpu_fit(seed, n, workers)
+    return {"value": 1.0 / sec, "unit": "fits/s", "cores": workers, "kind": "port",
+            "sample": (f"one full fit of the benchmark workload by the CPU oracle (numpy/scipy "
+                       f"restatement of the reference path, C gridding): N=1e6, grid 512^2, all "
+                       f"32 bandwidths, data seed {seed} (the GPU arm's data), {sec:.1f} s"),
+            "seconds_per_fit": sec, "phase_seconds": {k: round(v, 3) for k, v in t.items()},
+            "oracle": o}
+
+
+# ---------------------------------------------------------------------------
+# Parity against the CPU oracle: largest relative errors of every output
+# (max-normalised for arrays, element-wise for GCV/LCV scores).  Used by the
+# cpu_baseline leg of the benchmark and by the configuration parity tests.
+# ---------------------------------------------------------------------------
+TOL = {"fp32": 1e-5, "fp64": 1e-9}
+
+
+def _rel(a, b) -> float:
+    a, b = np.asarray(a), np.asarray(b)
+    den = float(np.max(np.abs(b))) if b.size else 0.0
+    return float(np.max(np.abs(a - b)) / (den if den > 0 else 1.0)) if b.size else 0.0
+
+
+def _erel(a, b) -> float:
+    a, b = np.asarray(a, dtype=complex), np.asarray(b, dtype=complex)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+
+
+def lpr_parity(r, o, tol: float) -> dict:
+    """RegressionOutput `r` against the oracle's result `o` of the same fit."""
+    e = {"yhat": _rel(r.yhat, o["yhat"]),
+         "grid_values": _rel(r.fpp_yhat.values, o["grid_values"]),
+         "gcv": _erel(r.gcv_yhat["gcv_m"], o["gcv_m"]),
+         "dof": _rel(r.gcv_yhat["dof"], o["dof_all"]),
+         "s0": _rel(r.s0, o["s0"])}
+    if o.get("d") is not None:
+        e["variance_scale"] = abs(r.d - o["d"]) / abs(o["d"])
+    same = bool(r.gcv_yhat["id1se"] == o["id1se"])
+    worst = max(e.values())
+    return {"max_rel_err": worst, "tol": tol, "same_bandwidth": same,
+            "ok": bool(worst <= tol and same), **e}
+
+
+def kde_parity(k, o, tol: float) -> dict:
+    e = {"density": _rel(k.metadata["fhat_all"], o["fhat_all"]),
+         "lcv": _erel(k.lcv["lcv_m"], o["lcv_m"])}
+    same = bool(k.lcv["id1se"] == o["id1se"])
+    worst = max(e.values())
+    return {"max_rel_err": worst, "tol": tol, "same_bandwidth": same,
+            "ok": bool(worst <= tol and same), **e}
+
+
+def hetero_bandwidth_sample(H: int, sel: int, count: int = 6) -> np.ndarray:
+    """Bandwidth indices of the 2-D local-quadratic parity case: the
+    smallest, the largest, the full sweep's choice and its neighbours, filled
+    up evenly to `count`."""
+    idx = {0, H - 1, sel, max(sel - 1, 0), min(sel + 1, H - 1)}
+    for v in np.linspace(0, H - 1, count).round().astype(int):
+        if len(idx) >= count:
+            break
+        idx.add(int(v))
+    return np.array(sorted(idx))
+
+
+def batched_sample(count: int = 16):
+    """The first `count` problems of the batched workload (1-D and 2-D,
+    orders 0-2, complex responses, N from 9e3 to 8.3e5 for 16)."""
+    return batched_workload(count=512)[:count]
+
+
+def parity_hetero2d(dev, workers: int, full_sel: int = None):
+    """2-D local-quadratic heteroscedastic configuration at full size
+    (N = 2e6, grid 512^2) on a sample of its 32 bandwidths: the mean fit,
+    then the variance fit of the squared residuals, GPU (FP64, the order-2
+    default) against the oracle on identical inputs."""
+    import fastlpr_b200
+    import oracle
+    x, y, h, o = config_workloads()["lpr2d_o2_hetero"]
+    opts = dict(o, device=str(dev))
+    if full_sel is None:
+        full_sel = int(fastlpr_b200.cv_fastlpr(x, y, h, opts).gcv_yhat["id1se"])
+    hs = h[hetero_bandwidth_sample(len(h), full_sel)]
+    r = fastlpr_b200.cv_fastlpr(x, y, hs, opts)
+    om = oracle.cv_fastlpr(x, y, hs, o, workers=workers)
+    yv = (y - r.yhat) ** 2
+    v = fastlpr_b200.cv_fastlpr(x, yv, hs, dict(opts, y_type_out="variance"))
+    ov = oracle.cv_fastlpr(x, yv, hs, dict(o, y_type_out="variance"), workers=workers)
+    return {"mean": lpr_parity(r, om, TOL["fp64"]), "variance": lpr_parity(v, ov, TOL["fp64"]),
+            "bandwidths": [int(i) for i in hetero_bandwidth_sample(len(h), full_sel)],
+            "points": int(x.shape[0]), "precision": "fp64"}
+
+
+def parity_lpr1d(dev, workers: int):
+    """1-D local-linear configuration at full size (N = 1e5, grid 1024,
+    20 bandwidths), default precision (FP32 grids)."""
+    import fastlpr_b200
+    import oracle
+    x, y, h, o = config_workloads()["lpr1d"]
+    r = fastlpr_b200.cv_fastlpr(x, y, h, dict(o, device=str(dev)))
+    return dict(lpr_parity(r, oracle.cv_fastlpr(x, y, h, o, workers=workers), TOL["fp32"]),
+                precision=r.metadata["precision"])
+
+
+def parity_kde3d(dev, workers: int, n: int = 1_000_000):
+    """3-D KDE configuration (mixture of 8 anisotropic Gaussians plus 10%
+    uniform background, grid 128^3, 16 bandwidths) at N = 1e6 points."""
+    import fastlpr_b200
+    import oracle
+    x, h, o = kde3d_workload(n)
+    k = fastlpr_b200.cv_fastkde(x, h, dict(o, device=str(dev)))
+    return dict(kde_parity(k, oracle.cv_fastkde(x, h, o, workers=workers), TOL["fp32"]),
+                points=n, precision=k.metadata["precision"])
+
+
+def parity_batched(results, probs, workers: int) -> dict:
+    """Batched-workload results (RegressionOutputs of `probs`, in order)
+    against the oracle, problem by problem; worst case per precision."""
+    import oracle
+    out = {}
+    for r, (x, y, h, o) in zip(results, probs):
+        prec = r.metadata["precision"]
+        p = lpr_parity(r, oracle.cv_fastlpr(x, y, h, o, workers=workers), TOL[prec])
+        q = out.setdefault(prec, {"problems": 0, "max_rel_err": 0.0, "tol": TOL[prec],
+                                  "all_same_bandwidth": True, "ok": True})
+        q["problems"] += 1
+        q["max_rel_err"] = max(q["max_rel_err"], p["max_rel_err"])
+        q["all_same_bandwidth"] = q["all_same_bandwidth"] and p["same_bandwidth"]
+        q["ok"] = q["ok"] and p["ok"]
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -218,42 +343,58 @@ def max_over_ranks(ms: float, world: int, device) -> float:
     return float(t.item())
 
 
+def bench_config(world: int) -> dict:
+    """The `config` of the benchmark line (both arms print the same one)."""
+    return {"workload": "2-D local-linear GCV sweep (plain full sweep), N=1e6, grid 512^2, "
+                        "32 isotropic h in [0.005,0.5], 10 Hutchinson probes",
+            "global_batch": world, "parallelism": f"replicas x{world}",
+            "l2": "working set (spectra, S/T planes) far larger than the 126 MB L2"}
+
+
 def run_reference(args):
+    """The reference path on the host cores: every step is one full fit of
+    the benchmark workload (all 32 bandwidths, the data set rank 0 of the GPU
+    arm fits) by the CPU oracle, with all host cores; W warm-up fits first.
+    Rank 0 alone runs and prints under torchrun."""
     world, rank, _ = _dist_env()
     if rank != 0:
         return 0
+    seed = replica_seed(0)
+    workers = os.cpu_count() or 1
     for _ in range(args.warmup):
-        pass  # the oracle has no JIT; warm-up steps are not needed
-    vals = []
-    last = None
-    for _ in range(max(1, args.steps)):
-        last = cpu_baseline(h_sample=2)
-        vals.append(last["value"])
-    v = statistics.median(vals)
+        cpu_fit(seed, workers=workers)
+    secs = [cpu_fit(seed, workers=workers)[0] for _ in range(max(1, args.steps))]
+    total = sum(secs)
+    v = len(secs) / total
     line = {
         "impl": "reference",
         "metric": METRIC,
         "value": v,
         "unit": "fits/s",
         "n_gpus": args.gpus,
-        "steps": args.steps,
+        "steps": len(secs),
         "warmup": args.warmup,
-        "ms_per_step": 1000.0 / v,
+        "ms_per_step": 1000.0 * total / len(secs),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded numpy), x~U[0,1]^2, y=sin(2pi x1)cos(2pi x2)+0.1N(0,1)",
-        "config": {"workload": "2-D local-linear GCV sweep, N=1e6, grid 512^2, 32 h, 10 probes",
-                   "parallelism": "host cores"},
-        "cpu_baseline": {k: last[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "config": bench_config(args.gpus),
+        "cpu_baseline": {"value": v, "unit": "fits/s", "cores": workers, "kind": "port",
+                         "sample": (f"{len(secs)} full fits of the benchmark workload (all 32 "
+                                    f"bandwidths, data seed {seed}) by the CPU oracle on "
+                                    f"{workers} host threads, after {args.warmup} warm-up fits; "
+                                    f"median {statistics.median(secs):.2f} s per fit")},
         "e2e": {"value": v, "unit": "fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "seconds_per_fit": [round(t, 3) for t in secs],
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_batched(args, dev, world: int = 1, rank: int = 0, barrier=lambda: None):
+def run_batched(args, dev, world: int = 1, rank: int = 0, barrier=lambda: None,
+                keep: dict = None):
     """The batched uneven workload through LprPlan: every problem's
     y-dependent work captured in one CUDA graph over concurrent streams and
     replayed; each step replaces all responses (fresh noise, pinned staging,
@@ -297,6 +438,11 @@ def run_batched(args, dev, world: int = 1, rank: int = 0, barrier=lambda: None):
     torch.cuda.synchronize(dev)
     seq_ms = max_over_ranks(1000.0 * (time.perf_counter() - t0), world, dev)
     npts = int(sum(p[0].shape[0] for p in allp))
+    if keep is not None:
+        # one more run on the first responses: its results, in problem order,
+        # for the parity check of the cpu_baseline leg
+        keep["results"] = plan.run(ys[0])
+        keep["problems"] = probs
     return {
         "workload": (f"{count} independent problems: half 1-D (grid 1024), half 2-D (grid 256^2), "
                      "N lognormal median 5e4 clipped [1e3,1e6], orders 0-2, 25% complex, 24 h; "
@@ -351,7 +497,7 @@ def config_workloads():
             "kde3d": (x3, None, h3, o3)}
 
 
-def run_configs(args, dev, steps: int = 3):
+def run_configs(args, dev, steps: int = 3, keep: dict = None):
     """Each other configuration through the public API with host arrays
     (cv_fastlpr / cv_fastkde; uploads and downloads included), after one
     warm-up call: seconds per fit by wall clock around synchronised calls."""
@@ -374,12 +520,14 @@ def run_configs(args, dev, steps: int = 3):
             else:
                 def step():
                     return fastlpr_b200.cv_fastlpr(x, y, h, opts)
-            step()
+            last = step()
             torch.cuda.synchronize(dev)
             t0 = time.perf_counter()
             for _ in range(steps):
                 step()
             torch.cuda.synchronize(dev)
+            if keep is not None:
+                keep[name] = last
             sec = (time.perf_counter() - t0) / steps
             out[name] = {"seconds_per_fit": sec, "fits_per_s": 1.0 / sec, "steps": steps,
                          "points": int(x.shape[0]), "bandwidths": int(len(h))}
@@ -554,12 +702,13 @@ def run_ours(args):
         learned = {"unavailable": "no trained bandwidth network (fastlpr_b200/data/bandwidth_mlp.npz)"}
 
     batched = None
+    kept_batched, kept_configs = {}, {}
     if args.batched and not args.bandwidths and args.points == N_POINTS:
-        batched = run_batched(args, dev, world, rank, barrier)
+        batched = run_batched(args, dev, world, rank, barrier, keep=kept_batched)
     # the other configurations, one GPU only (informational, end to end)
     configs = None
     if world == 1 and not args.no_configs and not args.bandwidths and args.points == N_POINTS:
-        configs = run_configs(args, dev)
+        configs = run_configs(args, dev, keep=kept_configs)
 
     per_step_ms = ms_dev / args.steps
     value = world * 1000.0 / per_step_ms
@@ -598,11 +747,8 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded numpy), x~U[0,1]^2, y=sin(2pi x1)cos(2pi x2)+0.1N(0,1)",
-        "config": {"workload": "2-D local-linear GCV sweep (plain full sweep), N=1e6, grid 512^2, "
-                               "32 isotropic h in [0.005,0.5], 10 Hutchinson probes",
-                   "global_batch": world, "parallelism": f"replicas x{world}",
-                   "l2": "working set (spectra, S/T planes) far larger than the 126 MB L2",
-                   "precision": "FP32 grids/FFT/products, FP64 solve and reductions"},
+        "config": bench_config(world),
+        "precision": "FP32 grids/FFT/products, FP64 solve and reductions",
         "e2e": {"value": e2e_value, "unit": "fits/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
@@ -627,9 +773,32 @@ def run_ours(args):
     if args.points != N_POINTS or args.grid or args.bandwidths:
         line["config"]["workload"] = (f"profiling case: N={args.points}, grid {opts['N']}, "
                                       f"{len(h)} bandwidths (not the benchmark workload)")
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline(h_sample=2)
+    if (rank == 0 and world == 1 and not args.no_cpu_baseline and not args.grid
+            and not args.bandwidths):
+        # the CPU oracle on the same data: its timing is the CPU baseline and
+        # its outputs are the parity check of the fit timed above; the other
+        # configurations are checked against it the same way
+        workers = os.cpu_count() or 1
+        cb = cpu_baseline(replica_seed(rank), args.points)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        parity = {"metric": dict(lpr_parity(res["r"], cb["oracle"], TOL["fp32"]),
+                                 precision="fp32", bandwidths=len(h), points=args.points)}
+        if res.get("l") is not None:
+            # the learned search's fit against the oracle's full sweep
+            parity["metric_learned"] = {
+                "yhat": _rel(res["l"].yhat, cb["oracle"]["yhat"]), "tol": TOL["fp32"],
+                "same_bandwidth": bool(np.allclose(res["l"].h, cb["oracle"]["h_sel"]))}
+        if configs is not None and not args.no_parity:
+            parity["lpr1d"] = parity_lpr1d(dev, workers)
+            hs = kept_configs.get("lpr2d_o2_hetero")
+            parity["lpr2d_o2_hetero"] = parity_hetero2d(
+                dev, workers, int(hs[0].gcv_yhat["id1se"]) if hs is not None else None)
+            parity["kde3d"] = parity_kde3d(dev, workers)
+        if kept_batched.get("results") is not None and not args.no_parity:
+            ns = min(16, len(kept_batched["results"]))
+            parity["batched_sample"] = parity_batched(kept_batched["results"][:ns],
+                                                      kept_batched["problems"][:ns], workers)
+        line["parity"] = parity
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -644,7 +813,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU oracle (CPU baseline and every parity check)")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="check only the benchmark fit against the oracle (not the other "
+                         "configurations)")
     ap.add_argument("--batched", type=int, default=512,
                     help="problems of the batched workload leg (0: skip)")
     ap.add_argument("--no-configs", action="store_true",

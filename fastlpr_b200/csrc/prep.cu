@@ -1,6 +1,9 @@
 // Point statistics and small elementwise helpers.
 #include "common.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 namespace flpr {
 
 struct Moments {
@@ -111,23 +114,58 @@ constexpr int kNoAllocMaxBlocks = 1024;
 constexpr int kNoAllocMaxDims = 8;
 static __device__ __align__(256) Moments g_noalloc_partials[kNoAllocMaxBlocks * kNoAllocMaxDims];
 
-// Device address of g_noalloc_partials per device ordinal.  Host code must not
-// pass the symbol itself to a kernel: on the host it is only a stand-in.
+// Device address of g_noalloc_partials, looked up once per device context.
+// Host code must not pass the symbol itself to a kernel: on the host it is
+// only a stand-in.  The cache is keyed by the unique id of the current
+// context (cuCtxGetId), so a context created after a device reset, or a
+// caller's own driver-API context, looks the address up again.
 constexpr int kNoAllocMaxDevices = 64;
 static std::mutex g_noalloc_mu;
-static Moments* g_noalloc_addr[kNoAllocMaxDevices] = {nullptr};
+struct NoAllocSlot {
+  unsigned long long ctx_id;
+  Moments* addr;
+};
+static NoAllocSlot g_noalloc_slot[kNoAllocMaxDevices] = {};
+
+// Unique id of the current context (0 when none is current yet).  Resolved
+// through the runtime's driver entry points, so the library does not link
+// the driver library itself.
+static int current_context_id(unsigned long long* id) {
+  static PFN_cuCtxGetCurrent_v4000 get_current = nullptr;
+  static PFN_cuCtxGetId_v12000 get_id = nullptr;
+  if (get_current == nullptr || get_id == nullptr) {
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+    FLPR_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault,
+                                      &q1));
+    FLPR_CUDA(cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q2));
+    FLPR_CHECK_ARG(q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess,
+                   "point_stats_noalloc: driver entry points cuCtxGetCurrent/cuCtxGetId missing");
+  }
+  CUcontext ctx = nullptr;
+  FLPR_CHECK_ARG(get_current(&ctx) == CUDA_SUCCESS, "point_stats_noalloc: cuCtxGetCurrent failed");
+  *id = 0;
+  if (ctx != nullptr)
+    FLPR_CHECK_ARG(get_id(ctx, id) == CUDA_SUCCESS, "point_stats_noalloc: cuCtxGetId failed");
+  return FLPR_OK;
+}
 
 static int noalloc_scratch(Moments** out) {
   int dev = 0;
   FLPR_CUDA(cudaGetDevice(&dev));
   FLPR_CHECK_ARG(dev >= 0 && dev < kNoAllocMaxDevices, "point_stats_noalloc: device %d", dev);
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (g_noalloc_addr[dev] == nullptr) {
+  unsigned long long id = 0;
+  FLPR_TRY(current_context_id(&id));
+  NoAllocSlot& slot = g_noalloc_slot[dev];
+  if (id == 0 || slot.addr == nullptr || slot.ctx_id != id) {
+    // the lookup makes the device's primary context current when none is
     void* p = nullptr;
     FLPR_CUDA(cudaGetSymbolAddress(&p, g_noalloc_partials));
-    g_noalloc_addr[dev] = static_cast<Moments*>(p);
+    FLPR_TRY(current_context_id(&id));
+    slot.addr = static_cast<Moments*>(p);
+    slot.ctx_id = id;
   }
-  *out = g_noalloc_addr[dev];
+  *out = slot.addr;
   return FLPR_OK;
 }
 

@@ -120,6 +120,10 @@ class LprPlan:
             self._finite = None
             self._write_y([p.su.y_arr for p in self.probs])
             self._check_finite(self._finite)
+            # whether the responses on the device passed their NaN/Inf check
+            # (a rejected run leaves them there; a replay without new
+            # responses would fit them)
+            self._y_ok = True
             self.graph = None
             self.outs = None
             self.tuning = None
@@ -302,6 +306,9 @@ class LprPlan:
         """Fit every problem (with new responses `ys` if given)."""
         with torch.cuda.device(self.device):
             finite = None
+            if ys is None and not self._y_ok:
+                raise ValueError("Response y contains NaN or Inf values (the last responses "
+                                 "given to run were rejected; pass new responses)")
             if ys is not None:
                 if len(ys) != len(self.probs):
                     raise ValueError(f"expected {len(self.probs)} responses, got {len(ys)}")
@@ -321,6 +328,8 @@ class LprPlan:
                 pends.append({k: (api._to_host(v) if isinstance(v, torch.Tensor) and v.is_cuda
                                   else v) for k, v in pend.items()})
             torch.cuda.current_stream(self.device).synchronize()
+            if finite is not None:
+                self._y_ok = bool(finite[0])
             self._check_finite(finite[0] if finite is not None else None)
             ev = api._PhaseEvents(None)
             return [api._finalize_build(self._ctx, outs[i][0], outs[i][1], pends[i], ev, None)

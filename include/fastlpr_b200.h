@@ -85,6 +85,9 @@ int flpr_point_stats(int d, int64_t n, const double* d_x, double* d_stats,
  * rejected with FLPR_ERR_ARG and a message); any n.  The first call on a
  * device looks up that array's device address (cudaGetSymbolAddress), so
  * make the first call on each device before any stream capture begins.
+ * The address is cached per device context (its cuCtxGetId): after a
+ * device reset, or under another context of the same device, the next call
+ * looks it up again, so again call it once before capturing there.
  * All calls share the array: two calls whose kernels overlap on the GPU
  * (different streams, no ordering between them) race and may return wrong
  * statistics; calls on one stream are ordered and safe. */

@@ -226,7 +226,8 @@ def channel_spectra(xmod: np.ndarray, chans: np.ndarray, L, accuracy: int, n_poi
     msp, tau, ratio = spread_params(L, accuracy)
     grid = spread_grid(xmod, chans, np.asarray(L) * ratio, msp, tau)
     if ratio > 1:
-        return nufft_spectra_oversampled(grid, n_points, L, ratio, tau, workers)
+        return hermitian_part(nufft_spectra_oversampled(grid, n_points, L, ratio, tau, workers),
+                              range(1, grid.ndim))
     return nufft_spectra(grid, n_points, workers)
 
 
@@ -371,19 +372,45 @@ def kernel_spectra(x_scaled, h, G, order: int, flag_power2: bool = True, workers
     return spectra, dict(L=L, qin=qin, qout=qout, h=h, ihbad=ihbad, G=G)
 
 
+def hermitian_part(spec: np.ndarray, axes: Sequence[int]) -> np.ndarray:
+    """(X[f] + conj(X[-f])) / 2 over the frequency `axes`.  The reference
+    keeps the real part of the inverse transform of K X (K Hermitian);
+    that real part is the inverse transform of K times this part of X, which
+    makes the half-spectrum convolution below exact for spectra that are not
+    Hermitian (the cropped oversampled spectra of accuracy >= 7)."""
+    conj_neg = np.conj(spec)
+    for ax in axes:
+        conj_neg = np.roll(np.flip(conj_neg, axis=ax), 1, axis=ax)
+    return 0.5 * (spec + conj_neg)
+
+
 def convolve(spec_c: np.ndarray, kdf: np.ndarray, qout, G, real: bool = True, workers: int = 1):
     """nufft_convolve (convolution.py:907-951): product, inverse FFT per axis, crop.
 
-    spec_c: (*L, C), kdf: (*L, H) -> (*G, H, C).
+    spec_c: (*L, C), kdf: (*L, H) -> (*G, H, C).  The reference forms the
+    full product, inverts every axis and keeps the real part.  For Hermitian
+    spectra (transforms of real grids; see hermitian_part) that real part is
+    obtained from the half spectrum along the last axis: the leading axes are
+    inverted on the kept columns and cropped, the last axis by a real inverse
+    transform of length L.  Same values up to rounding, a third of the work.
     """
     dims = kdf.ndim - 1
-    prod = kdf[..., :, None] * spec_c[..., None, :]
-    for ax in range(dims):
+    if not real:
+        prod = kdf[..., :, None] * spec_c[..., None, :]
+        for ax in range(dims):
+            prod = sfft.ifft(prod, axis=ax, workers=workers, overwrite_x=True)
+        sl = tuple(slice(qout[0, d], qout[0, d] + G[d]) for d in range(dims))
+        return prod[sl]
+    Ll = kdf.shape[dims - 1]
+    half = (slice(None),) * (dims - 1) + (slice(0, Ll // 2 + 1),)
+    prod = kdf[half][..., :, None] * spec_c[half][..., None, :]
+    for ax in range(dims - 1):
         prod = sfft.ifft(prod, axis=ax, workers=workers, overwrite_x=True)
-    if real:
-        prod = prod.real
-    sl = tuple(slice(qout[0, d], qout[0, d] + G[d]) for d in range(dims))
-    return prod[sl]
+        crop = (slice(None),) * ax + (slice(qout[0, ax], qout[0, ax] + G[ax]),)
+        prod = prod[crop]
+    out = sfft.irfft(prod, n=Ll, axis=dims - 1, workers=workers)
+    crop = (slice(None),) * (dims - 1) + (slice(qout[0, dims - 1], qout[0, dims - 1] + G[dims - 1]),)
+    return out[crop]
 
 
 # --------------------------------------------------------------------------
@@ -409,16 +436,46 @@ def solve_system(S: List[np.ndarray], T: List[np.ndarray], order: int, regulariz
             di = k * nt - k * (k - 1) // 2
             max_diag = max(max_diag, float(np.max(np.abs(S[di]))))
         lam = 1e-6 * max_diag
-    shape = S[0].shape
-    M = np.empty(shape + (nt, nt))
+    A = {}
     for k, (i, j) in enumerate(design_pairs(nt)):
-        M[..., i, j] = S[k]
-        M[..., j, i] = S[k]
-    for k in range(nt):
-        M[..., k, k] += lam
-    Tm = np.stack(T, axis=-2)  # (*G, H, nt, C)
-    beta = np.linalg.solve(M, Tm)
-    return beta[..., 0, :], lam
+        A[i, j] = A[j, i] = S[k] + (lam if i == j else 0.0)
+    if nt > 4:
+        # 2-D order 2: the reference's closed form reads a data file its
+        # package does not ship (lwp_formulas.py:436-444); solve directly
+        M = np.empty(S[0].shape + (nt, nt))
+        for (i, j), v in A.items():
+            M[..., i, j] = v
+        beta = np.linalg.solve(M, np.stack(T, axis=-2))   # T: (*G, H, nt, C)
+        return beta[..., 0, :], lam
+    # Cramer's rule, the form of the reference's closed-form estimators
+    # (lwp_formulas.py:133-380): the first row of (S + lambda I)^-1 is the
+    # first column of cofactors over the determinant (S is symmetric)
+    cof = [_cofactor0(A, nt, j) for j in range(nt)]
+    det = sum(A[0, j] * cof[j] for j in range(nt))
+    num = cof[0][..., None] * T[0]
+    for j in range(1, nt):
+        num += cof[j][..., None] * T[j]
+    num /= det[..., None]
+    return num, lam
+
+
+def _det(A, rows, cols):
+    """Determinant of the sub-matrix of the element arrays A[i, j]."""
+    if len(rows) == 1:
+        return A[rows[0], cols[0]]
+    out = 0.0
+    for k, c in enumerate(cols):
+        sub = _det(A, rows[1:], cols[:k] + cols[k + 1:])
+        out = out + (A[rows[0], c] * sub if k % 2 == 0 else -(A[rows[0], c] * sub))
+    return out
+
+
+def _cofactor0(A, nt, j):
+    """Cofactor (0, j) of the nt x nt element arrays A."""
+    rows = list(range(1, nt))
+    cols = [c for c in range(nt) if c != j]
+    m = _det(A, rows, cols)
+    return m if j % 2 == 0 else -m
 
 
 # --------------------------------------------------------------------------
@@ -670,7 +727,8 @@ def cv_fastlpr(x, y, h=None, options: Optional[Dict] = None, workers: int = 1,
         msp, tau, ratio = spread_params(L, acc)
         grid = spread_grid(xmod, np.column_stack([np.ones(n), ycols, p]),
                            np.asarray(L) * ratio, msp, tau)
-        spec = (nufft_spectra_oversampled(grid, n, L, ratio, tau, workers) if ratio > 1
+        spec = (hermitian_part(nufft_spectra_oversampled(grid, n, L, ratio, tau, workers),
+                               range(1, dims + 1)) if ratio > 1
                 else nufft_spectra(grid, n, workers))
     else:
         s_ones_p = channel_spectra(xmod, np.column_stack([np.ones(n), p]), L, acc_default, n,
@@ -828,7 +886,9 @@ def cv_fastkde(x, h=None, options: Optional[Dict] = None, workers: int = 1,
     xmod = knot_coordinates(xs, L, G, qin)
     grid = spread_grid(xmod, np.ones((n, 1)), np.asarray(L) * ratio, msp, tau)
     if ratio > 1:
-        spec = np.moveaxis(nufft_spectra_oversampled(grid, n, L, ratio, tau, workers), 0, -1)
+        spec = np.moveaxis(hermitian_part(nufft_spectra_oversampled(grid, n, L, ratio, tau,
+                                                                    workers),
+                                          range(1, dims + 1)), 0, -1)
     else:
         spec = np.moveaxis(nufft_spectra(grid, n, workers), 0, -1)
     s = np.empty(tuple(G) + (H,))

@@ -1,8 +1,9 @@
 """Generate golden fixtures by running the reference fastLPR Python package.
 
 This script is the only committed file that executes the reference.  It
-imports ``fastlpr`` from a read-only checkout (default
-``/root/reference/fastLPR_py/src``, override with ``FASTLPR_REF_SRC``), runs
+imports ``fastlpr`` from a read-only checkout of the reference (the
+``fastLPR_py/src`` directory, given in the environment variable
+``FASTLPR_REF_SRC``), runs
 it on small seeded inputs and stores inputs and outputs as ``.npz`` files
 next to this script.  The fixtures pin the CPU oracle (``oracle/``) and the
 GPU path without needing the reference at test time.
@@ -18,7 +19,7 @@ Two patches are applied to the reference, both to its FP64 configuration:
   ``numpy.linalg.solve`` of ``e1' (S + lambda I)^-1 T`` -- the definition the
   closed form implements (``py/lwp_formulas.py:12-14``).
 
-Run:  python tests/golden/make_golden.py
+Run:  FASTLPR_REF_SRC=<checkout>/fastLPR_py/src python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -29,10 +30,12 @@ import warnings
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = os.environ.get("FASTLPR_REF_SRC", "/root/reference/fastLPR_py/src")
+REF_SRC = os.environ.get("FASTLPR_REF_SRC")
 
 
 def _import_reference():
+    if not REF_SRC:
+        raise SystemExit("set FASTLPR_REF_SRC to the reference's fastLPR_py/src directory")
     os.environ.setdefault("FASTLPR_QUIET", "1")
     os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")
     sys.path.insert(0, REF_SRC)

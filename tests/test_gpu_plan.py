@@ -113,6 +113,10 @@ def test_plan_rejects_nonfinite_responses_and_recovers(cuda_ok):
     bad[3][5] = np.inf
     with pytest.raises(ValueError, match="NaN or Inf"):
         plan.run(bad)
+    # the rejected responses are still on the device: a run without new
+    # responses must refuse them too
+    with pytest.raises(ValueError, match="NaN or Inf"):
+        plan.run()
     out = plan.run([p[1] for p in probs])
     for (x, y, h, opts), r in zip(probs, out):
         _same(r, fastlpr_b200.cv_fastlpr(x, y, h, opts), _tol(opts))

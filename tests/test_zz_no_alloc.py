@@ -39,8 +39,11 @@ def test_noalloc_point_stats_matches_workspace_version(cuda_ok):
     lib = _lib.load()
     torch.cuda.set_device(0)
     rng = np.random.default_rng(99)
-    # two calls in a row with different shapes: the second reuses the scratch
-    for n, d in ((300_000, 2), (12_345, 3)):
+    # calls in a row with different shapes: each reuses the scratch; d = 8 is
+    # the largest axis count the scratch holds, and 2e6 points fill every
+    # block of the grid (4 per SM; the 1024-block clamp of the scratch is
+    # above that on this part)
+    for n, d in ((300_000, 2), (12_345, 3), (2_000_000, 8), (777, 8)):
         x = rng.standard_normal((n, d)) * np.arange(1, d + 1) + 5.0
         ref, got = _stats_both(lib, _lib, torch, x)
         np.testing.assert_allclose(got, ref, rtol=1e-12, atol=0)
