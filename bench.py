@@ -458,6 +458,83 @@ def run_batched(args, dev, world: int = 1, rank: int = 0, barrier=lambda: None,
     }
 
 
+def run_learned_batched(args, dev, plain_fits_per_s: float):
+    """The learned search over a batch of benchmark-shaped data sets (N = 1e6,
+    grid 512^2, the 32 bandwidths, each its own seed) through one LprPlan:
+    binned sums, features, the network (one batch) and every window chosen
+    and evaluated inside one CUDA graph; each step stages new responses for
+    every data set (host-to-device copies inside the timed region), replays
+    and returns every result.  The same data sets through a full-sweep
+    LprPlan give the swept GCV optimum each choice is judged against."""
+    import torch
+
+    import fastlpr_b200
+    count = args.learned_batched
+    probs, ys2 = [], []
+    for k in range(count):
+        x, y, h, o = workload(2000 + k)
+        rng = np.random.default_rng(3000 + k)
+        probs.append((x, y, h, dict(o, precision="fp32", bandwidth_search="learned")))
+        ys2.append(np.sin(2 * np.pi * x[:, 0]) * np.cos(2 * np.pi * x[:, 1])
+                   + 0.1 * rng.standard_normal(x.shape[0]))
+    ys = [[p[1] for p in probs], ys2]
+    t0 = time.perf_counter()
+    plan = fastlpr_b200.LprPlan(probs, device=dev)
+    build_s = time.perf_counter() - t0
+    try:
+        for k in range(2):
+            plan.run(ys[k % 2])
+        torch.cuda.synchronize(dev)
+        steps = max(2, min(args.steps, 5))
+        t0 = time.perf_counter()
+        for k in range(steps):
+            res = plan.run(ys[k % 2])
+        ms = 1000.0 * (time.perf_counter() - t0) / steps
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        plan.graph.replay()
+        e.record()
+        e.synchronize()
+        replay_ms = s.elapsed_time(e)
+        last = plan.run(ys[0])
+    finally:
+        plan.close()
+    # the full sweep of the same data sets judges every choice
+    fprobs = [(x, y, h, dict(o, bandwidth_search="full")) for (x, y, h, o) in probs]
+    fplan = fastlpr_b200.LprPlan(fprobs, device=dev)
+    try:
+        fplan.run(ys[0])
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        full = fplan.run(ys[0])
+        full_ms = 1000.0 * (time.perf_counter() - t0)
+    finally:
+        fplan.close()
+    ratios, accepted, evaluated, same = [], 0, [], 0
+    for lr, fr in zip(last, full):
+        bs = lr.metadata["bandwidth_search"]
+        accepted += int(bool(bs.get("accepted")))
+        evaluated.append(int(bs.get("evaluated", len(fr.gcv_yhat["gcv_m"]))))
+        ratios.append(float(np.min(lr.gcv_yhat["gcv_m"]) / np.min(fr.gcv_yhat["gcv_m"])))
+        same += int(np.allclose(lr.h, fr.h))
+    value = count * 1000.0 / ms
+    return {
+        "workload": (f"{count} data sets of the benchmark shape (N=1e6, grid 512^2, 32 isotropic h "
+                     f"in [0.005,0.5], 10 probes, seeds 2000..{1999 + count}), learned search in "
+                     "one LprPlan graph; new responses every step"),
+        "value": value, "unit": "fits/s", "ms_per_batch": ms, "graph_replay_ms": replay_ms,
+        "speedup_vs_plain": value / plain_fits_per_s,
+        "full_sweep_batched_fits_per_s": count * 1000.0 / full_ms,
+        "speedup_vs_full_sweep_batched": full_ms / ms,
+        "accepted": accepted, "bandwidths_evaluated_mean": float(np.mean(evaluated)),
+        "gcv_ratio_vs_full_sweep_max": float(np.max(ratios)),
+        "all_within_1pct_gcv": bool(np.max(ratios) <= 1.01),
+        "same_bandwidth_as_full_sweep": same, "plan_build_s": build_s,
+        "timing": "wall clock per step (staging, replay, outputs), after 2 warm-up steps",
+    }
+
+
 def kde3d_workload(n: int, seed: int = 5):
     """The 3-D KDE case: a mixture of 8 anisotropic Gaussians (means
     U[0.2,0.8]^3, per-axis std U[0.02,0.1], equal weights) plus 10% uniform
@@ -701,6 +778,9 @@ def run_ours(args):
     elif not have_net:
         learned = {"unavailable": "no trained bandwidth network (fastlpr_b200/data/bandwidth_mlp.npz)"}
 
+    learned_batched = None
+    if args.learned_batched and not args.bandwidths and args.points == N_POINTS and have_net:
+        learned_batched = run_learned_batched(args, dev, world * 1000.0 / (ms_dev / args.steps))
     batched = None
     kept_batched, kept_configs = {}, {}
     if args.batched and not args.bandwidths and args.points == N_POINTS:
@@ -765,6 +845,7 @@ def run_ours(args):
                                "frac": achieved_fit / hbm,
                                "algorithmic_bytes": bf},
         "learned": learned,
+        "learned_batched": learned_batched,
         "batched": batched,
         "configs": configs,
         "phase_ms": {k: round(v, 3) for k, v in phases.items()},
@@ -818,6 +899,8 @@ def main():
     ap.add_argument("--no-parity", action="store_true",
                     help="check only the benchmark fit against the oracle (not the other "
                          "configurations)")
+    ap.add_argument("--learned-batched", type=int, default=32,
+                    help="data sets of the learned-search batch leg (0: skip)")
     ap.add_argument("--batched", type=int, default=512,
                     help="problems of the batched workload leg (0: skip)")
     ap.add_argument("--no-configs", action="store_true",

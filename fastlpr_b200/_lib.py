@@ -78,6 +78,9 @@ SIGNATURES = [
     ("flpr_log_shift", _I, [_I64, _VP, _D, _VP, _VP]),
     ("flpr_exp_weighted_sum", _I, [_I64, _VP, _VP, _VP, _VP]),
     ("flpr_bin_moments", _I, [_I, _I64, _VP, _VP, _VP, _VP, _VP]),
+    ("flpr_learned_features", _I, [_I, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    ("flpr_learned_window", _I, [_I, _VP, _D, _D, _I, _VP, _I, _VP, _VP, _I, _VP, _VP, _VP]),
+    ("flpr_copy_rows", _I, [_VP, _VP, _I64, _I, _VP, _VP]),
     ("flpr_mlp_gemm", _I, [_I, _I, _I, _VP, _I, _I, _VP, _I, _I, _VP, _I, _VP, _I, _VP, _VP, _I,
                            _VP]),
     ("flpr_mlp_param_count", _I64, [_I, _PI]),

@@ -1364,11 +1364,15 @@ def _side_stream(device: torch.device) -> torch.cuda.Stream:
     return _SIDE_STREAMS[idx]
 
 
-def _start_summary(ctx, pending: dict, dx, ycols, stats, n, d, d_stats=None) -> None:
-    """Binned moment sums of the data on a side stream, copied to pinned
-    host memory, overlapping the spread that the main stream runs next."""
+def _start_summary(ctx, pending: dict, dx, ycols, stats, n, d, d_stats=None, model=None,
+                   order: int = 0, log_h=None) -> None:
+    """The proposal chain on a side stream, overlapping the spread that the
+    main stream runs next: binned moment sums of the data, their feature
+    vector, the network and the window start in the bandwidth list
+    (learned.DeviceProposal), copied to pinned host memory.  Nothing here
+    waits for the device."""
     from . import learned as _learned
-    if len(ycols) != 1 or d > 2:
+    if len(ycols) != 1 or d > 2 or model is None or log_h is None:
         return
     side = _side_stream(ctx.device)
     ready = torch.cuda.Event()
@@ -1379,68 +1383,122 @@ def _start_summary(ctx, pending: dict, dx, ycols, stats, n, d, d_stats=None) -> 
         ycols[0].record_stream(side)
         if d_stats is None:
             d_stats = ctx.upload(np.ascontiguousarray(stats[:2].ravel()))
-        bins = _learned.bin_moments(dx, ycols[0], d_stats, n, d, side.cuda_stream)
-        host = torch.empty(bins.shape, dtype=bins.dtype, pin_memory=True)
-        host.copy_(bins, non_blocking=True)
+        prop = _learned.DeviceProposal(model, [(d, order, n)], [log_h], ctx.device)
+        _lib.check(ctx.lib.flpr_bin_moments(d, n, dx.data_ptr(), ycols[0].data_ptr(),
+                                            d_stats.data_ptr(), prop.bins.data_ptr(),
+                                            side.cuda_stream), "flpr_bin_moments")
+        prop.enqueue(side.cuda_stream)
+        lo_h, t_h = _to_host(prop.lo), _to_host(prop.t)
         done = torch.cuda.Event()
         done.record(side)
-    pending.update(side=side, host=host, done=done, keep=(bins, d_stats))
+    pending.update(side=side, prop=prop, lo=lo_h, t=t_h, done=done, keep=(d_stats,))
+
+
+def _window_filter(ctx, st: _LprState, filt_all, lo_dev: torch.Tensor, W: int):
+    """Kernel factors of the W consecutive bandwidths starting at the index
+    in lo_dev (on the device) of a filter over the whole list, gathered on
+    the device (flpr_copy_rows), and their bandwidth sums.  The returned
+    filter's bandwidth rows are placeholders until the host knows the
+    window."""
+    kern, bw, keep, _ = filt_all
+    H, npow = kern.H, kern.npow
+    data = ctx.empty((int(sum(W * npow * int(La) for La in st.geom.L)), 2))
+    src, dst = kern.data_ptr(), data.data_ptr()
+    for La in st.geom.L:
+        row = npow * int(La) * 16
+        ctx.check(ctx.lib.flpr_copy_rows(src, dst, row, W, lo_dev.data_ptr(), ctx.stream),
+                  "flpr_copy_rows")
+        src += H * row
+        dst += W * row
+    hs_all = st.__dict__.get("_hsum_all")
+    if hs_all is None or hs_all.shape[0] != H:
+        hs = torch.from_numpy(np.ascontiguousarray(np.sum(bw[keep], axis=1))).pin_memory()
+        hs_all = hs.to(ctx.device, non_blocking=True)
+    hsum = ctx.empty(W)
+    ctx.check(ctx.lib.flpr_copy_rows(hs_all.data_ptr(), hsum.data_ptr(), 8, W, lo_dev.data_ptr(),
+                                     ctx.stream), "flpr_copy_rows")
+    kw = _Kernel(kern.kid, data, W, npow, kern.scale)
+    return (kw, bw[keep][:W], np.arange(W), np.zeros(W, dtype=bool)), hsum, hs_all
 
 
 def _learned_search(ctx, st: _LprState, bandwidths: np.ndarray, model, ev, pending: dict):
     """Proposal + five-bandwidth window, walked toward an edge minimum (the
     next window shares the edge bandwidth) at most _MAX_WALKS times; returns
     (evaluation, search record, pending outputs or None) or None when the
-    full sweep must run.  The first window is evaluated speculatively: its
-    GCV, 1-SE choice and output stage are enqueued on the device together
-    and one synchronisation brings back the scores that decide acceptance
-    with the outputs (used as they are when the window is accepted)."""
+    full sweep must run.  The first window is chosen and evaluated without a
+    host round trip: the proposal chain ran on the side stream
+    (_start_summary), the window's kernel factors are gathered on the device
+    at the start index it wrote, and GCV, the 1-SE choice and the output
+    stage are enqueued behind them; one synchronisation brings back the
+    window, its scores and the outputs (used as they are when the window is
+    accepted)."""
     from . import learned as _learned
     if not (st.calc_dof and st.ny == 1 and not st.y_is_complex and st.d <= 2
-            and st.kid == 0) or not pending:
+            and st.kid == 0) or not pending.get("prop"):
         return None
-    lh = _learned.isotropic_log_h(bandwidths)
-    if lh is None:
-        return None
-    # the summary was enqueued on the side stream before the spread: waiting
-    # for it does not wait for the main stream
-    pending["done"].synchronize()
-    feats = _learned.summarize(pending["host"].numpy(), st.d, st.n, st.order)
-    with torch.cuda.stream(pending["side"]):
-        t = float(model.predict(feats)[0])
-    ev.mark("proposal")
     nlist = int(bandwidths.shape[0])
-    window = _learned.refine_window(t, lh)
-    record = {"mode": "learned", "proposal_index": t, "windows": [], "nlist": nlist,
-              "accepted": False}
+    npow = 2 * st.order + 1
+    filt_all = _filter_bandwidths(ctx, st.geom, bandwidths, npow, st.kid)
+    if len(filt_all[2]) != nlist:
+        return None                         # a bandwidth of the list is filtered out
+    R = _learned.REFINE
+    torch.cuda.current_stream(ctx.device).wait_event(pending["done"])
+    filt_w, hsum, _ = _window_filter(ctx, st, filt_all, pending["prop"].lo, R)
+    r = _evaluate_device(ctx, st, filt_w, ev)
+    pend = _finalize_enqueue(ctx, st, r, ev, device_select=True, hsum_dev=hsum)
+    torch.cuda.current_stream(ctx.device).synchronize()
+    ev.mark("proposal")
+    return _learned_finish(ctx, st, bandwidths, r, pend, int(pending["lo"].numpy()[0]),
+                           float(pending["t"].numpy()[0]), ev)
+
+
+def _learned_finish(ctx, st: _LprState, bandwidths: np.ndarray, r: dict, pend: dict, lo: int,
+                    t: float, ev):
+    """Acceptance of a first window evaluated on the device (start index lo,
+    proposal t; r / pend its evaluation and output stage, complete), then the
+    walks toward an edge minimum: (evaluation, search record, pending
+    outputs or None) or None when the full sweep must run."""
+    from . import learned as _learned
+    R = _learned.REFINE
+    nlist = int(bandwidths.shape[0])
+    window = np.arange(lo, lo + R)
+    r["bw_k"] = bandwidths[window]
+    record = {"mode": "learned", "proposal_index": t, "windows": [[int(i) for i in window]],
+              "nlist": nlist, "accepted": False}
+    gcv_m = pend["gcv"].numpy()[:R]
     for walk in range(_MAX_WALKS + 1):
-        record["windows"].append([int(i) for i in window])
-        filt = _filter_bandwidths(ctx, st.geom, bandwidths[window], 2 * st.order + 1, st.kid)
-        if len(filt[2]) != len(window):
-            return None                     # a bandwidth of the window was filtered out
-        pend = None
-        if walk == 0:
-            r = _evaluate_device(ctx, st, filt, ev)
-            pend = _finalize_enqueue(ctx, st, r, ev, device_select=True)
-            torch.cuda.current_stream(ctx.device).synchronize()
-            gcv_m = pend["gcv"].numpy()[:len(window)]
-        else:
-            r = _evaluate_device(ctx, st, filt, ev)
-            r = _evaluate_host(st, r, r["packed"].cpu().numpy())
-            gcv_m = r["gcv"]["gcv_m"]
         pos = int(np.argmin(gcv_m))
         if _learned.accept_window(window, pos, nlist):
             record["accepted"] = True
             record["evaluated"] = len({i for w in record["windows"] for i in w})
-            return r, record, pend
-        step = _learned.REFINE - 1
+            return r, record, (pend if walk == 0 else None)
+        if walk == _MAX_WALKS:
+            break
+        step = R - 1
         lo = int(window[0]) + (step if pos == len(window) - 1 else -step)
-        lo = int(np.clip(lo, 0, nlist - _learned.REFINE))
-        nxt = np.arange(lo, lo + _learned.REFINE)
+        lo = int(np.clip(lo, 0, nlist - R))
+        nxt = np.arange(lo, lo + R)
         if np.array_equal(nxt, window):
             return None
         window = nxt
+        record["windows"].append([int(i) for i in window])
+        filt = _filter_bandwidths(ctx, st.geom, bandwidths[window], 2 * st.order + 1, st.kid)
+        r = _evaluate_device(ctx, st, filt, ev)
+        r = _evaluate_host(st, r, r["packed"].cpu().numpy())
+        gcv_m = r["gcv"]["gcv_m"]
     return None
+
+
+def _full_sweep(ctx, st: _LprState, bandwidths: np.ndarray, ev, search,
+                filt=None) -> RegressionOutput:
+    """Every bandwidth of the list: GCV, the 1-SE choice and the output stage
+    are enqueued on the device behind the reductions; one synchronisation."""
+    if filt is None:
+        filt = _filter_bandwidths(ctx, st.geom, bandwidths, 2 * st.order + 1, st.kid)
+    r = _evaluate_device(ctx, st, filt, ev)
+    pend = _finalize_enqueue(ctx, st, r, ev, device_select=True)
+    torch.cuda.current_stream(ctx.device).synchronize()
+    return _finalize_build(ctx, st, r, pend, ev, search)
 
 
 def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_is_complex,
@@ -1453,8 +1511,12 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
     pending = {}
     hook = None
     if learned is not None:
+        from . import learned as _learned
+        lh = _learned.isotropic_log_h(bandwidths)
+
         def hook(dx, ycols, stats, n, d, d_stats=None):
-            _start_summary(ctx, pending, dx, ycols, stats, n, d, d_stats=d_stats)
+            _start_summary(ctx, pending, dx, ycols, stats, n, d, d_stats=d_stats, model=learned,
+                           order=order, log_h=lh)
     st = _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_complex,
                       dev_inputs, ev, hook=hook)
     found = (_learned_search(ctx, st, bandwidths, learned, ev, pending)
@@ -1464,15 +1526,9 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
         if pend is not None:
             return _finalize_build(ctx, st, r, pend, ev, search)
         return _finalize_lpr(ctx, st, r, ev, search)
-    # full sweep: GCV, the 1-SE choice and the output stage are enqueued on
-    # the device behind the reductions; one synchronisation at the end
     search = None if learned is None else {"mode": "learned", "accepted": False,
                                            "fallback": "full sweep"}
-    filt = _filter_bandwidths(ctx, st.geom, bandwidths, 2 * st.order + 1, st.kid)
-    r = _evaluate_device(ctx, st, filt, ev)
-    pend = _finalize_enqueue(ctx, st, r, ev, device_select=True)
-    torch.cuda.current_stream(ctx.device).synchronize()
-    return _finalize_build(ctx, st, r, pend, ev, search)
+    return _full_sweep(ctx, st, bandwidths, ev, search)
 
 
 def _gcv_from_sums(n, rss, pdot, pp, dy, y_is_complex, opts):

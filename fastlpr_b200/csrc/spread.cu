@@ -474,6 +474,35 @@ __device__ __forceinline__ void shared_add(long long* p, long long v) {
 }
 __device__ __forceinline__ void shared_add(double* p, double v) { atomicAdd(p, v); }
 
+// Register accumulators of the 2-D path.  Fixed point: the product v w is
+// rounded once to the nearest integer by the fused multiply-add
+// t = v w + 1.5 * 2^52 (every double in [2^52, 2^53) is an integer, and
+// |v w| < 2^50 keeps t there), and the bit pattern of t is
+// bits(1.5 * 2^52) + round(v w), so the register adds the bit patterns in
+// integer arithmetic (modulo 2^64) and the flush subtracts the bias once per
+// add it received.  One FP64 instruction per product; the sum is exact and
+// independent of the order of the points.  Float64 accumulation adds the
+// fused product.
+template <typename Acc>
+struct Reg2;
+template <>
+struct Reg2<long long> {
+  using T = unsigned long long;
+  static constexpr unsigned long long kBias = 0x4338000000000000ull;  // bits(1.5 * 2^52)
+  __device__ static void add(T& a, double v, double w) {
+    a += (unsigned long long)__double_as_longlong(__fma_rn(v, w, 6755399441055744.0));
+  }
+  __device__ static long long value(T a, int adds) {
+    return (long long)(a - (unsigned long long)adds * kBias);
+  }
+};
+template <>
+struct Reg2<double> {
+  using T = double;
+  __device__ static void add(T& a, double v, double w) { a = __fma_rn(v, w, a); }
+  __device__ static double value(T a, int) { return a; }
+};
+
 // Halo-row stride (odd) and channel stride (odd) of the shared tile.
 __host__ __device__ constexpr int row_stride2(int nt1) { return (kT2 + nt1 - 1) | 1; }
 __host__ __device__ constexpr int chan_stride2(int w0, int nt1) { return (w0 * row_stride2(nt1)) | 1; }
@@ -579,11 +608,11 @@ tile_accumulate_2d_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, 
       const int grp = gb * GPL + gsub;
       const bool active = lane < NT1 * GPL && grp < ngrp;
       const int c0 = grp * kUnitCh;
-      double a[kUnitCh][NACC];
+      typename Reg2<Acc>::T a[kUnitCh][NACC];
 #pragma unroll
       for (int k = 0; k < kUnitCh; ++k)
 #pragma unroll
-        for (int j = 0; j < NACC; ++j) a[k][j] = 0.0;
+        for (int j = 0; j < NACC; ++j) a[k][j] = 0;
       const int rowbase = l0 * kT2;
 #pragma unroll
       for (int cr = 0; cr < kT2; ++cr) {
@@ -598,19 +627,30 @@ tile_accumulate_2d_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, 
           for (int jx = 0; jx < NT1; ++jx) {
             const double w = wx[pp * NT1 + jx];
 #pragma unroll
-            for (int k = 0; k < kUnitCh; ++k) reg_add<Acc>(a[k][cr + jx], v[k] * w);
+            for (int k = 0; k < kUnitCh; ++k) Reg2<Acc>::add(a[k][cr + jx], v[k], w);
           }
         }
       }
       if (active) {
+        // adds register j received: one per point of the cell rows cr with
+        // 0 <= j - cr < NT1
+        int rows[kT2];
+#pragma unroll
+        for (int cr = 0; cr < kT2; ++cr) rows[cr] = off[rowbase + cr + 1] - off[rowbase + cr];
         Acc* rowp = acc + (size_t)(l0 + jy) * RS;
 #pragma unroll
-        for (int k = 0; k < kUnitCh; ++k) {
-          if (c0 + k >= nc) break;
+        for (int j = 0; j < NACC; ++j) {
+          int adds = 0;
 #pragma unroll
-          for (int j = 0; j < NACC; ++j)
-            if (a[k][j] != 0.0)
-              shared_add(rowp + (size_t)(c0 + k) * CS + j, reg_value<Acc>(a[k][j]));
+          for (int cr = 0; cr < kT2; ++cr)
+            if (j - cr >= 0 && j - cr < NT1) adds += rows[cr];
+#pragma unroll
+          for (int k = 0; k < kUnitCh; ++k) {
+            if (c0 + k < nc) {
+              const Acc val = Reg2<Acc>::value(a[k][j], adds);
+              if (val != Acc(0)) shared_add(rowp + (size_t)(c0 + k) * CS + j, val);
+            }
+          }
         }
       }
     }

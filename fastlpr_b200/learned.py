@@ -330,3 +330,62 @@ def accept_window(window: np.ndarray, idmin: int, nlist: int) -> bool:
     or sits at an end of the whole list."""
     g = int(window[idmin])
     return (0 < idmin < len(window) - 1) or g == 0 or g == nlist - 1
+
+
+# ---------------------------------------------------------------- device chain
+
+class DeviceProposal:
+    """The proposal chain of B data sets on the device, without a host round
+    trip: binned sums (filled per data set by ``bin_moments``), feature
+    vectors and their standardised BF16 copy (``flpr_learned_features``), the
+    network (``flpr_mlp_fwd``, one batch for all data sets) and the window
+    start of the local sweep in each data set's own bandwidth list
+    (``flpr_learned_window``).  Every buffer lives as long as this object, so
+    the chain can be captured in a CUDA graph and replayed."""
+
+    def __init__(self, model: "BandwidthMLP", metas, log_hs, device):
+        """metas: (d, order, n) per data set; log_hs: each data set's log
+        bandwidths.  The small tables go up with non-blocking copies on the
+        current stream (no host wait)."""
+        self.lib = _lib.load()
+        self.model = model
+        self.device = torch.device(device)
+        B = len(metas)
+        self.B = B
+        dev = self.device
+
+        def up(a):
+            return torch.from_numpy(np.ascontiguousarray(a)).pin_memory().to(dev, non_blocking=True)
+
+        self.bins = torch.zeros((B, 3, CELLS), dtype=torch.float64, device=dev)
+        self.meta = up(np.asarray(metas, dtype=np.int32).reshape(B, 3))
+        self.lmax = max(REFINE, max(len(v) for v in log_hs))
+        lh = np.zeros((B, self.lmax))
+        for i, v in enumerate(log_hs):
+            lh[i, :len(v)] = v
+        self.logh = up(lh)
+        self.nlist = up(np.asarray([len(v) for v in log_hs], dtype=np.int32))
+        self.loggrid = up(np.log(HGRID))
+        self.x16 = torch.empty((B, model.dims[0]), dtype=torch.bfloat16, device=dev)
+        self.out = torch.empty((B, model.dims[-1]), dtype=torch.float32, device=dev)
+        self.lo = torch.zeros(B, dtype=torch.int32, device=dev)
+        self.t = torch.zeros(B, dtype=torch.float64, device=dev)
+        nb = int(self.lib.flpr_mlp_ws(model.nl, model._dims_c, B))
+        self.ws = torch.empty(max(nb, 256), dtype=torch.uint8, device=dev)
+
+    def enqueue(self, stream) -> None:
+        """Features, network and window starts of every data set (their
+        binned sums must be in ``bins``)."""
+        m, lib = self.model, self.lib
+        _lib.check(lib.flpr_learned_features(self.B, self.bins.data_ptr(), self.meta.data_ptr(),
+                                             m.fmean.data_ptr(), m.fstd.data_ptr(), None,
+                                             self.x16.data_ptr(), stream),
+                   "flpr_learned_features")
+        _lib.check(lib.flpr_mlp_fwd(m.nl, m._dims_c, m.p16.data_ptr(), m.p32.data_ptr(), self.B,
+                                    self.x16.data_ptr(), self.out.data_ptr(), self.ws.data_ptr(),
+                                    self.ws.numel(), stream), "flpr_mlp_fwd")
+        _lib.check(lib.flpr_learned_window(self.B, self.out.data_ptr(), T_SCALE, T_CENTER,
+                                           len(HGRID), self.loggrid.data_ptr(), self.lmax,
+                                           self.nlist.data_ptr(), self.logh.data_ptr(), REFINE,
+                                           self.lo.data_ptr(), self.t.data_ptr(), stream),
+                   "flpr_learned_window")

@@ -81,7 +81,11 @@ class LprPlan:
     """A set of LPR fits captured as one CUDA graph (see the module docstring).
 
     problems: sequence of (x, y, h, options) exactly as for cv_fastlpr
-    (h explicit; 'bandwidth_search' other than 'full' is not allowed).
+    (h explicit).  Problems with bandwidth_search='learned' take the
+    learned search: binned sums, features, the network (one batch for all
+    of them) and the window choice run inside the graph, and each evaluates
+    its five-bandwidth window there; acceptance is checked after the replay
+    and the rare walks or full-sweep fallbacks run eagerly.
     streams: concurrent streams inside the graph (default: up to 8).
     graph: capture a CUDA graph (True) or issue eagerly on every run.
     autotune: pick the number of streams and the spread work-item size by
@@ -101,9 +105,9 @@ class LprPlan:
             setups = []
             for (x, y, h, options) in problems:
                 opts = dict(options or {})
-                if str(opts.get("bandwidth_search", "full")) != "full":
-                    raise ValueError("LprPlan runs the full GCV sweep ('bandwidth_search' must "
-                                     "be 'full')")
+                if str(opts.get("bandwidth_search", "full")) not in ("full", "learned"):
+                    raise ValueError(f"bandwidth_search must be 'full' or 'learned', got "
+                                     f"{opts.get('bandwidth_search')!r}")
                 opts["device"] = str(self.device)
                 if h is None:
                     raise ValueError("LprPlan needs explicit bandwidths for every problem")
@@ -116,6 +120,7 @@ class LprPlan:
                                 su.opts.get("dof_seed", 42), None)
             for su in setups:
                 self.probs.append(self._build(ctx, su))
+            self._setup_learned()
             self._pool = None
             self._finite = None
             self._write_y([p.su.y_arr for p in self.probs])
@@ -196,6 +201,36 @@ class LprPlan:
         return rec
 
     # -- construction -------------------------------------------------------
+    def _setup_learned(self) -> None:
+        """Problems with bandwidth_search='learned' that the proposal network
+        serves (one real response, d <= 2, Gaussian kernel, DoF on, an
+        increasing isotropic bandwidth list none of which the grid filter
+        removes) share one device proposal chain (learned.DeviceProposal);
+        the others run the full sweep."""
+        from . import learned as _learned
+        self.prop = None
+        metas, lhs = [], []
+        for p in self.probs:
+            su = p.su
+            p.lidx = None
+            if str(su.opts.get("bandwidth_search", "full")) != "learned":
+                continue
+            lh = _learned.isotropic_log_h(su.bandwidths)
+            ok = (lh is not None and bool(su.opts.get("calc_dof", True)) and su.dy == 1
+                  and not su.y_is_complex and su.d <= 2 and api._kernel_id(su.opts) == 0
+                  and len(p.filt[2]) == su.bandwidths.shape[0])
+            if not ok:
+                continue
+            p.lidx = len(metas)
+            metas.append((su.d, su.order, su.n))
+            lhs.append(lh)
+            p.dstats = torch.from_numpy(np.ascontiguousarray(p.stats[:2].ravel())).to(self.device)
+        if metas:
+            model = _learned.default_model(self.device)
+            self.prop = _learned.DeviceProposal(model, metas, lhs, self.device)
+            self.lo_h = torch.empty(len(metas), dtype=torch.int32, pin_memory=True)
+            self.t_h = torch.empty(len(metas), dtype=torch.float64, pin_memory=True)
+
     def _build(self, ctx, su) -> _Problem:
         p = _Problem()
         p.su = su
@@ -277,11 +312,16 @@ class LprPlan:
 
     def _issue(self):
         """Enqueue the y-dependent stages of every problem on its stream, up
-        to its outputs in the pinned buffers."""
+        to its outputs in the pinned buffers.  Problems with the learned
+        search stop after their binned sums; the proposal chain then runs
+        once for all of them on the main stream, and each evaluates the
+        window it chose (kernel factors gathered on the device) up to its
+        outputs."""
         main = torch.cuda.current_stream(self.device)
         for s in self.streams:
             s.wait_stream(main)
         outs = [None] * len(self.probs)
+        states = {}
         for i in self.order:
             p = self.probs[i]
             su = p.su
@@ -291,12 +331,42 @@ class LprPlan:
                 st = api._prepare_lpr(ctx, None, None, su.dy, su.opts, su.order, su.prec,
                                       su.variance, su.y_is_complex, (p.dx, list(p.ycols)),
                                       ev, stats=p.stats, probes=p.probes)
+                if p.lidx is not None:
+                    _lib.check(ctx.lib.flpr_bin_moments(
+                        su.d, su.n, p.dx.data_ptr(), st.ycols[0].data_ptr(), p.dstats.data_ptr(),
+                        self.prop.bins[p.lidx].data_ptr(), ctx.stream), "flpr_bin_moments")
+                    states[i] = st
+                    continue
                 r = api._evaluate_device(ctx, st, p.filt, ev)
                 if p.bufs is None:
                     p.bufs = api._output_bufs(st, r["H"])
                 pend = api._finalize_enqueue(ctx, st, r, ev, device_select=True, bufs=p.bufs,
                                              hsum_dev=p.hsum)
                 outs[i] = (st, r, pend)
+        if states:
+            from . import learned as _learned
+            for s in self.streams:
+                main.wait_stream(s)
+            self.prop.enqueue(main.cuda_stream)
+            self.lo_h.copy_(self.prop.lo, non_blocking=True)
+            self.t_h.copy_(self.prop.t, non_blocking=True)
+            for s in self.streams:
+                s.wait_stream(main)
+            for i in self.order:
+                if i not in states:
+                    continue
+                p, st = self.probs[i], states[i]
+                with torch.cuda.stream(self.streams[self.assign[i]]):
+                    ctx = api._Ctx(self.device)
+                    ev = api._PhaseEvents(None)
+                    filt_w, hsum, _ = api._window_filter(
+                        ctx, st, p.filt, self.prop.lo[p.lidx:p.lidx + 1], _learned.REFINE)
+                    r = api._evaluate_device(ctx, st, filt_w, ev)
+                    if p.bufs is None:
+                        p.bufs = api._output_bufs(st, r["H"])
+                    pend = api._finalize_enqueue(ctx, st, r, ev, device_select=True,
+                                                 bufs=p.bufs, hsum_dev=hsum)
+                    outs[i] = (st, r, pend)
         for s in self.streams:
             main.wait_stream(s)
         return outs
@@ -332,8 +402,30 @@ class LprPlan:
                 self._y_ok = bool(finite[0])
             self._check_finite(finite[0] if finite is not None else None)
             ev = api._PhaseEvents(None)
-            return [api._finalize_build(self._ctx, outs[i][0], outs[i][1], pends[i], ev, None)
-                    for i in range(len(self.probs))]
+            res = []
+            for i, p in enumerate(self.probs):
+                st, r, _ = outs[i]
+                if p.lidx is None:
+                    res.append(api._finalize_build(self._ctx, st, r, pends[i], ev, None))
+                else:
+                    res.append(self._finish_learned(p, st, r, pends[i], ev))
+            return res
+
+    def _finish_learned(self, p, st, r, pend, ev) -> RegressionOutput:
+        """Acceptance of a learned problem's window after the replay; the
+        rare walks and full-sweep fallbacks run eagerly on its prepared state
+        (valid until the next replay)."""
+        ctx = self._ctx
+        bw = p.su.bandwidths
+        found = api._learned_finish(ctx, st, bw, dict(r), pend, int(self.lo_h[p.lidx]),
+                                    float(self.t_h[p.lidx]), ev)
+        if found is None:
+            return api._full_sweep(ctx, st, bw, ev, {"mode": "learned", "accepted": False,
+                                                      "fallback": "full sweep"}, filt=p.filt)
+        r2, record, pend2 = found
+        if pend2 is not None:
+            return api._finalize_build(ctx, st, r2, pend2, ev, record)
+        return api._finalize_lpr(ctx, st, r2, ev, record)
 
 
 def cv_fastlpr_many(problems: Sequence, device=None,

@@ -411,6 +411,36 @@ int flpr_exp_weighted_sum(int64_t n, const double* d_yraw, const double* d_yhat,
 int flpr_bin_moments(int d, int64_t n, const double* d_x, const double* d_y,
                      const double* d_stats, double* d_out, void* stream);
 
+/* Feature vectors of B data sets from their binned sums, on the device (the
+ * summary learned.summarize forms on the host: per-axis 64-bin count / mean /
+ * mean-square profiles of the standardised response, 12 lag-roughness values
+ * raw and noise-corrected, the pooled within-cell variance and its log,
+ * log10 n, order and dimension one-hots).  d_bins: (B, 3, 4096) from
+ * flpr_bin_moments; d_meta: (B, 3) int {d, order, n}; d_fmean / d_fstd: the
+ * network's feature standardisation (416 each).  d_feat (optional, may be
+ * NULL): (B, 416) FP32 raw features; d_x16: (B, 416) BF16 standardised
+ * network inputs.  One CTA per data set. */
+int flpr_learned_features(int B, const double* d_bins, const int* d_meta, const float* d_fmean,
+                          const float* d_fstd, float* d_feat, void* d_x16, void* stream);
+
+/* Window start of the short local sweep for each of B data sets from the
+ * network output d_raw (B): t = clip(raw * t_scale + t_center, 0, ngrid-1)
+ * on the canonical grid d_loggrid (ngrid log bandwidths), the target log h
+ * linearly interpolated there, the nearest entry c of the data set's own
+ * list d_logh (B x lmax, d_nlist[b] valid entries, first on ties) and
+ * d_lo[b] = clip(c - refine/2, 0, nlist - refine).  d_t (optional): the
+ * unclipped t. */
+int flpr_learned_window(int B, const float* d_raw, double t_scale, double t_center, int ngrid,
+                        const double* d_loggrid, int lmax, const int* d_nlist,
+                        const double* d_logh, int refine, int* d_lo, double* d_t,
+                        void* stream);
+
+/* Copy `rows` rows of row_bytes (a multiple of 8) starting at row *d_start
+ * (read on the device) of d_src to d_dst: the window's slice of a per-
+ * bandwidth table chosen on the device, inside a captured graph. */
+int flpr_copy_rows(const void* d_src, void* d_dst, int64_t row_bytes, int rows,
+                   const int* d_start, void* stream);
+
 /* Dense ReLU network h_{l+1} = relu(h_l W_l^T + b_l) (no ReLU on the last
  * layer) with dims[0..nlayers].  Parameters are packed per layer as
  * W_l (dims[l+1] x dims[l], row-major) then b_l; d_params32 is the FP32

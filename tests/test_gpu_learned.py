@@ -164,6 +164,16 @@ def _problem(seed, n=200000):
     return x, y
 
 
+def _constant_net(t):
+    """A network whose output is the proposal t for every input: zero
+    weights, the last bias set (the biases are added in FP32)."""
+    from fastlpr_b200 import learned
+    base = learned.BandwidthMLP(device="cuda")
+    p = np.zeros(base.nparams, np.float32)
+    p[-1] = (t - learned.T_CENTER) / learned.T_SCALE
+    return learned.BandwidthMLP(device="cuda", params=p)
+
+
 def test_learned_search_window_walk_and_fallback(cuda_ok, monkeypatch):
     """A proposal on the minimum is accepted at once; a far proposal walks its
     window to the minimum; with walking disabled it falls back to the full
@@ -177,20 +187,25 @@ def test_learned_search_window_walk_and_fallback(cuda_ok, monkeypatch):
     full = fastlpr_b200.cv_fastlpr(x, y, h, opts)
     best = int(np.argmin(full.gcv_yhat["gcv_m"]))
     assert 4 < best < 27
-    net = learned.BandwidthMLP(device="cuda")
-    monkeypatch.setattr(learned, "default_model", lambda device: net)
     lopts = dict(opts, bandwidth_search="learned")
     # on the minimum: one window
-    monkeypatch.setattr(net, "predict", lambda feats: np.array([float(best)]))
+    net = _constant_net(float(best))
+    monkeypatch.setattr(learned, "default_model", lambda device: net)
     res = fastlpr_b200.cv_fastlpr(x, y, h, lopts)
     bs = res.metadata["bandwidth_search"]
     assert bs["accepted"] is True and len(bs["windows"]) == 1
+    assert bs["windows"][0] == list(range(best - 2, best + 3))
+    assert abs(bs["proposal_index"] - best) < 1e-5
     assert len(res.gcv_yhat["bandwidths"]) == 5
     assert np.allclose(res.h, full.h)
     assert res.gcv_yhat["gcv_m"].min() <= 1.01 * full.gcv_yhat["gcv_m"].min()
+    # the window's outputs equal the full sweep's at the same bandwidths
+    w = bs["windows"][0]
+    assert np.allclose(res.gcv_yhat["gcv_m"], full.gcv_yhat["gcv_m"][w], rtol=1e-9)
     # far away: the window walks toward the minimum
     far = 0.0 if best > 15 else 31.0
-    monkeypatch.setattr(net, "predict", lambda feats: np.array([far]))
+    net = _constant_net(far)
+    monkeypatch.setattr(learned, "default_model", lambda device: net)
     monkeypatch.setattr(api, "_MAX_WALKS", 10)
     res = fastlpr_b200.cv_fastlpr(x, y, h, lopts)
     bs = res.metadata["bandwidth_search"]
@@ -203,6 +218,82 @@ def test_learned_search_window_walk_and_fallback(cuda_ok, monkeypatch):
     assert np.array_equal(res.yhat, full.yhat)
     # (the adjoint deposits use FP64 atomics: equal up to summation order)
     assert np.allclose(res.gcv_yhat["gcv_m"], full.gcv_yhat["gcv_m"], rtol=1e-12, atol=0.0)
+
+
+@pytest.mark.parametrize("d", [1, 2])
+def test_device_features_match_host_summary(cuda_ok, d):
+    """flpr_learned_features equals learned.summarize on the same binned
+    sums (float32 features) and the network's standardised BF16 inputs."""
+    from fastlpr_b200 import learned
+    L, lib = _lib()
+    net = learned.default_model(torch.device("cuda"))
+    s = torch.cuda.current_stream().cuda_stream
+    bins, metas, want = [], [], []
+    for k, (n, order) in enumerate([(300000, 1), (5000, 0), (20000, 2)]):
+        rng = np.random.default_rng(50 + 3 * d + k)
+        x = rng.random((n, d)) ** (1 + k)
+        y = np.sin(5 * x[:, 0]) + (0.5 + k) * rng.standard_normal(n)
+        dx, dy = torch.tensor(x, device="cuda"), torch.tensor(y, device="cuda")
+        st = torch.tensor(np.concatenate([x.min(0), x.max(0)]), device="cuda")
+        b = torch.empty((3, 4096), dtype=torch.float64, device="cuda")
+        L.check(lib.flpr_bin_moments(d, n, dx.data_ptr(), dy.data_ptr(), st.data_ptr(),
+                                     b.data_ptr(), s))
+        bins.append(b)
+        metas.append((d, order, n))
+        want.append(learned.summarize(b.cpu().numpy(), d, n, order))
+    B = len(bins)
+    db = torch.stack(bins)
+    meta = torch.tensor(np.asarray(metas, np.int32), device="cuda")
+    feat = torch.empty((B, learned.FEATURE_DIM), dtype=torch.float32, device="cuda")
+    x16 = torch.empty((B, learned.FEATURE_DIM), dtype=torch.bfloat16, device="cuda")
+    L.check(lib.flpr_learned_features(B, db.data_ptr(), meta.data_ptr(), net.fmean.data_ptr(),
+                                      net.fstd.data_ptr(), feat.data_ptr(), x16.data_ptr(), s))
+    got = feat.cpu().numpy()
+    want = np.stack(want)
+    np.testing.assert_allclose(got, want, rtol=2e-6, atol=1e-7)
+    ref16 = net._inputs(want).float().cpu().numpy()
+    diff = np.abs(x16.float().cpu().numpy() - ref16)
+    # a feature within an ulp of a BF16 rounding boundary may round the other way
+    assert np.mean(diff == 0) > 0.995
+    assert np.max(diff) <= 2 ** -7 * np.maximum(np.abs(ref16), 1e-3).max()
+
+
+def test_device_window_matches_host(cuda_ok):
+    """flpr_learned_window equals learned.refine_window for proposals all
+    over (and beyond) the canonical grid and lists of several lengths."""
+    from fastlpr_b200 import learned
+    L, lib = _lib()
+    rng = np.random.default_rng(60)
+    B = 200
+    raw = rng.uniform(-2.5, 2.5, B).astype(np.float32)
+    raw[:5] = (np.array([0, 3, 15.5, 28, 31]) - learned.T_CENTER) / learned.T_SCALE
+    lists = [np.log(np.logspace(np.log10(rng.uniform(0.002, 0.02)),
+                                np.log10(rng.uniform(0.2, 0.9)), int(rng.integers(5, 40))))
+             for _ in range(B)]
+    prop = learned.DeviceProposal(learned.default_model(torch.device("cuda")),
+                                  [(2, 1, 1000)] * B, lists, "cuda")
+    out = torch.tensor(raw, device="cuda")
+    L.check(lib.flpr_learned_window(B, out.data_ptr(), learned.T_SCALE, learned.T_CENTER,
+                                    len(learned.HGRID), prop.loggrid.data_ptr(), prop.lmax,
+                                    prop.nlist.data_ptr(), prop.logh.data_ptr(), learned.REFINE,
+                                    prop.lo.data_ptr(), prop.t.data_ptr(),
+                                    torch.cuda.current_stream().cuda_stream))
+    lo = prop.lo.cpu().numpy()
+    t = prop.t.cpu().numpy()
+    for b in range(B):
+        tb = float(np.float64(raw[b]) * learned.T_SCALE + learned.T_CENTER)
+        assert t[b] == tb
+        assert lo[b] == learned.refine_window(tb, lists[b])[0], b
+
+
+def test_copy_rows_from_device_start(cuda_ok):
+    L, lib = _lib()
+    src = torch.arange(7 * 24, dtype=torch.float64, device="cuda").reshape(7, 24)
+    dst = torch.zeros((3, 24), dtype=torch.float64, device="cuda")
+    start = torch.tensor([4], dtype=torch.int32, device="cuda")
+    L.check(lib.flpr_copy_rows(src.data_ptr(), dst.data_ptr(), 24 * 8, 3, start.data_ptr(),
+                               torch.cuda.current_stream().cuda_stream))
+    assert torch.equal(dst, src[4:7])
 
 
 def test_trained_network_gains_over_full_sweep(cuda_ok):

@@ -173,3 +173,57 @@ def test_tune_fit_applies_a_candidate(cuda_ok, tmp_path, monkeypatch):
         assert os.path.exists(tmp_path / "c.json")
     finally:
         autotune.set_params(saved)
+
+
+def _learned_problems(seed=70):
+    """Data sets for the learned search in a plan: 1-D and 2-D, orders 0-2,
+    uneven n, the canonical bandwidth list; plus a complex response (the
+    network does not serve it: full sweep) and a plain full-sweep problem."""
+    from fastlpr_b200 import learned
+    rng = np.random.default_rng(seed)
+    out = []
+    for k, (d, n, order) in enumerate([(1, 40000, 1), (2, 120000, 1), (1, 9000, 2),
+                                       (2, 30000, 0), (1, 70000, 0), (2, 60000, 1)]):
+        x = rng.random((n, d))
+        f = np.sin(2 * np.pi * (1 + k % 3) * x[:, 0]) * (np.cos(np.pi * x[:, 1]) if d == 2 else 1)
+        y = f + (0.05 + 0.1 * k) * rng.standard_normal(n)
+        h = np.column_stack([learned.HGRID] * d)
+        out.append((x, y, h, {"order": order, "N": 512 if d == 1 else [96, 96],
+                              "bandwidth_search": "learned"}))
+    x = rng.random((20000, 1))
+    y = np.exp(2j * np.pi * x[:, 0]) + 0.1 * rng.standard_normal(20000)
+    out.append((x, y, np.column_stack([learned.HGRID]), {"order": 1, "N": 256,
+                                                         "bandwidth_search": "learned"}))
+    x = rng.random((15000, 2))
+    out.append((x, np.cos(3 * x[:, 0]) + 0.1 * rng.standard_normal(15000),
+                np.column_stack([learned.HGRID[::3]] * 2), {"order": 1, "N": [64, 64]}))
+    return out
+
+
+def test_plan_learned_search_matches_single_fits(cuda_ok):
+    """The learned search inside the graph (proposal chain for all problems
+    in one batch, windows chosen and evaluated on the device) gives each
+    problem the single-fit learned search's window, choice and outputs;
+    replays with new responses agree with fresh single fits too."""
+    import fastlpr_b200
+    probs = _learned_problems()
+    plan = fastlpr_b200.LprPlan(probs, streams=4)
+    try:
+        for run in range(2):
+            ys = [p[1] for p in probs] if run == 0 else [
+                (p[1] * 1.3 + 0.2) if not np.iscomplexobj(p[1]) else p[1] * np.exp(0.4j)
+                for p in probs]
+            got = plan.run(ys)
+            for (x, _, h, o), y, g in zip(probs, ys, got):
+                ref = fastlpr_b200.cv_fastlpr(x, y, h, o)
+                gs, rs = g.metadata["bandwidth_search"], ref.metadata["bandwidth_search"]
+                assert gs.get("mode") == rs.get("mode")
+                assert gs.get("accepted") == rs.get("accepted")
+                assert gs.get("windows") == rs.get("windows")
+                if gs.get("mode") == "learned" and "proposal_index" in rs:
+                    assert abs(gs["proposal_index"] - rs["proposal_index"]) < 1e-4
+                _same(g, ref, _tol(o))
+        learned_count = sum(1 for r in got if r.metadata["bandwidth_search"].get("accepted"))
+        assert learned_count >= 4
+    finally:
+        plan.close()
