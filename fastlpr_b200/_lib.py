@@ -67,6 +67,7 @@ SIGNATURES = [
     ("flpr_interp_reduce", _I, [_I, _I64, _VP, _PD, _PI, _I, _I, _I, _VP, _PVP, _PVP, _VP, _VP,
                                 _VP, _VP, _SZ, _VP]),
     ("flpr_interp_eval", _I, [_I, _I64, _VP, _PD, _PI, _I, _VP, _VP, _VP]),
+    ("flpr_interp_eval_extrap", _I, [_I, _I64, _VP, _PD, _PI, _I, _VP, _VP, _VP]),
     ("flpr_spline_prefilter", _I, [_I, _PI, _I64, _I, _VP, _VP, _VP]),
     ("flpr_gcv_select", _I, [_I, _I, _I, _I, _I, _I, _D, _D, _VP, _VP, _VP, _VP, _VP]),
     ("flpr_select_grid", _I, [_I64, _I, _I, _I, _VP, _VP, _I, _VP, _VP, _VP, _VP]),
@@ -91,6 +92,8 @@ SIGNATURES = [
                            C.c_float, C.c_float, _I, _VP]),
     ("flpr_mlp_mse", _I, [_I, _VP, _VP, _VP, _VP, _VP]),
     ("flpr_to_bf16", _I, [_I64, _VP, _VP, _VP]),
+    ("flpr_mlp_infer_supported", _I, [_I, _PI]),
+    ("flpr_mlp_infer", _I, [_I, _PI, _VP, _VP, _I, _VP, _VP, _VP, _VP]),
 ]
 
 

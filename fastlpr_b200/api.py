@@ -675,10 +675,8 @@ def _check_supported(dims: int, opts) -> None:
         raise NotImplementedError(
             f"fastlpr_b200 supports 1-3 predictor dimensions on the GPU; got dx={dims}")
     acc = int(opts["accuracy"])
-    if acc < 0 or acc > 12 or (dims == 3 and acc > 6):
-        raise NotImplementedError(
-            f"accuracy={acc} is not supported on the GPU (supported: 0-12 in 1-D/2-D, "
-            "0-6 in 3-D)")
+    if acc < 0 or acc > 12:
+        raise NotImplementedError(f"accuracy={acc} is not supported on the GPU (supported: 0-12)")
     _kernel_id(opts)
 
 

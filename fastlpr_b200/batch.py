@@ -145,11 +145,29 @@ def cv_fastlpr_batch(shared: SharedData, return_all_grid_values: bool = False) -
     return out
 
 
+def _batch_method(shared: SharedData, key: str) -> str:
+    """Interpolation of the batch helpers (batch.py:646-651, 718-720): the
+    option `key`, else linear in 1-D and the cubic spline otherwise."""
+    d = shared.x_raw.shape[1]
+    return str(shared.options.get(key, "linear" if d == 1 else "cubic"))
+
+
+def _rgi(shared: SharedData, values: np.ndarray, method: str) -> GridInterpolant:
+    """scipy's RegularGridInterpolator(fill_value=None) on the GPU: the
+    cubic spline with extended end pieces, or linear continuing the edge
+    cells beyond the grid."""
+    if method not in ("linear", "cubic"):
+        raise NotImplementedError(f"interpolation method {method!r}: only 'linear' and 'cubic'")
+    return GridInterpolant(shared.grid_axes_raw, values, shared._ctx.device, method=method,
+                           extrapolate=True)
+
+
 def batch_evaluate_at_points(shared: SharedData, eval_points,
                              bandwidth_indices: Optional[Sequence[int]] = None) -> np.ndarray:
     """Fitted surfaces of the chosen bandwidths at new points, (M, k) (or
-    (M, k, dy)); clamped multilinear interpolation on the GPU (reference
-    batch.py:595-669)."""
+    (M, k, dy)), interpolated on the GPU like the reference (batch.py:595-669:
+    option 'interp_method', default linear in 1-D and cubic otherwise,
+    continued beyond the grid)."""
     r, _ = _evaluate_all(shared)
     grids = _grids(shared, r)
     H = grids.shape[0]
@@ -159,7 +177,7 @@ def batch_evaluate_at_points(shared: SharedData, eval_points,
     sel = np.moveaxis(grids[idx], 0, -2)               # G... x k x dy
     if sel.shape[-1] == 1:
         sel = sel[..., 0]
-    interp = GridInterpolant(shared.grid_axes_raw, sel, shared._ctx.device)
+    interp = _rgi(shared, sel, _batch_method(shared, "interp_method"))
     return interp(np.atleast_2d(np.asarray(eval_points, dtype=float)))
 
 
@@ -169,13 +187,15 @@ def compute_gcv_scores_batch(shared: SharedData, m_all: np.ndarray, dof_all: np.
     """GCV score and standard error per bandwidth from given fitted grids and
     degrees of freedom (reference batch.py:672-760, regression.py:280-471):
     GCV = (RSS/N) / max(clip(1 - dof/N, 0, 1), 0.01)^2, stderr = (RSS/N) x
-    penalty_std, columns aggregated by the ``gcv_selection`` option."""
+    penalty_std, columns aggregated by the ``gcv_selection`` option; fitted
+    values interpolated with option 'gcv_interp_method' (default linear in
+    1-D, cubic otherwise)."""
     m = np.asarray(m_all)
     gshape = tuple(int(g) for g in shared.grid_shape)
     H = len(np.atleast_1d(dof_all))
     if m.shape[:len(gshape)] != gshape:
         raise ValueError(f"m_all must start with the grid shape {gshape}, got {m.shape}")
-    interp = GridInterpolant(shared.grid_axes_raw, m, shared._ctx.device)
+    interp = _rgi(shared, m, _batch_method(shared, "gcv_interp_method"))
     yhat = interp(shared.x_raw)                        # (N, H) or (N, H, dy)
     y = np.asarray(shared.y_raw)
     N = y.shape[0]

@@ -161,12 +161,46 @@ __global__ void probe_norm_kernel(int64_t n, int R, ColPtrs pc, double* __restri
   }
 }
 
+// Edge-cell continuation on one axis (scipy's RegularGridInterpolator with
+// fill_value=None): the cell index clamped to [0, nx - 2], the fraction not.
+__device__ __forceinline__ void axis_cell_extrap(double xi, double x0, double dx, int nx, int* ix,
+                                                 double* fr) {
+  const double t = (xi - x0) / dx;
+  int i = (int)floor(t);
+  const int top = nx - 2 < 0 ? 0 : nx - 2;
+  i = i < 0 ? 0 : (i > top ? top : i);
+  *ix = i;
+  *fr = t - (double)i;
+}
+
+template <bool kExtrap>
 __global__ void interp_eval_kernel(InterpGeom g, int64_t n, const double* __restrict__ x, int nval,
                                    const double* __restrict__ vals, double* __restrict__ out) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     Stencil st;
-    make_stencil(g, x, i, st);
+    if (kExtrap) {
+      int ix[3] = {0, 0, 0};
+      double fr[3] = {0, 0, 0};
+      for (int a = 0; a < g.d; ++a)
+        axis_cell_extrap(x[i * g.d + a], g.x0[a], g.dx[a], g.G[a], &ix[a], &fr[a]);
+      st.ncorner = 1 << g.d;
+      for (int c = 0; c < st.ncorner; ++c) {
+        int64_t idx = 0;
+        double w = 1.0;
+        for (int a = 0; a < g.d; ++a) {
+          const int bit = (c >> (g.d - 1 - a)) & 1;
+          int ia = ix[a] + bit;
+          if (ia >= g.G[a]) ia = g.G[a] - 1;  // single-point axis
+          idx = idx * g.G[a] + ia;
+          w *= bit ? fr[a] : (1.0 - fr[a]);
+        }
+        st.base[c] = idx;
+        st.w[c] = w;
+      }
+    } else {
+      make_stencil(g, x, i, st);
+    }
     for (int v = 0; v < nval; ++v) {
       const double* vv = vals + (int64_t)v * g.M;
       double r = 0.0;
@@ -504,8 +538,20 @@ int flpr_interp_eval(int d, int64_t n, const double* d_x, const double* h_ax, co
   InterpGeom g;
   FLPR_TRY(make_geom(g, d, h_ax, h_G));
   FLPR_CHECK_ARG(n >= 1 && nval >= 1, "interp_eval: n=%lld nval=%d", (long long)n, nval);
-  interp_eval_kernel<<<pt_blocks(n, 8), 256, 0, as_stream(stream)>>>(g, n, d_x, nval, d_vals,
-                                                                      d_out);
+  interp_eval_kernel<false><<<pt_blocks(n, 8), 256, 0, as_stream(stream)>>>(g, n, d_x, nval,
+                                                                             d_vals, d_out);
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
+int flpr_interp_eval_extrap(int d, int64_t n, const double* d_x, const double* h_ax,
+                            const int* h_G, int nval, const double* d_vals, double* d_out,
+                            void* stream) {
+  InterpGeom g;
+  FLPR_TRY(make_geom(g, d, h_ax, h_G));
+  FLPR_CHECK_ARG(n >= 1 && nval >= 1, "interp_eval_extrap: n=%lld nval=%d", (long long)n, nval);
+  interp_eval_kernel<true><<<pt_blocks(n, 8), 256, 0, as_stream(stream)>>>(g, n, d_x, nval,
+                                                                            d_vals, d_out);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }

@@ -20,8 +20,13 @@ from . import _lib, spline
 
 
 class GridInterpolant:
+    """extrapolate=True continues the edge cells' linear functions beyond the
+    grid instead of clamping (scipy's RegularGridInterpolator with
+    fill_value=None, used by the reference's batch helpers); the spline
+    always extends its end pieces."""
+
     def __init__(self, axes: Sequence[np.ndarray], values: np.ndarray, device: torch.device,
-                 method: str = "linear"):
+                 method: str = "linear", extrapolate: bool = False):
         self.grid_axes = tuple(np.asarray(a, dtype=float).ravel() for a in axes)
         self.ndim = len(self.grid_axes)
         self.values = np.ascontiguousarray(values)
@@ -34,6 +39,7 @@ class GridInterpolant:
         self._extra = extra
         self._dvals = None  # device copy (spline coefficients if cubic), made at first use
         self._cubic = str(method) == "cubic"
+        self._extrap = bool(extrapolate)
         self._spl = None
         ax = []
         for a in self.grid_axes:
@@ -71,9 +77,10 @@ class GridInterpolant:
                                                 nval, self._dvals.data_ptr(), out.data_ptr(),
                                                 stream), "flpr_spline_eval")
             else:
-                _lib.check(lib.flpr_interp_eval(self.ndim, n, dx.data_ptr(), _lib.dvec(self._ax),
-                                                _lib.ivec(self._G), nval, self._dvals.data_ptr(),
-                                                out.data_ptr(), stream), "flpr_interp_eval")
+                fn = lib.flpr_interp_eval_extrap if self._extrap else lib.flpr_interp_eval
+                _lib.check(fn(self.ndim, n, dx.data_ptr(), _lib.dvec(self._ax),
+                              _lib.ivec(self._G), nval, self._dvals.data_ptr(), out.data_ptr(),
+                              stream), "flpr_interp_eval")
             res = out.cpu().numpy()
         k = nval // 2 if self.is_complex else nval
         vals = res[:k] + 1j * res[k:] if self.is_complex else res

@@ -370,7 +370,11 @@ class DeviceProposal:
         self.out = torch.empty((B, model.dims[-1]), dtype=torch.float32, device=dev)
         self.lo = torch.zeros(B, dtype=torch.int32, device=dev)
         self.t = torch.zeros(B, dtype=torch.float64, device=dev)
-        nb = int(self.lib.flpr_mlp_ws(model.nl, model._dims_c, B))
+        # the fused tensor-core inference kernel when the network's shape
+        # allows it (the shipped one does), else the layer-by-layer products
+        self.fused = bool(self.lib.flpr_mlp_infer_supported(model.nl, model._dims_c))
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        nb = 0 if self.fused else int(self.lib.flpr_mlp_ws(model.nl, model._dims_c, B))
         self.ws = torch.empty(max(nb, 256), dtype=torch.uint8, device=dev)
 
     def enqueue(self, stream) -> None:
@@ -381,9 +385,15 @@ class DeviceProposal:
                                              m.fmean.data_ptr(), m.fstd.data_ptr(), None,
                                              self.x16.data_ptr(), stream),
                    "flpr_learned_features")
-        _lib.check(lib.flpr_mlp_fwd(m.nl, m._dims_c, m.p16.data_ptr(), m.p32.data_ptr(), self.B,
-                                    self.x16.data_ptr(), self.out.data_ptr(), self.ws.data_ptr(),
-                                    self.ws.numel(), stream), "flpr_mlp_fwd")
+        if self.fused:
+            _lib.check(lib.flpr_mlp_infer(m.nl, m._dims_c, m.p16.data_ptr(), m.p32.data_ptr(),
+                                          self.B, self.x16.data_ptr(), self.out.data_ptr(),
+                                          self.status.data_ptr(), stream), "flpr_mlp_infer")
+        else:
+            _lib.check(lib.flpr_mlp_fwd(m.nl, m._dims_c, m.p16.data_ptr(), m.p32.data_ptr(),
+                                        self.B, self.x16.data_ptr(), self.out.data_ptr(),
+                                        self.ws.data_ptr(), self.ws.numel(), stream),
+                       "flpr_mlp_fwd")
         _lib.check(lib.flpr_learned_window(self.B, self.out.data_ptr(), T_SCALE, T_CENTER,
                                            len(HGRID), self.loggrid.data_ptr(), self.lmax,
                                            self.nlist.data_ptr(), self.logh.data_ptr(), REFINE,

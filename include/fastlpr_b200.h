@@ -325,6 +325,13 @@ int flpr_stencil_quad(int d, const int* h_G, int H, int ny, const double* d_m, c
  * the fpp_yhat / fpp interpolant and the final yhat of api.py:760-763. */
 int flpr_interp_eval(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G,
                      int nval, const double* d_vals, double* d_out, void* stream);
+/* The same evaluation continuing the edge cells' linear functions beyond
+ * the grid (cell index clamped, fraction not): scipy's
+ * RegularGridInterpolator(method='linear', fill_value=None), which the
+ * reference's batch helpers use (batch.py:595-760). */
+int flpr_interp_eval_extrap(int d, int64_t n, const double* d_x, const double* h_ax,
+                            const int* h_G, int nval, const double* d_vals, double* d_out,
+                            void* stream);
 
 /* (8b) Not-a-knot cubic spline interpolation: the 'cubic' GCV / DoF
  * interpolation of api.py:594-600 / api.py:651-657 (regression.py:1015-1020;
@@ -479,6 +486,20 @@ int flpr_mlp_step(int64_t nparams, float* d_params32, void* d_params16, const fl
 int flpr_mlp_mse(int batch, const float* d_y, const float* d_t, float* d_dy, float* d_loss,
                  void* stream);
 int flpr_to_bf16(int64_t n, const float* d_x, void* d_y, void* stream);
+
+/* Inference of the same network in one launch on the fifth-generation
+ * tensor cores (tcgen05.mma, accumulators in tensor memory): each CTA takes
+ * 128 rows of the batch through every layer, the activations staying on
+ * chip.  Supported shapes (flpr_mlp_infer_supported): input width <= 448
+ * and a multiple of 8, every hidden width 256, one output.  d_x16:
+ * (batch, dims[0]) BF16; d_out: (batch) FP32.  d_status (optional): set to
+ * FLPR_ERR_TIMEOUT if a bounded wait of the kernel ran out (the outputs are
+ * then not written).  No reference counterpart (the learned proposal is not
+ * part of the reference). */
+int flpr_mlp_infer_supported(int nlayers, const int* h_dims);
+int flpr_mlp_infer(int nlayers, const int* h_dims, const void* d_params16,
+                   const float* d_params32, int batch, const void* d_x16, float* d_out,
+                   int* d_status, void* stream);
 
 #ifdef __cplusplus
 }

@@ -921,3 +921,87 @@ def cv_fastkde(x, h=None, options: Optional[Dict] = None, workers: int = 1,
                 lcv_sd=lcv_sd, idmax=int(np.argmax(lcv_m)), id1se=int(sel), axes_raw=ax_raw,
                 bandwidths=bw, S=s, spec=spec, grid=grid, L=L, qin=qin, qout=qout, G=G,
                 mean=mean, std=std, x_scaled=xs)
+
+
+# --------------------------------------------------------------------------
+# Shared-data batch helpers -- batch.py:139-760
+# --------------------------------------------------------------------------
+def rgi_interp(axes: Sequence[np.ndarray], values: np.ndarray, pts: np.ndarray,
+               method: str) -> np.ndarray:
+    """scipy's RegularGridInterpolator(method, fill_value=None): 'linear'
+    continues the edge cells beyond the grid (cell index clamped to
+    [0, n - 2], fraction unclamped), 'cubic' is the not-a-knot spline with
+    its end pieces extended."""
+    pts = np.atleast_2d(pts)
+    if method == "cubic":
+        return cubic_interp(axes, values, pts)
+    if method != "linear":
+        raise ValueError(f"interpolation method {method!r} is not restated")
+    dims = len(axes)
+    idx, frac = [], []
+    for d in range(dims):
+        ax = np.asarray(axes[d], dtype=float)
+        i = np.clip(np.searchsorted(ax, pts[:, d], side="right") - 1, 0, len(ax) - 2)
+        idx.append(i)
+        frac.append((pts[:, d] - ax[i]) / (ax[i + 1] - ax[i]))
+    extra = values.shape[dims:]
+    out = np.zeros((pts.shape[0],) + extra, dtype=np.result_type(values.dtype, np.float64))
+    for corner in np.ndindex(*([2] * dims)):
+        w = np.ones(pts.shape[0])
+        ii = []
+        for d, c in enumerate(corner):
+            w = w * (frac[d] if c else (1.0 - frac[d]))
+            ii.append(idx[d] + c)
+        out += w.reshape((-1,) + (1,) * len(extra)) * values[tuple(ii)]
+    return out
+
+
+def batch_method(dims: int, opts: Dict, key: str) -> str:
+    """batch.py:646-651 / 718-720: the option, else linear in 1-D, cubic otherwise."""
+    return str(opts.get(key, "linear" if dims == 1 else "cubic"))
+
+
+def batch_evaluate_at_points(x, y, h, options, eval_points, bandwidth_indices=None,
+                             workers: int = 1) -> np.ndarray:
+    """batch.py:595-669: the fitted grids of the chosen bandwidths evaluated
+    at new points with RegularGridInterpolator (fill_value=None)."""
+    o = cv_fastlpr(x, y, h, dict(options, calc_dof=False), workers=workers)
+    m = o["m"]                                   # (*G, H, C)
+    dims = len(o["G"])
+    ny = (1 if np.asarray(y).ndim == 1 else np.asarray(y).shape[1])
+    idx = list(range(m.shape[dims])) if bandwidth_indices is None else list(bandwidth_indices)
+    vals = m[..., idx, :ny]
+    vals = vals[..., 0] if ny == 1 else vals
+    return rgi_interp(o["axes_raw"], vals, eval_points,
+                      batch_method(dims, o["opts"], "interp_method"))
+
+
+def compute_gcv_scores_batch(axes_raw, x_raw, y_raw, m_all, dof_all, dof_stderr_all,
+                             penalty_std_all, opts) -> Tuple[np.ndarray, np.ndarray]:
+    """batch.py:672-760 with compute_gcv (regression.py:280-471)."""
+    dims = len(axes_raw)
+    yhat = rgi_interp(axes_raw, np.asarray(m_all), x_raw,
+                      batch_method(dims, opts, "gcv_interp_method"))
+    y = np.asarray(y_raw)
+    if y.ndim == 1:
+        y = y[:, None]
+    N = y.shape[0]
+    agg = str(opts.get("gcv_selection", "first"))
+    H = len(np.atleast_1d(dof_all))
+    scores, errs = np.empty(H), np.empty(H)
+    for k in range(H):
+        yh = yhat[:, k] if yhat.ndim == 2 else yhat[:, k, :]
+        yh = yh[:, None] if yh.ndim == 1 else yh
+        mse = np.sum(np.abs(y - yh) ** 2, axis=0) / N
+        pdof = float(np.clip(1.0 - float(np.atleast_1d(dof_all)[k]) / N, 0.0, 1.0))
+        g = mse / max(pdof, 0.01) ** 2
+        if agg == "first":
+            s, ms = g[0], mse[0]
+        elif agg == "average":
+            s, ms = np.mean(g), np.mean(mse)
+        else:
+            s, ms = np.sum(g), np.sum(mse)
+        ps = float(np.atleast_1d(penalty_std_all)[k])
+        scores[k] = s
+        errs[k] = ms * ps if ps > 0 else 0.0
+    return scores, errs

@@ -237,6 +237,9 @@ def main():
 
     _intermediates_case(fastlpr, "inter2d_o1")
     interval_case(fastlpr)
+    accuracy3d_cases(fastlpr)
+    extrapolation_cases(fastlpr)
+    batch_cases(fastlpr)
     accuracy_cases(fastlpr)
     cubic_cases(fastlpr)
     kernel_cases(fastlpr)
@@ -291,6 +294,92 @@ def accuracy_cases(fastlpr):
     _lpr_case(fastlpr, "lpr2d_o1_acc7", x2, y2, h2, {"order": 1, "N": [32, 32], "accuracy": 7})
     xk = rng.standard_normal((3000, 2))
     _kde_case(fastlpr, "kde2d_acc7", xk, h2, {"N": [32, 32], "accuracy": 7})
+
+
+def accuracy3d_cases(fastlpr):
+    """Accuracy >= 7 in 3-D (oversampling ratio 2 / 3 with Gaussian
+    deconvolution on a 3-D grid, nufftn_type1.py:693-770).  The reference's
+    response grids come out about 1e3 times too large on this path; the
+    fixtures pin that behaviour, which the oracle and the GPU reproduce."""
+    rng = np.random.default_rng(97)
+    n = 20000
+    x = rng.random((n, 3)) * np.array([1.0, 2.0, 0.5])
+    y = np.sin(3 * x[:, 0]) + x[:, 1] * x[:, 2] + 0.1 * rng.standard_normal(n)
+    hv = np.array([0.3, 0.6, 1.2])
+    h = np.column_stack([hv, hv, hv])
+    _lpr_case(fastlpr, "lpr3d_o1_acc7", x, y, h, {"order": 1, "N": [16, 14, 12], "accuracy": 7})
+    xk = rng.standard_normal((8000, 3))
+    _kde_case(fastlpr, "kde3d_acc12", xk, h, {"N": [16, 14, 12], "accuracy": 12})
+
+
+def extrapolation_cases(fastlpr):
+    """opts['xrange'] narrower than the data, so that points lie beyond the
+    grid.  With the DoF on, the reference raises here: its finite-difference
+    extrapolation of the probe fits (regression.py:1074) cannot broadcast
+    the (bandwidth, probe) axes ("operands could not be broadcast
+    together").  Without the DoF it returns the fit at the first bandwidth,
+    the fitted values from the clamped linear interpolant
+    (interp_optimized.py:60-215); these fixtures pin that."""
+    from fastlpr import get_hlist
+
+    rng = np.random.default_rng(123)
+    n = 3000
+    x1 = rng.random((n, 1))
+    y1 = np.sin(2 * np.pi * x1[:, 0]) + 0.1 * rng.standard_normal(n)
+    _lpr_case(fastlpr, "lpr1d_o1_xrange", x1, y1, get_hlist(3, [0.05, 0.3]),
+              {"order": 1, "N": 128, "xrange": [[0.1, 0.85]], "calc_dof": False})
+    n2 = 6000
+    x2 = rng.random((n2, 2))
+    y2 = np.sin(2 * np.pi * x2[:, 0]) * np.cos(2 * np.pi * x2[:, 1]) + 0.1 * rng.standard_normal(n2)
+    hv = np.array([0.1, 0.2])
+    _lpr_case(fastlpr, "lpr2d_o1_xrange", x2, y2, np.column_stack([hv, hv]),
+              {"order": 1, "N": [40, 36], "xrange": [[0.1, 0.9], [0.05, 0.8]],
+               "calc_dof": False})
+
+
+def batch_cases(fastlpr):
+    """Shared-data batch API (batch.py:139-760): the fields of
+    precompute_shared, batch_evaluate_at_points at points inside and beyond
+    the grid (RegularGridInterpolator, linear in 1-D and cubic otherwise,
+    fill_value=None) and compute_gcv_scores_batch on given fitted grids and
+    DoF.  (cv_fastlpr_batch itself stops at batch.py:417, unpacking three
+    values from a four-value return.)"""
+    from fastlpr import get_hlist
+    from fastlpr.batch import (batch_evaluate_at_points, compute_gcv_scores_batch,
+                               precompute_shared)
+
+    rng = np.random.default_rng(321)
+    for d, n, G, name in ((1, 2000, 128, "batch1d"), (2, 3000, [40, 36], "batch2d")):
+        fastlpr.clear_fastlpr_caches()
+        x = rng.random((n, d))
+        y = np.sin(2 * np.pi * x[:, 0]) * (np.cos(np.pi * x[:, -1]) if d == 2 else 1.0)
+        y = y + 0.1 * rng.standard_normal(n)
+        hv = np.logspace(np.log10(0.06), np.log10(0.5), 5)
+        h = np.column_stack([hv] * d)
+        opts = {"order": 1, "N": G}
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            sh = precompute_shared(x, y, h, dict(opts))
+            pts = np.vstack([rng.random((40, d)), rng.uniform(-0.2, 1.2, (20, d))])
+            ev = batch_evaluate_at_points(sh, pts, [0, 2, 4])
+            gshape = tuple(int(g) for g in sh.grid_shape)
+            axes = np.meshgrid(*sh.grid_axes_raw, indexing="ij")
+            m_all = np.stack([np.sin((1 + k) * axes[0]) + (axes[-1] ** 2 if d == 2 else 0.0)
+                              for k in range(len(hv))], axis=-1)
+            dof = np.linspace(5.0, 80.0, len(hv))
+            sc, se = compute_gcv_scores_batch(sh, m_all, dof, 0.1 * dof, np.full(len(hv), 0.3))
+        out = dict(kind="batch", x=x, y=y, h=h, opts=repr(opts),
+                   x_scaled=np.asarray(sh.x_scaled), mean=np.asarray(sh.mean),
+                   std=np.asarray(sh.std), bandwidths_filtered=np.asarray(sh.bandwidths_filtered),
+                   grid_shape=np.asarray(sh.grid_shape), L=np.asarray(sh.kdf_params["L"]),
+                   qin=np.asarray(sh.kdf_params["qin"]), qout=np.asarray(sh.kdf_params["qout"]),
+                   eval_points=pts, eval_values=np.asarray(ev), m_all=m_all, dof=dof,
+                   gcv_scores=np.asarray(sc), gcv_stderr=np.asarray(se))
+        for k, ax in enumerate(sh.grid_axes_raw):
+            out[f"axis{k}"] = np.asarray(ax)
+            out[f"axis_scaled{k}"] = np.asarray(sh.grid_axes_scaled[k])
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print(f"{name}: N={n} d={d} H={len(hv)} eval {np.asarray(ev).shape}")
 
 
 def cubic_cases(fastlpr):
@@ -358,5 +447,11 @@ if __name__ == "__main__":
         interval_case(_import_reference())
     elif "--only-accuracy" in sys.argv:
         accuracy_cases(_import_reference())
+    elif "--only-accuracy3d" in sys.argv:
+        accuracy3d_cases(_import_reference())
+    elif "--only-extrapolation" in sys.argv:
+        extrapolation_cases(_import_reference())
+    elif "--only-batch" in sys.argv:
+        batch_cases(_import_reference())
     else:
         main()

@@ -21,6 +21,10 @@ def test_batch_sweep_equals_cv_fastlpr(cuda_ok, d, precision):
     hv = np.logspace(np.log10(0.02), np.log10(0.5), 8)
     h = np.column_stack([hv] * d)
     opts = {"order": 1, "N": 256 if d == 1 else [96, 96], "precision": precision}
+    if d == 2:
+        # the batch helpers default to the cubic spline in 2-D (batch.py:646);
+        # linear here so that their values are the fit's own interpolation
+        opts.update(interp_method="linear", gcv_interp_method="linear")
     ref = fl.cv_fastlpr(x, y, h, opts)
     shared = fl.precompute_shared(x, y, h, opts)
     assert shared.kdf_params["dh"] == 8 and np.allclose(shared.bandwidths_filtered, h)
@@ -51,3 +55,52 @@ def test_batch_sweep_equals_cv_fastlpr(cuda_ok, d, precision):
     pen = 1.0 / np.maximum(np.clip(1 - dof / len(y), 0, 1), 0.01) ** 2
     assert np.allclose(sc, mse * pen, rtol=1e-10)
     assert np.allclose(se, mse * 0.1, rtol=1e-10)
+
+
+@pytest.mark.parametrize("name", ["batch1d", "batch2d"])
+def test_batch_api_matches_reference(cuda_ok, name):
+    """precompute_shared's fields, batch_evaluate_at_points (inside and
+    beyond the grid) and compute_gcv_scores_batch against the reference's
+    own outputs (tests/golden/batch*.npz, made by running its batch.py).  In
+    2-D the batch helpers default to scipy's cubic spline, whose iterative
+    coefficient solve (gcrotmk, atol 1e-6) the GPU replaces by the exact
+    one: inside the grid they agree to that residual, beyond it the values
+    are checked against the oracle's exact spline."""
+    import os
+
+    import oracle
+    import fastlpr_b200 as fl
+    from conftest import GOLDEN, elem_rel_err, load_golden, rel_err
+    z = load_golden(os.path.join(GOLDEN, name + ".npz"))
+    d = z["x"].shape[1]
+    opts = dict(z["opts"], precision="fp64")
+    sh = fl.precompute_shared(z["x"], z["y"], z["h"], opts)
+    np.testing.assert_allclose(sh.x_scaled, z["x_scaled"], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(sh.mean, z["mean"], rtol=1e-15)
+    np.testing.assert_allclose(sh.std, z["std"], rtol=1e-14)
+    np.testing.assert_array_equal(sh.bandwidths_filtered, z["bandwidths_filtered"])
+    np.testing.assert_array_equal(sh.grid_shape, z["grid_shape"])
+    np.testing.assert_array_equal(sh.kdf_params["L"], z["L"])
+    np.testing.assert_array_equal(sh.kdf_params["qin"], z["qin"])
+    np.testing.assert_array_equal(sh.kdf_params["qout"], z["qout"])
+    for k in range(d):
+        np.testing.assert_allclose(sh.grid_axes_raw[k], z[f"axis{k}"], rtol=1e-14)
+        np.testing.assert_allclose(sh.grid_axes_scaled[k], z[f"axis_scaled{k}"], rtol=0,
+                                   atol=1e-13)
+    pts = z["eval_points"]
+    ev = fl.batch_evaluate_at_points(sh, pts, [0, 2, 4])
+    axes = [z[f"axis{k}"] for k in range(d)]
+    inside = np.all([(pts[:, k] >= axes[k][0]) & (pts[:, k] <= axes[k][-1]) for k in range(d)],
+                    axis=0)
+    if d == 1:
+        assert rel_err(ev, z["eval_values"]) < 1e-9
+    else:
+        assert rel_err(ev[inside], z["eval_values"][inside]) < 2e-5
+        want = oracle.lpr.batch_evaluate_at_points(z["x"], z["y"], z["h"], z["opts"], pts,
+                                                   [0, 2, 4])
+        assert rel_err(ev, want) < 1e-9
+    sc, se = fl.compute_gcv_scores_batch(sh, z["m_all"], z["dof"], 0.1 * z["dof"],
+                                         np.full(len(z["dof"]), 0.3))
+    tol = 1e-12 if d == 1 else 2e-5
+    assert elem_rel_err(sc, z["gcv_scores"]) < tol
+    assert elem_rel_err(se, z["gcv_stderr"]) < tol

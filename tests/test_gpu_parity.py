@@ -574,3 +574,4 @@ def test_device_gcv_select_matches_host(cuda_ok, dual, cplx, R, agg):
     for k, key in enumerate(("gcv_m", "gcv_sd", "dof", "dof_stderr")):
         np.testing.assert_allclose(g4[k], want[key], rtol=1e-13, atol=1e-13, err_msg=key)
     assert int(sel.cpu()[0]) == wsel
+

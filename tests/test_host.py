@@ -67,9 +67,6 @@ def test_unsupported_paths_raise_not_implemented():
     x1 = rng.random((50, 1))
     with pytest.raises(NotImplementedError):
         api.cv_fastlpr(x1, rng.random(50), [[0.3]], {"accuracy": 13})
-    x3 = rng.random((50, 3))
-    with pytest.raises(NotImplementedError):
-        api.cv_fastlpr(x3, rng.random(50), [[0.3] * 3], {"accuracy": 7})
     # the reference calls kernel_function without options: polynomial fails there
     with pytest.raises(ValueError, match="Polynomial"):
         api.cv_fastlpr(x1, rng.random(50), [[0.3]], {"kernel_type": "polynomial"})

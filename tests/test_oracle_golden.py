@@ -92,3 +92,34 @@ def test_oracle_spline_is_scipys_exact_spline():
         want = make_ndbspl(tuple(axes), vals, 3, solver=ssl.spsolve)(pts)
         got = spline.cubic_interp(axes, vals, pts)
         assert np.abs(got - want).max() < 1e-11 * max(1.0, np.abs(want).max())
+
+
+@pytest.mark.parametrize("path", golden_files("batch"), ids=os.path.basename)
+def test_oracle_batch_helpers_match_reference(path):
+    """batch_evaluate_at_points (points inside and beyond the grid) and
+    compute_gcv_scores_batch of the reference's shared-data batch API.  In
+    2-D their default is scipy's cubic spline, whose coefficients scipy
+    solves iteratively (gcrotmk, atol 1e-6); the oracle solves them exactly,
+    so inside the grid the two agree to that solver's residual, and beyond
+    it the extended end pieces magnify the residual (checked against the
+    exact spline instead)."""
+    z = load_golden(path)
+    d = z["x"].shape[1]
+    axes = [z[f"axis{k}"] for k in range(d)]
+    ev = oracle.lpr.batch_evaluate_at_points(z["x"], z["y"], z["h"], z["opts"], z["eval_points"],
+                                             [0, 2, 4])
+    pts = z["eval_points"]
+    inside = np.all([(pts[:, k] >= axes[k][0]) & (pts[:, k] <= axes[k][-1]) for k in range(d)],
+                    axis=0)
+    assert inside.sum() >= 30 and (~inside).sum() >= 5
+    if d == 1:
+        assert rel_err(ev, z["eval_values"]) < 1e-12
+    else:
+        assert rel_err(ev[inside], z["eval_values"][inside]) < CUBIC_SOLVER_TOL
+    opts = dict(z["opts"])
+    sc, se = oracle.lpr.compute_gcv_scores_batch(axes, z["x"], z["y"], z["m_all"], z["dof"],
+                                                 0.1 * z["dof"], np.full(len(z["dof"]), 0.3),
+                                                 opts)
+    tol = 1e-12 if d == 1 else CUBIC_SOLVER_TOL
+    assert elem_rel_err(sc, z["gcv_scores"]) < tol
+    assert elem_rel_err(se, z["gcv_stderr"]) < tol
