@@ -307,12 +307,16 @@ def parity_batched(results, probs, workers: int) -> dict:
     against the oracle, problem by problem; worst case per precision."""
     import oracle
     out = {}
-    for r, (x, y, h, o) in zip(results, probs):
+    for k, (r, (x, y, h, o)) in enumerate(zip(results, probs)):
         prec = r.metadata["precision"]
         p = lpr_parity(r, oracle.cv_fastlpr(x, y, h, o, workers=workers), TOL[prec])
         q = out.setdefault(prec, {"problems": 0, "max_rel_err": 0.0, "tol": TOL[prec],
                                   "all_same_bandwidth": True, "ok": True})
         q["problems"] += 1
+        if p["max_rel_err"] >= q["max_rel_err"]:
+            fields = {f: v for f, v in p.items() if isinstance(v, float)}
+            q["worst"] = {"problem": k, "field": max(fields, key=fields.get),
+                          "fp64_bandwidths": int(r.metadata.get("fp64_bandwidths", 0))}
         q["max_rel_err"] = max(q["max_rel_err"], p["max_rel_err"])
         q["all_same_bandwidth"] = q["all_same_bandwidth"] and p["same_bandwidth"]
         q["ok"] = q["ok"] and p["ok"]

@@ -12,6 +12,7 @@ CUDA library through its C ABI (``_lib``):
 """
 from __future__ import annotations
 
+import copy
 import math
 import time
 import warnings
@@ -551,12 +552,14 @@ def _spread_params(L: np.ndarray, kmap: np.ndarray, accuracy: int):
 
 def _spread_fft(ctx: _Ctx, geom: _Geom, dx: torch.Tensor, cols: List[torch.Tensor], prec: int,
                 ev=None, accuracy: Optional[int] = None, ones: bool = True,
-                kmap_dev: Optional[torch.Tensor] = None):
+                kmap_dev: Optional[torch.Tensor] = None, keep: Optional[dict] = None):
     """Spread {1 (if ones), cols...} at `accuracy` and transform: returns the
     (C, L.., L_last/2+1) spectra.  Oversampled accuracies spread on the
     ratio*L grid and keep its central deconvolved L frequencies.  kmap_dev:
     the knot maps on the device (flpr_knot_map; accuracy <= 6 only), in
-    which case `geom` needs only d, n, L and accuracy."""
+    which case `geom` needs only d, n, L and accuracy.  keep (a dict, FP32
+    without oversampling): receives the spread workspace and its arguments,
+    from which _grid64 forms the exact FP64 grid later."""
     d, n = geom.d, geom.n
     acc = geom.accuracy if accuracy is None else int(accuracy)
     msp, tau, ratio, kmap = _spread_params(geom.L, None if kmap_dev is not None else geom.kmap,
@@ -582,6 +585,8 @@ def _spread_fft(ctx: _Ctx, geom: _Geom, dx: torch.Tensor, cols: List[torch.Tenso
                                       _lib.ivec(Lsp), msp, _lib.dvec(tau), C, 1 if ones else 0,
                                       chans, grid.data_ptr(), prec, ws.data_ptr(), ws.numel(),
                                       ctx.stream), "flpr_spread")
+    if keep is not None and prec == _lib.FLPR_PREC_F32 and ratio == 1:
+        keep.update(ws=ws, d=d, n=n, L=Lsp.copy(), msp=msp, C=C)
     del ws
     if ev is not None:
         ev.mark("spread")
@@ -604,6 +609,50 @@ def _spread_fft(ctx: _Ctx, geom: _Geom, dx: torch.Tensor, cols: List[torch.Tenso
     if ev is not None:
         ev.mark("fft")
     return spec
+
+
+def _grid64(ctx: _Ctx, kept: dict) -> torch.Tensor:
+    """(C, cells) FP64 grid from the exact fixed-point sums of an FP32 spread
+    (flpr_spread_grid64; `kept` from _spread_fft)."""
+    cells = int(np.prod(kept["L"]))
+    out = ctx.empty((kept["C"], cells))
+    ws = kept["ws"]
+    ctx.check(ctx.lib.flpr_spread_grid64(kept["d"], kept["n"], _lib.ivec(kept["L"]), kept["msp"],
+                                         kept["C"], ws.data_ptr(), ws.numel(), out.data_ptr(),
+                                         ctx.stream), "flpr_spread_grid64")
+    return out
+
+
+def _spectra64(ctx: _Ctx, st) -> torch.Tensor:
+    """FP64 spectra of every channel (D2Z of the FP64 grid), formed once."""
+    if getattr(st, "spec64", None) is None:
+        geom, d = st.geom, st.geom.d
+        cells = int(np.prod(geom.L))
+        half = cells // int(geom.L[-1]) * (int(geom.L[-1]) // 2 + 1)
+        C = st.grid64.shape[0]
+        spec = ctx.empty((C, half, 2))
+        ws = ctx.ws(ctx.lib.flpr_forward_fft_ws(ctx.handle, d, _lib.ivec(geom.L), C,
+                                                _lib.FLPR_PREC_F64))
+        ctx.check(ctx.lib.flpr_forward_fft(ctx.handle, d, _lib.ivec(geom.L), C,
+                                           st.grid64.data_ptr(), spec.data_ptr(),
+                                           _lib.FLPR_PREC_F64, ws.data_ptr(), ws.numel(),
+                                           ctx.stream), "flpr_forward_fft")
+        st.spec64 = spec
+    return st.spec64
+
+
+# Bandwidths whose kernel covers fewer data points than this (n times the
+# kernel's +-h box over the data box) are evaluated with FP64 planes on the
+# FP32 path: there the local moment matrices are nearly empty and FP32 planes
+# carry relative errors far above 1e-5.
+SPARSE_POINTS = 4.0
+
+
+def _sparse_bandwidths(geom, n: int, bw: np.ndarray) -> np.ndarray:
+    """Per bandwidth row: does its kernel cover fewer than SPARSE_POINTS points?"""
+    span = np.maximum(np.asarray(geom.hi, float) - np.asarray(geom.lo, float), 1e-300)
+    frac = np.minimum(1.0, 2.0 * np.asarray(bw, float) / span[None, :])
+    return n * np.prod(frac, axis=1) < SPARSE_POINTS
 
 
 # 2-D separable kernels take the two-pass convolution unless this is set
@@ -880,7 +929,8 @@ class _LprState:
 
 
 def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_complex,
-                 dev_inputs, ev, hook=None, stats=None, probes=None) -> _LprState:
+                 dev_inputs, ev, hook=None, stats=None, probes=None,
+                 bandwidths: Optional[np.ndarray] = None) -> _LprState:
     """Bandwidth-independent stage.  `hook(dx, ycols, stats, n, d, d_stats=None)`
     runs once the point statistics exist, before the spread is enqueued (the
     learned search starts its data summary there, on a side stream); on the
@@ -888,9 +938,13 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
     statistics (d_stats: minima then maxima) instead of the host ones.  With `stats` (the
     point statistics of these device inputs, already checked) nothing here
     waits for the device, so the stage can be captured in a CUDA graph
-    (`probes`: the (tensor, R) of _probes for these points, formed earlier)."""
+    (`probes`: the (tensor, R) of _probes for these points, formed earlier).
+    `bandwidths`: the list the fit will evaluate; on the FP32 path, when
+    some of them cover few points (_sparse_bandwidths), the exact FP64 grid
+    of the spread is kept for their FP64 planes."""
     lib = ctx.lib
     st = _LprState()
+    kept = {}
     if dev_inputs is not None:
         dx, ycols = dev_inputs
         n, d = dx.shape
@@ -957,7 +1011,7 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
         if hook is not None:
             hook(dx, ycols, None, n, d, d_stats=st_dev[:2 * d])
         pre = SimpleNamespace(n=n, d=d, L=L, accuracy=accuracy, kmap=None)
-        spec = _spread_fft(ctx, pre, dx, ycols + pcols, prec, ev, kmap_dev=kmap_dev)
+        spec = _spread_fft(ctx, pre, dx, ycols + pcols, prec, ev, kmap_dev=kmap_dev, keep=kept)
         st_ready.synchronize()
         stats = st_host.numpy().reshape(4, d)
     elif stats is None:
@@ -970,7 +1024,7 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
         if hook is not None:
             hook(dx, ycols, stats, n, d)
         if geom.accuracy == acc_default:
-            spec = _spread_fft(ctx, geom, dx, ycols + pcols, prec, ev)
+            spec = _spread_fft(ctx, geom, dx, ycols + pcols, prec, ev, keep=kept)
         else:
             spec_s = _spread_fft(ctx, geom, dx, pcols, prec, ev, accuracy=acc_default, ones=True)
             spec_y = _spread_fft(ctx, geom, dx, ycols, prec, ev, accuracy=geom.accuracy,
@@ -979,6 +1033,11 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
             del spec_s, spec_y
     axes_raw = _raw_axes(geom, opts)
     methods = _check_interp_methods(opts, d, n)
+    st.grid64 = None
+    st.spec64 = None
+    if kept and bandwidths is not None and bool(np.any(_sparse_bandwidths(geom, n, bandwidths))):
+        st.grid64 = _grid64(ctx, kept)
+    kept.clear()
     st.__dict__.update(dict(
         n=n, d=d, dx=dx, ycols=ycols, pcols=pcols, R=R, ny=ny, y_raw_dev=y_raw_dev,
         stats=stats, geom=geom, spec=spec, calc_dof=calc_dof, order=order, prec=prec,
@@ -1015,7 +1074,26 @@ def _evaluate_lpr(ctx, st: _LprState, bandwidths: np.ndarray, ev) -> dict:
 def _evaluate_device(ctx, st: _LprState, filt, ev) -> dict:
     """Device part of the evaluation: convolutions, solves and the GCV/DoF
     reductions, packed into one device vector (``packed``).  `filt` is the
-    result of _filter_bandwidths.  Nothing here waits for the device."""
+    result of _filter_bandwidths.  Nothing here waits for the device.
+
+    On the FP32 path, bandwidths whose kernel covers few points
+    (_sparse_bandwidths; the FP64 grid was kept for them) get FP64 planes:
+    the leading ones of an increasing list as a separate group sharing the
+    regularisation of the whole list (_evaluate_split), otherwise the whole
+    list in FP64."""
+    kern0, bw0, keep0, _ = filt
+    if (st.prec == _lib.FLPR_PREC_F32 and getattr(st, "grid64", None) is not None
+            and not getattr(kern0, "device_window", False)):
+        mask = _sparse_bandwidths(st.geom, st.n, bw0[keep0])
+        k64 = int(mask.sum())
+        if k64:
+            if (k64 < len(mask) and bool(np.all(mask[:k64])) and st.dual and kern0.separable):
+                return _evaluate_split(ctx, st, filt, k64, ev)
+            st64 = copy.copy(st)
+            st64.spec = _spectra64(ctx, st)
+            st64.prec = _lib.FLPR_PREC_F64
+            st64.grid64 = None
+            return dict(_evaluate_device(ctx, st64, filt, ev), fp64_bandwidths=len(mask))
     lib = ctx.lib
     d, n, ny, R, order, prec = st.d, st.n, st.ny, st.R, st.order, st.prec
     geom, spec, opts, calc_dof = st.geom, st.spec, st.opts, st.calc_dof
@@ -1113,6 +1191,86 @@ def _evaluate_device(ctx, st: _LprState, filt, ev) -> dict:
                                 red[st.methods["dof"]][2].reshape(-1)])
     return dict(keep=keep, bw_k=bw_k, H=H, m=m, S=S, ns=ns, mstride=mstride, packed=packed,
                 dual=st.dual)
+
+
+def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev) -> dict:
+    """_evaluate_device with the first k64 bandwidths in FP64 (planes from
+    the FP64 spectra) and the rest on the FP32 path; lambda (or max s) is
+    the larger of the two groups' (the reference's, over all bandwidths)."""
+    lib = ctx.lib
+    kern, bw, keep, _ = filt
+    d, ny, R, order = st.d, st.ny, st.R, st.order
+    geom = st.geom
+    bw_k = bw[keep]
+    H = len(keep)
+    H32 = H - k64
+    npow = 2 * order + 1
+    f64 = _filter_bandwidths(ctx, geom, bw_k[:k64], npow, st.kid)
+    f32 = _filter_bandwidths(ctx, geom, bw_k[k64:], npow, st.kid)
+    if len(f64[2]) != k64 or len(f32[2]) != H32:
+        st64 = copy.copy(st)
+        st64.spec, st64.prec, st64.grid64 = _spectra64(ctx, st), _lib.FLPR_PREC_F64, None
+        return dict(_evaluate_device(ctx, st64, filt, ev), fp64_bandwidths=H)
+    k64k, k32k = f64[0], f32[0]
+    epw = _element_powers(d, order)
+    ns = len(epw)
+    nt = 1 if order == 0 else len(_design_powers(d, order))
+    Cv = ny + R
+    M = geom.M
+    F32, F64 = _lib.FLPR_PREC_F32, _lib.FLPR_PREC_F64
+    spec64 = _spectra64(ctx, st)
+    S64 = _conv(ctx, geom, spec64, k64k, [(0, hk, epw[k]) for k in range(ns) for hk in range(k64)],
+                F64, order == 0)
+    T64 = _conv(ctx, geom, spec64, k64k,
+                [(1 + c, hk, epw[i]) for i in range(nt) for c in range(Cv) for hk in range(k64)],
+                F64, False)
+    scal64 = ctx.empty(1)
+    ctx.check(lib.flpr_scalar_of(order, nt, k64, M, S64.data_ptr(), F64, None, scal64.data_ptr(),
+                                 ctx.stream), "flpr_scalar_of")
+    reg = float(st.opts["regularization"])
+    m = ctx.empty((H, M, ny))
+    m32 = m.data_ptr() + k64 * M * ny * 8
+    dots64 = ctx.empty((Cv, k64))
+    dots32 = ctx.empty((Cv, H32))
+    scalar = ctx.empty(1)
+    Lq = (_lib.ivec(geom.G), _lib.ivec(geom.L), _lib.ivec(geom.qout[0]))
+    use_fused = (d == 2 and not st.opts.get("_no_fused", False)
+                 and lib.flpr_lpr2d_fused_supported(*Lq, H32, order, Cv) == 1)
+    if use_fused:
+        S32 = ctx.empty((ns, H32, M), dtype=torch.float32)
+        ws = ctx.ws(lib.flpr_lpr2d_fused_ws(*Lq, H32, order, Cv))
+        ctx.check(lib.flpr_lpr2d_fused_floor(*Lq, H32, npow, order, Cv, ny, st.spec.data_ptr(),
+                                             k32k.data_ptr(), k32k.scale, st.Q.data_ptr(), reg,
+                                             S32.data_ptr(), m32, dots32.data_ptr(),
+                                             scalar.data_ptr(), scal64.data_ptr(), ws.data_ptr(),
+                                             ws.numel(), ctx.stream), "flpr_lpr2d_fused_floor")
+        del ws
+    else:
+        S32 = _conv(ctx, geom, st.spec, k32k,
+                    [(0, hk, epw[k]) for k in range(ns) for hk in range(H32)], F32, order == 0)
+        T32 = _conv(ctx, geom, st.spec, k32k,
+                    [(1 + c, hk, epw[i]) for i in range(nt) for c in range(Cv) for hk in range(H32)],
+                    F32, False)
+        ctx.check(lib.flpr_scalar_of(order, nt, H32, M, S32.data_ptr(), F32, scal64.data_ptr(),
+                                     scalar.data_ptr(), ctx.stream), "flpr_scalar_of")
+        ctx.check(lib.flpr_solve_reduce_given(order, nt, H32, H32, M, Cv, S32.data_ptr(),
+                                              T32.data_ptr(), reg, ny, m32, st.Q.data_ptr(),
+                                              dots32.data_ptr(), scalar.data_ptr(), F32,
+                                              ctx.stream), "flpr_solve_reduce_given")
+    ctx.check(lib.flpr_solve_reduce_given(order, nt, k64, k64, M, Cv, S64.data_ptr(),
+                                          T64.data_ptr(), reg, ny, m.data_ptr(), st.Q.data_ptr(),
+                                          dots64.data_ptr(), scalar.data_ptr(), F64, ctx.stream),
+              "flpr_solve_reduce_given")
+    ev.mark("conv_solve")
+    dots = torch.cat([dots64, dots32], dim=1)
+    quad = ctx.empty((H, ny))
+    ctx.check(lib.flpr_stencil_quad(d, st.G_arg, H, ny, m.data_ptr(), st.Bst.data_ptr(),
+                                    quad.data_ptr(), ctx.stream), "flpr_stencil_quad")
+    ev.mark("interp_reduce")
+    packed = torch.cat([st.sq.reshape(-1), dots.reshape(-1), quad.reshape(-1)])
+    S0 = torch.cat([S64.view(ns, k64, M)[0], S32.view(ns, H32, M)[0].to(torch.float64)], dim=0)
+    return dict(keep=keep, bw_k=bw_k, H=H, m=m, S=S0.view(1, H, M), ns=1, mstride=ny,
+                packed=packed, dual=True, fp64_bandwidths=k64)
 
 
 def _evaluate_host(st: _LprState, r: dict, packed: Optional[np.ndarray]) -> dict:
@@ -1341,6 +1499,8 @@ def _finalize_build(ctx, st: _LprState, r: dict, pend: dict, ev, search,
         "dof": dof,
         "dof_stderr": dof_se,
         "precision": "fp32" if st.prec == _lib.FLPR_PREC_F32 else "fp64",
+        # FP32 path: bandwidths whose kernel covers few points, evaluated in FP64
+        "fp64_bandwidths": int(r.get("fp64_bandwidths", 0)),
         "bandwidth_search": search if search is not None else {"mode": "full"},
     }
     return RegressionOutput(yhat=yhat, grid=tuple(st.axes_raw), h=selected, gcv_yhat=gcv_result,
@@ -1416,6 +1576,7 @@ def _window_filter(ctx, st: _LprState, filt_all, lo_dev: torch.Tensor, W: int):
     ctx.check(ctx.lib.flpr_copy_rows(hs_all.data_ptr(), hsum.data_ptr(), 8, W, lo_dev.data_ptr(),
                                      ctx.stream), "flpr_copy_rows")
     kw = _Kernel(kern.kid, data, W, npow, kern.scale)
+    kw.device_window = True     # bandwidths chosen on the device: no host-side split
     return (kw, bw[keep][:W], np.arange(W), np.zeros(W, dtype=bool)), hsum, hs_all
 
 
@@ -1516,7 +1677,7 @@ def _fit_lpr(ctx, x_arr, y_arr, dy, bandwidths, opts, order, prec, variance, y_i
             _start_summary(ctx, pending, dx, ycols, stats, n, d, d_stats=d_stats, model=learned,
                            order=order, log_h=lh)
     st = _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_complex,
-                      dev_inputs, ev, hook=hook)
+                      dev_inputs, ev, hook=hook, bandwidths=bandwidths)
     found = (_learned_search(ctx, st, bandwidths, learned, ev, pending)
              if learned is not None else None)
     if found is not None:

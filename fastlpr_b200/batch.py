@@ -100,7 +100,7 @@ def precompute_shared(x, y, h=None, options: Optional[dict] = None,
     ctx = _Ctx(_device(opts))
     with torch.cuda.device(ctx.device):
         st = _prepare_lpr(ctx, x_arr, y_arr, y_arr.shape[1], opts, order, prec, variance,
-                          y_is_complex, None, _PhaseEvents(None))
+                          y_is_complex, None, _PhaseEvents(None), bandwidths=bandwidths)
         _, bw, keep, _ = _filter_bandwidths(ctx, st.geom, bandwidths, 2 * order + 1, st.kid)
     g = st.geom
     axes_scaled = [np.linspace(g.lo[a], g.hi[a], int(g.G[a])) for a in range(dims)]

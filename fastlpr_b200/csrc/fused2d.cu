@@ -22,6 +22,7 @@ namespace flpr {
 
 int global_scalar(int order, int nt, int H, int64_t M, const void* d_S, double* d_scalar, int prec,
                   cudaStream_t s);
+int scalar_floor(double* d_scalar, const double* d_floor, cudaStream_t s);
 
 namespace {
 
@@ -793,7 +794,7 @@ template <int E0, int E1>
 static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow, int order, int C,
                      int ny, const float2* spec, const double2* F, double scale, const double* Q,
                      double reg, float* S, double* my, double* dots, double* scalar,
-                     const FusedBuffers& b, cudaStream_t s) {
+                     const double* scalar_floor_in, const FusedBuffers& b, cudaStream_t s) {
   const int nt = tb.nt;
   twiddle_table_kernel<<<(twiddle_entries(fg.L0) + 255) / 256, 256, 0, s>>>(fg.L0, b.tab0);
   FLPR_LAUNCH_CHECK();
@@ -838,6 +839,7 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
     FLPR_TRY(launch_row_s<E1>(ra, hc, H, hc, b.W, F1f, b.tab1, kcut1, S, s));
   }
   FLPR_TRY(global_scalar(order, nt, H, fg.M, S, scalar, FLPR_PREC_F32, s));
+  FLPR_TRY(scalar_floor(scalar, scalar_floor_in, s));
   {
     const int64_t HM = (int64_t)H * fg.M;
     int nb = (int)((HM + 255) / 256);
@@ -882,11 +884,12 @@ template <int E0>
 static int dispatch_e1(int E1, const FusedTables& tb, const FusedGeom& fg, int H, int npow,
                        int order, int C, int ny, const float2* spec, const double2* F,
                        double scale, const double* Q, double reg, float* S, double* my,
-                       double* dots, double* scalar, const FusedBuffers& b, cudaStream_t s) {
+                       double* dots, double* scalar, const double* floor_in, const FusedBuffers& b,
+                       cudaStream_t s) {
 #define FLPR_E1(V)                                                                          \
   case V:                                                                                   \
     return run_fused<E0, V>(tb, fg, H, npow, order, C, ny, spec, F, scale, Q, reg, S, my,   \
-                            dots, scalar, b, s);
+                            dots, scalar, floor_in, b, s);
   switch (E1) {
     FLPR_E1(2)
     FLPR_E1(4)
@@ -948,10 +951,11 @@ size_t flpr_lpr2d_fused_ws(const int* h_G, const int* h_L, const int* h_qout, in
   return ar.used;
 }
 
-int flpr_lpr2d_fused(const int* h_G, const int* h_L, const int* h_qout, int H, int npow, int order,
-                     int C, int ny, const void* d_spec, const void* d_F, double scale,
-                     const double* d_Q, double reg, float* d_S, double* d_my, double* d_dots,
-                     double* d_scalar, void* d_ws, size_t ws_bytes, void* stream) {
+int flpr_lpr2d_fused_floor(const int* h_G, const int* h_L, const int* h_qout, int H, int npow,
+                           int order, int C, int ny, const void* d_spec, const void* d_F,
+                           double scale, const double* d_Q, double reg, float* d_S, double* d_my,
+                           double* d_dots, double* d_scalar, const double* d_scalar_floor,
+                           void* d_ws, size_t ws_bytes, void* stream) {
   FusedTables tb;
   FusedGeom fg;
   FLPR_TRY(fused2d_check(h_G, h_L, h_qout, H, order, C, &tb, &fg));
@@ -973,7 +977,7 @@ int flpr_lpr2d_fused(const int* h_G, const int* h_L, const int* h_qout, int H, i
 #define FLPR_E0(V)                                                                             \
   case V:                                                                                      \
     return dispatch_e1<V>(fg.L1 / 32, tb, fg, H, npow, order, C, ny, spec, F, scale, d_Q, reg, \
-                          d_S, d_my, d_dots, d_scalar, b, s);
+                          d_S, d_my, d_dots, d_scalar, d_scalar_floor, b, s);
     FLPR_E0(2)
     FLPR_E0(4)
     FLPR_E0(8)
@@ -984,6 +988,14 @@ int flpr_lpr2d_fused(const int* h_G, const int* h_L, const int* h_qout, int H, i
       set_error("fused2d: unsupported L0");
       return FLPR_ERR_ARG;
   }
+}
+
+int flpr_lpr2d_fused(const int* h_G, const int* h_L, const int* h_qout, int H, int npow, int order,
+                     int C, int ny, const void* d_spec, const void* d_F, double scale,
+                     const double* d_Q, double reg, float* d_S, double* d_my, double* d_dots,
+                     double* d_scalar, void* d_ws, size_t ws_bytes, void* stream) {
+  return flpr_lpr2d_fused_floor(h_G, h_L, h_qout, H, npow, order, C, ny, d_spec, d_F, scale, d_Q,
+                                reg, d_S, d_my, d_dots, d_scalar, nullptr, d_ws, ws_bytes, stream);
 }
 
 }  // extern "C"

@@ -203,6 +203,20 @@ static int blocks_for(int64_t total, int per_sm) {
   return (int)b;
 }
 
+__global__ void scalar_max_kernel(double* __restrict__ scalar, const double* __restrict__ floor_) {
+  const double a = scalar[0], b = floor_[0];
+  scalar[0] = a > b ? a : b;
+}
+
+// *d_scalar = max(*d_scalar, *d_floor): the regularisation scalar over the
+// union of two bandwidth groups (lambda grows with max |diag S|)
+int scalar_floor(double* d_scalar, const double* d_floor, cudaStream_t s) {
+  if (d_floor == nullptr) return FLPR_OK;
+  scalar_max_kernel<<<1, 1, 0, s>>>(d_scalar, d_floor);
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
 int global_scalar(int order, int nt, int H, int64_t M, const void* d_S, double* d_scalar,
                   int prec, cudaStream_t s) {
   unsigned long long* bits = reinterpret_cast<unsigned long long*>(d_scalar);
@@ -232,9 +246,10 @@ using namespace flpr;
 
 extern "C" {
 
-int flpr_solve_reduce(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,
-                      const void* d_T, double reg, int nkeep, double* d_mkeep, const double* d_Q,
-                      double* d_dots, double* d_scalar, int prec, void* stream) {
+static int solve_reduce_impl(int order, int nt, int H, int HT, int64_t M, int C,
+                             const void* d_S, const void* d_T, double reg, int nkeep,
+                             double* d_mkeep, const double* d_Q, double* d_dots,
+                             double* d_scalar, bool scalar_given, int prec, void* stream) {
   FLPR_CHECK_ARG(order >= 0 && order <= 2, "solve_reduce: order=%d", order);
   FLPR_CHECK_ARG(nt >= 1 && nt <= kMaxNt, "solve_reduce: nt=%d", nt);
   FLPR_CHECK_ARG(order > 0 || nt == 1, "solve_reduce: order 0 needs nt=1");
@@ -242,7 +257,7 @@ int flpr_solve_reduce(int order, int nt, int H, int HT, int64_t M, int C, const 
   FLPR_CHECK_ARG(HT >= 1 && HT <= H, "solve_reduce: HT=%d", HT);
   FLPR_CHECK_ARG(nkeep >= 0 && nkeep <= C, "solve_reduce: nkeep=%d", nkeep);
   cudaStream_t s = as_stream(stream);
-  FLPR_TRY(global_scalar(order, nt, H, M, d_S, d_scalar, prec, s));
+  if (!scalar_given) FLPR_TRY(global_scalar(order, nt, H, M, d_S, d_scalar, prec, s));
   FLPR_CUDA(cudaMemsetAsync(d_dots, 0, sizeof(double) * (size_t)C * HT, s));
   int per_h = (blocks_for(M * HT, 4) + HT - 1) / HT;
   if (per_h < 2) per_h = 2;
@@ -262,6 +277,31 @@ int flpr_solve_reduce(int order, int nt, int H, int HT, int64_t M, int C, const 
       set_error("solve_reduce: nt=%d not supported", nt);
       return FLPR_ERR_ARG;
   }
+}
+
+int flpr_solve_reduce(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,
+                      const void* d_T, double reg, int nkeep, double* d_mkeep, const double* d_Q,
+                      double* d_dots, double* d_scalar, int prec, void* stream) {
+  return solve_reduce_impl(order, nt, H, HT, M, C, d_S, d_T, reg, nkeep, d_mkeep, d_Q, d_dots,
+                           d_scalar, false, prec, stream);
+}
+
+int flpr_solve_reduce_given(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,
+                            const void* d_T, double reg, int nkeep, double* d_mkeep,
+                            const double* d_Q, double* d_dots, const double* d_scalar, int prec,
+                            void* stream) {
+  FLPR_CHECK_ARG(d_scalar != nullptr, "solve_reduce_given: null scalar");
+  return solve_reduce_impl(order, nt, H, HT, M, C, d_S, d_T, reg, nkeep, d_mkeep, d_Q, d_dots,
+                           const_cast<double*>(d_scalar), true, prec, stream);
+}
+
+int flpr_scalar_of(int order, int nt, int H, int64_t M, const void* d_S, int prec,
+                   const double* d_floor, double* d_scalar, void* stream) {
+  FLPR_CHECK_ARG(order >= 0 && order <= 2 && nt >= 1 && nt <= kMaxNt, "scalar_of: order/nt");
+  FLPR_CHECK_ARG(H >= 1 && M >= 1 && d_S && d_scalar, "scalar_of: H=%d", H);
+  cudaStream_t s = as_stream(stream);
+  FLPR_TRY(global_scalar(order, nt, H, M, d_S, d_scalar, prec, s));
+  return scalar_floor(d_scalar, d_floor, s);
 }
 
 int flpr_solve(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,

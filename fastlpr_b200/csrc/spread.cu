@@ -1187,6 +1187,31 @@ int flpr_spread_dkmap(int d, int64_t n, const double* d_x, const double* d_kmap,
                      d_grid_out, prec, d_ws, ws_bytes, stream);
 }
 
+int flpr_spread_grid64(int d, int64_t n, const int* h_L, int msp, int nchan, const void* d_ws,
+                       size_t ws_bytes, double* d_grid64, void* stream) {
+  FLPR_CHECK_ARG(d >= 1 && d <= 3, "spread_grid64: d=%d not in [1,3]", d);
+  FLPR_CHECK_ARG(n >= 1 && nchan >= 1 && nchan <= FLPR_MAX_CHANNELS, "spread_grid64: n/nchan");
+  FLPR_CHECK_ARG(d_ws != nullptr && d_grid64 != nullptr, "spread_grid64: null pointer");
+  for (int a = 0; a < d; ++a) FLPR_CHECK_ARG(h_L[a] >= 1, "spread_grid64: L[%d]=%d", a, h_L[a]);
+  if (ws_bytes < flpr_spread_ws(d, n, h_L, msp, nchan, FLPR_PREC_F32)) {
+    set_error("spread_grid64: workspace too small");
+    return FLPR_ERR_WORKSPACE;
+  }
+  SpreadGeom g;
+  double tau[3] = {1, 1, 1}, kmap[27] = {0};
+  make_geom(g, d, h_L, msp, tau, kmap);
+  Arena ar(const_cast<void*>(d_ws), ws_bytes);
+  SpreadWs w;
+  spread_layout(ar, d, n, g.ntiles, nchan, g.cells, 8, &w);
+  int64_t fb64 = (g.cells + 255) / 256;
+  if (fb64 > 16 * sm_count()) fb64 = 16 * sm_count();
+  finalize_kernel<long long, double, true><<<(int)fb64, 256, 0, as_stream(stream)>>>(
+      nchan, g.cells, (const long long*)w.gacc, w.absum, margin_bits_for(g), 1.0 / (double)n,
+      d_grid64);
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
 int flpr_knot_map(int d, int64_t n, const double* d_stats, const double* h_ks,
                   const double* h_r0, const double* h_hx, double* d_kmap, void* stream) {
   FLPR_CHECK_ARG(d >= 1 && d <= 3, "knot_map: d=%d not in [1,3]", d);

@@ -330,7 +330,8 @@ class LprPlan:
                 ev = api._PhaseEvents(None)
                 st = api._prepare_lpr(ctx, None, None, su.dy, su.opts, su.order, su.prec,
                                       su.variance, su.y_is_complex, (p.dx, list(p.ycols)),
-                                      ev, stats=p.stats, probes=p.probes)
+                                      ev, stats=p.stats, probes=p.probes,
+                                      bandwidths=su.bandwidths)
                 if p.lidx is not None:
                     _lib.check(ctx.lib.flpr_bin_moments(
                         su.d, su.n, p.dx.data_ptr(), st.ycols[0].data_ptr(), p.dstats.data_ptr(),

@@ -129,6 +129,14 @@ int flpr_spread_dkmap(int d, int64_t n, const double* d_x, const double* d_kmap,
                       const double* h_hx, const int* h_L, int msp, const double* h_tau,
                       int nchan, int ones_channel, const double* const* h_cols,
                       void* d_grid_out, int prec, void* d_ws, size_t ws_bytes, void* stream);
+/* The FP64 grid of the last FLPR_PREC_F32 spread that used this
+ * workspace with the same d, n, L, msp and nchan: the exact fixed-point sums
+ * (before their rounding to FP32) times 1/n, as (nchan, L...) float64.  The
+ * FP32 path evaluates bandwidths whose kernel covers few points with FP64
+ * planes; this gives them their grids without a second spread.  No
+ * reference counterpart (the reference spreads once, in one precision). */
+int flpr_spread_grid64(int d, int64_t n, const int* h_L, int msp, int nchan, const void* d_ws,
+                       size_t ws_bytes, double* d_grid64, void* stream);
 /* Knot maps d_kmap (d x 9) from the point statistics d_stats (4 x d:
  * minimum, maximum, mean, M2 as flpr_point_stats writes them) and the
  * host-known per-axis constants of the grid (ks, r0: the knot range of
@@ -255,6 +263,19 @@ int flpr_solve(int order, int nt, int H, int HT, int64_t M, int C, const void* d
 int flpr_solve_reduce(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,
                       const void* d_T, double reg, int nkeep, double* d_mkeep, const double* d_Q,
                       double* d_dots, double* d_scalar, int prec, void* stream);
+/* (6b') The same with lambda (or max s) given in d_scalar instead of formed
+ * from these planes: when the bandwidths of one sweep are split between an
+ * FP64 group (kernels covering few points) and the FP32 group, the
+ * reference's lambda over all bandwidths (regression.py:243-267) is the
+ * larger of the two groups' (flpr_scalar_of). */
+int flpr_solve_reduce_given(int order, int nt, int H, int HT, int64_t M, int C, const void* d_S,
+                            const void* d_T, double reg, int nkeep, double* d_mkeep,
+                            const double* d_Q, double* d_dots, const double* d_scalar, int prec,
+                            void* stream);
+/* lambda (order >= 1) or max s (order 0) of the planes d_S (ns, H, M), as
+ * flpr_solve forms it, raised to *d_floor when d_floor is not NULL. */
+int flpr_scalar_of(int order, int nt, int H, int64_t M, const void* d_S, int prec,
+                   const double* d_floor, double* d_scalar, void* stream);
 
 /* (6c) Fused 2-D FP32 convolution + solve + dual-form reductions: the
  * whole inverse-transform / solve stage of a 2-D GCV sweep in one call,
@@ -280,6 +301,14 @@ int flpr_lpr2d_fused(const int* h_G, const int* h_L, const int* h_qout, int H, i
                      int C, int ny, const void* d_spec, const void* d_F, double scale,
                      const double* d_Q, double reg, float* d_S, double* d_my, double* d_dots,
                      double* d_scalar, void* d_ws, size_t ws_bytes, void* stream);
+/* The same with lambda raised to *d_scalar_floor (the other group's, see
+ * flpr_solve_reduce_given) before the solves; d_scalar receives the
+ * union's value. */
+int flpr_lpr2d_fused_floor(const int* h_G, const int* h_L, const int* h_qout, int H, int npow,
+                           int order, int C, int ny, const void* d_spec, const void* d_F,
+                           double scale, const double* d_Q, double reg, float* d_S, double* d_my,
+                           double* d_dots, double* d_scalar, const double* d_scalar_floor,
+                           void* d_ws, size_t ws_bytes, void* stream);
 
 /* ---------------------------------------------------------------------
  * (7) Interpolation + GCV / Hutchinson reductions over the points.

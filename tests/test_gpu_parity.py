@@ -575,3 +575,27 @@ def test_device_gcv_select_matches_host(cuda_ok, dual, cplx, R, agg):
         np.testing.assert_allclose(g4[k], want[key], rtol=1e-13, atol=1e-13, err_msg=key)
     assert int(sel.cpu()[0]) == wsel
 
+
+
+@pytest.mark.parametrize("d,order,n", [(2, 1, 20000), (2, 0, 20000), (1, 1, 500)])
+def test_sparse_bandwidths_take_fp64_planes(cuda_ok, d, order, n):
+    """Few points per kernel (bandwidths below the grid spacing on sparse
+    data): the FP32 path evaluates those bandwidths with FP64 planes from
+    the exact fixed-point spread (same lambda over the whole list) and stays
+    within 1e-5 of the oracle; the rest of the list stays FP32."""
+    rng = np.random.default_rng(60 + 3 * d + order)
+    x = rng.random((n, d))
+    y = np.sin(2 * np.pi * x[:, 0]) * (np.cos(2 * np.pi * x[:, -1]) if d == 2 else 1.0)
+    y = y + 0.1 * rng.standard_normal(n)
+    hv = np.logspace(np.log10(0.005), np.log10(0.5), 12)
+    h = np.column_stack([hv] * d)
+    opts = {"order": order, "N": [256, 256] if d == 2 else 1024}
+    o = oracle.cv_fastlpr(x, y, h, opts)
+    r = _fastlpr().cv_fastlpr(x, y, h, opts)
+    assert r.metadata["precision"] == "fp32"
+    assert 0 < r.metadata["fp64_bandwidths"] < len(h)
+    _compare_to_oracle(r, o, TOL["fp32"])
+    assert rel_err(r.s0, o["s0"]) < TOL["fp32"]
+    # the explicit FP64 path agrees with both
+    r64 = _fastlpr().cv_fastlpr(x, y, h, dict(opts, precision="fp64"))
+    _compare_to_oracle(r64, o, TOL["fp64"])
