@@ -314,7 +314,8 @@ def parity_batched(results, probs, workers: int) -> dict:
                                   "all_same_bandwidth": True, "ok": True})
         q["problems"] += 1
         if p["max_rel_err"] >= q["max_rel_err"]:
-            fields = {f: v for f, v in p.items() if isinstance(v, float)}
+            fields = {f: v for f, v in p.items()
+                      if isinstance(v, float) and f not in ("tol", "max_rel_err")}
             q["worst"] = {"problem": k, "field": max(fields, key=fields.get),
                           "fp64_bandwidths": int(r.metadata.get("fp64_bandwidths", 0))}
         q["max_rel_err"] = max(q["max_rel_err"], p["max_rel_err"])
