@@ -585,8 +585,8 @@ def _spread_fft(ctx: _Ctx, geom: _Geom, dx: torch.Tensor, cols: List[torch.Tenso
                                       _lib.ivec(Lsp), msp, _lib.dvec(tau), C, 1 if ones else 0,
                                       chans, grid.data_ptr(), prec, ws.data_ptr(), ws.numel(),
                                       ctx.stream), "flpr_spread")
-    if keep is not None and prec == _lib.FLPR_PREC_F32 and ratio == 1:
-        keep.update(ws=ws, d=d, n=n, L=Lsp.copy(), msp=msp, C=C)
+    if keep is not None and ratio == 1:
+        keep.update(ws=ws, d=d, n=n, L=Lsp.copy(), msp=msp, C=C, prec=prec)
     del ws
     if ev is not None:
         ev.mark("spread")
@@ -609,6 +609,18 @@ def _spread_fft(ctx: _Ctx, geom: _Geom, dx: torch.Tensor, cols: List[torch.Tenso
     if ev is not None:
         ev.mark("fft")
     return spec
+
+
+def _node0_cells(geom) -> List[int]:
+    """Spreading cell of raw-grid node 0 per axis (where x = min lands: the
+    knot map at xs = lo), the window hint of flpr_deposit_sorted."""
+    out = []
+    for a in range(geom.d):
+        _, _, _, _, _, _, r0, shift, hx = geom.kmap[a]
+        xn = np.mod(r0 + 0.5, 1.0) - 0.5
+        k = np.mod((xn + shift) * (2 * np.pi), 2 * np.pi)
+        out.append(int(np.rint(k / hx)) % int(geom.L[a]))
+    return out
 
 
 def _grid64(ctx: _Ctx, kept: dict) -> torch.Tensor:
@@ -1035,9 +1047,9 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
     methods = _check_interp_methods(opts, d, n)
     st.grid64 = None
     st.spec64 = None
-    if kept and bandwidths is not None and bool(np.any(_sparse_bandwidths(geom, n, bandwidths))):
+    if (kept and kept["prec"] == _lib.FLPR_PREC_F32 and bandwidths is not None
+            and bool(np.any(_sparse_bandwidths(geom, n, bandwidths)))):
         st.grid64 = _grid64(ctx, kept)
-    kept.clear()
     st.__dict__.update(dict(
         n=n, d=d, dx=dx, ycols=ycols, pcols=pcols, R=R, ny=ny, y_raw_dev=y_raw_dev,
         stats=stats, geom=geom, spec=spec, calc_dof=calc_dof, order=order, prec=prec,
@@ -1056,11 +1068,25 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
         st.Q = ctx.empty((M, Cv))
         st.Bst = ctx.empty((M, npair))
         st.sq = ctx.empty(Cv)
-        ctx.check(lib.flpr_deposit(d, n, dx.data_ptr(), st.ax_arg, st.G_arg, Cv,
-                                   _lib.pvec([c.data_ptr() for c in ycols + pcols]),
-                                   st.Q.data_ptr(), st.Bst.data_ptr(), st.sq.data_ptr(),
-                                   ctx.stream), "flpr_deposit")
+        if kept and d <= 2 and kept["C"] == 1 + Cv:
+            # from the spread's tile-sorted records: exact and order-free
+            ws2 = ctx.ws(lib.flpr_deposit_sorted_ws(d, n, _lib.ivec(kept["L"]), kept["msp"],
+                                                    kept["C"]))
+            ctx.check(lib.flpr_deposit_sorted(d, n, dx.data_ptr(), _lib.ivec(kept["L"]),
+                                              kept["msp"], kept["C"], 1, kept["ws"].data_ptr(),
+                                              kept["ws"].numel(), st.ax_arg, st.G_arg,
+                                              _lib.ivec(_node0_cells(geom)), st.Q.data_ptr(),
+                                              st.Bst.data_ptr(), st.sq.data_ptr(),
+                                              ws2.data_ptr(), ws2.numel(), ctx.stream),
+                      "flpr_deposit_sorted")
+            del ws2
+        else:
+            ctx.check(lib.flpr_deposit(d, n, dx.data_ptr(), st.ax_arg, st.G_arg, Cv,
+                                       _lib.pvec([c.data_ptr() for c in ycols + pcols]),
+                                       st.Q.data_ptr(), st.Bst.data_ptr(), st.sq.data_ptr(),
+                                       ctx.stream), "flpr_deposit")
         ev.mark("deposit")
+    kept.clear()
     return st
 
 

@@ -247,7 +247,8 @@ __global__ void bin_scatter_kernel(SpreadGeom g, int64_t n, const double* __rest
                                    const double* __restrict__ d_kmap,
                                    const int* __restrict__ offsets, int* __restrict__ cursor,
                                    int nv, ChanPtrs cp, int* __restrict__ rec_base,
-                                   Real* __restrict__ rec_frac, Real* __restrict__ rec_val) {
+                                   int* __restrict__ rec_idx, Real* __restrict__ rec_frac,
+                                   Real* __restrict__ rec_val) {
   __shared__ KnotAxis s_ax[3];
   load_axes(g, d_kmap, s_ax);
   __syncthreads();
@@ -265,6 +266,7 @@ __global__ void bin_scatter_kernel(SpreadGeom g, int64_t n, const double* __rest
       rec_frac[(int64_t)a * n + pos] = (Real)dsub(k[a], dmul(g.ax[a].hx, (double)m[a]));
     }
     rec_base[pos] = packed;
+    rec_idx[pos] = (int)i;
     for (int c = 0; c < nv; ++c) rec_val[(int64_t)c * n + pos] = (Real)cp.col[c][i];
   }
 }
@@ -896,6 +898,7 @@ struct SpreadWs {
   int* items;
   int* cursor;
   int* rec_base;
+  int* rec_idx;
   void* rec_frac;
   void* rec_val;
   double* absum;
@@ -915,6 +918,7 @@ static void spread_layout(A& ar, int d, int64_t n, int ntiles, int nchan, int64_
   auto p7 = ar.template take<char>((size_t)(nchan > 1 ? nchan - 1 : 1) * n * real_bytes);
   auto p8 = ar.template take<double>(FLPR_MAX_CHANNELS);
   auto p9 = ar.template take<double>((size_t)nchan * cells);
+  auto p10 = ar.template take<int>(n);
   if (w) {
     w->point_tile = (int*)p0;
     w->counts = (int*)p1;
@@ -926,6 +930,7 @@ static void spread_layout(A& ar, int d, int64_t n, int ntiles, int nchan, int64_
     w->rec_val = (void*)p7;
     w->absum = (double*)p8;
     w->gacc = (void*)p9;
+    w->rec_idx = (int*)p10;
   }
 }
 
@@ -1088,8 +1093,10 @@ static int spread_impl(int d, int64_t n, const double* d_x, const double* h_kmap
 
   int nb = (int)((n + 255) / 256);
   if (nb > 8 * sm_count()) nb = 8 * sm_count();
+  // per-channel sums of |v|: the fixed-point scales of the FP32 grid and of
+  // the sorted adjoint deposits (flpr_deposit_sorted) in either precision
   bin_count_kernel<<<nb, 256, 0, s>>>(g, n, d_x, d_kmap, w.point_tile, w.counts, nchan, ones_channel, cp,
-                                      fixed ? w.absum : nullptr);
+                                      w.absum);
   FLPR_LAUNCH_CHECK();
   tile_scan_kernel<<<1, 1024, 0, s>>>(g.ntiles, g.item_points, w.counts, w.offsets, w.items,
                                       w.cursor);
@@ -1102,7 +1109,7 @@ static int spread_impl(int d, int64_t n, const double* d_x, const double* h_kmap
   int nbs = (int)((n + 255) / 256);
   if (nbs > 32 * sm_count()) nbs = 32 * sm_count();
   bin_scatter_kernel<double><<<nbs, 256, 0, s>>>(g, n, d_x, d_kmap, w.offsets, w.cursor, nv, cp,
-                                                w.rec_base, (double*)w.rec_frac,
+                                                w.rec_base, w.rec_idx, (double*)w.rec_frac,
                                                 (double*)w.rec_val);
   FLPR_LAUNCH_CHECK();
 
@@ -1251,3 +1258,328 @@ static int finalize(const SpreadGeom& g, int64_t n, int nchan, bool fixed, int m
 }
 
 }  // namespace flpr
+
+// ---- adjoint deposits from the tile-sorted records --------------------------
+// The dual form of the GCV / Hutchinson sums (see flpr_deposit) needs, per
+// cell g of the raw grid, Q[g][c] = sum_i w_ig v_ic and the corner-pair
+// weights B of the multilinear stencils.  Here one CTA takes the same work
+// item as the spread (the points of one spreading tile, in tile order, with
+// their point indices and channel values already in the records) and
+// accumulates its deposits in a shared-memory window of the raw grid around
+// the tile; the window goes to the global sums with one atomic per non-zero
+// cell.  Every contribution is rounded to a 64-bit fixed-point integer
+// (quantum 2^-62 of the channel's absolute sum; of n for the pair weights),
+// so the sums are exact and do not depend on the order of the points: the
+// deposits, and with them the FP32 fit, are bitwise reproducible.  The
+// output arrays Q and B hold the integers until the finishing pass turns
+// them into doubles in place.
+namespace flpr {
+
+constexpr int kDepThreads = 256;
+constexpr int kDepHalo = 2;       // raw-grid cells of margin around a spreading tile
+constexpr int kDepMaxChan = 32;
+
+struct DepositGeom {
+  int G[2];
+  double x0[2], dx[2];
+  int m0[2];     // spreading cell of raw-grid node 0, per axis (a window hint only)
+  int win[2];    // window extent (raw-grid cells) per axis
+  int C;         // value channels
+  int ones;      // 1: spread channel 0 was the constant (not deposited)
+};
+
+__host__ __device__ constexpr int dep_pairs(int D) { return (1 << D) * ((1 << D) + 1) / 2; }
+
+__device__ __forceinline__ double dep_scale(double absum, int extra_bits) {
+  if (!(absum > 0.0)) return 1.0;
+  int e = 0;
+  frexp(absum, &e);  // absum < 2^e
+  return ldexp(1.0, 62 - extra_bits - e);
+}
+
+template <int D>
+__global__ void __launch_bounds__(kDepThreads)
+tile_deposit_kernel(SpreadGeom g, DepositGeom dg, int64_t n, const double* __restrict__ x,
+                    const int* __restrict__ offsets, const int* __restrict__ items,
+                    const int* __restrict__ rec_idx, const double* __restrict__ rec_val,
+                    const double* __restrict__ absum, unsigned long long* __restrict__ qacc,
+                    unsigned long long* __restrict__ bacc, double* __restrict__ part) {
+  constexpr int NC = 1 << D;
+  constexpr int NP = dep_pairs(D);
+  extern __shared__ __align__(16) unsigned long long sacc[];  // window cells x (C + NP)
+  __shared__ double s_scale[kDepMaxChan + 1];
+  __shared__ double red[kDepThreads / 32];
+  const int C = dg.C, stride = C + NP;
+  const int W0 = dg.win[0], W1 = D == 2 ? dg.win[1] : 1;
+  const int item = blockIdx.x;
+  if (item >= items[g.ntiles]) return;
+  int lo = 0, hi = g.ntiles;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (items[mid] <= item) lo = mid; else hi = mid;
+  }
+  const int tile = lo;
+  const int p_begin = offsets[tile] + (item - items[tile]) * g.item_points;
+  const int p_end = min(offsets[tile + 1], p_begin + g.item_points);
+  // raw-grid window of the tile: node j sits at spreading cell (m0 + j) mod L
+  // (the knots are centred on the periodic grid); points whose stencil
+  // leaves the window go straight to the global sums
+  int org[2] = {0, 0};
+  {
+    int tc[2] = {tile, 0};
+    if (D == 2) {
+      tc[0] = tile / g.ntile[1];
+      tc[1] = tile - tc[0] * g.ntile[1];
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      int j = (tc[a] * g.T[a] - dg.m0[a]) % g.L[a];
+      if (j < 0) j += g.L[a];
+      org[a] = j - kDepHalo;
+    }
+  }
+  for (int i = threadIdx.x; i < W0 * W1 * stride; i += kDepThreads) sacc[i] = 0ull;
+  if (threadIdx.x < C) s_scale[threadIdx.x] = dep_scale(absum[dg.ones + threadIdx.x], 0);
+  if (threadIdx.x == 0) s_scale[C] = dep_scale((double)n, 1);  // pair weights: sum <= n
+  __syncthreads();
+  for (int p = p_begin + threadIdx.x; p < p_end; p += kDepThreads) {
+    const int64_t i = rec_idx[p];
+    int ix[2] = {0, 0};
+    double fr[2] = {0.0, 0.0};
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      // the clamped cell of interp_optimized.py:60-78 (the fitted values' stencil)
+      const double t = (x[i * D + a] - dg.x0[a]) / dg.dx[a];
+      if (t < 0.0) {
+        ix[a] = 0;
+        fr[a] = 0.0;
+      } else if (t >= (double)(dg.G[a] - 1)) {
+        ix[a] = dg.G[a] - 2;
+        fr[a] = 1.0;
+      } else {
+        ix[a] = (int)t;
+        fr[a] = t - (double)ix[a];
+      }
+    }
+    double w[NC];
+    int gcell[NC], lcell[NC];
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      const int l = ix[a] - org[a];
+      inside = inside && l >= 0 && l + 1 < dg.win[a];
+    }
+#pragma unroll
+    for (int k = 0; k < NC; ++k) {
+      double wk = 1.0;
+      int gi = 0, li = 0;
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        const int bit = (k >> (D - 1 - a)) & 1;
+        wk *= bit ? fr[a] : (1.0 - fr[a]);
+        gi = gi * dg.G[a] + ix[a] + bit;
+        li = li * dg.win[a] + ix[a] + bit - org[a];
+      }
+      w[k] = wk;
+      gcell[k] = gi;
+      lcell[k] = li;
+    }
+    for (int c = 0; c < C; ++c) {
+      const double vs = rec_val[(int64_t)c * n + p] * s_scale[c];
+#pragma unroll
+      for (int k = 0; k < NC; ++k) {
+        const long long q = __double2ll_rn(w[k] * vs);
+        if (q == 0) continue;
+        if (inside)
+          atomicAdd(&sacc[lcell[k] * stride + c], (unsigned long long)q);
+        else
+          atomicAdd(&qacc[(int64_t)gcell[k] * C + c], (unsigned long long)q);
+      }
+    }
+    int pr = 0;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) {
+#pragma unroll
+      for (int k2 = k; k2 < NC; ++k2, ++pr) {
+        const long long q = __double2ll_rn((k == k2 ? 1.0 : 2.0) * w[k] * w[k2] * s_scale[C]);
+        if (q == 0) continue;
+        if (inside)
+          atomicAdd(&sacc[lcell[0] * stride + C + pr], (unsigned long long)q);
+        else
+          atomicAdd(&bacc[(int64_t)gcell[0] * NP + pr], (unsigned long long)q);
+      }
+    }
+  }
+  __syncthreads();
+  // window -> global sums, one atomic per non-zero entry
+  for (int e = threadIdx.x; e < W0 * W1 * stride; e += kDepThreads) {
+    const unsigned long long v = sacc[e];
+    if (v == 0ull) continue;
+    const int cell = e / stride, j = e - cell * stride;
+    const int l0 = D == 2 ? cell / W1 : cell, l1 = D == 2 ? cell - l0 * W1 : 0;
+    const int g0 = org[0] + l0, g1 = org[1] + l1;
+    if (g0 < 0 || g0 >= dg.G[0] || (D == 2 && (g1 < 0 || g1 >= dg.G[1]))) continue;  // stays 0
+    const int64_t gc = D == 2 ? (int64_t)g0 * dg.G[1] + g1 : g0;
+    if (j < C)
+      atomicAdd(&qacc[gc * C + j], v);
+    else
+      atomicAdd(&bacc[gc * NP + (j - C)], v);
+  }
+  // sum of squares of every channel over this item's points (fixed order)
+  for (int c = 0; c < C; ++c) {
+    double sq = 0.0;
+    for (int p = p_begin + threadIdx.x; p < p_end; p += kDepThreads) {
+      const double v = rec_val[(int64_t)c * n + p];
+      sq += v * v;
+    }
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < kDepThreads / 32; ++k) t += red[k];
+      part[(int64_t)item * C + c] = t;
+    }
+  }
+}
+
+// integers -> doubles in place (Q (M, C), B (M, NP))
+__global__ void deposit_finish_kernel(int64_t M, int C, int NP, const double* __restrict__ absum,
+                                      int ones, int64_t n, double* __restrict__ Q,
+                                      double* __restrict__ B) {
+  __shared__ double inv[kDepMaxChan + 1];
+  if (threadIdx.x < C) inv[threadIdx.x] = 1.0 / dep_scale(absum[ones + threadIdx.x], 0);
+  if (threadIdx.x == 0) inv[C] = 1.0 / dep_scale((double)n, 1);
+  __syncthreads();
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M * C;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const long long v = reinterpret_cast<const long long*>(Q)[i];
+    Q[i] = (double)v * inv[i % C];
+  }
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < M * NP;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const long long v = reinterpret_cast<const long long*>(B)[i];
+    B[i] = (double)v * inv[C];
+  }
+}
+
+// sq[c] = sum over the items' partials, in item order (one block per channel)
+__global__ void deposit_sq_kernel(int nitems, int C, const double* __restrict__ part,
+                                  double* __restrict__ sq) {
+  __shared__ double sh[256];
+  const int c = blockIdx.x;
+  double s = 0.0;
+  for (int it = threadIdx.x; it < nitems; it += blockDim.x) s += part[(int64_t)it * C + c];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if (threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sq[c] = sh[0];
+}
+
+static int64_t max_items_of(const SpreadGeom& g, int64_t n) {
+  return (int64_t)g.ntiles + (n + g.item_points - 1) / g.item_points;
+}
+
+}  // namespace flpr
+
+extern "C" {
+
+size_t flpr_deposit_sorted_ws(int d, int64_t n, const int* h_L, int msp, int nchan) {
+  if (d < 1 || d > 2 || n < 1 || nchan < 1) return 0;
+  SpreadGeom g;
+  double tau[3] = {1, 1, 1}, kmap[27] = {0};
+  make_geom(g, d, h_L, msp, tau, kmap);
+  // the spread shrinks its work items on grids with few tiles; the items of
+  // the default size bound them from above
+  const int64_t items = (int64_t)g.ntiles + n;
+  return align_up(sizeof(double) * (size_t)items * (size_t)nchan);
+}
+
+int flpr_deposit_sorted(int d, int64_t n, const double* d_x, const int* h_L, int msp, int nchan,
+                        int ones_channel, const void* d_spread_ws, size_t spread_ws_bytes,
+                        const double* h_ax, const int* h_G, const int* h_m0, double* d_Q,
+                        double* d_B, double* d_sq, void* d_ws, size_t ws_bytes, void* stream) {
+  FLPR_CHECK_ARG(d == 1 || d == 2, "deposit_sorted: d=%d (1 or 2)", d);
+  FLPR_CHECK_ARG(ones_channel == 0 || ones_channel == 1, "deposit_sorted: ones_channel");
+  const int C = nchan - ones_channel;
+  FLPR_CHECK_ARG(n >= 1 && C >= 1 && C <= kDepMaxChan, "deposit_sorted: n=%lld C=%d",
+                 (long long)n, C);
+  FLPR_CHECK_ARG(d_x && d_spread_ws && h_ax && h_G && h_m0 && d_Q && d_B && d_sq && d_ws,
+                 "deposit_sorted: null pointer");
+  for (int a = 0; a < d; ++a)
+    FLPR_CHECK_ARG(h_G[a] >= 2 && h_L[a] >= 1, "deposit_sorted: G[%d]=%d", a, h_G[a]);
+  if (spread_ws_bytes < flpr_spread_ws(d, n, h_L, msp, nchan, FLPR_PREC_F32) ||
+      ws_bytes < flpr_deposit_sorted_ws(d, n, h_L, msp, nchan)) {
+    set_error("deposit_sorted: workspace too small");
+    return FLPR_ERR_WORKSPACE;
+  }
+  cudaStream_t s = as_stream(stream);
+  SpreadGeom g;
+  double tau[3] = {1, 1, 1}, kmap[27] = {0};
+  make_geom(g, d, h_L, msp, tau, kmap);
+  {
+    // the work items the spread used (it shrinks them on grids with few tiles)
+    const int64_t target = 4LL * sm_count();
+    if (g.ntiles < target) {
+      const int64_t per = (n + target - 1) / target;
+      int ip = 256;
+      while (ip < per && ip < g.item_points) ip <<= 1;
+      if (ip < g.item_points) g.item_points = ip;
+    }
+  }
+  Arena ar(const_cast<void*>(d_spread_ws), spread_ws_bytes);
+  SpreadWs w;
+  spread_layout(ar, d, n, g.ntiles, nchan, g.cells, 8, &w);
+  DepositGeom dg;
+  memset(&dg, 0, sizeof(dg));
+  int64_t M = 1;
+  for (int a = 0; a < d; ++a) {
+    dg.G[a] = h_G[a];
+    dg.x0[a] = h_ax[2 * a];
+    dg.dx[a] = h_ax[2 * a + 1];
+    dg.m0[a] = h_m0[a];
+    dg.win[a] = g.T[a] + 2 * kDepHalo;
+    M *= h_G[a];
+  }
+  dg.C = C;
+  dg.ones = ones_channel;
+  const int NP = dep_pairs(d);
+  const int wcells = dg.win[0] * (d == 2 ? dg.win[1] : 1);
+  const size_t smem = sizeof(unsigned long long) * (size_t)wcells * (size_t)(C + NP);
+  FLPR_CHECK_ARG(smem <= (size_t)200 * 1024, "deposit_sorted: window does not fit shared memory");
+  FLPR_CUDA(cudaMemsetAsync(d_Q, 0, sizeof(double) * (size_t)M * C, s));
+  FLPR_CUDA(cudaMemsetAsync(d_B, 0, sizeof(double) * (size_t)M * NP, s));
+  const int64_t nitems = max_items_of(g, n);
+  FLPR_CHECK_ARG(nitems <= (int64_t)g.ntiles + n, "deposit_sorted: work items");
+  double* part = static_cast<double*>(d_ws);
+  FLPR_CUDA(cudaMemsetAsync(part, 0, sizeof(double) * (size_t)nitems * C, s));
+  if (d == 2) {
+    auto k = tile_deposit_kernel<2>;
+    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<(unsigned)nitems, kDepThreads, smem, s>>>(
+        g, dg, n, d_x, w.offsets, w.items, w.rec_idx, (const double*)w.rec_val, w.absum,
+        reinterpret_cast<unsigned long long*>(d_Q), reinterpret_cast<unsigned long long*>(d_B),
+        part);
+  } else {
+    auto k = tile_deposit_kernel<1>;
+    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<(unsigned)nitems, kDepThreads, smem, s>>>(
+        g, dg, n, d_x, w.offsets, w.items, w.rec_idx, (const double*)w.rec_val, w.absum,
+        reinterpret_cast<unsigned long long*>(d_Q), reinterpret_cast<unsigned long long*>(d_B),
+        part);
+  }
+  FLPR_LAUNCH_CHECK();
+  int64_t fb = (M * (C > NP ? C : NP) + 255) / 256;
+  if (fb > 8 * sm_count()) fb = 8 * sm_count();
+  deposit_finish_kernel<<<(int)fb, 256, 0, s>>>(M, C, NP, w.absum, ones_channel, n, d_Q, d_B);
+  FLPR_LAUNCH_CHECK();
+  deposit_sq_kernel<<<C, 256, 0, s>>>((int)nitems, C, part, d_sq);
+  FLPR_LAUNCH_CHECK();
+  return FLPR_OK;
+}
+
+}  // extern "C"

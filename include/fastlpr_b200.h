@@ -343,6 +343,23 @@ int flpr_interp_reduce(int d, int64_t n, const double* d_x, const double* h_ax, 
 int flpr_deposit(int d, int64_t n, const double* d_x, const double* h_ax, const int* h_G, int C,
                  const double* const* h_cols, double* d_Q, double* d_B, double* d_sq,
                  void* stream);
+/* (5b) The same deposits (and d_sq) from the records of the last
+ * flpr_spread / flpr_spread_dkmap call (either precision) with the same d,
+ * n, L, msp, nchan and workspace d_spread_ws: one CTA per spreading work
+ * item accumulates its points' deposits in shared memory, exact 64-bit
+ * fixed point (quantum 2^-62 of each channel's absolute sum), so the
+ * result is independent of the order of the points (bitwise reproducible)
+ * and no point takes a global atomic of its own.  The deposited channels
+ * are the spread's value channels (nchan - ones_channel <= 32).  h_ax,
+ * h_G: the raw grid as for flpr_deposit; h_m0: per axis the spreading cell
+ * of raw-grid node 0 (a placement hint: any value gives the same sums).
+ * d = 1 or 2.  d_ws: flpr_deposit_sorted_ws bytes.  No reference
+ * counterpart beyond flpr_deposit's. */
+size_t flpr_deposit_sorted_ws(int d, int64_t n, const int* h_L, int msp, int nchan);
+int flpr_deposit_sorted(int d, int64_t n, const double* d_x, const int* h_L, int msp, int nchan,
+                        int ones_channel, const void* d_spread_ws, size_t spread_ws_bytes,
+                        const double* h_ax, const int* h_G, const int* h_m0, double* d_Q,
+                        double* d_B, double* d_sq, void* d_ws, size_t ws_bytes, void* stream);
 /* quad[h][c] = sum_b sum_pairs B[b][p] m(b+c_k) m(b+c_k') for m (H, M, ny),
  * ny <= 4; d_quad (H, ny) overwritten. */
 int flpr_stencil_quad(int d, const int* h_G, int H, int ny, const double* d_m, const double* d_B,

@@ -599,3 +599,70 @@ def test_sparse_bandwidths_take_fp64_planes(cuda_ok, d, order, n):
     # the explicit FP64 path agrees with both
     r64 = _fastlpr().cv_fastlpr(x, y, h, dict(opts, precision="fp64"))
     _compare_to_oracle(r64, o, TOL["fp64"])
+
+
+@pytest.mark.parametrize("d,G,prec", [(1, [300], 0), (2, [64, 48], 0), (2, [64, 48], 1),
+                                      (2, [512, 512], 0)])
+def test_sorted_deposits_match_pointwise_deposits(cuda_ok, d, G, prec):
+    """flpr_deposit_sorted (from the spread's tile-sorted records, exact
+    fixed point, shared-memory windows) equals flpr_deposit (one FP64
+    atomic per point, corner and channel) and is bitwise reproducible."""
+    import torch
+    from fastlpr_b200 import _lib, api
+    rng = np.random.default_rng(70 + d + prec)
+    n = 50000 if G[0] < 512 else 1_000_000
+    x = rng.random((n, d)) * np.arange(1, d + 1) - 0.4
+    cols = np.column_stack([np.sin(3 * x[:, 0]), rng.standard_normal((n, 3))])
+    ctx = api._Ctx(torch.device("cuda", 0))
+    dx = ctx.upload(x)
+    stats = api._point_stats(ctx, dx, n, d)
+    geom = api._make_geom(stats, n, d, np.asarray(G), 4, True)
+    dcols = [ctx.upload(np.ascontiguousarray(c)) for c in cols.T]
+    C = 1 + len(dcols)
+    spec_dt = torch.float32 if prec == _lib.FLPR_PREC_F32 else torch.float64
+    grid = ctx.empty((C, int(np.prod(geom.L))), dtype=spec_dt)
+    ws = ctx.ws(ctx.lib.flpr_spread_ws(d, n, _lib.ivec(geom.L), geom.msp, C, prec))
+    _lib.check(ctx.lib.flpr_spread(d, n, dx.data_ptr(), _lib.dvec(geom.kmap.ravel()),
+                                   _lib.ivec(geom.L), geom.msp, _lib.dvec(geom.tau), C, 1,
+                                   _lib.pvec([c.data_ptr() for c in dcols]), grid.data_ptr(), prec,
+                                   ws.data_ptr(), ws.numel(), ctx.stream), "spread")
+    axes = api._raw_axes(geom, {})
+    ax = _lib.dvec(api._axes_arg(axes))
+    M, Cv, npair = int(np.prod(G)), C - 1, (2 ** d) * (2 ** d + 1) // 2
+    outs = []
+    for rep in range(2):
+        Q, B, sq = ctx.empty((M, Cv)), ctx.empty((M, npair)), ctx.empty(Cv)
+        ws2 = ctx.ws(ctx.lib.flpr_deposit_sorted_ws(d, n, _lib.ivec(geom.L), geom.msp, C))
+        _lib.check(ctx.lib.flpr_deposit_sorted(d, n, dx.data_ptr(), _lib.ivec(geom.L), geom.msp,
+                                               C, 1, ws.data_ptr(), ws.numel(), ax,
+                                               _lib.ivec(G), _lib.ivec(api._node0_cells(geom)),
+                                               Q.data_ptr(), B.data_ptr(), sq.data_ptr(),
+                                               ws2.data_ptr(), ws2.numel(), ctx.stream),
+                   "deposit_sorted")
+        outs.append((Q, B, sq))
+    Qr, Br, sqr = ctx.empty((M, Cv)), ctx.empty((M, npair)), ctx.empty(Cv)
+    _lib.check(ctx.lib.flpr_deposit(d, n, dx.data_ptr(), ax, _lib.ivec(G), Cv,
+                                    _lib.pvec([c.data_ptr() for c in dcols]), Qr.data_ptr(),
+                                    Br.data_ptr(), sqr.data_ptr(), ctx.stream), "deposit")
+    torch.cuda.synchronize()
+    for a, b in zip(outs[0], outs[1]):
+        assert torch.equal(a, b)                     # bitwise reproducible
+    for a, b in zip(outs[0], (Qr, Br, sqr)):
+        assert rel_err(a.cpu().numpy(), b.cpu().numpy()) < 1e-12
+
+
+def test_fp32_fit_is_bitwise_reproducible(cuda_ok):
+    """Spread and deposits sum exactly in fixed point: the whole FP32 fit
+    repeats bit for bit."""
+    rng = np.random.default_rng(81)
+    n = 200000
+    x = rng.random((n, 2))
+    y = np.sin(2 * np.pi * x[:, 0]) * np.cos(2 * np.pi * x[:, 1]) + 0.1 * rng.standard_normal(n)
+    hv = np.logspace(np.log10(0.01), np.log10(0.4), 6)
+    h = np.column_stack([hv, hv])
+    opts = {"order": 1, "N": [128, 128], "precision": "fp32"}
+    a = _fastlpr().cv_fastlpr(x, y, h, opts)
+    b = _fastlpr().cv_fastlpr(x, y, h, opts)
+    np.testing.assert_array_equal(a.yhat, b.yhat)
+    np.testing.assert_array_equal(a.gcv_yhat["gcv_m"], b.gcv_yhat["gcv_m"])
+    np.testing.assert_array_equal(a.gcv_yhat["dof"], b.gcv_yhat["dof"])
