@@ -66,6 +66,8 @@ SIGNATURES = [
     ("flpr_deposit_sorted", _I, [_I, _I64, _VP, _PI, _I, _I, _I, _VP, _SZ, _PD, _PI, _PI, _VP,
                                  _VP, _VP, _VP, _SZ, _VP]),
     ("flpr_stencil_quad", _I, [_I, _PI, _I, _I, _VP, _VP, _VP, _VP]),
+    ("flpr_stencil_quad_fixed_ws", _SZ, [_I, _PI, _I, _I]),
+    ("flpr_stencil_quad_fixed", _I, [_I, _PI, _I, _I, _VP, _VP, _VP, _VP, _SZ, _VP]),
     ("flpr_lpr2d_fused_supported", _I, [_PI, _PI, _PI, _I, _I, _I]),
     ("flpr_lpr2d_fused_ws", _SZ, [_PI, _PI, _PI, _I, _I, _I]),
     ("flpr_lpr2d_fused", _I, [_PI, _PI, _PI, _I, _I, _I, _I, _I, _VP, _VP, _D, _VP, _D, _VP, _VP,

@@ -1171,8 +1171,7 @@ def _evaluate_device(ctx, st: _LprState, filt, ev) -> dict:
                                             ctx.stream), "flpr_solve_reduce")
             ev.mark("solve")
         quad = ctx.empty((H, ny))
-        ctx.check(lib.flpr_stencil_quad(d, st.G_arg, H, ny, m.data_ptr(), st.Bst.data_ptr(),
-                                        quad.data_ptr(), ctx.stream), "flpr_stencil_quad")
+        _stencil_quad(ctx, st, H, ny, m, quad)
         ev.mark("interp_reduce")
         # one device -> host read for the three reductions
         packed = torch.cat([st.sq.reshape(-1), dots.reshape(-1), quad.reshape(-1)])
@@ -1219,6 +1218,30 @@ def _evaluate_device(ctx, st: _LprState, filt, ev) -> dict:
                 dual=st.dual)
 
 
+def _stencil_quad(ctx, st, H: int, ny: int, m: torch.Tensor, quad: torch.Tensor) -> None:
+    """sum B m m of the dual form, reduced in a fixed order."""
+    lib = ctx.lib
+    ws = ctx.ws(lib.flpr_stencil_quad_fixed_ws(st.d, st.G_arg, H, ny))
+    ctx.check(lib.flpr_stencil_quad_fixed(st.d, st.G_arg, H, ny, m.data_ptr(), st.Bst.data_ptr(),
+                                          quad.data_ptr(), ws.data_ptr(), ws.numel(), ctx.stream),
+              "flpr_stencil_quad_fixed")
+
+
+def _kernel_rows(kern: _Kernel, rows: np.ndarray, geom) -> _Kernel:
+    """The per-axis factors of a consecutive subset of a separable kernel's
+    bandwidths, sliced on the device (no upload: usable inside a capture)."""
+    r0, r1 = int(rows[0]), int(rows[-1]) + 1
+    parts, off = [], 0
+    for La in geom.L:
+        seg = int(kern.H) * kern.npow * int(La)
+        parts.append(kern.data[off:off + seg].view(kern.H, kern.npow * int(La), 2)[r0:r1]
+                     .reshape(-1, 2))
+        off += seg
+    if not np.array_equal(np.asarray(rows), np.arange(r0, r1)):
+        raise ValueError("kernel rows must be consecutive")
+    return _Kernel(kern.kid, torch.cat(parts, dim=0).contiguous(), r1 - r0, kern.npow, kern.scale)
+
+
 def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev) -> dict:
     """_evaluate_device with the first k64 bandwidths in FP64 (planes from
     the FP64 spectra) and the rest on the FP32 path; lambda (or max s) is
@@ -1231,13 +1254,8 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev) -> dict:
     H = len(keep)
     H32 = H - k64
     npow = 2 * order + 1
-    f64 = _filter_bandwidths(ctx, geom, bw_k[:k64], npow, st.kid)
-    f32 = _filter_bandwidths(ctx, geom, bw_k[k64:], npow, st.kid)
-    if len(f64[2]) != k64 or len(f32[2]) != H32:
-        st64 = copy.copy(st)
-        st64.spec, st64.prec, st64.grid64 = _spectra64(ctx, st), _lib.FLPR_PREC_F64, None
-        return dict(_evaluate_device(ctx, st64, filt, ev), fp64_bandwidths=H)
-    k64k, k32k = f64[0], f32[0]
+    k64k = _kernel_rows(kern, keep[:k64], geom)
+    k32k = _kernel_rows(kern, keep[k64:], geom)
     epw = _element_powers(d, order)
     ns = len(epw)
     nt = 1 if order == 0 else len(_design_powers(d, order))
@@ -1290,8 +1308,7 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev) -> dict:
     ev.mark("conv_solve")
     dots = torch.cat([dots64, dots32], dim=1)
     quad = ctx.empty((H, ny))
-    ctx.check(lib.flpr_stencil_quad(d, st.G_arg, H, ny, m.data_ptr(), st.Bst.data_ptr(),
-                                    quad.data_ptr(), ctx.stream), "flpr_stencil_quad")
+    _stencil_quad(ctx, st, H, ny, m, quad)
     ev.mark("interp_reduce")
     packed = torch.cat([st.sq.reshape(-1), dots.reshape(-1), quad.reshape(-1)])
     S0 = torch.cat([S64.view(ns, k64, M)[0], S32.view(ns, H32, M)[0].to(torch.float64)], dim=0)

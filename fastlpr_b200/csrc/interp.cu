@@ -394,9 +394,13 @@ struct QuadChunk {
   static constexpr int value = D == 3 ? 4 : 8;
 };
 
+// part == nullptr: block sums added into quad (atomics); otherwise each
+// block's sums go to part[(h * ny + c) * gridDim.x + blockIdx.x] for a
+// fixed-order reduction (quad_reduce_kernel): bitwise reproducible
 template <int D>
 __global__ void stencil_quad_kernel(InterpGeom g, int H, int ny, const double* __restrict__ m,
-                                    const double* __restrict__ B, double* __restrict__ quad) {
+                                    const double* __restrict__ B, double* __restrict__ quad,
+                                    double* __restrict__ part) {
   constexpr int NC = 1 << D;
   constexpr int NP = NC * (NC + 1) / 2;
   constexpr int QB = QuadChunk<D>::value;
@@ -456,10 +460,25 @@ __global__ void stencil_quad_kernel(InterpGeom g, int H, int ny, const double* _
     for (int c = 0; c < 4; ++c) {
       if (h0 + q < H && c < ny) {
         const double s = block_sum(acc[q][c], sh);
-        if (threadIdx.x == 0) atomicAdd(&quad[(h0 + q) * ny + c], s);
+        if (threadIdx.x == 0) {
+          if (part != nullptr)
+            part[((int64_t)(h0 + q) * ny + c) * gridDim.x + blockIdx.x] = s;
+          else
+            atomicAdd(&quad[(h0 + q) * ny + c], s);
+        }
       }
     }
   }
+}
+
+// quad[k] = sum of the nb block partials of entry k, in block order
+__global__ void quad_reduce_kernel(int nk, int nb, const double* __restrict__ part,
+                                   double* __restrict__ quad) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nk) return;
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s += part[(int64_t)k * nb + b];
+  quad[k] = s;
 }
 
 static int make_geom(InterpGeom& g, int d, const double* ax, const int* G) {
@@ -575,26 +594,63 @@ int flpr_deposit(int d, int64_t n, const double* d_x, const double* h_ax, const 
   return FLPR_OK;
 }
 
-int flpr_stencil_quad(int d, const int* h_G, int H, int ny, const double* d_m, const double* d_B,
-                      double* d_quad, void* stream) {
+static int quad_grid(const InterpGeom& g, int H, int* per, int* nchunk) {
+  const int qb = g.d == 3 ? QuadChunk<3>::value : QuadChunk<2>::value;
+  *nchunk = (H + qb - 1) / qb;
+  int p = (pt_blocks(g.M, 4) + *nchunk - 1) / *nchunk;
+  if (p < 4) p = 4;
+  *per = p;
+  return FLPR_OK;
+}
+
+static int stencil_quad_impl(int d, const int* h_G, int H, int ny, const double* d_m,
+                             const double* d_B, double* d_quad, double* d_part, void* stream) {
   InterpGeom g;
   double ax[6] = {0, 1, 0, 1, 0, 1};
   FLPR_TRY(make_geom(g, d, ax, h_G));
   FLPR_CHECK_ARG(H >= 1 && ny >= 1 && ny <= 4, "stencil_quad: H=%d ny=%d", H, ny);
   cudaStream_t s = as_stream(stream);
-  FLPR_CUDA(cudaMemsetAsync(d_quad, 0, sizeof(double) * H * ny, s));
   FLPR_CHECK_ARG(g.M < ((int64_t)1 << 31), "stencil_quad: grid too large");
-  const int qb = d == 3 ? QuadChunk<3>::value : QuadChunk<2>::value;
-  const int nchunk = (H + qb - 1) / qb;
-  int per = (pt_blocks(g.M, 4) + nchunk - 1) / nchunk;
-  if (per < 4) per = 4;
+  int per, nchunk;
+  quad_grid(g, H, &per, &nchunk);
+  if (d_part == nullptr) FLPR_CUDA(cudaMemsetAsync(d_quad, 0, sizeof(double) * H * ny, s));
   switch (d) {
-    case 1: stencil_quad_kernel<1><<<dim3(per, nchunk), 256, 0, s>>>(g, H, ny, d_m, d_B, d_quad); break;
-    case 2: stencil_quad_kernel<2><<<dim3(per, nchunk), 256, 0, s>>>(g, H, ny, d_m, d_B, d_quad); break;
-    default: stencil_quad_kernel<3><<<dim3(per, nchunk), 256, 0, s>>>(g, H, ny, d_m, d_B, d_quad); break;
+    case 1: stencil_quad_kernel<1><<<dim3(per, nchunk), 256, 0, s>>>(g, H, ny, d_m, d_B, d_quad, d_part); break;
+    case 2: stencil_quad_kernel<2><<<dim3(per, nchunk), 256, 0, s>>>(g, H, ny, d_m, d_B, d_quad, d_part); break;
+    default: stencil_quad_kernel<3><<<dim3(per, nchunk), 256, 0, s>>>(g, H, ny, d_m, d_B, d_quad, d_part); break;
   }
   FLPR_LAUNCH_CHECK();
+  if (d_part != nullptr) {
+    const int nk = H * ny;
+    quad_reduce_kernel<<<(nk + 127) / 128, 128, 0, s>>>(nk, per, d_part, d_quad);
+    FLPR_LAUNCH_CHECK();
+  }
   return FLPR_OK;
+}
+
+int flpr_stencil_quad(int d, const int* h_G, int H, int ny, const double* d_m, const double* d_B,
+                      double* d_quad, void* stream) {
+  return stencil_quad_impl(d, h_G, H, ny, d_m, d_B, d_quad, nullptr, stream);
+}
+
+size_t flpr_stencil_quad_fixed_ws(int d, const int* h_G, int H, int ny) {
+  InterpGeom g;
+  double ax[6] = {0, 1, 0, 1, 0, 1};
+  if (make_geom(g, d, ax, h_G) != FLPR_OK || H < 1 || ny < 1) return 0;
+  int per, nchunk;
+  quad_grid(g, H, &per, &nchunk);
+  return align_up(sizeof(double) * (size_t)per * (size_t)H * (size_t)ny);
+}
+
+int flpr_stencil_quad_fixed(int d, const int* h_G, int H, int ny, const double* d_m,
+                            const double* d_B, double* d_quad, void* d_ws, size_t ws_bytes,
+                            void* stream) {
+  FLPR_CHECK_ARG(d_ws != nullptr, "stencil_quad_fixed: null workspace");
+  if (ws_bytes < flpr_stencil_quad_fixed_ws(d, h_G, H, ny)) {
+    set_error("stencil_quad_fixed: workspace too small");
+    return FLPR_ERR_WORKSPACE;
+  }
+  return stencil_quad_impl(d, h_G, H, ny, d_m, d_B, d_quad, static_cast<double*>(d_ws), stream);
 }
 
 size_t flpr_kde_ws(int64_t n, int H, int64_t M) {

@@ -849,6 +849,14 @@ static void make_geom(SpreadGeom& g, int d, const int* L, int msp, const double*
     if (a < d) {
       g.L[a] = L[a];
       int T = d == 1 ? 256 : (d == 2 ? (path2 ? kT2 : tile2[a]) : tile3[a]);
+      if (d == 3) {
+        // wide stencils (oversampled accuracies): smaller tiles, so that one
+        // channel's tile plus halo fits shared memory
+        const size_t kMax3 = (size_t)200 * 1024;
+        while (T > 1 && sizeof(long long) * (size_t)(T + 2 * msp) * (T + 2 * msp) *
+                                (T + 2 * msp) > kMax3)
+          T >>= 1;
+      }
       if (T > L[a]) T = L[a];
       g.T[a] = T;
       g.ntile[a] = (L[a] + T - 1) / T;
@@ -876,8 +884,10 @@ static int margin_bits_for(const SpreadGeom& g) {
 }
 
 static int channel_group(const SpreadGeom& g, int nchan, size_t acc_bytes) {
-  // 1-D/2-D: four CTAs per SM; 3-D tiles are larger: two CTAs per SM
+  // 1-D/2-D: four CTAs per SM; 3-D tiles are larger: two CTAs per SM, or
+  // one when a wide stencil's tile needs more
   size_t budget = (g.d == 3 ? 110 : 55) * 1024;
+  if (g.d == 3 && acc_bytes * (size_t)g.tile_cells > budget) budget = (size_t)200 * 1024;
   int cg = (int)(budget / (acc_bytes * (size_t)g.tile_cells));
   if (cg > 32) cg = 32;  // fixed-point scales of one group live in 32 shared slots
   if (cg > nchan) cg = nchan;

@@ -364,6 +364,12 @@ int flpr_deposit_sorted(int d, int64_t n, const double* d_x, const int* h_L, int
  * ny <= 4; d_quad (H, ny) overwritten. */
 int flpr_stencil_quad(int d, const int* h_G, int H, int ny, const double* d_m, const double* d_B,
                       double* d_quad, void* stream);
+/* The same sums reduced in a fixed order (block partials in d_ws, then one
+ * ordered pass): bitwise reproducible. */
+size_t flpr_stencil_quad_fixed_ws(int d, const int* h_G, int H, int ny);
+int flpr_stencil_quad_fixed(int d, const int* h_G, int H, int ny, const double* d_m,
+                            const double* d_B, double* d_quad, void* d_ws, size_t ws_bytes,
+                            void* stream);
 
 /* (8) Evaluate one grid (values (M) float64 at every grid point, times
  * nval interleaved value sets, layout (nval, M)) at n points: d_out (nval, n).

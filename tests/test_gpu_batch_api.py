@@ -76,7 +76,7 @@ def test_batch_api_matches_reference(cuda_ok, name):
     opts = dict(z["opts"], precision="fp64")
     sh = fl.precompute_shared(z["x"], z["y"], z["h"], opts)
     np.testing.assert_allclose(sh.x_scaled, z["x_scaled"], rtol=0, atol=1e-13)
-    np.testing.assert_allclose(sh.mean, z["mean"], rtol=1e-15)
+    np.testing.assert_allclose(sh.mean, z["mean"], rtol=1e-14)
     np.testing.assert_allclose(sh.std, z["std"], rtol=1e-14)
     np.testing.assert_array_equal(sh.bandwidths_filtered, z["bandwidths_filtered"])
     np.testing.assert_array_equal(sh.grid_shape, z["grid_shape"])
