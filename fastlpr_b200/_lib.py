@@ -63,8 +63,8 @@ SIGNATURES = [
     ("flpr_scalar_of", _I, [_I, _I, _I, _I64, _VP, _I, _VP, _VP, _VP]),
     ("flpr_deposit", _I, [_I, _I64, _VP, _PD, _PI, _I, _PVP, _VP, _VP, _VP, _VP]),
     ("flpr_deposit_sorted_ws", _SZ, [_I, _I64, _PI, _I, _I]),
-    ("flpr_deposit_sorted", _I, [_I, _I64, _VP, _PI, _I, _I, _I, _VP, _SZ, _PD, _PI, _PI, _VP,
-                                 _VP, _VP, _VP, _SZ, _VP]),
+    ("flpr_deposit_sorted", _I, [_I, _I64, _VP, _PI, _I, _I, _I, _PVP, _VP, _SZ, _PD, _PI, _PI,
+                                 _VP, _VP, _VP, _VP, _SZ, _VP]),
     ("flpr_stencil_quad", _I, [_I, _PI, _I, _I, _VP, _VP, _VP, _VP]),
     ("flpr_stencil_quad_fixed_ws", _SZ, [_I, _PI, _I, _I]),
     ("flpr_stencil_quad_fixed", _I, [_I, _PI, _I, _I, _VP, _VP, _VP, _VP, _SZ, _VP]),

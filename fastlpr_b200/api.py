@@ -1073,7 +1073,9 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
             ws2 = ctx.ws(lib.flpr_deposit_sorted_ws(d, n, _lib.ivec(kept["L"]), kept["msp"],
                                                     kept["C"]))
             ctx.check(lib.flpr_deposit_sorted(d, n, dx.data_ptr(), _lib.ivec(kept["L"]),
-                                              kept["msp"], kept["C"], 1, kept["ws"].data_ptr(),
+                                              kept["msp"], kept["C"], 1,
+                                              _lib.pvec([c.data_ptr() for c in ycols + pcols]),
+                                              kept["ws"].data_ptr(),
                                               kept["ws"].numel(), st.ax_arg, st.G_arg,
                                               _lib.ivec(_node0_cells(geom)), st.Q.data_ptr(),
                                               st.Bst.data_ptr(), st.sq.data_ptr(),

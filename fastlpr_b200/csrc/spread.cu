@@ -1313,12 +1313,11 @@ tile_deposit_kernel(SpreadGeom g, DepositGeom dg, int64_t n, const double* __res
                     const int* __restrict__ offsets, const int* __restrict__ items,
                     const int* __restrict__ rec_idx, const double* __restrict__ rec_val,
                     const double* __restrict__ absum, unsigned long long* __restrict__ qacc,
-                    unsigned long long* __restrict__ bacc, double* __restrict__ part) {
+                    unsigned long long* __restrict__ bacc) {
   constexpr int NC = 1 << D;
   constexpr int NP = dep_pairs(D);
   extern __shared__ __align__(16) unsigned long long sacc[];  // window cells x (C + NP)
   __shared__ double s_scale[kDepMaxChan + 1];
-  __shared__ double red[kDepThreads / 32];
   const int C = dg.C, stride = C + NP;
   const int W0 = dg.win[0], W1 = D == 2 ? dg.win[1] : 1;
   const int item = blockIdx.x;
@@ -1435,11 +1434,19 @@ tile_deposit_kernel(SpreadGeom g, DepositGeom dg, int64_t n, const double* __res
     else
       atomicAdd(&bacc[gc * NP + (j - C)], v);
   }
-  // sum of squares of every channel over this item's points (fixed order)
+}
+
+// per-block sums of squares of every channel over a fixed range of point
+// indices (the columns in their own order: the result does not depend on
+// the order of the sorted records); part[b * C + c]
+__global__ void sumsq_kernel(int64_t n, int C, ChanPtrs cp, double* __restrict__ part) {
+  __shared__ double red[kDepThreads / 32];
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t i0 = blockIdx.x * chunk, i1 = min(n, i0 + chunk);
   for (int c = 0; c < C; ++c) {
     double sq = 0.0;
-    for (int p = p_begin + threadIdx.x; p < p_end; p += kDepThreads) {
-      const double v = rec_val[(int64_t)c * n + p];
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += kDepThreads) {
+      const double v = cp.col[c][i];
       sq += v * v;
     }
     for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
@@ -1449,7 +1456,7 @@ tile_deposit_kernel(SpreadGeom g, DepositGeom dg, int64_t n, const double* __res
     if (threadIdx.x == 0) {
       double t = 0.0;
       for (int k = 0; k < kDepThreads / 32; ++k) t += red[k];
-      part[(int64_t)item * C + c] = t;
+      part[(int64_t)blockIdx.x * C + c] = t;
     }
   }
 }
@@ -1490,6 +1497,8 @@ __global__ void deposit_sq_kernel(int nitems, int C, const double* __restrict__ 
   if (threadIdx.x == 0) sq[c] = sh[0];
 }
 
+constexpr int kSumsqBlocks = 512;
+
 static int64_t max_items_of(const SpreadGeom& g, int64_t n) {
   return (int64_t)g.ntiles + (n + g.item_points - 1) / g.item_points;
 }
@@ -1503,14 +1512,12 @@ size_t flpr_deposit_sorted_ws(int d, int64_t n, const int* h_L, int msp, int nch
   SpreadGeom g;
   double tau[3] = {1, 1, 1}, kmap[27] = {0};
   make_geom(g, d, h_L, msp, tau, kmap);
-  // the spread shrinks its work items on grids with few tiles; the items of
-  // the default size bound them from above
-  const int64_t items = (int64_t)g.ntiles + n;
-  return align_up(sizeof(double) * (size_t)items * (size_t)nchan);
+  return align_up(sizeof(double) * (size_t)kSumsqBlocks * (size_t)nchan);
 }
 
 int flpr_deposit_sorted(int d, int64_t n, const double* d_x, const int* h_L, int msp, int nchan,
-                        int ones_channel, const void* d_spread_ws, size_t spread_ws_bytes,
+                        int ones_channel, const double* const* h_cols,
+                        const void* d_spread_ws, size_t spread_ws_bytes,
                         const double* h_ax, const int* h_G, const int* h_m0, double* d_Q,
                         double* d_B, double* d_sq, void* d_ws, size_t ws_bytes, void* stream) {
   FLPR_CHECK_ARG(d == 1 || d == 2, "deposit_sorted: d=%d (1 or 2)", d);
@@ -1518,7 +1525,7 @@ int flpr_deposit_sorted(int d, int64_t n, const double* d_x, const int* h_L, int
   const int C = nchan - ones_channel;
   FLPR_CHECK_ARG(n >= 1 && C >= 1 && C <= kDepMaxChan, "deposit_sorted: n=%lld C=%d",
                  (long long)n, C);
-  FLPR_CHECK_ARG(d_x && d_spread_ws && h_ax && h_G && h_m0 && d_Q && d_B && d_sq && d_ws,
+  FLPR_CHECK_ARG(d_x && h_cols && d_spread_ws && h_ax && h_G && h_m0 && d_Q && d_B && d_sq && d_ws,
                  "deposit_sorted: null pointer");
   for (int a = 0; a < d; ++a)
     FLPR_CHECK_ARG(h_G[a] >= 2 && h_L[a] >= 1, "deposit_sorted: G[%d]=%d", a, h_G[a]);
@@ -1564,30 +1571,31 @@ int flpr_deposit_sorted(int d, int64_t n, const double* d_x, const int* h_L, int
   FLPR_CUDA(cudaMemsetAsync(d_Q, 0, sizeof(double) * (size_t)M * C, s));
   FLPR_CUDA(cudaMemsetAsync(d_B, 0, sizeof(double) * (size_t)M * NP, s));
   const int64_t nitems = max_items_of(g, n);
-  FLPR_CHECK_ARG(nitems <= (int64_t)g.ntiles + n, "deposit_sorted: work items");
   double* part = static_cast<double*>(d_ws);
-  FLPR_CUDA(cudaMemsetAsync(part, 0, sizeof(double) * (size_t)nitems * C, s));
+  ChanPtrs cp;
+  memset(&cp, 0, sizeof(cp));
+  for (int c = 0; c < C; ++c) cp.col[c] = h_cols[c];
   if (d == 2) {
     auto k = tile_deposit_kernel<2>;
     FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<(unsigned)nitems, kDepThreads, smem, s>>>(
         g, dg, n, d_x, w.offsets, w.items, w.rec_idx, (const double*)w.rec_val, w.absum,
-        reinterpret_cast<unsigned long long*>(d_Q), reinterpret_cast<unsigned long long*>(d_B),
-        part);
+        reinterpret_cast<unsigned long long*>(d_Q), reinterpret_cast<unsigned long long*>(d_B));
   } else {
     auto k = tile_deposit_kernel<1>;
     FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<(unsigned)nitems, kDepThreads, smem, s>>>(
         g, dg, n, d_x, w.offsets, w.items, w.rec_idx, (const double*)w.rec_val, w.absum,
-        reinterpret_cast<unsigned long long*>(d_Q), reinterpret_cast<unsigned long long*>(d_B),
-        part);
+        reinterpret_cast<unsigned long long*>(d_Q), reinterpret_cast<unsigned long long*>(d_B));
   }
   FLPR_LAUNCH_CHECK();
   int64_t fb = (M * (C > NP ? C : NP) + 255) / 256;
   if (fb > 8 * sm_count()) fb = 8 * sm_count();
   deposit_finish_kernel<<<(int)fb, 256, 0, s>>>(M, C, NP, w.absum, ones_channel, n, d_Q, d_B);
   FLPR_LAUNCH_CHECK();
-  deposit_sq_kernel<<<C, 256, 0, s>>>((int)nitems, C, part, d_sq);
+  sumsq_kernel<<<kSumsqBlocks, kDepThreads, 0, s>>>(n, C, cp, part);
+  FLPR_LAUNCH_CHECK();
+  deposit_sq_kernel<<<C, 256, 0, s>>>(kSumsqBlocks, C, part, d_sq);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }

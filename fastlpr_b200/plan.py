@@ -23,6 +23,7 @@ streams, no capture).
 from __future__ import annotations
 
 import os
+import time
 from concurrent.futures import ThreadPoolExecutor
 from typing import List, Optional, Sequence
 
@@ -373,8 +374,20 @@ class LprPlan:
         return outs
 
     # -- execution ----------------------------------------------------------
-    def run(self, ys: Optional[Sequence] = None) -> List[RegressionOutput]:
-        """Fit every problem (with new responses `ys` if given)."""
+    def run(self, ys: Optional[Sequence] = None,
+            timings: Optional[dict] = None) -> List[RegressionOutput]:
+        """Fit every problem (with new responses `ys` if given).  timings
+        (optional dict): accumulates host wall seconds of the stages
+        'stage' (responses to the device), 'enqueue' (replay and downloads
+        issued), 'wait' (device done) and 'results'."""
+        clock = [time.perf_counter()]
+
+        def mark(name):
+            if timings is not None:
+                now = time.perf_counter()
+                timings[name] = timings.get(name, 0.0) + now - clock[0]
+                clock[0] = now
+
         with torch.cuda.device(self.device):
             finite = None
             if ys is None and not self._y_ok:
@@ -387,6 +400,7 @@ class LprPlan:
                     p.staged.synchronize()
                 self._write_y(ys)
                 finite = api._to_host(self._finite.reshape(1))
+            mark("stage")
             if self.graph is not None:
                 self.graph.replay()
                 outs = self.outs
@@ -398,7 +412,9 @@ class LprPlan:
             for st, r, pend in outs:
                 pends.append({k: (api._to_host(v) if isinstance(v, torch.Tensor) and v.is_cuda
                                   else v) for k, v in pend.items()})
+            mark("enqueue")
             torch.cuda.current_stream(self.device).synchronize()
+            mark("wait")
             if finite is not None:
                 self._y_ok = bool(finite[0])
             self._check_finite(finite[0] if finite is not None else None)
@@ -410,6 +426,7 @@ class LprPlan:
                     res.append(api._finalize_build(self._ctx, st, r, pends[i], ev, None))
                 else:
                     res.append(self._finish_learned(p, st, r, pends[i], ev))
+            mark("results")
             return res
 
     def _finish_learned(self, p, st, r, pend, ev) -> RegressionOutput:

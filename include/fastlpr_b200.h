@@ -350,14 +350,16 @@ int flpr_deposit(int d, int64_t n, const double* d_x, const double* h_ax, const 
  * fixed point (quantum 2^-62 of each channel's absolute sum), so the
  * result is independent of the order of the points (bitwise reproducible)
  * and no point takes a global atomic of its own.  The deposited channels
- * are the spread's value channels (nchan - ones_channel <= 32).  h_ax,
+ * are the spread's value channels (nchan - ones_channel <= 32; h_cols: their
+ * device columns, for the sums of squares in d_sq, taken in point order).  h_ax,
  * h_G: the raw grid as for flpr_deposit; h_m0: per axis the spreading cell
  * of raw-grid node 0 (a placement hint: any value gives the same sums).
  * d = 1 or 2.  d_ws: flpr_deposit_sorted_ws bytes.  No reference
  * counterpart beyond flpr_deposit's. */
 size_t flpr_deposit_sorted_ws(int d, int64_t n, const int* h_L, int msp, int nchan);
 int flpr_deposit_sorted(int d, int64_t n, const double* d_x, const int* h_L, int msp, int nchan,
-                        int ones_channel, const void* d_spread_ws, size_t spread_ws_bytes,
+                        int ones_channel, const double* const* h_cols,
+                        const void* d_spread_ws, size_t spread_ws_bytes,
                         const double* h_ax, const int* h_G, const int* h_m0, double* d_Q,
                         double* d_B, double* d_sq, void* d_ws, size_t ws_bytes, void* stream);
 /* quad[h][c] = sum_b sum_pairs B[b][p] m(b+c_k) m(b+c_k') for m (H, M, ny),

@@ -634,7 +634,8 @@ def test_sorted_deposits_match_pointwise_deposits(cuda_ok, d, G, prec):
         Q, B, sq = ctx.empty((M, Cv)), ctx.empty((M, npair)), ctx.empty(Cv)
         ws2 = ctx.ws(ctx.lib.flpr_deposit_sorted_ws(d, n, _lib.ivec(geom.L), geom.msp, C))
         _lib.check(ctx.lib.flpr_deposit_sorted(d, n, dx.data_ptr(), _lib.ivec(geom.L), geom.msp,
-                                               C, 1, ws.data_ptr(), ws.numel(), ax,
+                                               C, 1, _lib.pvec([c.data_ptr() for c in dcols]),
+                                               ws.data_ptr(), ws.numel(), ax,
                                                _lib.ivec(G), _lib.ivec(api._node0_cells(geom)),
                                                Q.data_ptr(), B.data_ptr(), sq.data_ptr(),
                                                ws2.data_ptr(), ws2.numel(), ctx.stream),
