@@ -125,7 +125,12 @@ class LprPlan:
             self._pool = None
             self._finite = None
             self._write_y([p.su.y_arr for p in self.probs])
-            self._check_finite(self._finite)
+            for p in self.probs:
+                self._check_finite(bool(np.all(np.isfinite(p.staging.numpy()))))
+            # downloads of each problem's outputs, issued behind its last
+            # kernel (an event recorded in the graph) so they overlap the
+            # rest of the replay
+            self._copy = torch.cuda.Stream(self.device)
             # whether the responses on the device passed their NaN/Inf check
             # (a rejected run leaves them there; a replay without new
             # responses would fit them)
@@ -214,8 +219,12 @@ class LprPlan:
         for p in self.probs:
             su = p.su
             p.lidx = None
+            p.search = None
             if str(su.opts.get("bandwidth_search", "full")) != "learned":
                 continue
+            # what a single learned fit records when the network does not
+            # serve the problem
+            p.search = {"mode": "learned", "accepted": False, "fallback": "full sweep"}
             lh = _learned.isotropic_log_h(su.bandwidths)
             ok = (lh is not None and bool(su.opts.get("calc_dof", True)) and su.dy == 1
                   and not su.y_is_complex and su.d <= 2 and api._kernel_id(su.opts) == 0
@@ -265,9 +274,9 @@ class LprPlan:
 
     def _write_y(self, ys) -> None:
         """Copy the responses into the pinned staging rows (a few host threads:
-        numpy's copies release the GIL) and on to the device; their NaN/Inf
-        check runs on the device (self._finite, read with the outputs)."""
-        stream = torch.cuda.current_stream(self.device)
+        numpy's copies release the GIL).  The upload to the device and the
+        NaN/Inf check are part of the issued work (_upload_y), so in a graph
+        they overlap the other problems' kernels."""
         arrs = []
         for p, y in zip(self.probs, ys):
             y_arr = np.asarray(y)
@@ -295,16 +304,14 @@ class LprPlan:
         if self._pool is None:
             self._pool = ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1)))
         list(self._pool.map(stage, range(len(self.probs))))
-        flags = []
-        for p in self.probs:
-            for c, col in enumerate(p.ycols):
-                col.copy_(p.staging[c], non_blocking=True)
-                flags.append(torch.isfinite(col).all())
-            # the staging rows are reused by the next run
-            ev = torch.cuda.Event()
-            ev.record(stream)
-            p.staged = ev
-        self._finite = torch.stack(flags).all()
+
+    @staticmethod
+    def _upload_y(p) -> torch.Tensor:
+        """On the current stream: the staged responses of problem p to its
+        device columns, and whether all of them are finite (device flag)."""
+        for c, col in enumerate(p.ycols):
+            col.copy_(p.staging[c], non_blocking=True)
+        return torch.isfinite(torch.stack(p.ycols)).all()
 
     @staticmethod
     def _check_finite(flag) -> None:
@@ -323,10 +330,14 @@ class LprPlan:
             s.wait_stream(main)
         outs = [None] * len(self.probs)
         states = {}
+        flags = []
         for i in self.order:
             p = self.probs[i]
             su = p.su
+            if getattr(p, "done", None) is None:
+                p.done = torch.cuda.Event(external=True)
             with torch.cuda.stream(self.streams[self.assign[i]]):
+                flags.append(self._upload_y(p))
                 ctx = api._Ctx(self.device)
                 ev = api._PhaseEvents(None)
                 st = api._prepare_lpr(ctx, None, None, su.dy, su.opts, su.order, su.prec,
@@ -344,6 +355,7 @@ class LprPlan:
                     p.bufs = api._output_bufs(st, r["H"])
                 pend = api._finalize_enqueue(ctx, st, r, ev, device_select=True, bufs=p.bufs,
                                              hsum_dev=p.hsum)
+                p.done.record()
                 outs[i] = (st, r, pend)
         if states:
             from . import learned as _learned
@@ -368,9 +380,11 @@ class LprPlan:
                         p.bufs = api._output_bufs(st, r["H"])
                     pend = api._finalize_enqueue(ctx, st, r, ev, device_select=True,
                                                  bufs=p.bufs, hsum_dev=hsum)
+                    p.done.record()
                     outs[i] = (st, r, pend)
         for s in self.streams:
             main.wait_stream(s)
+        self._finite = torch.stack(flags).all().reshape(1)
         return outs
 
     # -- execution ----------------------------------------------------------
@@ -378,8 +392,8 @@ class LprPlan:
             timings: Optional[dict] = None) -> List[RegressionOutput]:
         """Fit every problem (with new responses `ys` if given).  timings
         (optional dict): accumulates host wall seconds of the stages
-        'stage' (responses to the device), 'enqueue' (replay and downloads
-        issued), 'wait' (device done) and 'results'."""
+        'stage' (responses into the pinned staging rows), 'enqueue' (replay
+        and downloads issued), 'wait' (device done) and 'results'."""
         clock = [time.perf_counter()]
 
         def mark(name):
@@ -389,41 +403,42 @@ class LprPlan:
                 clock[0] = now
 
         with torch.cuda.device(self.device):
-            finite = None
             if ys is None and not self._y_ok:
                 raise ValueError("Response y contains NaN or Inf values (the last responses "
                                  "given to run were rejected; pass new responses)")
             if ys is not None:
                 if len(ys) != len(self.probs):
                     raise ValueError(f"expected {len(self.probs)} responses, got {len(ys)}")
-                for p in self.probs:
-                    p.staged.synchronize()
                 self._write_y(ys)
-                finite = api._to_host(self._finite.reshape(1))
             mark("stage")
             if self.graph is not None:
                 self.graph.replay()
                 outs = self.outs
             else:
                 outs = self._issue()
-            # the large outputs go into fresh pinned memory (no host copies;
-            # the results stay valid after later runs)
+            finite = api._to_host(self._finite)
+            # each problem's outputs go into fresh pinned memory (no host
+            # copies; the results stay valid after later runs) on the copy
+            # stream, as soon as that problem's last kernel is done
             pends = []
-            for st, r, pend in outs:
-                pends.append({k: (api._to_host(v) if isinstance(v, torch.Tensor) and v.is_cuda
-                                  else v) for k, v in pend.items()})
+            with torch.cuda.stream(self._copy):
+                for p, (st, r, pend) in zip(self.probs, outs):
+                    self._copy.wait_event(p.done)
+                    pends.append({k: (api._to_host(v) if isinstance(v, torch.Tensor)
+                                      and v.is_cuda else v) for k, v in pend.items()})
             mark("enqueue")
             torch.cuda.current_stream(self.device).synchronize()
+            self._copy.synchronize()
             mark("wait")
-            if finite is not None:
-                self._y_ok = bool(finite[0])
-            self._check_finite(finite[0] if finite is not None else None)
+            self._y_ok = bool(finite[0])
+            self._check_finite(finite[0])
             ev = api._PhaseEvents(None)
             res = []
             for i, p in enumerate(self.probs):
                 st, r, _ = outs[i]
                 if p.lidx is None:
-                    res.append(api._finalize_build(self._ctx, st, r, pends[i], ev, None))
+                    res.append(api._finalize_build(self._ctx, st, r, pends[i], ev,
+                                                   dict(p.search) if p.search else None))
                 else:
                     res.append(self._finish_learned(p, st, r, pends[i], ev))
             mark("results")
@@ -435,6 +450,9 @@ class LprPlan:
         (valid until the next replay)."""
         ctx = self._ctx
         bw = p.su.bandwidths
+        # FP64 spectra formed eagerly after an earlier replay hold that
+        # replay's responses: form them again from this replay's grid
+        st.spec64 = None
         found = api._learned_finish(ctx, st, bw, dict(r), pend, int(self.lo_h[p.lidx]),
                                     float(self.t_h[p.lidx]), ev)
         if found is None:

@@ -303,6 +303,25 @@ def test_fused_2d_path_matches_cufft_path_and_oracle(cuda_ok, order, G):
     assert rel_err(fused.yhat, plain.yhat) < tol
 
 
+def test_fused_2d_band_classes_match_oracle(cuda_ok):
+    """1024-point row and column transforms (grid 512 x 400) over bandwidths
+    whose kernel spectra end in every band class of the pruned first pass
+    (1, 2 and 4 slots per side, and all slots) agree with the oracle."""
+    rng = np.random.default_rng(77)
+    n = 200000
+    x = rng.random((n, 2))
+    y = np.sin(2 * np.pi * x[:, 0]) * np.cos(2 * np.pi * x[:, 1]) + 0.1 * rng.standard_normal(n)
+    hv = np.logspace(np.log10(0.006), np.log10(0.5), 8)
+    h = np.column_stack([hv, 1.1 * hv])
+    opts = {"order": 1, "N": [512, 400], "precision": "fp32"}
+    r = _fastlpr().cv_fastlpr(x, y, h, opts)
+    assert r.metadata.get("fp64_bandwidths", 0) == 0
+    o = oracle.cv_fastlpr(x, y, h, {"order": 1, "N": [512, 400]})
+    assert rel_err(r.yhat, o["yhat"]) < 1e-5
+    assert elem_rel_err(r.gcv_yhat["gcv_m"], o["gcv_m"]) < 1e-5
+    assert rel_err(r.gcv_yhat["dof"], o["dof_all"]) < 1e-5
+
+
 @pytest.mark.parametrize("bad", [np.nan, np.inf])
 def test_validation_rejects_nonfinite(cuda_ok, bad):
     """NaN/Inf inputs raise the reference's ValueError (checked on the device)."""
