@@ -84,88 +84,6 @@ __device__ __forceinline__ void dif_slots(float2 (&v)[E], const float2* __restri
   }
 }
 
-// Band-limited inputs: a transform whose input entries k (lane l, slot s:
-// k = 32 s + l) are zero outside min(k, N - k) <= kc has nonzero slots only
-// in [0, NZ) and [E - NZ, E) for NZ = kc / 32 + 1.  The first DIF pass then
-// skips the butterflies whose inputs are both zero and does half the work
-// of those with one zero input (a + 0 = a, a - 0 = a and 0 - b = -b are
-// exact, so the results are those of the full pass).  nz_before: the slots
-// that can be nonzero when the stage of span `span` starts.
-__host__ __device__ constexpr unsigned long long nz_initial(int E, int NZ) {
-  unsigned long long m = 0;
-  for (int s = 0; s < E; ++s)
-    if (s < NZ || s >= E - NZ) m |= 1ull << s;
-  return m;
-}
-__host__ __device__ constexpr unsigned long long nz_before(int E, int NZ, int span) {
-  unsigned long long m = nz_initial(E, NZ);
-  for (int sp = E / 2; sp > span; sp >>= 1) {
-    unsigned long long r = m;
-    for (int s = 0; s < E; ++s)
-      if ((s & sp) == 0 && (((m >> s) | (m >> (s + sp))) & 1ull)) r |= (1ull << s) | (1ull << (s + sp));
-    m = r;
-  }
-  return m;
-}
-
-template <int E, int NZ, int SPAN>
-__device__ __forceinline__ void dif_stage_nz(float2 (&v)[E], const float2* __restrict__ tw32) {
-  constexpr unsigned long long m = nz_before(E, NZ, SPAN);
-#pragma unroll
-  for (int s = 0; s < E; ++s) {
-    if ((s & SPAN) == 0) {
-      const bool an = (m >> s) & 1ull, bn = (m >> (s + SPAN)) & 1ull;
-      const int tw = (s & (SPAN - 1)) * (16 / SPAN);
-      if (an && bn) {
-        const float2 a = v[s], b = v[s + SPAN];
-        v[s] = cadd(a, b);
-        v[s + SPAN] = rot32(csub(a, b), tw, tw32);
-      } else if (an) {
-        v[s + SPAN] = rot32(v[s], tw, tw32);
-      } else if (bn) {
-        const float2 b = v[s + SPAN];
-        v[s] = b;
-        v[s + SPAN] = rot32(make_float2(-b.x, -b.y), tw, tw32);
-      }
-    }
-  }
-  if constexpr (SPAN > 1) dif_stage_nz<E, NZ, SPAN / 2>(v, tw32);
-}
-
-// dif_slots<E> for an input with nonzero slots only in [0, NZ) and
-// [E - NZ, E) (NZ = E / 2: every slot, the full pass).
-template <int E, int NZ>
-__device__ __forceinline__ void dif_slots_nz(float2 (&v)[E], const float2* __restrict__ tw32) {
-  static_assert(NZ >= 1 && 2 * NZ <= E, "band class");
-  if constexpr (E >= 2) dif_stage_nz<E, NZ, E / 2>(v, tw32);
-}
-
-// Band class of a transform input with cutoff kc: the slots per side, a
-// power of two, at most E / 2.
-template <int E>
-__host__ __device__ constexpr int nz_cap(int c) { return c < E / 2 ? c : E / 2; }
-
-// Runs BODY (which names the constant NZ) for the band class of kc: one of
-// 1, 2 or 4 slots per side, or every slot.  kc is uniform across the CTA,
-// so every warp takes the same branch.
-#define FLPR_BAND_CLASS(E, kc, BODY)                  \
-  do {                                                \
-    const int need_ = (kc) / 32 + 1;                  \
-    if (need_ <= 1) {                                 \
-      constexpr int NZ = nz_cap<E>(1);                \
-      BODY;                                           \
-    } else if (need_ <= 2) {                          \
-      constexpr int NZ = nz_cap<E>(2);                \
-      BODY;                                           \
-    } else if (need_ <= 4) {                          \
-      constexpr int NZ = nz_cap<E>(4);                \
-      BODY;                                           \
-    } else {                                          \
-      constexpr int NZ = (E) / 2;                     \
-      BODY;                                           \
-    }                                                 \
-  } while (0)
-
 // Output index held by lane t, slot s after warp_ifft<E>.
 template <int E>
 __device__ __forceinline__ int out_index(int lane, int s) {
@@ -175,17 +93,16 @@ __device__ __forceinline__ int out_index(int lane, int s) {
 }
 
 // Inverse (unnormalised) FFT of length N = 32 E held by one warp.  On entry
-// lane l, slot s holds x[32 s + l] (zero outside the slots of band class
-// NZ); on exit lane t, slot s holds X[out_index<E>(t, s)].  buf: this
-// warp's warp_buf_stride(E) floats, free again when the function returns.
-template <int E, int NZ = E / 2>
+// lane l, slot s holds x[32 s + l]; on exit lane t, slot s holds
+// X[out_index<E>(t, s)].  buf: this warp's warp_buf_stride(E) floats, free
+// again when the function returns.
+template <int E>
 __device__ __forceinline__ void warp_ifft(float2 (&v)[E], const float2* __restrict__ tw2,
                                           const float2* __restrict__ tw32, float* buf, int lane) {
   constexpr int EB = ilog2(E);
   constexpr int P = 32 / E;
-  // DFT over n1 (n = 32 n1 + n2) for each n2 = lane; slots outside the
-  // input's band class are zero
-  dif_slots_nz<E, NZ>(v, tw32);
+  // DFT over n1 (n = 32 n1 + n2) for each n2 = lane
+  dif_slots<E>(v, tw32);
   // twiddle W_N^(n2 k1), k1 = brev(s)
 #pragma unroll
   for (int s = 1; s < E; ++s) v[s] = cmul(v[s], tw2[brev(s, EB) * 32 + lane]);
@@ -323,36 +240,16 @@ struct ColArgs {
 // W layout: [slot][hz][r][w1], r = x0 - q0 in [0, G0).  Each warp stages its
 // cropped column in its own transpose buffer; the CTA then writes 8-column
 // row segments.
-// The column's product with the axis-0 factor, band-limited at kc0 (entries
-// of the factor below kBandEps of its peak are left out), and its inverse
-// transform for band class NZ.
-template <int E, int NZ>
-__device__ __forceinline__ void col_fft(const float2* __restrict__ col, const float2* __restrict__ f,
-                                        int kc0, const float2* s_tw2, const float2* s_tw32,
-                                        float* buf, int lane, float2 (&v)[E]) {
-  constexpr int N = 32 * E;
-#pragma unroll
-  for (int s = 0; s < E; ++s) {
-    v[s] = make_float2(0.0f, 0.0f);
-    if (s < NZ || s >= E - NZ) {
-      const int w0 = 32 * s + lane;
-      if (min(w0, N - w0) <= kc0) v[s] = cmul(col[32 * s], f[32 * s]);
-    }
-  }
-  warp_ifft<E, NZ>(v, s_tw2, s_tw32, buf, lane);
-}
-
 template <int E>
 __global__ void __launch_bounds__(kColWarps * 32, 2)
 colpass_kernel(ColArgs ca, const float2* __restrict__ Yt, const float2* __restrict__ F0f,
-               const float2* __restrict__ tab, const int* __restrict__ kcut0,
-               const int* __restrict__ kcut1, float2* __restrict__ W) {
+               const float2* __restrict__ tab, const int* __restrict__ kcut1,
+               float2* __restrict__ W) {
   constexpr int N = 32 * E;
   constexpr int SW = warp_buf_stride(E);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // columns beyond the axis-1 band limit are never read by the row pass
   const int kc1 = kcut1[ca.hbase + blockIdx.z];
-  const int kc0 = kcut0[ca.hbase + blockIdx.z];
   if (blockIdx.x * kColWarps > kc1) return;
   float2* s_tw2 = reinterpret_cast<float2*>(smem_raw);
   float2* s_tw32 = s_tw2 + N;
@@ -368,7 +265,9 @@ colpass_kernel(ColArgs ca, const float2* __restrict__ Yt, const float2* __restri
     const float2* col = Yt + ((size_t)c * ca.L1h + w1) * N + lane;
     const float2* f = F0f + ((size_t)h * ca.npow + a0) * N + lane;
     float2 v[E];
-    FLPR_BAND_CLASS(E, kc0, (col_fft<E, NZ>(col, f, kc0, s_tw2, s_tw32, buf, lane, v)));
+#pragma unroll
+    for (int s = 0; s < E; ++s) v[s] = cmul(col[32 * s], f[32 * s]);
+    warp_ifft<E>(v, s_tw2, s_tw32, buf, lane);
     float2* stage = reinterpret_cast<float2*>(buf);
 #pragma unroll
     for (int s = 0; s < E; ++s) {
@@ -383,6 +282,34 @@ colpass_kernel(ColArgs ca, const float2* __restrict__ Yt, const float2* __restri
     const int colw = blockIdx.x * kColWarps + wl;
     if (colw < ca.L1h && colw <= kc1)
       out[(size_t)r * ca.L1h + colw] = reinterpret_cast<const float2*>(bufs + wl * SW)[r];
+  }
+}
+
+// Solve vectors z = (S + lam I)^-1 e1 per (bandwidth, grid point); order 0
+// stores 1/max(s, max(s) reg).  S: (ns, H, M) float; z: (H, M, NT) double.
+template <int NT>
+__global__ void zvec_kernel(int order, int H, int64_t M, const float* __restrict__ S,
+                            const double* __restrict__ scalar, double reg, double* __restrict__ z) {
+  constexpr int NS = NT * (NT + 1) / 2;
+  const int64_t HM = (int64_t)H * M;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < HM;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    double zz[NT];
+    if (order == 0) {
+      const double thr = scalar[0] * reg;
+      const double s = (double)S[t];
+      zz[0] = 1.0 / (s > thr ? s : thr);
+    } else {
+      double Ap[NS];
+#pragma unroll
+      for (int k = 0; k < NS; ++k) Ap[k] = (double)S[(int64_t)k * HM + t];
+      if (!solve_e1_fixed<NT>(Ap, scalar[0], zz)) {
+#pragma unroll
+        for (int i = 0; i < NT; ++i) zz[i] = NAN;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NT; ++i) z[t * NT + i] = zz[i];
   }
 }
 
@@ -422,14 +349,13 @@ __device__ __forceinline__ float2 herm_product(const float2* __restrict__ wlo,
 
 // One warp: the inverse transform of job jb for row r; on return lane t,
 // slot s holds the products a (real part) and b (imaginary part) at
-// x1 = out_index(t, s).  Entries beyond the band limit kc are zero, so only
-// the slots of band class NZ are loaded and transformed in the first pass.
-template <int E, int NZ>
-__device__ __forceinline__ void row_fft_nz(const RowArgs& ra, const RowJob& jb, int r, int hz,
-                                           int h, int nslots_w, const float2* __restrict__ W,
-                                           const float2* __restrict__ F1f, const float2* s_tw2,
-                                           const float2* s_tw32, float* buf, int lane, int kc,
-                                           float2 (&v)[E]) {
+// x1 = out_index(t, s).
+template <int E>
+__device__ __forceinline__ void row_fft(const RowArgs& ra, const RowJob& jb, int r, int hz, int h,
+                                        int nslots_w, const float2* __restrict__ W,
+                                        const float2* __restrict__ F1f, const float2* s_tw2,
+                                        const float2* s_tw32, float* buf, int lane, int kc,
+                                        float2 (&v)[E]) {
   constexpr int N = 32 * E;
   const size_t rowstride = (size_t)ra.L1h;
   const float2* wa = W + (((size_t)jb.slot_a * nslots_w + hz) * ra.G0 + r) * rowstride;
@@ -439,35 +365,18 @@ __device__ __forceinline__ void row_fft_nz(const RowArgs& ra, const RowJob& jb, 
     const float2* fb = F1f + ((size_t)h * ra.npow + jb.pow_b) * N;
 #pragma unroll
     for (int s = 0; s < E; ++s) {
-      v[s] = make_float2(0.0f, 0.0f);
-      if (s < NZ || s >= E - NZ) {
-        const float2 pa =
-            herm_product<E>(wa + lane, fa + lane, wa + N - lane, fa + N - lane, s, lane, kc);
-        const float2 pb =
-            herm_product<E>(wb + lane, fb + lane, wb + N - lane, fb + N - lane, s, lane, kc);
-        v[s] = make_float2(pa.x - pb.y, pa.y + pb.x);
-      }
+      const float2 pa =
+          herm_product<E>(wa + lane, fa + lane, wa + N - lane, fa + N - lane, s, lane, kc);
+      const float2 pb =
+          herm_product<E>(wb + lane, fb + lane, wb + N - lane, fb + N - lane, s, lane, kc);
+      v[s] = make_float2(pa.x - pb.y, pa.y + pb.x);
     }
   } else {
 #pragma unroll
-    for (int s = 0; s < E; ++s) {
-      v[s] = make_float2(0.0f, 0.0f);
-      if (s < NZ || s >= E - NZ)
-        v[s] = herm_product<E>(wa + lane, fa + lane, wa + N - lane, fa + N - lane, s, lane, kc);
-    }
+    for (int s = 0; s < E; ++s)
+      v[s] = herm_product<E>(wa + lane, fa + lane, wa + N - lane, fa + N - lane, s, lane, kc);
   }
-  warp_ifft<E, NZ>(v, s_tw2, s_tw32, buf, lane);
-}
-
-// row_fft_nz for the band class of kc (uniform across the CTA).
-template <int E>
-__device__ __forceinline__ void row_fft(const RowArgs& ra, const RowJob& jb, int r, int hz, int h,
-                                        int nslots_w, const float2* __restrict__ W,
-                                        const float2* __restrict__ F1f, const float2* s_tw2,
-                                        const float2* s_tw32, float* buf, int lane, int kc,
-                                        float2 (&v)[E]) {
-  FLPR_BAND_CLASS(E, kc, (row_fft_nz<E, NZ>(ra, jb, r, hz, h, nslots_w, W, F1f, s_tw2, s_tw32,
-                                            buf, lane, kc, v)));
+  warp_ifft<E>(v, s_tw2, s_tw32, buf, lane);
 }
 
 // S pass: grid (ceil(G0 * njobs / 8), Hc); warp w takes item blockIdx.x*8+w =
@@ -509,15 +418,14 @@ rowpass_s_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
   }
 }
 
-// Shared memory of the T pass: twiddles, two transpose buffers per warp
+// Shared memory of the T pass: twiddles and two transpose buffers per warp
 // (rounds alternate between them; a warp's job leaves its two cropped
-// products there) and the row's solve vectors (nt doubles per grid point).
-__host__ __device__ inline size_t t_buf_bytes(int E, int nwarps) {
+// products there).
+inline size_t t_smem_bytes(int E, int nwarps, int njobs, int G1) {
+  (void)njobs;
+  (void)G1;
   return sizeof(float2) * (size_t)twiddle_entries(32 * E) +
          sizeof(float) * (size_t)2 * nwarps * warp_buf_stride(E);
-}
-inline size_t t_smem_bytes(int E, int nwarps, int nt, int G1) {
-  return ((t_buf_bytes(E, nwarps) + 15) & ~(size_t)15) + sizeof(double) * (size_t)nt * G1;
 }
 
 // Warps of a T-pass CTA: rounds of kTWarps jobs, or one round when there
@@ -525,43 +433,37 @@ inline size_t t_smem_bytes(int E, int nwarps, int nt, int G1) {
 // an SM (16 warps; six-warp CTAs are allocated as eight warps, two CTAs).
 inline int t_warps(int njobs) { return njobs < kTWarps ? njobs : kTWarps; }
 
-// T pass fused with the solve and the dual-form reductions: grid (G0, Hc),
-// t_warps(njobs) warps.  First the row's solve vectors z = (S + lam I)^-1 e1
-// (order 0: 1 / max(s, max(s) reg)) go to shared memory from the S planes
-// (ns, H, M).  Product p = c * NT + i is half p % 2 of job p / 2.  In round
-// k the warps compute jobs k * nwarps + w, each leaving its two cropped
-// products in its buffer of parity k % 2; then, for the channels completed
-// in that round, m_c(x1) = sum_i z_i(x1) T(p, x1), the response fits go to
-// `my`, and sum_x1 m_c Q_c accumulates into one partial per (c, h, row).  A
-// channel's NT products span at most two consecutive rounds
-// (NT <= 2 nwarps + 1), so the buffers of the previous round still hold its
-// earlier products.
+// T pass fused with the solve and the dual-form reductions: grid (Hc, G0),
+// t_warps(njobs) warps.  Product p = c * NT + i is half p % 2 of job p / 2.
+// In round k the warps compute jobs k * nwarps + w, each leaving its two
+// cropped products in its buffer of parity k % 2; then, for the channels
+// completed in that round, m_c(x1) = sum_i z_i(x1) T(p, x1) with z the row's
+// solve vectors, the response fits go to `my`, and sum_x1 m_c Q_c
+// accumulates into one partial per (c, h, row).  A channel's NT products
+// span at most two consecutive rounds (NT <= 2 nwarps + 1), so the buffers
+// of the previous round still hold its earlier products.
 template <int E, int NT>
 __global__ void __maxnreg__(112)
 rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
                        const float2* __restrict__ F1f, const float2* __restrict__ tab,
-                       const int* __restrict__ kcut1, int C, int ny, int order,
-                       const float* __restrict__ S, const double* __restrict__ scalar, double reg,
+                       const int* __restrict__ kcut1, int C, int ny, const double* __restrict__ zg,
                        const double* __restrict__ Q, double* __restrict__ my,
                        double* __restrict__ dpart) {
   constexpr int N = 32 * E;
   constexpr int SW = warp_buf_stride(E);
-  constexpr int NS = NT * (NT + 1) / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double red[kTWarps * 32];
   float2* s_tw2 = reinterpret_cast<float2*>(smem_raw);
   float2* s_tw32 = s_tw2 + N;
   float* bufs = reinterpret_cast<float*>(s_tw2 + twiddle_entries(N));
   const int nwarps = blockDim.x >> 5;
-  double* zs = reinterpret_cast<double*>(smem_raw + ((t_buf_bytes(E, nwarps) + 15) & ~(size_t)15));
-  // row fastest: the CTAs resident on an SM share the bandwidth's factor
-  // rows (in L1) and its band class (the same instructions)
-  const int r = blockIdx.x, hz = blockIdx.y, h = ra.hbase + hz;
+  // bandwidth fastest: the CTAs of one row (sharing its deposits Q) run together
+  const int hz = blockIdx.x, r = blockIdx.y, h = ra.hbase + hz;
   const int64_t M = (int64_t)ra.G0 * ra.G1;
   const int G1 = ra.G1, njobs = ra.njobs;
   {
-    // start every W row this row's jobs read (up to the band limit) on its
-    // way into L2 before the first transform
+    // start every W row this row's jobs read (up to the band limit) and the
+    // row's solve vectors on their way into L2 before the first transform
     const int lines = ((kcut1[h] + 1) * (int)sizeof(float2) + 127) / 128;
     const int per_job = 2 * lines;
     for (int t = threadIdx.x; t < njobs * per_job; t += blockDim.x) {
@@ -573,30 +475,12 @@ rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict
           W + (((size_t)slot * nslots_w + hz) * ra.G0 + r) * (size_t)ra.L1h);
       asm volatile("prefetch.global.L2 [%0];" ::"l"(row + 128 * l));
     }
+    const char* zr = reinterpret_cast<const char*>(zg + ((int64_t)h * M + (int64_t)r * G1) * NT);
+    const int zl = (G1 * NT * (int)sizeof(double) + 127) / 128;
+    for (int l = threadIdx.x; l < zl; l += blockDim.x)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(zr + 128 * l));
   }
   load_twiddles<E>(s_tw2, tab);
-  {
-    const int64_t HM = (int64_t)H * M;
-    const int64_t t0 = (int64_t)h * M + (int64_t)r * G1;
-    for (int x = threadIdx.x; x < G1; x += blockDim.x) {
-      double zz[NT];
-      if (order == 0) {
-        const double thr = scalar[0] * reg;
-        const double sv = (double)S[t0 + x];
-        zz[0] = 1.0 / (sv > thr ? sv : thr);
-      } else {
-        double Ap[NS];
-#pragma unroll
-        for (int k = 0; k < NS; ++k) Ap[k] = (double)S[(int64_t)k * HM + t0 + x];
-        if (!solve_e1_fixed<NT>(Ap, scalar[0], zz)) {
-#pragma unroll
-          for (int i = 0; i < NT; ++i) zz[i] = NAN;
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < NT; ++i) zs[x * NT + i] = zz[i];
-    }
-  }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int kc = kcut1[h];
@@ -632,7 +516,7 @@ rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict
       double acc = 0.0;
       for (int x = threadIdx.x; x < G1; x += blockDim.x) {
         const int64_t g = (int64_t)r * G1 + x;
-        const double* z = zs + x * NT;
+        const double* z = zg + ((int64_t)h * M + g) * NT;
         double m = 0.0;
 #pragma unroll
         for (int i = 0; i < NT; ++i) m += z[i] * (double)src[i][x];
@@ -687,12 +571,12 @@ static size_t warp_pass_smem(int E, int nwarps) {
 
 template <int E>
 static int launch_col(const ColArgs& ca, int ncolblk, int nslots, int Hc, const float2* Yt,
-                      const float2* F0f, const float2* tab, const int* kcut0, const int* kcut1,
-                      float2* W, cudaStream_t s) {
+                      const float2* F0f, const float2* tab, const int* kcut1, float2* W,
+                      cudaStream_t s) {
   const size_t smem = warp_pass_smem(E, kColWarps);
   FLPR_TRY(set_smem(colpass_kernel<E>, smem, kColWarps * 32));
   colpass_kernel<E><<<dim3(ncolblk, nslots, Hc), kColWarps * 32, smem, s>>>(ca, Yt, F0f, tab,
-                                                                          kcut0, kcut1, W);
+                                                                          kcut1, W);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
@@ -710,39 +594,28 @@ static int launch_row_s(const RowArgs& ra, int Hc, int H, int nslots_w, const fl
   return FLPR_OK;
 }
 
-// Arguments of the T pass's solve and reductions.
-struct TSolveArgs {
-  int C, ny, order;
-  const float* S;
-  const double* scalar;
-  double reg;
-  const double* Q;
-  double* my;
-  double* dpart;
-};
-
 template <int E, int NT>
 static int launch_row_t_nt(const RowArgs& ra, int Hc, int H, int nslots_w, const float2* W,
-                           const float2* F1f, const float2* tab, const int* kcut1,
-                           const TSolveArgs& ta, cudaStream_t s) {
+                           const float2* F1f, const float2* tab, const int* kcut1, int C, int ny,
+                           const double* z, const double* Q, double* my, double* dpart,
+                           cudaStream_t s) {
   const int nwarps = t_warps(ra.njobs);
-  const size_t smem = t_smem_bytes(E, nwarps, NT, ra.G1);
+  const size_t smem = t_smem_bytes(E, nwarps, ra.njobs, ra.G1);
   FLPR_TRY(set_smem(rowpass_t_solve_kernel<E, NT>, smem, nwarps * 32));
-  rowpass_t_solve_kernel<E, NT><<<dim3(ra.G0, Hc), nwarps * 32, smem, s>>>(
-      ra, H, nslots_w, W, F1f, tab, kcut1, ta.C, ta.ny, ta.order, ta.S, ta.scalar, ta.reg, ta.Q,
-      ta.my, ta.dpart);
+  rowpass_t_solve_kernel<E, NT><<<dim3(Hc, ra.G0), nwarps * 32, smem, s>>>(
+      ra, H, nslots_w, W, F1f, tab, kcut1, C, ny, z, Q, my, dpart);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;
 }
 
 template <int E>
 static int launch_row_t(int nt, const RowArgs& ra, int Hc, int H, int nslots_w, const float2* W,
-                        const float2* F1f, const float2* tab, const int* kc, const TSolveArgs& ta,
-                        cudaStream_t s) {
+                        const float2* F1f, const float2* tab, const int* kc, int C, int ny,
+                        const double* z, const double* Q, double* my, double* dp, cudaStream_t s) {
   switch (nt) {
-    case 1: return launch_row_t_nt<E, 1>(ra, Hc, H, nslots_w, W, F1f, tab, kc, ta, s);
-    case 3: return launch_row_t_nt<E, 3>(ra, Hc, H, nslots_w, W, F1f, tab, kc, ta, s);
-    case 6: return launch_row_t_nt<E, 6>(ra, Hc, H, nslots_w, W, F1f, tab, kc, ta, s);
+    case 1: return launch_row_t_nt<E, 1>(ra, Hc, H, nslots_w, W, F1f, tab, kc, C, ny, z, Q, my, dp, s);
+    case 3: return launch_row_t_nt<E, 3>(ra, Hc, H, nslots_w, W, F1f, tab, kc, C, ny, z, Q, my, dp, s);
+    case 6: return launch_row_t_nt<E, 6>(ra, Hc, H, nslots_w, W, F1f, tab, kc, C, ny, z, Q, my, dp, s);
     default: set_error("fused2d: nt=%d", nt); return FLPR_ERR_ARG;
   }
 }
@@ -900,7 +773,7 @@ static int fused_geom(const int* G, const int* L, const int* qout, int H, const 
 // Workspace carve-up, shared by the size query and the run.
 struct FusedBuffers {
   float2 *Yt, *W, *tab0, *tab1, *Ff;
-  double* dpart;
+  double *z, *dpart;
   int* kcut;
 };
 
@@ -912,6 +785,7 @@ static void carve(A& ar, const FusedTables& tb, const FusedGeom& fg, int H, int 
   b->tab0 = ar.template take<float2>(twiddle_entries(fg.L0));
   b->tab1 = ar.template take<float2>(twiddle_entries(fg.L1));
   b->Ff = ar.template take<float2>((size_t)H * npow * (fg.L0 + fg.L1));
+  b->z = ar.template take<double>((size_t)H * fg.M * tb.nt);
   b->dpart = ar.template take<double>((size_t)C * H * fg.G0);
   b->kcut = ar.template take<int>(2 * (size_t)H);
 }
@@ -961,12 +835,23 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
     const int hc = H - h0 < fg.Hc_s ? H - h0 : fg.Hc_s;
     ca.hbase = h0;
     ra.hbase = h0;
-    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.s_nslots, hc, b.Yt, F0f, b.tab0, b.kcut, kcut1, b.W,
-                              s));
+    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.s_nslots, hc, b.Yt, F0f, b.tab0, kcut1, b.W, s));
     FLPR_TRY(launch_row_s<E1>(ra, hc, H, hc, b.W, F1f, b.tab1, kcut1, S, s));
   }
   FLPR_TRY(global_scalar(order, nt, H, fg.M, S, scalar, FLPR_PREC_F32, s));
   FLPR_TRY(scalar_floor(scalar, scalar_floor_in, s));
+  {
+    const int64_t HM = (int64_t)H * fg.M;
+    int nb = (int)((HM + 255) / 256);
+    if (nb > 16 * sm_count()) nb = 16 * sm_count();
+    switch (nt) {
+      case 1: zvec_kernel<1><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, b.z); break;
+      case 3: zvec_kernel<3><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, b.z); break;
+      case 6: zvec_kernel<6><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, b.z); break;
+      default: set_error("fused2d: nt=%d", nt); return FLPR_ERR_ARG;
+    }
+    FLPR_LAUNCH_CHECK();
+  }
   // T pass fused with the solve
   ca = tb.t_col;
   ca.L0 = fg.L0;
@@ -986,10 +871,9 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
     const int hc = H - h0 < fg.Hc_t ? H - h0 : fg.Hc_t;
     ca.hbase = h0;
     ra.hbase = h0;
-    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.t_nslots, hc, b.Yt, F0f, b.tab0, b.kcut, kcut1, b.W,
-                              s));
-    const TSolveArgs ta{C, ny, order, S, scalar, reg, Q, my, b.dpart};
-    FLPR_TRY(launch_row_t<E1>(nt, ra, hc, H, hc, b.W, F1f, b.tab1, kcut1, ta, s));
+    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.t_nslots, hc, b.Yt, F0f, b.tab0, kcut1, b.W, s));
+    FLPR_TRY(launch_row_t<E1>(nt, ra, hc, H, hc, b.W, F1f, b.tab1, kcut1, C, ny, b.z, Q, my,
+                              b.dpart, s));
   }
   dots_reduce_kernel<<<C * H, 256, 0, s>>>(C * H, fg.G0, b.dpart, dots);
   FLPR_LAUNCH_CHECK();
@@ -1034,7 +918,7 @@ int fused2d_check(const int* G, const int* L, const int* qout, int H, int order,
   FLPR_CHECK_ARG(order >= 0 && order <= 2 && C >= 1 && C <= 32 && H >= 1, "fused2d: order/C/H");
   FLPR_CHECK_ARG(build_tables(order, C, tb) == FLPR_OK, "fused2d: too many slots or jobs");
   const int nwarps = t_warps(tb->t_row.njobs);
-  FLPR_CHECK_ARG(t_smem_bytes(L[1] / 32, nwarps, tb->nt, G[1]) <= kMaxSmem,
+  FLPR_CHECK_ARG(t_smem_bytes(L[1] / 32, nwarps, tb->t_row.njobs, G[1]) <= kMaxSmem,
                  "fused2d: T row tile does not fit shared memory");
   // a channel's products span at most two consecutive T rounds
   FLPR_CHECK_ARG(tb->t_row.njobs <= kTWarps || tb->nt <= 2 * kTWarps + 1,
