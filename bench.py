@@ -657,6 +657,65 @@ def run_profile_case(args, dev):
             "h": [float(v) for v in np.atleast_1d(r.h)]}
 
 
+def mlp_timing(dev, reps: int = 200) -> dict:
+    """Forward pass of the trained proposal network on batches of 1 and
+    1024 rows: the one-launch tensor-core kernel (flpr_mlp_infer:
+    tcgen05.mma, accumulators in tensor memory) beside the layer-by-layer
+    kernels (flpr_mlp_fwd: mma.sync), each the mean of `reps` launches
+    timed with CUDA events on the launching stream after warm-up."""
+    import torch
+    from fastlpr_b200 import _lib
+    from fastlpr_b200 import learned as _learned
+    lib = _lib.load()
+    model = _learned.default_model(dev)
+    dims = [int(v) for v in model.dims]
+    flops_row = 2.0 * sum(dims[i] * dims[i + 1] for i in range(len(dims) - 1))
+    stream = torch.cuda.current_stream(dev)
+    out = {"dims": dims, "flops_per_row": flops_row}
+    fused_ok = bool(lib.flpr_mlp_infer_supported(model.nl, model._dims_c))
+    for rows in (1, 1024):
+        x16 = torch.randn((rows, dims[0]), device=dev).to(torch.bfloat16)
+        y = torch.empty(rows, dtype=torch.float32, device=dev)
+        y2 = torch.empty((rows, 1), dtype=torch.float32, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        ws = torch.empty(lib.flpr_mlp_ws(model.nl, model._dims_c, rows), dtype=torch.uint8,
+                         device=dev)
+
+        def tc():
+            _lib.check(lib.flpr_mlp_infer(model.nl, model._dims_c, model.p16.data_ptr(),
+                                          model.p32.data_ptr(), rows, x16.data_ptr(),
+                                          y.data_ptr(), status.data_ptr(), stream.cuda_stream),
+                       "flpr_mlp_infer")
+
+        def layers():
+            _lib.check(lib.flpr_mlp_fwd(model.nl, model._dims_c, model.p16.data_ptr(),
+                                        model.p32.data_ptr(), rows, x16.data_ptr(),
+                                        y2.data_ptr(), ws.data_ptr(), ws.numel(),
+                                        stream.cuda_stream), "flpr_mlp_fwd")
+
+        rec = {}
+        for name, fn in (("tcgen05_one_launch", tc), ("mma_sync_layers", layers)):
+            if name == "tcgen05_one_launch" and not fused_ok:
+                continue
+            for _ in range(10):
+                fn()
+            torch.cuda.synchronize(dev)
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            for _ in range(reps):
+                fn()
+            e.record(stream)
+            e.synchronize()
+            us = 1000.0 * s.elapsed_time(e) / reps
+            rec[name] = {"us": us, "tflops": flops_row * rows / (us * 1e-6) / 1e12}
+        if fused_ok:
+            torch.cuda.synchronize(dev)
+            rec["status_ok"] = int(status.item()) == 0
+        out[f"rows_{rows}"] = rec
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -784,6 +843,7 @@ def run_ours(args):
             "yhat_max_rel_diff_vs_full_sweep": float(
                 np.max(np.abs(lr_r.yhat - full_r.yhat)) / np.max(np.abs(full_r.yhat))),
         }
+        learned["network_inference"] = mlp_timing(dev)
     elif not have_net:
         learned = {"unavailable": "no trained bandwidth network (fastlpr_b200/data/bandwidth_mlp.npz)"}
 
