@@ -2,20 +2,33 @@
 // tensor cores (tcgen05, sm_100a).
 //
 // The network h_{l+1} = relu(h_l W_l^T + b_l) with hidden width 256 and one
-// output runs in ONE launch: a CTA of four warps takes 128 rows of the batch
-// (the UMMA M), keeps their activations in shared memory as the A operand of
-// the next layer (BF16, K-major, 128-byte swizzle) and accumulates every
-// layer's 128 x 256 product in tensor memory (256 FP32 columns).  Weights
-// stream through a ring of three 64-deep K chunks (256 rows x 128 bytes
-// each) loaded with cp.async; one elected thread issues the tcgen05.mma
-// instructions (M = 128, N = 256, K = 16, BF16 x BF16 -> FP32) and commits
-// them to a per-stage mbarrier.  The epilogue of each layer reads the
-// accumulator with tcgen05.ld (each warp its 32 TMEM lanes = rows), adds the
-// FP32 bias, applies the ReLU and rounds to BF16 into the next A operand;
-// the last layer (one output) is a dot product of the last hidden row with
-// the output weights in registers.  Every wait on an mbarrier is bounded:
-// on expiry the CTA records FLPR_ERR_TIMEOUT in the status word, waits for
-// its own copies, frees its tensor memory and returns.
+// output runs in ONE launch: a CTA takes 128 rows of the batch (the UMMA M),
+// keeps their activations in shared memory as the A operand of the next
+// layer (BF16, K-major, 128-byte swizzle) and accumulates every layer's
+// 128 x 256 product in tensor memory (256 FP32 columns).  The CTA is warp
+// specialised:
+//   - warp 4 (one lane) streams the weights through a ring of three 64-deep
+//     K chunks (256 rows x 128 bytes) with tensor-map copies
+//     (cp.async.bulk.tensor, 128-byte swizzle: the copy engine writes the
+//     UMMA operand layout itself, columns of W beyond its K read as zero),
+//     and the 128 input rows the same way;
+//   - warp 5 (one lane) issues the tcgen05.mma instructions (M = 128,
+//     N = 256, K = 16, BF16 x BF16 -> FP32) as soon as a chunk has landed,
+//     committing each chunk to its stage's "empty" barrier (the producer
+//     refills the stage after it) and each layer's last chunk to the
+//     accumulator barrier;
+//   - warps 0-3 (one per 32 TMEM lanes = rows) run each layer's epilogue:
+//     tcgen05.ld of the accumulator, FP32 bias (cached in shared memory),
+//     ReLU and rounding to BF16 into the next layer's A operand, then one
+//     arrival each on the "A ready" barrier the next layer's first MMA waits
+//     on; the last layer (one output) is a dot product of the last hidden
+//     row with the output weights in registers.
+// The weights of the next layer stream in while the epilogue runs.  Every
+// wait on an mbarrier is bounded: on expiry the CTA records
+// FLPR_ERR_TIMEOUT in the status word, the producer waits (bounded) for its
+// copies in flight, the MMA issuer for its products, and the tensor memory
+// is freed before the CTA returns.
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -28,7 +41,10 @@ constexpr int kHid = 256;                // hidden width (UMMA N)
 constexpr int kKC = 64;                  // K elements per chunk: one 128-byte swizzle row
 constexpr int kMaxInChunks = 7;          // input width <= 448
 constexpr int kStages = 3;               // weight chunk ring
-constexpr int kThreads = 128;            // four warps: one per 32 TMEM lanes
+constexpr int kEpiWarps = 4;             // warps 0-3: TMEM lanes 0-127
+constexpr int kProdWarp = 4;             // tensor-map copies
+constexpr int kMmaWarp = 5;              // tcgen05.mma issue
+constexpr int kThreads = 32 * 6;
 constexpr int kMaxLayersTc = 8;
 constexpr int kAChunk = kTM * 128;       // 16 KB
 constexpr int kBChunk = kHid * 128;      // 32 KB
@@ -40,22 +56,24 @@ constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) |
                             ((uint32_t)(kHid >> 3) << 17) | ((uint32_t)(kTM >> 4) << 24);
 
 struct TcArgs {
+  CUtensorMap tm_w[kMaxLayersTc];  // W_l (K_l columns x 256 rows), boxes of 64 x 256
+  CUtensorMap tm_x;                // inputs (K_0 columns x batch rows), boxes of 64 x 128
   int nlayers;
   int dims[kMaxLayersTc + 1];
-  int64_t w_off[kMaxLayersTc];   // BF16 element offsets of W_l in the packed parameters
-  int64_t b_off[kMaxLayersTc];   // FP32 element offsets of b_l
-  int nchunks[kMaxLayersTc];     // K chunks of each hidden layer
+  int64_t w_off[kMaxLayersTc];     // BF16 element offsets of W_l in the packed parameters
+  int64_t b_off[kMaxLayersTc];     // FP32 element offsets of b_l
+  int nchunks[kMaxLayersTc];       // K chunks of each hidden layer
   int total_chunks;
   int batch;
   const __nv_bfloat16* p16;
   const float* p32;
-  const __nv_bfloat16* x16;
   float* out;
   int* status;
 };
 
 // byte offset of (row, 16-byte column c16) in a K-major 128-byte-swizzled
 // tile: 8-row groups 1024 bytes apart, the 16-byte column XORed with row % 8
+// (the layout the tensor-map copies with 128-byte swizzle write)
 __device__ __forceinline__ uint32_t sw128(int row, int c16) {
   return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((c16 ^ (row & 7)) << 4));
 }
@@ -76,21 +94,6 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_wait_pending(int n) {
-  // wait until at most n groups of this thread are pending (n < kStages)
-  switch (n) {
-    case 0: asm volatile("cp.async.wait_group 0;\n" ::: "memory"); break;
-    case 1: asm volatile("cp.async.wait_group 1;\n" ::: "memory"); break;
-    default: asm volatile("cp.async.wait_group 2;\n" ::: "memory"); break;
-  }
-}
 __device__ __forceinline__ void fence_async_shared() {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
@@ -106,8 +109,25 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
                : "memory");
 }
 
-// bounded wait for the given phase parity of an mbarrier
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\t"
+      "mbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\t"
+      "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}\n" ::"r"(smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+// bounded wait for the given phase parity of an mbarrier; gives up early
+// when another role of the CTA has given up (abort flag)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          const volatile int* abort_flag) {
   const uint32_t a = smem_u32(bar);
   for (uint32_t it = 0; it < kSpinLimit; ++it) {
     uint32_t done;
@@ -119,8 +139,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((it & 1023u) == 1023u && *abort_flag) return false;
   }
   return false;
+}
+
+// 2-D tensor-map copy of one box into shared memory, completing on `bar`
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* tm, int c0, int c1,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      : "memory");
 }
 
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db,
@@ -142,9 +173,9 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
       : "memory");
 }
 
-// 16 consecutive FP32 accumulator columns of this thread's TMEM lane
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
+// 16 consecutive FP32 accumulator columns of this thread's TMEM lane (no
+// wait: the caller issues tcgen05.wait::ld before using them)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
       "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
@@ -152,9 +183,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
         "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // the global chunk sequence: layer of chunk j and its K index within the layer
@@ -168,40 +199,47 @@ __device__ __forceinline__ void chunk_of(const TcArgs& a, int j, int* layer, int
   *kc = j;
 }
 
-// issue the cp.async copies of weight chunk j into ring stage s (rows of
-// W_l beyond its K are zero-filled)
-__device__ __forceinline__ void load_w_chunk(const TcArgs& a, int j, uint32_t sB) {
-  int l, kc;
-  chunk_of(a, j, &l, &kc);
-  const int K = a.dims[l];
-  const __nv_bfloat16* W = a.p16 + a.w_off[l];
-  for (int v = threadIdx.x; v < kHid * 8; v += kThreads) {
-    const int n = v >> 3, c16 = v & 7;
-    const int k = kc * kKC + c16 * 8;
-    const int bytes = k < K ? 16 : 0;   // K is a multiple of 8
-    cp_async16(sB + sw128(n, c16), bytes ? (const void*)(W + (int64_t)n * K + k) : (const void*)W,
-               bytes);
-  }
-}
-
-__global__ void __launch_bounds__(kThreads, 1) mlp_infer_tc_kernel(TcArgs a) {
+__global__ void __launch_bounds__(kThreads, 1)
+    mlp_infer_tc_kernel(const __grid_constant__ TcArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  // 1024-aligned operand region: A chunks, then the B ring
+  // 1024-aligned operand region: A chunks, then the B ring, then barriers
+  // and the FP32 bias / output-weight cache
   const uint32_t base_u32 = smem_u32(smem_raw);
   const uint32_t pad = (1024u - (base_u32 & 1023u)) & 1023u;
   unsigned char* smem = smem_raw + pad;
   const uint32_t sA = base_u32 + pad;
   const uint32_t sB = sA + kMaxInChunks * kAChunk;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kMaxInChunks * kAChunk + kStages * kBChunk);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kStages);
-  __shared__ int s_abort;
+  uint64_t* full = bars;                      // [kStages] chunk landed
+  uint64_t* empty = bars + kStages;           // [kStages] chunk's products done
+  uint64_t* in_full = bars + 2 * kStages;     // input rows landed
+  uint64_t* acc_full = in_full + 1;           // a layer's accumulator complete
+  uint64_t* a_ready = in_full + 2;            // next A operand written, accumulator read
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(in_full + 3);
+  float* s_bias = reinterpret_cast<float*>(tmem_slot + 4);   // [nlayers - 1][256]
+  float* s_wout = s_bias + (kMaxLayersTc - 1) * kHid;         // [256]
+  __shared__ volatile int s_abort;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row0 = blockIdx.x * kTM;
+  const int nhid = a.nlayers - 1;  // layers with 256 outputs
   if (threadIdx.x == 0) {
     s_abort = 0;
-    for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(in_full, 1);
+    mbar_init(acc_full, 1);
+    mbar_init(a_ready, kEpiWarps * 32);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (threadIdx.x == kProdWarp * 32) {
+    asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&a.tm_x))
+                 : "memory");
+    for (int l = 0; l < nhid; ++l)
+      asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&a.tm_w[l]))
+                   : "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
@@ -210,104 +248,138 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_infer_tc_kernel(TcArgs a) {
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
-  // input rows of this CTA (zero beyond the batch and beyond K0), with the
-  // first weight chunk, as the first copy group
-  {
-    const int K0 = a.dims[0];
-    const int nc0 = a.nchunks[0];
-    for (int v = threadIdx.x; v < kTM * nc0 * 8; v += kThreads) {
-      const int kc = v / (kTM * 8), r = v % (kTM * 8);
-      const int m = r >> 3, c16 = r & 7;
-      const int k = kc * kKC + c16 * 8;
-      const int gm = row0 + m;
-      const int bytes = (gm < a.batch && k < K0) ? 16 : 0;
-      cp_async16(sA + kc * kAChunk + sw128(m, c16),
-                 bytes ? (const void*)(a.x16 + (int64_t)gm * K0 + k) : (const void*)a.x16, bytes);
+  if (warp < kEpiWarps) {
+    for (int i = threadIdx.x; i < nhid * kHid; i += kEpiWarps * 32) {
+      const int l = i / kHid, c = i - l * kHid;
+      s_bias[i] = a.p32[a.b_off[l] + c];
     }
-  }
-  int issued = 0;
-  for (; issued < kStages && issued < a.total_chunks; ++issued) {
-    load_w_chunk(a, issued, sB + (issued % kStages) * kBChunk);
-    cp_async_commit();
+    const __nv_bfloat16* wout = a.p16 + a.w_off[a.nlayers - 1];
+    for (int c = threadIdx.x; c < kHid; c += kEpiWarps * 32) s_wout[c] = __bfloat162float(wout[c]);
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  uint32_t phase[kStages] = {0u, 0u, 0u};
-  float acc_out = 0.0f;   // last-layer output of this thread's row
 
-  for (int j = 0; j < a.total_chunks; ++j) {
-    const int s = j % kStages;
-    int l, kc;
-    chunk_of(a, j, &l, &kc);
-    // chunk j (and, for j = 0, the input) has landed: this thread's copies,
-    // then everyone's through the barrier; the proxy fence makes the
-    // generic-proxy writes visible to the tensor core's reads
-    cp_async_wait_pending(issued - j - 1);
-    fence_async_shared();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      tc_fence_after();
-#pragma unroll
-      for (int kk = 0; kk < kKC / 16; ++kk) {
-        const uint64_t da = umma_desc(sA + kc * kAChunk + kk * 32);
-        const uint64_t db = umma_desc(sB + s * kBChunk + kk * 32);
-        umma_bf16(tmem, da, db, (kc > 0 || kk > 0) ? 1u : 0u);
+  if (warp == kProdWarp) {
+    if (lane == 0) {
+      // the 128 input rows (rows beyond the batch and columns beyond K_0
+      // read as zero), then the weight chunks in order, up to three ahead
+      mbar_expect_tx(in_full, (uint32_t)(a.nchunks[0] * kAChunk));
+      for (int kc = 0; kc < a.nchunks[0]; ++kc)
+        tma_load_2d(sA + kc * kAChunk, &a.tm_x, kc * kKC, row0, in_full);
+      int issued = 0;
+      for (int j = 0; j < a.total_chunks; ++j) {
+        const int s = j % kStages;
+        if (j >= kStages && !mbar_wait(&empty[s], (uint32_t)((j / kStages) - 1) & 1u, &s_abort)) {
+          s_abort = 1;
+          break;
+        }
+        int l, kc;
+        chunk_of(a, j, &l, &kc);
+        mbar_expect_tx(&full[s], (uint32_t)kBChunk);
+        tma_load_2d(sB + s * kBChunk, &a.tm_w[l], kc * kKC, 0, &full[s]);
+        issued = j + 1;
       }
-      umma_commit(&bars[s]);
+      // the copies in flight land before the CTA can leave
+      for (int j = issued - 1; j >= 0 && j >= issued - kStages; --j)
+        mbar_wait(&full[j % kStages], (uint32_t)(j / kStages) & 1u, &s_abort);
+      mbar_wait(in_full, 0u, &s_abort);
     }
-    // the products of chunk j are done: stage s is free and, after the
-    // layer's last chunk, the accumulator is complete
-    if (!mbar_wait(&bars[s], phase[s])) s_abort = 1;
-    phase[s] ^= 1u;
-    __syncthreads();
-    if (s_abort) break;
-    tc_fence_after();
-    if (kc == a.nchunks[l] - 1) {
-      const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-      const int m = warp * 32 + lane;
-      const float* bias = a.p32 + a.b_off[l];
-      const bool last_hidden = (l == a.nlayers - 2);
-      if (last_hidden) acc_out = a.p32[a.b_off[l + 1]];
-      const __nv_bfloat16* wout = a.p16 + a.w_off[a.nlayers - 1];
-      for (int c0 = 0; c0 < kHid; c0 += 16) {
-        float v[16];
-        tmem_ld16(trow + (uint32_t)c0, v);
-        __align__(16) __nv_bfloat16 h[16];
+  } else if (warp == kMmaWarp) {
+    if (lane == 0) {
+      int last = -1;
+      if (!mbar_wait(in_full, 0u, &s_abort)) {
+        s_abort = 1;
+      } else {
+        for (int j = 0; j < a.total_chunks; ++j) {
+          const int s = j % kStages;
+          int l, kc;
+          chunk_of(a, j, &l, &kc);
+          // a new layer reads the A operand and overwrites the accumulator
+          // the previous layer's epilogue was working on
+          if (kc == 0 && l > 0 && !mbar_wait(a_ready, (uint32_t)(l - 1) & 1u, &s_abort)) {
+            s_abort = 1;
+            break;
+          }
+          if (!mbar_wait(&full[s], (uint32_t)(j / kStages) & 1u, &s_abort)) {
+            s_abort = 1;
+            break;
+          }
+          tc_fence_after();
 #pragma unroll
-        for (int i = 0; i < 16; ++i) h[i] = __float2bfloat16_rn(fmaxf(v[i] + bias[c0 + i], 0.0f));
-        if (last_hidden) {
-#pragma unroll
-          for (int i = 0; i < 16; ++i)
-            acc_out += __bfloat162float(h[i]) * __bfloat162float(wout[c0 + i]);
-        } else {
-          // next layer's A operand: K index c0..c0+15 of row m
-          const int kcn = c0 / kKC, c16 = (c0 % kKC) / 8;
-          unsigned char* dst = smem + kcn * kAChunk;
-          *reinterpret_cast<uint4*>(dst + sw128(m, c16)) = *reinterpret_cast<const uint4*>(h);
-          *reinterpret_cast<uint4*>(dst + sw128(m, c16 + 1)) =
-              *reinterpret_cast<const uint4*>(h + 8);
+          for (int kk = 0; kk < kKC / 16; ++kk) {
+            const uint64_t da = umma_desc(sA + kc * kAChunk + kk * 32);
+            const uint64_t db = umma_desc(sB + s * kBChunk + kk * 32);
+            umma_bf16(tmem, da, db, (kc > 0 || kk > 0) ? 1u : 0u);
+          }
+          umma_commit(&empty[s]);
+          if (kc == a.nchunks[l] - 1) umma_commit(acc_full);
+          last = j;
         }
       }
-      tc_fence_before();
+      // every product issued is complete before the tensor memory is freed
+      if (last >= 0)
+        mbar_wait(&empty[last % kStages], (uint32_t)(last / kStages) & 1u, &s_abort);
     }
-    // refill stage s with chunk j + kStages
-    if (issued < a.total_chunks) {
-      load_w_chunk(a, issued, sB + (issued % kStages) * kBChunk);
-      ++issued;
+  } else {
+    // epilogue warps: warp w reads TMEM lanes 32 w .. 32 w + 31 (its rows)
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    const int m = warp * 32 + lane;
+    float acc_out = 0.0f;
+    bool ok = true;
+    for (int l = 0; l < nhid; ++l) {
+      if (!mbar_wait(acc_full, (uint32_t)l & 1u, &s_abort)) {
+        s_abort = 1;
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const float* bias = s_bias + l * kHid;
+      const bool last_hidden = (l == nhid - 1);
+      if (last_hidden) acc_out = a.p32[a.b_off[l + 1]];
+      for (int c0 = 0; c0 < kHid; c0 += 64) {
+        uint32_t r[4][16];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) tmem_ld16(trow + (uint32_t)(c0 + 16 * q), r[q]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          __align__(16) __nv_bfloat16 hv[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            hv[i] = __float2bfloat16_rn(
+                fmaxf(__uint_as_float(r[q][i]) + bias[c0 + 16 * q + i], 0.0f));
+          if (last_hidden) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              acc_out += __bfloat162float(hv[i]) * s_wout[c0 + 16 * q + i];
+          } else {
+            // next layer's A operand: chunk c0 / 64, 16-byte columns 2q, 2q + 1
+            unsigned char* dst = smem + (c0 / kKC) * kAChunk;
+            *reinterpret_cast<uint4*>(dst + sw128(m, 2 * q)) =
+                *reinterpret_cast<const uint4*>(hv);
+            *reinterpret_cast<uint4*>(dst + sw128(m, 2 * q + 1)) =
+                *reinterpret_cast<const uint4*>(hv + 8);
+          }
+        }
+      }
+      if (!last_hidden) {
+        // generic-proxy writes of the A operand, then the accumulator reads,
+        // ordered before the next layer's products
+        fence_async_shared();
+        tc_fence_before();
+        mbar_arrive(a_ready);
+      }
     }
-    cp_async_commit();   // (an empty group keeps the pending count uniform)
+    if (ok && !s_abort) {
+      const int gm = row0 + m;
+      if (gm < a.batch) a.out[gm] = acc_out;
+    }
   }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
   tc_fence_before();
   __syncthreads();
-  if (!s_abort) {
-    const int gm = row0 + warp * 32 + lane;
-    if (gm < a.batch) a.out[gm] = acc_out;
-  } else if (threadIdx.x == 0 && a.status != nullptr) {
-    atomicExch(a.status, FLPR_ERR_TIMEOUT);
-  }
+  if (s_abort && threadIdx.x == 0 && a.status != nullptr) atomicExch(a.status, FLPR_ERR_TIMEOUT);
   if (warp == 0) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
@@ -316,8 +388,47 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_infer_tc_kernel(TcArgs a) {
   }
 }
 
-constexpr size_t kTcSmem = (size_t)kMaxInChunks * kAChunk + (size_t)kStages * kBChunk +
-                           1024 /* alignment */ + kStages * sizeof(uint64_t) + 16;
+constexpr size_t kTcSmem = 1024 /* alignment */ + (size_t)kMaxInChunks * kAChunk +
+                           (size_t)kStages * kBChunk + (2 * kStages + 3) * sizeof(uint64_t) +
+                           4 * sizeof(uint32_t) + sizeof(float) * (size_t)kMaxLayersTc * kHid;
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static int encode_fn(EncodeTiledFn* out) {
+  static EncodeTiledFn fn = nullptr;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  if (fn == nullptr) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    FLPR_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    FLPR_CHECK_ARG(q == cudaDriverEntryPointSuccess && p != nullptr,
+                   "mlp_infer: driver entry point cuTensorMapEncodeTiled missing");
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  *out = fn;
+  return FLPR_OK;
+}
+
+// K-major BF16 matrix of `rows` rows and K columns (row stride K elements)
+// read in boxes of 64 columns x box_rows rows with the 128-byte swizzle;
+// entries outside the matrix read as zero
+static int encode_bf16_2d(EncodeTiledFn fn, CUtensorMap* tm, const void* base, int K, int rows,
+                          int box_rows) {
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)K * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)kKC, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = fn(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
+                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  FLPR_CHECK_ARG(r == CUDA_SUCCESS, "mlp_infer: cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return FLPR_OK;
+}
 
 }  // namespace
 }  // namespace flpr
@@ -352,7 +463,7 @@ int flpr_mlp_infer(int nlayers, const int* h_dims, const void* d_params16,
     off += (int64_t)h_dims[l] * h_dims[l + 1];
     a.b_off[l] = off;
     off += h_dims[l + 1];
-    // the operand copies move 16-byte vectors of the weight rows
+    // tensor maps start on 16-byte boundaries
     FLPR_CHECK_ARG(((uintptr_t)d_params16 + 2 * (uintptr_t)a.w_off[l]) % 16 == 0,
                    "mlp_infer: weights of layer %d not 16-byte aligned", l);
   }
@@ -362,10 +473,15 @@ int flpr_mlp_infer(int nlayers, const int* h_dims, const void* d_params16,
     a.nchunks[l] = (h_dims[l] + kKC - 1) / kKC;
     a.total_chunks += a.nchunks[l];
   }
+  EncodeTiledFn fn = nullptr;
+  FLPR_TRY(encode_fn(&fn));
+  const __nv_bfloat16* p16 = static_cast<const __nv_bfloat16*>(d_params16);
+  for (int l = 0; l < nlayers - 1; ++l)
+    FLPR_TRY(encode_bf16_2d(fn, &a.tm_w[l], p16 + a.w_off[l], h_dims[l], kHid, kHid));
+  FLPR_TRY(encode_bf16_2d(fn, &a.tm_x, d_x16, h_dims[0], batch, kTM));
   a.batch = batch;
-  a.p16 = static_cast<const __nv_bfloat16*>(d_params16);
+  a.p16 = p16;
   a.p32 = d_params32;
-  a.x16 = static_cast<const __nv_bfloat16*>(d_x16);
   a.out = d_out;
   a.status = d_status;
   FLPR_CUDA(cudaFuncSetAttribute(mlp_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
