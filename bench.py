@@ -261,8 +261,9 @@ def batched_sample(count: int = 16):
 def parity_hetero2d(dev, workers: int, full_sel: int = None):
     """2-D local-quadratic heteroscedastic configuration at full size
     (N = 2e6, grid 512^2) on a sample of its 32 bandwidths: the mean fit,
-    then the variance fit of the squared residuals, GPU (FP64, the order-2
-    default) against the oracle on identical inputs."""
+    then the variance fit of the squared residuals, GPU (default precision:
+    FP32 value channels, FP64 moment planes and solves) against the oracle
+    on identical inputs, each at the tolerance of the precision it ran in."""
     import fastlpr_b200
     import oracle
     x, y, h, o = config_workloads()["lpr2d_o2_hetero"]
@@ -275,9 +276,12 @@ def parity_hetero2d(dev, workers: int, full_sel: int = None):
     yv = (y - r.yhat) ** 2
     v = fastlpr_b200.cv_fastlpr(x, yv, hs, dict(opts, y_type_out="variance"))
     ov = oracle.cv_fastlpr(x, yv, hs, dict(o, y_type_out="variance"), workers=workers)
-    return {"mean": lpr_parity(r, om, TOL["fp64"]), "variance": lpr_parity(v, ov, TOL["fp64"]),
+    return {"mean": lpr_parity(r, om, TOL[r.metadata["precision"]]),
+            "variance": lpr_parity(v, ov, TOL[v.metadata["precision"]]),
             "bandwidths": [int(i) for i in hetero_bandwidth_sample(len(h), full_sel)],
-            "points": int(x.shape[0]), "precision": "fp64"}
+            "points": int(x.shape[0]), "precision": r.metadata["precision"],
+            "moment_planes": r.metadata.get("moment_planes"),
+            "fp64_bandwidths": int(r.metadata.get("fp64_bandwidths", 0))}
 
 
 def parity_lpr1d(dev, workers: int):

@@ -38,6 +38,7 @@ SIGNATURES = [
     ("flpr_spread_dkmap", _I, [_I, _I64, _VP, _VP, _PD, _PI, _I, _PD, _I, _I, _PVP, _VP, _I, _VP,
                                _SZ, _VP]),
     ("flpr_spread_grid64", _I, [_I, _I64, _PI, _I, _I, _VP, _SZ, _VP, _VP]),
+    ("flpr_spread_grid64_channels", _I, [_I, _I64, _PI, _I, _I, _I, _VP, _SZ, _VP, _VP]),
     ("flpr_knot_map", _I, [_I, _I64, _VP, _PD, _PD, _PD, _VP, _VP]),
     ("flpr_forward_fft_ws", _SZ, [_VP, _I, _PI, _I, _I]),
     ("flpr_forward_fft", _I, [_VP, _I, _PI, _I, _VP, _VP, _I, _VP, _SZ, _VP]),
@@ -74,6 +75,8 @@ SIGNATURES = [
                               _VP, _VP, _VP, _SZ, _VP]),
     ("flpr_lpr2d_fused_floor", _I, [_PI, _PI, _PI, _I, _I, _I, _I, _I, _VP, _VP, _D, _VP, _D,
                                     _VP, _VP, _VP, _VP, _VP, _VP, _SZ, _VP]),
+    ("flpr_lpr2d_fused_t", _I, [_PI, _PI, _PI, _I, _I, _I, _I, _I, _VP, _VP, _D, _VP, _D, _VP,
+                                _VP, _VP, _VP, _VP, _SZ, _VP]),
     ("flpr_interp_reduce_ws", _SZ, [_I64, _I, _I, _I]),
     ("flpr_interp_reduce", _I, [_I, _I64, _VP, _PD, _PI, _I, _I, _I, _VP, _PVP, _PVP, _VP, _VP,
                                 _VP, _VP, _SZ, _VP]),

@@ -623,15 +623,18 @@ def _node0_cells(geom) -> List[int]:
     return out
 
 
-def _grid64(ctx: _Ctx, kept: dict) -> torch.Tensor:
-    """(C, cells) FP64 grid from the exact fixed-point sums of an FP32 spread
-    (flpr_spread_grid64; `kept` from _spread_fft)."""
+def _grid64(ctx: _Ctx, kept: dict, nout: Optional[int] = None) -> torch.Tensor:
+    """(nout, cells) FP64 grid of the first nout channels (default all) from
+    the exact fixed-point sums of an FP32 spread (flpr_spread_grid64_channels;
+    `kept` from _spread_fft)."""
     cells = int(np.prod(kept["L"]))
-    out = ctx.empty((kept["C"], cells))
+    nout = kept["C"] if nout is None else int(nout)
+    out = ctx.empty((nout, cells))
     ws = kept["ws"]
-    ctx.check(ctx.lib.flpr_spread_grid64(kept["d"], kept["n"], _lib.ivec(kept["L"]), kept["msp"],
-                                         kept["C"], ws.data_ptr(), ws.numel(), out.data_ptr(),
-                                         ctx.stream), "flpr_spread_grid64")
+    ctx.check(ctx.lib.flpr_spread_grid64_channels(kept["d"], kept["n"], _lib.ivec(kept["L"]),
+                                                  kept["msp"], kept["C"], nout, ws.data_ptr(),
+                                                  ws.numel(), out.data_ptr(), ctx.stream),
+              "flpr_spread_grid64_channels")
     return out
 
 
@@ -713,14 +716,24 @@ def _conv(ctx: _Ctx, geom: _Geom, spec, kern: _Kernel, prods, prec: int, add_eps
     return out
 
 
-def _precision(opts) -> int:
+def _precision(opts, dims: Optional[int] = None) -> int:
     p = opts.get("precision", None)
     if p is None:
         # The reference grids are complex64 below accuracy 5 (type_utils.py:158-168).
-        # Local-quadratic (order 2) moment systems are ill-conditioned when h
-        # approaches the grid spacing: FP32 S or T planes then lose ~1e-2 in m,
-        # so order 2 keeps its grids in FP64 by default.
-        if int(opts["accuracy"]) < 5 and int(opts.get("order", 0)) < 2:
+        # Local-quadratic (order 2) moment systems are ill-conditioned: FP32 S
+        # planes lose ~1e-5 in m at the largest bandwidths and ~1e-2 where h
+        # approaches the grid spacing.  In 2-D with the full sweep and DoF,
+        # order-2 mean fits run the FP32 path with their moment planes in FP64
+        # (formed from the exact FP64 grid of the fixed-point spread) and the
+        # sparse bandwidths wholly in FP64 (_evaluate_device).  Variance fits
+        # return exp(m) of a log response (|m| ~ 5-10), so their relative
+        # error is the absolute error of m: FP32 value channels would give
+        # ~4e-5; they, and order 2 elsewhere, keep their grids in FP64.
+        order = int(opts.get("order", 0))
+        if int(opts["accuracy"]) < 5 and (
+                order < 2 or (dims == 2 and bool(opts.get("calc_dof", True))
+                              and str(opts.get("bandwidth_search", "full")) != "learned"
+                              and str(opts.get("y_type_out", "mean")) != "variance")):
             return _lib.FLPR_PREC_F32
         return _lib.FLPR_PREC_F64
     p = str(p).lower()
@@ -848,7 +861,7 @@ def _lpr_setup(x, y, h, options) -> _LprSetup:
     if variance and y_is_complex:
         raise NotImplementedError("variance mode needs a real response")
     _check_interp_methods(opts, dims, n)
-    prec = _precision(opts)
+    prec = _precision(opts, dims)
     return _LprSetup(x_arr=x_arr, y_arr=y_arr, dy=dy, bandwidths=bandwidths, opts=opts,
                      order=order, prec=prec, variance=variance, y_is_complex=y_is_complex,
                      n=n, d=dims)
@@ -919,7 +932,7 @@ def cv_fastlpr_device(x: torch.Tensor, y: torch.Tensor, h=None,
     _check_supported(dims, opts)
     if str(opts.get("y_type_out", "mean")) == "variance":
         raise NotImplementedError("variance mode: use cv_fastlpr")
-    prec = _precision(opts)
+    prec = _precision(opts, dims)
     ctx = _Ctx(x.device)
     search = str(opts.get("bandwidth_search", "full"))
     if search not in ("full", "learned"):
@@ -1047,9 +1060,6 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
     methods = _check_interp_methods(opts, d, n)
     st.grid64 = None
     st.spec64 = None
-    if (kept and kept["prec"] == _lib.FLPR_PREC_F32 and bandwidths is not None
-            and bool(np.any(_sparse_bandwidths(geom, n, bandwidths)))):
-        st.grid64 = _grid64(ctx, kept)
     st.__dict__.update(dict(
         n=n, d=d, dx=dx, ycols=ycols, pcols=pcols, R=R, ny=ny, y_raw_dev=y_raw_dev,
         stats=stats, geom=geom, spec=spec, calc_dof=calc_dof, order=order, prec=prec,
@@ -1058,6 +1068,16 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
         methods=methods, spl=None, kid=_kernel_id(opts),
         dual=(calc_dof and ny <= 4 and not opts.get("_direct_reduce", False)
               and methods["gcv"] == "linear" and methods["dof"] == "linear"), Q=None))
+    if kept and kept["prec"] == _lib.FLPR_PREC_F32 and bandwidths is not None:
+        sparse_any = bool(np.any(_sparse_bandwidths(geom, n, bandwidths)))
+        if order == 2 or sparse_any:
+            # the exact FP64 grid for FP64 planes; the ones channel alone
+            # when only the order-2 moment planes need it (_evaluate_device)
+            Lq = (_lib.ivec(geom.G), _lib.ivec(geom.L), _lib.ivec(geom.qout[0]))
+            ones_only = (order == 2 and not sparse_any and d == 2 and st.dual
+                         and st.kid in (0, 1) and not opts.get("_no_fused", False)
+                         and lib.flpr_lpr2d_fused_supported(*Lq, 1, 2, ny + R) == 1)
+            st.grid64 = _grid64(ctx, kept, 1 if ones_only else None)
     if "cubic" in methods.values():
         st.spl = spline.tables(axes_raw, ctx.device)
     if st.dual:
@@ -1114,8 +1134,22 @@ def _evaluate_device(ctx, st: _LprState, filt, ev) -> dict:
             and not getattr(kern0, "device_window", False)):
         mask = _sparse_bandwidths(st.geom, st.n, bw0[keep0])
         k64 = int(mask.sum())
+        leading = k64 < len(mask) and bool(np.all(mask[:k64]))
+        if st.order == 2:
+            # moment planes in FP64, value channels on the fused FP32 path
+            Lq = (_lib.ivec(st.geom.G), _lib.ivec(st.geom.L), _lib.ivec(st.geom.qout[0]))
+            if ((k64 == 0 or leading) and k64 < len(mask) and st.d == 2 and st.dual
+                    and kern0.separable and not st.opts.get("_no_fused", False)
+                    and ctx.lib.flpr_lpr2d_fused_supported(*Lq, len(mask) - k64, 2,
+                                                           st.ny + st.R) == 1):
+                return _evaluate_split(ctx, st, filt, k64, ev, s64_all=True)
+            # otherwise FP64 throughout
+            k64, leading = len(mask), False
         if k64:
-            if (k64 < len(mask) and bool(np.all(mask[:k64])) and st.dual and kern0.separable):
+            if st.grid64.shape[0] < 1 + st.ny + st.R:
+                raise _lib.FastLPRError("the FP64 grid holds only the ones channel but the "
+                                        "evaluation needs every channel in FP64")
+            if leading and st.dual and kern0.separable:
                 return _evaluate_split(ctx, st, filt, k64, ev)
             st64 = copy.copy(st)
             st64.spec = _spectra64(ctx, st)
@@ -1244,10 +1278,13 @@ def _kernel_rows(kern: _Kernel, rows: np.ndarray, geom) -> _Kernel:
     return _Kernel(kern.kid, torch.cat(parts, dim=0).contiguous(), r1 - r0, kern.npow, kern.scale)
 
 
-def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev) -> dict:
+def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev, s64_all: bool = False) -> dict:
     """_evaluate_device with the first k64 bandwidths in FP64 (planes from
     the FP64 spectra) and the rest on the FP32 path; lambda (or max s) is
-    the larger of the two groups' (the reference's, over all bandwidths)."""
+    the larger of the two groups' (the reference's, over all bandwidths).
+    s64_all: the FP32 group's moment planes S are FP64 too (from the FP64
+    spectra of the ones channel; flpr_lpr2d_fused_t), only its value
+    channels run in FP32; k64 may then be 0."""
     lib = ctx.lib
     kern, bw, keep, _ = filt
     d, ny, R, order = st.d, st.ny, st.R, st.order
@@ -1256,7 +1293,6 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev) -> dict:
     H = len(keep)
     H32 = H - k64
     npow = 2 * order + 1
-    k64k = _kernel_rows(kern, keep[:k64], geom)
     k32k = _kernel_rows(kern, keep[k64:], geom)
     epw = _element_powers(d, order)
     ns = len(epw)
@@ -1265,30 +1301,45 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev) -> dict:
     M = geom.M
     F32, F64 = _lib.FLPR_PREC_F32, _lib.FLPR_PREC_F64
     spec64 = _spectra64(ctx, st)
-    S64 = _conv(ctx, geom, spec64, k64k, [(0, hk, epw[k]) for k in range(ns) for hk in range(k64)],
-                F64, order == 0)
-    T64 = _conv(ctx, geom, spec64, k64k,
-                [(1 + c, hk, epw[i]) for i in range(nt) for c in range(Cv) for hk in range(k64)],
-                F64, False)
-    scal64 = ctx.empty(1)
-    ctx.check(lib.flpr_scalar_of(order, nt, k64, M, S64.data_ptr(), F64, None, scal64.data_ptr(),
-                                 ctx.stream), "flpr_scalar_of")
+    scal64 = None
+    if k64:
+        k64k = _kernel_rows(kern, keep[:k64], geom)
+        S64 = _conv(ctx, geom, spec64, k64k,
+                    [(0, hk, epw[k]) for k in range(ns) for hk in range(k64)], F64, order == 0)
+        T64 = _conv(ctx, geom, spec64, k64k,
+                    [(1 + c, hk, epw[i]) for i in range(nt) for c in range(Cv)
+                     for hk in range(k64)], F64, False)
+        scal64 = ctx.empty(1)
+        ctx.check(lib.flpr_scalar_of(order, nt, k64, M, S64.data_ptr(), F64, None,
+                                     scal64.data_ptr(), ctx.stream), "flpr_scalar_of")
     reg = float(st.opts["regularization"])
     m = ctx.empty((H, M, ny))
     m32 = m.data_ptr() + k64 * M * ny * 8
-    dots64 = ctx.empty((Cv, k64))
     dots32 = ctx.empty((Cv, H32))
     scalar = ctx.empty(1)
     Lq = (_lib.ivec(geom.G), _lib.ivec(geom.L), _lib.ivec(geom.qout[0]))
     use_fused = (d == 2 and not st.opts.get("_no_fused", False)
                  and lib.flpr_lpr2d_fused_supported(*Lq, H32, order, Cv) == 1)
-    if use_fused:
+    floor = scal64.data_ptr() if scal64 is not None else None
+    if s64_all:
+        S32 = _conv(ctx, geom, spec64, k32k,
+                    [(0, hk, epw[k]) for k in range(ns) for hk in range(H32)], F64, order == 0)
+        ctx.check(lib.flpr_scalar_of(order, nt, H32, M, S32.data_ptr(), F64, floor,
+                                     scalar.data_ptr(), ctx.stream), "flpr_scalar_of")
+        ws = ctx.ws(lib.flpr_lpr2d_fused_ws(*Lq, H32, order, Cv))
+        ctx.check(lib.flpr_lpr2d_fused_t(*Lq, H32, npow, order, Cv, ny, st.spec.data_ptr(),
+                                         k32k.data_ptr(), k32k.scale, st.Q.data_ptr(), reg,
+                                         S32.data_ptr(), scalar.data_ptr(), m32,
+                                         dots32.data_ptr(), ws.data_ptr(), ws.numel(),
+                                         ctx.stream), "flpr_lpr2d_fused_t")
+        del ws
+    elif use_fused:
         S32 = ctx.empty((ns, H32, M), dtype=torch.float32)
         ws = ctx.ws(lib.flpr_lpr2d_fused_ws(*Lq, H32, order, Cv))
         ctx.check(lib.flpr_lpr2d_fused_floor(*Lq, H32, npow, order, Cv, ny, st.spec.data_ptr(),
                                              k32k.data_ptr(), k32k.scale, st.Q.data_ptr(), reg,
                                              S32.data_ptr(), m32, dots32.data_ptr(),
-                                             scalar.data_ptr(), scal64.data_ptr(), ws.data_ptr(),
+                                             scalar.data_ptr(), floor, ws.data_ptr(),
                                              ws.numel(), ctx.stream), "flpr_lpr2d_fused_floor")
         del ws
     else:
@@ -1297,25 +1348,31 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev) -> dict:
         T32 = _conv(ctx, geom, st.spec, k32k,
                     [(1 + c, hk, epw[i]) for i in range(nt) for c in range(Cv) for hk in range(H32)],
                     F32, False)
-        ctx.check(lib.flpr_scalar_of(order, nt, H32, M, S32.data_ptr(), F32, scal64.data_ptr(),
+        ctx.check(lib.flpr_scalar_of(order, nt, H32, M, S32.data_ptr(), F32, floor,
                                      scalar.data_ptr(), ctx.stream), "flpr_scalar_of")
         ctx.check(lib.flpr_solve_reduce_given(order, nt, H32, H32, M, Cv, S32.data_ptr(),
                                               T32.data_ptr(), reg, ny, m32, st.Q.data_ptr(),
                                               dots32.data_ptr(), scalar.data_ptr(), F32,
                                               ctx.stream), "flpr_solve_reduce_given")
-    ctx.check(lib.flpr_solve_reduce_given(order, nt, k64, k64, M, Cv, S64.data_ptr(),
-                                          T64.data_ptr(), reg, ny, m.data_ptr(), st.Q.data_ptr(),
-                                          dots64.data_ptr(), scalar.data_ptr(), F64, ctx.stream),
-              "flpr_solve_reduce_given")
+    parts_dots, parts_s0 = [], []
+    if k64:
+        dots64 = ctx.empty((Cv, k64))
+        ctx.check(lib.flpr_solve_reduce_given(order, nt, k64, k64, M, Cv, S64.data_ptr(),
+                                              T64.data_ptr(), reg, ny, m.data_ptr(),
+                                              st.Q.data_ptr(), dots64.data_ptr(),
+                                              scalar.data_ptr(), F64, ctx.stream),
+                  "flpr_solve_reduce_given")
+        parts_dots.append(dots64)
+        parts_s0.append(S64.view(ns, k64, M)[0])
     ev.mark("conv_solve")
-    dots = torch.cat([dots64, dots32], dim=1)
+    dots = torch.cat(parts_dots + [dots32], dim=1)
     quad = ctx.empty((H, ny))
     _stencil_quad(ctx, st, H, ny, m, quad)
     ev.mark("interp_reduce")
     packed = torch.cat([st.sq.reshape(-1), dots.reshape(-1), quad.reshape(-1)])
-    S0 = torch.cat([S64.view(ns, k64, M)[0], S32.view(ns, H32, M)[0].to(torch.float64)], dim=0)
+    S0 = torch.cat(parts_s0 + [S32.view(ns, H32, M)[0].to(torch.float64)], dim=0)
     return dict(keep=keep, bw_k=bw_k, H=H, m=m, S=S0.view(1, H, M), ns=1, mstride=ny,
-                packed=packed, dual=True, fp64_bandwidths=k64)
+                packed=packed, dual=True, fp64_bandwidths=k64, s_planes_fp64=bool(s64_all))
 
 
 def _evaluate_host(st: _LprState, r: dict, packed: Optional[np.ndarray]) -> dict:
@@ -1546,6 +1603,9 @@ def _finalize_build(ctx, st: _LprState, r: dict, pend: dict, ev, search,
         "precision": "fp32" if st.prec == _lib.FLPR_PREC_F32 else "fp64",
         # FP32 path: bandwidths whose kernel covers few points, evaluated in FP64
         "fp64_bandwidths": int(r.get("fp64_bandwidths", 0)),
+        # FP32 path of order 2: moment planes S in FP64, value channels in FP32
+        "moment_planes": "fp64" if (st.prec == _lib.FLPR_PREC_F64
+                                    or r.get("s_planes_fp64", False)) else "fp32",
         "bandwidth_search": search if search is not None else {"mode": "full"},
     }
     return RegressionOutput(yhat=yhat, grid=tuple(st.axes_raw), h=selected, gcv_yhat=gcv_result,

@@ -286,9 +286,10 @@ colpass_kernel(ColArgs ca, const float2* __restrict__ Yt, const float2* __restri
 }
 
 // Solve vectors z = (S + lam I)^-1 e1 per (bandwidth, grid point); order 0
-// stores 1/max(s, max(s) reg).  S: (ns, H, M) float; z: (H, M, NT) double.
-template <int NT>
-__global__ void zvec_kernel(int order, int H, int64_t M, const float* __restrict__ S,
+// stores 1/max(s, max(s) reg).  S: (ns, H, M) float or double; z: (H, M, NT)
+// double.
+template <int NT, typename TS>
+__global__ void zvec_kernel(int order, int H, int64_t M, const TS* __restrict__ S,
                             const double* __restrict__ scalar, double reg, double* __restrict__ z) {
   constexpr int NS = NT * (NT + 1) / 2;
   const int64_t HM = (int64_t)H * M;
@@ -790,11 +791,15 @@ static void carve(A& ar, const FusedTables& tb, const FusedGeom& fg, int H, int 
   b->kcut = ar.template take<int>(2 * (size_t)H);
 }
 
+// S64 (optional): the S planes in FP64, (ns, H, M), formed by the caller
+// (with `scalar` already holding lambda / max s): the S pass is skipped and
+// the solve vectors come from them.
 template <int E0, int E1>
 static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow, int order, int C,
                      int ny, const float2* spec, const double2* F, double scale, const double* Q,
-                     double reg, float* S, double* my, double* dots, double* scalar,
-                     const double* scalar_floor_in, const FusedBuffers& b, cudaStream_t s) {
+                     double reg, float* S, const double* S64, double* my, double* dots,
+                     double* scalar, const double* scalar_floor_in, const FusedBuffers& b,
+                     cudaStream_t s) {
   const int nt = tb.nt;
   twiddle_table_kernel<<<(twiddle_entries(fg.L0) + 255) / 256, 256, 0, s>>>(fg.L0, b.tab0);
   FLPR_LAUNCH_CHECK();
@@ -831,25 +836,33 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
   ra.G1 = fg.G1;
   ra.q1 = fg.q1;
   ra.npow = npow;
-  for (int h0 = 0; h0 < H; h0 += fg.Hc_s) {
-    const int hc = H - h0 < fg.Hc_s ? H - h0 : fg.Hc_s;
-    ca.hbase = h0;
-    ra.hbase = h0;
-    FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.s_nslots, hc, b.Yt, F0f, b.tab0, kcut1, b.W, s));
-    FLPR_TRY(launch_row_s<E1>(ra, hc, H, hc, b.W, F1f, b.tab1, kcut1, S, s));
+  if (S64 == nullptr) {
+    for (int h0 = 0; h0 < H; h0 += fg.Hc_s) {
+      const int hc = H - h0 < fg.Hc_s ? H - h0 : fg.Hc_s;
+      ca.hbase = h0;
+      ra.hbase = h0;
+      FLPR_TRY(launch_col<E0>(ca, ncolblk, tb.s_nslots, hc, b.Yt, F0f, b.tab0, kcut1, b.W, s));
+      FLPR_TRY(launch_row_s<E1>(ra, hc, H, hc, b.W, F1f, b.tab1, kcut1, S, s));
+    }
+    FLPR_TRY(global_scalar(order, nt, H, fg.M, S, scalar, FLPR_PREC_F32, s));
+    FLPR_TRY(scalar_floor(scalar, scalar_floor_in, s));
   }
-  FLPR_TRY(global_scalar(order, nt, H, fg.M, S, scalar, FLPR_PREC_F32, s));
-  FLPR_TRY(scalar_floor(scalar, scalar_floor_in, s));
   {
     const int64_t HM = (int64_t)H * fg.M;
     int nb = (int)((HM + 255) / 256);
     if (nb > 16 * sm_count()) nb = 16 * sm_count();
+#define FLPR_ZVEC(NTV)                                                                  \
+  if (S64)                                                                              \
+    zvec_kernel<NTV, double><<<nb, 256, 0, s>>>(order, H, fg.M, S64, scalar, reg, b.z); \
+  else                                                                                  \
+    zvec_kernel<NTV, float><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, b.z);
     switch (nt) {
-      case 1: zvec_kernel<1><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, b.z); break;
-      case 3: zvec_kernel<3><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, b.z); break;
-      case 6: zvec_kernel<6><<<nb, 256, 0, s>>>(order, H, fg.M, S, scalar, reg, b.z); break;
+      case 1: FLPR_ZVEC(1) break;
+      case 3: FLPR_ZVEC(3) break;
+      case 6: FLPR_ZVEC(6) break;
       default: set_error("fused2d: nt=%d", nt); return FLPR_ERR_ARG;
     }
+#undef FLPR_ZVEC
     FLPR_LAUNCH_CHECK();
   }
   // T pass fused with the solve
@@ -883,12 +896,12 @@ static int run_fused(const FusedTables& tb, const FusedGeom& fg, int H, int npow
 template <int E0>
 static int dispatch_e1(int E1, const FusedTables& tb, const FusedGeom& fg, int H, int npow,
                        int order, int C, int ny, const float2* spec, const double2* F,
-                       double scale, const double* Q, double reg, float* S, double* my,
-                       double* dots, double* scalar, const double* floor_in, const FusedBuffers& b,
-                       cudaStream_t s) {
-#define FLPR_E1(V)                                                                          \
-  case V:                                                                                   \
-    return run_fused<E0, V>(tb, fg, H, npow, order, C, ny, spec, F, scale, Q, reg, S, my,   \
+                       double scale, const double* Q, double reg, float* S, const double* S64,
+                       double* my, double* dots, double* scalar, const double* floor_in,
+                       const FusedBuffers& b, cudaStream_t s) {
+#define FLPR_E1(V)                                                                            \
+  case V:                                                                                     \
+    return run_fused<E0, V>(tb, fg, H, npow, order, C, ny, spec, F, scale, Q, reg, S, S64, my, \
                             dots, scalar, floor_in, b, s);
   switch (E1) {
     FLPR_E1(2)
@@ -951,11 +964,11 @@ size_t flpr_lpr2d_fused_ws(const int* h_G, const int* h_L, const int* h_qout, in
   return ar.used;
 }
 
-int flpr_lpr2d_fused_floor(const int* h_G, const int* h_L, const int* h_qout, int H, int npow,
-                           int order, int C, int ny, const void* d_spec, const void* d_F,
-                           double scale, const double* d_Q, double reg, float* d_S, double* d_my,
-                           double* d_dots, double* d_scalar, const double* d_scalar_floor,
-                           void* d_ws, size_t ws_bytes, void* stream) {
+static int fused_entry(const int* h_G, const int* h_L, const int* h_qout, int H, int npow,
+                       int order, int C, int ny, const void* d_spec, const void* d_F,
+                       double scale, const double* d_Q, double reg, float* d_S,
+                       const double* d_S64, double* d_my, double* d_dots, double* d_scalar,
+                       const double* d_scalar_floor, void* d_ws, size_t ws_bytes, void* stream) {
   FusedTables tb;
   FusedGeom fg;
   FLPR_TRY(fused2d_check(h_G, h_L, h_qout, H, order, C, &tb, &fg));
@@ -977,7 +990,7 @@ int flpr_lpr2d_fused_floor(const int* h_G, const int* h_L, const int* h_qout, in
 #define FLPR_E0(V)                                                                             \
   case V:                                                                                      \
     return dispatch_e1<V>(fg.L1 / 32, tb, fg, H, npow, order, C, ny, spec, F, scale, d_Q, reg, \
-                          d_S, d_my, d_dots, d_scalar, d_scalar_floor, b, s);
+                          d_S, d_S64, d_my, d_dots, d_scalar, d_scalar_floor, b, s);
     FLPR_E0(2)
     FLPR_E0(4)
     FLPR_E0(8)
@@ -990,12 +1003,32 @@ int flpr_lpr2d_fused_floor(const int* h_G, const int* h_L, const int* h_qout, in
   }
 }
 
+int flpr_lpr2d_fused_floor(const int* h_G, const int* h_L, const int* h_qout, int H, int npow,
+                           int order, int C, int ny, const void* d_spec, const void* d_F,
+                           double scale, const double* d_Q, double reg, float* d_S, double* d_my,
+                           double* d_dots, double* d_scalar, const double* d_scalar_floor,
+                           void* d_ws, size_t ws_bytes, void* stream) {
+  FLPR_CHECK_ARG(d_S != nullptr, "fused2d: S planes missing");
+  return fused_entry(h_G, h_L, h_qout, H, npow, order, C, ny, d_spec, d_F, scale, d_Q, reg, d_S,
+                     nullptr, d_my, d_dots, d_scalar, d_scalar_floor, d_ws, ws_bytes, stream);
+}
+
 int flpr_lpr2d_fused(const int* h_G, const int* h_L, const int* h_qout, int H, int npow, int order,
                      int C, int ny, const void* d_spec, const void* d_F, double scale,
                      const double* d_Q, double reg, float* d_S, double* d_my, double* d_dots,
                      double* d_scalar, void* d_ws, size_t ws_bytes, void* stream) {
   return flpr_lpr2d_fused_floor(h_G, h_L, h_qout, H, npow, order, C, ny, d_spec, d_F, scale, d_Q,
                                 reg, d_S, d_my, d_dots, d_scalar, nullptr, d_ws, ws_bytes, stream);
+}
+
+int flpr_lpr2d_fused_t(const int* h_G, const int* h_L, const int* h_qout, int H, int npow,
+                       int order, int C, int ny, const void* d_spec, const void* d_F, double scale,
+                       const double* d_Q, double reg, const double* d_S64, const double* d_scalar,
+                       double* d_my, double* d_dots, void* d_ws, size_t ws_bytes, void* stream) {
+  FLPR_CHECK_ARG(d_S64 != nullptr && d_scalar != nullptr, "fused2d: S planes or scalar missing");
+  return fused_entry(h_G, h_L, h_qout, H, npow, order, C, ny, d_spec, d_F, scale, d_Q, reg,
+                     nullptr, d_S64, d_my, d_dots, const_cast<double*>(d_scalar), nullptr, d_ws,
+                     ws_bytes, stream);
 }
 
 }  // extern "C"

@@ -1206,8 +1206,16 @@ int flpr_spread_dkmap(int d, int64_t n, const double* d_x, const double* d_kmap,
 
 int flpr_spread_grid64(int d, int64_t n, const int* h_L, int msp, int nchan, const void* d_ws,
                        size_t ws_bytes, double* d_grid64, void* stream) {
+  return flpr_spread_grid64_channels(d, n, h_L, msp, nchan, nchan, d_ws, ws_bytes, d_grid64,
+                                     stream);
+}
+
+int flpr_spread_grid64_channels(int d, int64_t n, const int* h_L, int msp, int nchan, int nout,
+                                const void* d_ws, size_t ws_bytes, double* d_grid64,
+                                void* stream) {
   FLPR_CHECK_ARG(d >= 1 && d <= 3, "spread_grid64: d=%d not in [1,3]", d);
   FLPR_CHECK_ARG(n >= 1 && nchan >= 1 && nchan <= FLPR_MAX_CHANNELS, "spread_grid64: n/nchan");
+  FLPR_CHECK_ARG(nout >= 1 && nout <= nchan, "spread_grid64: nout=%d not in [1, %d]", nout, nchan);
   FLPR_CHECK_ARG(d_ws != nullptr && d_grid64 != nullptr, "spread_grid64: null pointer");
   for (int a = 0; a < d; ++a) FLPR_CHECK_ARG(h_L[a] >= 1, "spread_grid64: L[%d]=%d", a, h_L[a]);
   if (ws_bytes < flpr_spread_ws(d, n, h_L, msp, nchan, FLPR_PREC_F32)) {
@@ -1223,7 +1231,7 @@ int flpr_spread_grid64(int d, int64_t n, const int* h_L, int msp, int nchan, con
   int64_t fb64 = (g.cells + 255) / 256;
   if (fb64 > 16 * sm_count()) fb64 = 16 * sm_count();
   finalize_kernel<long long, double, true><<<(int)fb64, 256, 0, as_stream(stream)>>>(
-      nchan, g.cells, (const long long*)w.gacc, w.absum, margin_bits_for(g), 1.0 / (double)n,
+      nout, g.cells, (const long long*)w.gacc, w.absum, margin_bits_for(g), 1.0 / (double)n,
       d_grid64);
   FLPR_LAUNCH_CHECK();
   return FLPR_OK;

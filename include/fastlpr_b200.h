@@ -137,6 +137,11 @@ int flpr_spread_dkmap(int d, int64_t n, const double* d_x, const double* d_kmap,
  * reference counterpart (the reference spreads once, in one precision). */
 int flpr_spread_grid64(int d, int64_t n, const int* h_L, int msp, int nchan, const void* d_ws,
                        size_t ws_bytes, double* d_grid64, void* stream);
+/* The same for the first nout channels only, as (nout, L...) float64 (the
+ * ones channel alone gives the FP64 moment planes of order-2 fits). */
+int flpr_spread_grid64_channels(int d, int64_t n, const int* h_L, int msp, int nchan, int nout,
+                                const void* d_ws, size_t ws_bytes, double* d_grid64,
+                                void* stream);
 /* Knot maps d_kmap (d x 9) from the point statistics d_stats (4 x d:
  * minimum, maximum, mean, M2 as flpr_point_stats writes them) and the
  * host-known per-axis constants of the grid (ks, r0: the knot range of
@@ -309,6 +314,19 @@ int flpr_lpr2d_fused_floor(const int* h_G, const int* h_L, const int* h_qout, in
                            double scale, const double* d_Q, double reg, float* d_S, double* d_my,
                            double* d_dots, double* d_scalar, const double* d_scalar_floor,
                            void* d_ws, size_t ws_bytes, void* stream);
+
+/* The T pass of flpr_lpr2d_fused on FP64 S planes formed by the caller
+ * (d_S64: (ns, H, M) float64, the moment matrices of every kept bandwidth
+ * in FP64, e.g. from the exact FP64 grid of the ones channel) with lambda
+ * (order >= 1) or max s (order 0) already in *d_scalar: the FP32 column and
+ * row passes of the value channels, the per-point FP64 solves on the FP64
+ * moment matrices and the dual-form reductions.  The local-quadratic
+ * moment systems are then factorised from FP64 planes while the channels'
+ * transforms stay FP32.  Same workspace as flpr_lpr2d_fused. */
+int flpr_lpr2d_fused_t(const int* h_G, const int* h_L, const int* h_qout, int H, int npow,
+                       int order, int C, int ny, const void* d_spec, const void* d_F, double scale,
+                       const double* d_Q, double reg, const double* d_S64, const double* d_scalar,
+                       double* d_my, double* d_dots, void* d_ws, size_t ws_bytes, void* stream);
 
 /* ---------------------------------------------------------------------
  * (7) Interpolation + GCV / Hutchinson reductions over the points.

@@ -325,6 +325,30 @@ def test_fused_2d_band_classes_match_oracle(cuda_ok):
     assert rel_err(r.gcv_yhat["dof"], o["dof_all"]) < 1e-5
 
 
+@pytest.mark.parametrize("n,G", [(50000, [256, 256]), (300000, [200, 160])])
+def test_order2_2d_default_fp64_moment_planes_match_oracle(cuda_ok, n, G):
+    """2-D local quadratic at the default precision: FP32 value channels on
+    the fused path with the moment planes S and the solves in FP64 (the
+    sparse bandwidths wholly in FP64); every output within the FP32 bound of
+    the oracle."""
+    rng = np.random.default_rng(n)
+    x = rng.random((n, 2))
+    y = np.sin(2 * np.pi * (1.3 * x[:, 0] + 0.4 * x[:, 1])) + 0.1 * rng.standard_normal(n)
+    hv = np.logspace(np.log10(0.005), np.log10(0.5), 24)
+    h = np.column_stack([hv, hv])
+    opts = {"order": 2, "N": G}
+    r = _fastlpr().cv_fastlpr(x, y, h, opts)
+    assert r.metadata["precision"] == "fp32"
+    assert r.metadata["moment_planes"] == "fp64"
+    o = oracle.cv_fastlpr(x, y, h, opts, workers=8)
+    assert r.gcv_yhat["id1se"] == o["id1se"]
+    assert rel_err(r.yhat, o["yhat"]) < 1e-5
+    assert rel_err(r.fpp_yhat.values, o["grid_values"]) < 1e-5
+    assert elem_rel_err(r.gcv_yhat["gcv_m"], o["gcv_m"]) < 1e-5
+    assert rel_err(r.gcv_yhat["dof"], o["dof_all"]) < 1e-5
+    assert rel_err(r.s0, o["s0"]) < 1e-5
+
+
 @pytest.mark.parametrize("bad", [np.nan, np.inf])
 def test_validation_rejects_nonfinite(cuda_ok, bad):
     """NaN/Inf inputs raise the reference's ValueError (checked on the device)."""
