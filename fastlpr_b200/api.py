@@ -716,6 +716,24 @@ def _conv(ctx: _Ctx, geom: _Geom, spec, kern: _Kernel, prods, prec: int, add_eps
     return out
 
 
+def _conv_s(ctx: _Ctx, geom: _Geom, spec, kern: _Kernel, hks, epw, prec: int,
+            add_eps: bool) -> torch.Tensor:
+    """The moment planes S of the ones channel for the bandwidth rows `hks`
+    and every element power in `epw` -> (len(epw) * len(hks), M), element
+    major.  Elements with the same power (order 2: 21 elements, 15 powers)
+    are convolved once and their planes repeated."""
+    uniq = []
+    for e in epw:
+        if tuple(e) not in uniq:
+            uniq.append(tuple(e))
+    H = len(hks)
+    out = _conv(ctx, geom, spec, kern, [(0, hk, u) for u in uniq for hk in hks], prec, add_eps)
+    if len(uniq) == len(epw):
+        return out
+    blocks = [out[uniq.index(tuple(e)) * H:(uniq.index(tuple(e)) + 1) * H] for e in epw]
+    return torch.cat(blocks, dim=0)
+
+
 def _precision(opts, dims: Optional[int] = None) -> int:
     p = opts.get("precision", None)
     if p is None:
@@ -1175,8 +1193,7 @@ def _evaluate_device(ctx, st: _LprState, filt, ev) -> dict:
                  and not opts.get("_no_fused", False)
                  and lib.flpr_lpr2d_fused_supported(*Lq, H, order, Cv) == 1)
     if not use_fused:
-        S = _conv(ctx, geom, spec, kern,
-                  [(0, int(hk), epw[k]) for k in range(ns) for hk in keep], prec, order == 0)
+        S = _conv_s(ctx, geom, spec, kern, [int(hk) for hk in keep], epw, prec, order == 0)
         ev.mark("conv_S")
         T = _conv(ctx, geom, spec, kern,
                   [(1 + c, int(hk), epw[i]) for i in range(nt) for c in range(Cv) for hk in h_t],
@@ -1304,8 +1321,7 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev, s64_all: bool = Fals
     scal64 = None
     if k64:
         k64k = _kernel_rows(kern, keep[:k64], geom)
-        S64 = _conv(ctx, geom, spec64, k64k,
-                    [(0, hk, epw[k]) for k in range(ns) for hk in range(k64)], F64, order == 0)
+        S64 = _conv_s(ctx, geom, spec64, k64k, list(range(k64)), epw, F64, order == 0)
         T64 = _conv(ctx, geom, spec64, k64k,
                     [(1 + c, hk, epw[i]) for i in range(nt) for c in range(Cv)
                      for hk in range(k64)], F64, False)
@@ -1322,8 +1338,7 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev, s64_all: bool = Fals
                  and lib.flpr_lpr2d_fused_supported(*Lq, H32, order, Cv) == 1)
     floor = scal64.data_ptr() if scal64 is not None else None
     if s64_all:
-        S32 = _conv(ctx, geom, spec64, k32k,
-                    [(0, hk, epw[k]) for k in range(ns) for hk in range(H32)], F64, order == 0)
+        S32 = _conv_s(ctx, geom, spec64, k32k, list(range(H32)), epw, F64, order == 0)
         ctx.check(lib.flpr_scalar_of(order, nt, H32, M, S32.data_ptr(), F64, floor,
                                      scalar.data_ptr(), ctx.stream), "flpr_scalar_of")
         ws = ctx.ws(lib.flpr_lpr2d_fused_ws(*Lq, H32, order, Cv))
@@ -1343,8 +1358,7 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev, s64_all: bool = Fals
                                              ws.numel(), ctx.stream), "flpr_lpr2d_fused_floor")
         del ws
     else:
-        S32 = _conv(ctx, geom, st.spec, k32k,
-                    [(0, hk, epw[k]) for k in range(ns) for hk in range(H32)], F32, order == 0)
+        S32 = _conv_s(ctx, geom, st.spec, k32k, list(range(H32)), epw, F32, order == 0)
         T32 = _conv(ctx, geom, st.spec, k32k,
                     [(1 + c, hk, epw[i]) for i in range(nt) for c in range(Cv) for hk in range(H32)],
                     F32, False)
