@@ -77,6 +77,10 @@ SIGNATURES = [
                                     _VP, _VP, _VP, _VP, _VP, _VP, _SZ, _VP]),
     ("flpr_lpr2d_fused_t", _I, [_PI, _PI, _PI, _I, _I, _I, _I, _I, _VP, _VP, _D, _VP, _D, _VP,
                                 _VP, _VP, _VP, _VP, _SZ, _VP]),
+    ("flpr_lpr2d_fused_ex_supported", _I, [_I, _PI, _PI, _PI, _I, _I, _I]),
+    ("flpr_lpr2d_fused_ex_ws", _SZ, [_I, _PI, _PI, _PI, _I, _I, _I]),
+    ("flpr_lpr2d_fused_ex", _I, [_I, _I, _PI, _PI, _PI, _I, _I, _I, _I, _I, _VP, _VP, _D, _VP,
+                                 _D, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _SZ, _VP]),
     ("flpr_interp_reduce_ws", _SZ, [_I64, _I, _I, _I]),
     ("flpr_interp_reduce", _I, [_I, _I64, _VP, _PD, _PI, _I, _I, _I, _VP, _PVP, _PVP, _VP, _VP,
                                 _VP, _VP, _SZ, _VP]),

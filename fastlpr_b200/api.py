@@ -1189,9 +1189,7 @@ def _evaluate_device(ctx, st: _LprState, filt, ev) -> dict:
     Cv = ny + R
     M = geom.M
     Lq = (_lib.ivec(geom.G), _lib.ivec(geom.L), _lib.ivec(geom.qout[0]))
-    use_fused = (prec == _lib.FLPR_PREC_F32 and d == 2 and st.dual and kern.separable
-                 and not opts.get("_no_fused", False)
-                 and lib.flpr_lpr2d_fused_supported(*Lq, H, order, Cv) == 1)
+    use_fused = st.dual and kern.separable and _fused_ok(ctx, st, prec, H)
     if not use_fused:
         S = _conv_s(ctx, geom, spec, kern, [int(hk) for hk in keep], epw, prec, order == 0)
         ev.mark("conv_S")
@@ -1208,13 +1206,15 @@ def _evaluate_device(ctx, st: _LprState, filt, ev) -> dict:
         m = ctx.empty((H, M, ny))
         dots = ctx.empty((Cv, H))
         if use_fused:
-            S = ctx.empty((ns, H, M), dtype=torch.float32)
-            ws = ctx.ws(lib.flpr_lpr2d_fused_ws(*Lq, H, order, Cv))
-            ctx.check(lib.flpr_lpr2d_fused(*Lq, H, npow, order, Cv, ny, spec.data_ptr(),
-                                           kern.data_ptr(), kern.scale, st.Q.data_ptr(), reg,
-                                           S.data_ptr(), m.data_ptr(), dots.data_ptr(),
-                                           scalar.data_ptr(), ws.data_ptr(), ws.numel(),
-                                           ctx.stream), "flpr_lpr2d_fused")
+            S = ctx.empty((ns, H, M),
+                          dtype=torch.float32 if prec == _lib.FLPR_PREC_F32 else torch.float64)
+            ws = ctx.ws(lib.flpr_lpr2d_fused_ex_ws(prec, *Lq, H, order, Cv))
+            ctx.check(lib.flpr_lpr2d_fused_ex(prec, _FUSED_BOTH, *Lq, H, npow, order, Cv, ny,
+                                              spec.data_ptr(), kern.data_ptr(), kern.scale,
+                                              st.Q.data_ptr(), reg, S.data_ptr(), None,
+                                              m.data_ptr(), dots.data_ptr(), scalar.data_ptr(),
+                                              None, ws.data_ptr(), ws.numel(), ctx.stream),
+                      "flpr_lpr2d_fused_ex")
             del ws
             ev.mark("conv_solve")
         else:
@@ -1295,6 +1295,35 @@ def _kernel_rows(kern: _Kernel, rows: np.ndarray, geom) -> _Kernel:
     return _Kernel(kern.kid, torch.cat(parts, dim=0).contiguous(), r1 - r0, kern.npow, kern.scale)
 
 
+_FUSED_BOTH, _FUSED_S, _FUSED_T = 0, 1, 2
+
+
+def _fused_ok(ctx, st, prec: int, H: int) -> bool:
+    """Whether the fused 2-D passes serve this fit in `prec`."""
+    if st.d != 2 or st.opts.get("_no_fused", False) or H < 1:
+        return False
+    Lq = (_lib.ivec(st.geom.G), _lib.ivec(st.geom.L), _lib.ivec(st.geom.qout[0]))
+    return ctx.lib.flpr_lpr2d_fused_ex_supported(prec, *Lq, H, st.order, st.ny + st.R) == 1
+
+
+def _fused_s_planes(ctx, st, spec, kern: "_Kernel", prec: int) -> torch.Tensor:
+    """The S planes (ns, H, M) of the kernel's bandwidths from the ones
+    channel of `spec` by the fused S pass in `prec`."""
+    geom, order = st.geom, st.order
+    ns = len(_element_powers(st.d, order))
+    Cv = st.ny + st.R
+    Lq = (_lib.ivec(geom.G), _lib.ivec(geom.L), _lib.ivec(geom.qout[0]))
+    S = ctx.empty((ns, kern.H, geom.M),
+                  dtype=torch.float64 if prec == _lib.FLPR_PREC_F64 else torch.float32)
+    ws = ctx.ws(ctx.lib.flpr_lpr2d_fused_ex_ws(prec, *Lq, kern.H, order, Cv))
+    ctx.check(ctx.lib.flpr_lpr2d_fused_ex(prec, _FUSED_S, *Lq, kern.H, kern.npow, order, Cv, st.ny,
+                                          spec.data_ptr(), kern.data_ptr(), kern.scale, None,
+                                          float(st.opts["regularization"]), S.data_ptr(), None,
+                                          None, None, None, None, ws.data_ptr(), ws.numel(),
+                                          ctx.stream), "flpr_lpr2d_fused_ex")
+    return S
+
+
 def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev, s64_all: bool = False) -> dict:
     """_evaluate_device with the first k64 bandwidths in FP64 (planes from
     the FP64 spectra) and the rest on the FP32 path; lambda (or max s) is
@@ -1319,12 +1348,18 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev, s64_all: bool = Fals
     F32, F64 = _lib.FLPR_PREC_F32, _lib.FLPR_PREC_F64
     spec64 = _spectra64(ctx, st)
     scal64 = None
+    # the FP64 group on the fused FP64 passes (S planes first: its lambda
+    # floors the other group's), else on the cuFFT planes
+    fused64 = _fused_ok(ctx, st, F64, max(k64, H32))
     if k64:
         k64k = _kernel_rows(kern, keep[:k64], geom)
-        S64 = _conv_s(ctx, geom, spec64, k64k, list(range(k64)), epw, F64, order == 0)
-        T64 = _conv(ctx, geom, spec64, k64k,
-                    [(1 + c, hk, epw[i]) for i in range(nt) for c in range(Cv)
-                     for hk in range(k64)], F64, False)
+        if fused64:
+            S64 = _fused_s_planes(ctx, st, spec64, k64k, F64)
+        else:
+            S64 = _conv_s(ctx, geom, spec64, k64k, list(range(k64)), epw, F64, order == 0)
+            T64 = _conv(ctx, geom, spec64, k64k,
+                        [(1 + c, hk, epw[i]) for i in range(nt) for c in range(Cv)
+                         for hk in range(k64)], F64, False)
         scal64 = ctx.empty(1)
         ctx.check(lib.flpr_scalar_of(order, nt, k64, M, S64.data_ptr(), F64, None,
                                      scal64.data_ptr(), ctx.stream), "flpr_scalar_of")
@@ -1338,7 +1373,10 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev, s64_all: bool = Fals
                  and lib.flpr_lpr2d_fused_supported(*Lq, H32, order, Cv) == 1)
     floor = scal64.data_ptr() if scal64 is not None else None
     if s64_all:
-        S32 = _conv_s(ctx, geom, spec64, k32k, list(range(H32)), epw, F64, order == 0)
+        if fused64:
+            S32 = _fused_s_planes(ctx, st, spec64, k32k, F64)
+        else:
+            S32 = _conv_s(ctx, geom, spec64, k32k, list(range(H32)), epw, F64, order == 0)
         ctx.check(lib.flpr_scalar_of(order, nt, H32, M, S32.data_ptr(), F64, floor,
                                      scalar.data_ptr(), ctx.stream), "flpr_scalar_of")
         ws = ctx.ws(lib.flpr_lpr2d_fused_ws(*Lq, H32, order, Cv))
@@ -1371,11 +1409,21 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev, s64_all: bool = Fals
     parts_dots, parts_s0 = [], []
     if k64:
         dots64 = ctx.empty((Cv, k64))
-        ctx.check(lib.flpr_solve_reduce_given(order, nt, k64, k64, M, Cv, S64.data_ptr(),
-                                              T64.data_ptr(), reg, ny, m.data_ptr(),
-                                              st.Q.data_ptr(), dots64.data_ptr(),
-                                              scalar.data_ptr(), F64, ctx.stream),
-                  "flpr_solve_reduce_given")
+        if fused64:
+            ws = ctx.ws(lib.flpr_lpr2d_fused_ex_ws(F64, *Lq, k64, order, Cv))
+            ctx.check(lib.flpr_lpr2d_fused_ex(F64, _FUSED_T, *Lq, k64, npow, order, Cv, ny,
+                                              spec64.data_ptr(), k64k.data_ptr(), k64k.scale,
+                                              st.Q.data_ptr(), reg, None, S64.data_ptr(),
+                                              m.data_ptr(), dots64.data_ptr(), scalar.data_ptr(),
+                                              None, ws.data_ptr(), ws.numel(), ctx.stream),
+                      "flpr_lpr2d_fused_ex")
+            del ws
+        else:
+            ctx.check(lib.flpr_solve_reduce_given(order, nt, k64, k64, M, Cv, S64.data_ptr(),
+                                                  T64.data_ptr(), reg, ny, m.data_ptr(),
+                                                  st.Q.data_ptr(), dots64.data_ptr(),
+                                                  scalar.data_ptr(), F64, ctx.stream),
+                      "flpr_solve_reduce_given")
         parts_dots.append(dots64)
         parts_s0.append(S64.view(ns, k64, M)[0])
     ev.mark("conv_solve")

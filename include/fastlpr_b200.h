@@ -328,6 +328,25 @@ int flpr_lpr2d_fused_t(const int* h_G, const int* h_L, const int* h_qout, int H,
                        const double* d_Q, double reg, const double* d_S64, const double* d_scalar,
                        double* d_my, double* d_dots, void* d_ws, size_t ws_bytes, void* stream);
 
+/* The fused 2-D passes in either precision (prec FLPR_PREC_F32: float2
+ * spectra and transforms; FLPR_PREC_F64: complex128 spectra, FP64
+ * transforms, factor entries kept down to 1e-15 of their peak) and for a
+ * chosen part (mode): 0 = S pass, lambda (floored by *d_scalar_floor when
+ * given) and T pass, as flpr_lpr2d_fused_floor; 1 = the S planes only
+ * (d_S: (ns, H, M) in prec; d_spec may then hold the ones channel alone);
+ * 2 = the T pass on FP64 S planes d_S64 with lambda already in *d_scalar,
+ * as flpr_lpr2d_fused_t.  Same outputs and workspace rules as
+ * flpr_lpr2d_fused; the size query and support test take the precision. */
+int flpr_lpr2d_fused_ex_supported(int prec, const int* h_G, const int* h_L, const int* h_qout,
+                                  int H, int order, int C);
+size_t flpr_lpr2d_fused_ex_ws(int prec, const int* h_G, const int* h_L, const int* h_qout, int H,
+                              int order, int C);
+int flpr_lpr2d_fused_ex(int prec, int mode, const int* h_G, const int* h_L, const int* h_qout,
+                        int H, int npow, int order, int C, int ny, const void* d_spec,
+                        const void* d_F, double scale, const double* d_Q, double reg, void* d_S,
+                        const double* d_S64, double* d_my, double* d_dots, double* d_scalar,
+                        const double* d_scalar_floor, void* d_ws, size_t ws_bytes, void* stream);
+
 /* ---------------------------------------------------------------------
  * (7) Interpolation + GCV / Hutchinson reductions over the points.
  * Replaces the yhat interpolation and RSS of api.py:645-741 /

@@ -325,6 +325,31 @@ def test_fused_2d_band_classes_match_oracle(cuda_ok):
     assert rel_err(r.gcv_yhat["dof"], o["dof_all"]) < 1e-5
 
 
+@pytest.mark.parametrize("order", [0, 1, 2])
+@pytest.mark.parametrize("G", [[100, 60], [200, 160], [400, 300]])
+def test_fused_2d_fp64_passes_match_cufft_path_and_oracle(cuda_ok, order, G):
+    """The fused column/row passes in FP64 (transform lengths 256 to 1024)
+    agree with the cuFFT-plane FP64 path to rounding and with the oracle
+    within the FP64 bound."""
+    rng = np.random.default_rng(60 + order)
+    n = 30000
+    x = rng.random((n, 2))
+    y = np.sin(2 * np.pi * x[:, 0]) * np.cos(2 * np.pi * x[:, 1]) + 0.1 * rng.standard_normal(n)
+    hv = np.array([0.03, 0.08, 0.2, 0.5])
+    h = np.column_stack([hv, 0.8 * hv])
+    opts = {"order": order, "N": G, "precision": "fp64"}
+    fused = _fastlpr().cv_fastlpr(x, y, h, opts)
+    plain = _fastlpr().cv_fastlpr(x, y, h, dict(opts, _no_fused=True))
+    assert rel_err(fused.yhat, plain.yhat) < 1e-11
+    assert elem_rel_err(fused.gcv_yhat["gcv_m"], plain.gcv_yhat["gcv_m"]) < 1e-11
+    o = oracle.cv_fastlpr(x, y, h, {"order": order, "N": G})
+    assert fused.gcv_yhat["id1se"] == o["id1se"]
+    assert rel_err(fused.yhat, o["yhat"]) < 1e-9
+    assert elem_rel_err(fused.gcv_yhat["gcv_m"], o["gcv_m"]) < 1e-9
+    assert rel_err(fused.gcv_yhat["dof"], o["dof_all"]) < 1e-9
+    assert rel_err(fused.s0, o["s0"]) < 1e-9
+
+
 @pytest.mark.parametrize("n,G", [(50000, [256, 256]), (300000, [200, 160])])
 def test_order2_2d_default_fp64_moment_planes_match_oracle(cuda_ok, n, G):
     """2-D local quadratic at the default precision: FP32 value channels on
