@@ -223,7 +223,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row0 = blockIdx.x * kTM;
   const int nhid = a.nlayers - 1;  // layers with 256 outputs
-  if (threadIdx.x == 0) {
+  // the producer initialises the barriers and starts the first copies (the
+  // input rows and the first ring of weight chunks) before the CTA-wide
+  // set-up (tensor memory, bias cache) so their latency overlaps it
+  if (threadIdx.x == kProdWarp * 32) {
     s_abort = 0;
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
@@ -233,13 +236,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     mbar_init(acc_full, 1);
     mbar_init(a_ready, kEpiWarps * 32);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  if (threadIdx.x == kProdWarp * 32) {
-    asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&a.tm_x))
-                 : "memory");
-    for (int l = 0; l < nhid; ++l)
-      asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<uint64_t>(&a.tm_w[l]))
-                   : "memory");
+    mbar_expect_tx(in_full, (uint32_t)(a.nchunks[0] * kAChunk));
+    for (int kc = 0; kc < a.nchunks[0]; ++kc)
+      tma_load_2d(sA + kc * kAChunk, &a.tm_x, kc * kKC, row0, in_full);
+    for (int j = 0; j < kStages && j < a.total_chunks; ++j) {
+      int l, kc;
+      chunk_of(a, j, &l, &kc);
+      mbar_expect_tx(&full[j], (uint32_t)kBChunk);
+      tma_load_2d(sB + j * kBChunk, &a.tm_w[l], kc * kKC, 0, &full[j]);
+    }
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
@@ -263,15 +268,13 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == kProdWarp) {
     if (lane == 0) {
-      // the 128 input rows (rows beyond the batch and columns beyond K_0
-      // read as zero), then the weight chunks in order, up to three ahead
-      mbar_expect_tx(in_full, (uint32_t)(a.nchunks[0] * kAChunk));
-      for (int kc = 0; kc < a.nchunks[0]; ++kc)
-        tma_load_2d(sA + kc * kAChunk, &a.tm_x, kc * kKC, row0, in_full);
-      int issued = 0;
-      for (int j = 0; j < a.total_chunks; ++j) {
+      // the rest of the weight chunks in order, each into the stage the
+      // products three chunks earlier have released (the input rows and
+      // the first three chunks were issued before the set-up)
+      int issued = a.total_chunks < kStages ? a.total_chunks : kStages;
+      for (int j = kStages; j < a.total_chunks; ++j) {
         const int s = j % kStages;
-        if (j >= kStages && !mbar_wait(&empty[s], (uint32_t)((j / kStages) - 1) & 1u, &s_abort)) {
+        if (!mbar_wait(&empty[s], (uint32_t)((j / kStages) - 1) & 1u, &s_abort)) {
           s_abort = 1;
           break;
         }

@@ -1359,73 +1359,89 @@ tile_deposit_kernel(SpreadGeom g, DepositGeom dg, int64_t n, const double* __res
   if (threadIdx.x < C) s_scale[threadIdx.x] = dep_scale(absum[dg.ones + threadIdx.x], 0);
   if (threadIdx.x == 0) s_scale[C] = dep_scale((double)n, 1);  // pair weights: sum <= n
   __syncthreads();
-  for (int p = p_begin + threadIdx.x; p < p_end; p += kDepThreads) {
-    const int64_t i = rec_idx[p];
-    int ix[2] = {0, 0};
-    double fr[2] = {0.0, 0.0};
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      // the clamped cell of interp_optimized.py:60-78 (the fitted values' stencil)
-      const double t = (x[i * D + a] - dg.x0[a]) / dg.dx[a];
-      if (t < 0.0) {
-        ix[a] = 0;
-        fr[a] = 0.0;
-      } else if (t >= (double)(dg.G[a] - 1)) {
-        ix[a] = dg.G[a] - 2;
-        fr[a] = 1.0;
-      } else {
-        ix[a] = (int)t;
-        fr[a] = t - (double)ix[a];
-      }
-    }
-    double w[NC];
-    int gcell[NC], lcell[NC];
-    bool inside = true;
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      const int l = ix[a] - org[a];
-      inside = inside && l >= 0 && l + 1 < dg.win[a];
-    }
-#pragma unroll
-    for (int k = 0; k < NC; ++k) {
-      double wk = 1.0;
-      int gi = 0, li = 0;
+  // batches of kDepThreads points: first one thread per point forms its
+  // corner weights and cells (the window cell, or -1 - the global cell when
+  // the stencil leaves the window), then the (point, channel) deposits and
+  // the pair weights are spread over all threads
+  __shared__ double s_w[kDepThreads * (1 << D)];
+  __shared__ int s_cell[kDepThreads * (1 << D)];
+  for (int b0 = p_begin; b0 < p_end; b0 += kDepThreads) {
+    const int nb = min(kDepThreads, p_end - b0);
+    if (threadIdx.x < nb) {
+      const int p = b0 + threadIdx.x;
+      const int64_t i = rec_idx[p];
+      int ix[2] = {0, 0};
+      double fr[2] = {0.0, 0.0};
 #pragma unroll
       for (int a = 0; a < D; ++a) {
-        const int bit = (k >> (D - 1 - a)) & 1;
-        wk *= bit ? fr[a] : (1.0 - fr[a]);
-        gi = gi * dg.G[a] + ix[a] + bit;
-        li = li * dg.win[a] + ix[a] + bit - org[a];
+        // the clamped cell of interp_optimized.py:60-78 (the fitted values' stencil)
+        const double t = (x[i * D + a] - dg.x0[a]) / dg.dx[a];
+        if (t < 0.0) {
+          ix[a] = 0;
+          fr[a] = 0.0;
+        } else if (t >= (double)(dg.G[a] - 1)) {
+          ix[a] = dg.G[a] - 2;
+          fr[a] = 1.0;
+        } else {
+          ix[a] = (int)t;
+          fr[a] = t - (double)ix[a];
+        }
       }
-      w[k] = wk;
-      gcell[k] = gi;
-      lcell[k] = li;
-    }
-    for (int c = 0; c < C; ++c) {
-      const double vs = rec_val[(int64_t)c * n + p] * s_scale[c];
+      bool inside = true;
+#pragma unroll
+      for (int a = 0; a < D; ++a) {
+        const int l = ix[a] - org[a];
+        inside = inside && l >= 0 && l + 1 < dg.win[a];
+      }
 #pragma unroll
       for (int k = 0; k < NC; ++k) {
-        const long long q = __double2ll_rn(w[k] * vs);
-        if (q == 0) continue;
-        if (inside)
-          atomicAdd(&sacc[lcell[k] * stride + c], (unsigned long long)q);
-        else
-          atomicAdd(&qacc[(int64_t)gcell[k] * C + c], (unsigned long long)q);
+        double wk = 1.0;
+        int gi = 0, li = 0;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+          const int bit = (k >> (D - 1 - a)) & 1;
+          wk *= bit ? fr[a] : (1.0 - fr[a]);
+          gi = gi * dg.G[a] + ix[a] + bit;
+          li = li * dg.win[a] + ix[a] + bit - org[a];
+        }
+        s_w[threadIdx.x * NC + k] = wk;
+        s_cell[threadIdx.x * NC + k] = inside ? li : -1 - gi;
       }
     }
-    int pr = 0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < nb * (C + 1); e += kDepThreads) {
+      const int c = e / nb, t = e - c * nb;
+      const double* w = s_w + t * NC;
+      const int* cell = s_cell + t * NC;
+      if (c < C) {
+        const double vs = rec_val[(int64_t)c * n + b0 + t] * s_scale[c];
 #pragma unroll
-    for (int k = 0; k < NC; ++k) {
+        for (int k = 0; k < NC; ++k) {
+          const long long q = __double2ll_rn(w[k] * vs);
+          if (q == 0) continue;
+          if (cell[k] >= 0)
+            atomicAdd(&sacc[cell[k] * stride + c], (unsigned long long)q);
+          else
+            atomicAdd(&qacc[(int64_t)(-1 - cell[k]) * C + c], (unsigned long long)q);
+        }
+      } else {
+        int pr = 0;
 #pragma unroll
-      for (int k2 = k; k2 < NC; ++k2, ++pr) {
-        const long long q = __double2ll_rn((k == k2 ? 1.0 : 2.0) * w[k] * w[k2] * s_scale[C]);
-        if (q == 0) continue;
-        if (inside)
-          atomicAdd(&sacc[lcell[0] * stride + C + pr], (unsigned long long)q);
-        else
-          atomicAdd(&bacc[(int64_t)gcell[0] * NP + pr], (unsigned long long)q);
+        for (int k = 0; k < NC; ++k) {
+#pragma unroll
+          for (int k2 = k; k2 < NC; ++k2, ++pr) {
+            const long long q =
+                __double2ll_rn((k == k2 ? 1.0 : 2.0) * w[k] * w[k2] * s_scale[C]);
+            if (q == 0) continue;
+            if (cell[0] >= 0)
+              atomicAdd(&sacc[cell[0] * stride + C + pr], (unsigned long long)q);
+            else
+              atomicAdd(&bacc[(int64_t)(-1 - cell[0]) * NP + pr], (unsigned long long)q);
+          }
+        }
       }
     }
+    __syncthreads();  // the next batch overwrites the point table
   }
   __syncthreads();
   // window -> global sums, one atomic per non-zero entry

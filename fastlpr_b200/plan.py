@@ -302,7 +302,7 @@ class LprPlan:
                     st[c] = y_arr[:, c]
 
         if self._pool is None:
-            self._pool = ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1)))
+            self._pool = ThreadPoolExecutor(max_workers=max(1, min(16, os.cpu_count() or 1)))
         list(self._pool.map(stage, range(len(self.probs))))
 
     @staticmethod
