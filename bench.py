@@ -587,10 +587,11 @@ def config_workloads():
             "kde3d": (x3, None, h3, o3)}
 
 
-def run_configs(args, dev, steps: int = 3, keep: dict = None):
+def run_configs(args, dev, steps: int = 5, keep: dict = None):
     """Each other configuration through the public API with host arrays
-    (cv_fastlpr / cv_fastkde; uploads and downloads included), after one
-    warm-up call: seconds per fit by wall clock around synchronised calls."""
+    (cv_fastlpr / cv_fastkde; uploads and downloads included), after two
+    warm-up calls: seconds per fit, the median of `steps` calls timed by wall
+    clock around synchronised calls."""
     import torch
 
     import fastlpr_b200
@@ -610,15 +611,18 @@ def run_configs(args, dev, steps: int = 3, keep: dict = None):
             else:
                 def step():
                     return fastlpr_b200.cv_fastlpr(x, y, h, opts)
+            step()
             last = step()
             torch.cuda.synchronize(dev)
-            t0 = time.perf_counter()
+            times = []
             for _ in range(steps):
+                t0 = time.perf_counter()
                 step()
-            torch.cuda.synchronize(dev)
+                torch.cuda.synchronize(dev)
+                times.append(time.perf_counter() - t0)
             if keep is not None:
                 keep[name] = last
-            sec = (time.perf_counter() - t0) / steps
+            sec = float(np.median(times))
             out[name] = {"seconds_per_fit": sec, "fits_per_s": 1.0 / sec, "steps": steps,
                          "points": int(x.shape[0]), "bandwidths": int(len(h))}
         except Exception as e:  # an out-of-memory or unsupported case is reported, not fatal
