@@ -52,10 +52,6 @@ SIGNATURES = [
                             _VP, _SZ, _VP]),
     ("flpr_conv_ws", _SZ, [_VP, _I, _PI, _I, _I]),
     ("flpr_conv2d_sep_ws", _SZ, [_VP, _PI, _PI, _I, _I]),
-    ("flpr_conv2d_direct_supported", _I, [_PI, _PI, _PI, _PD, _PD, _I, _I, _PD]),
-    ("flpr_conv2d_direct_ws", _SZ, [_PI, _PI, _I, _I, _I]),
-    ("flpr_conv2d_direct", _I, [_PI, _PI, _PI, _PD, _PD, _I, _I, _PD, _D, _VP, _I, _PI, _PI,
-                                _PI, _PI, _I, _VP, _VP, _SZ, _VP]),
     ("flpr_conv2d_sep", _I, [_VP, _PI, _PI, _PI, _I, _I, _VP, _VP, _I, _PI, _PI, _PI, _D, _I, _VP,
                              _I, _VP, _SZ, _VP]),
     ("flpr_conv", _I, [_VP, _I, _PI, _PI, _PI, _I, _I, _VP, _VP, _I, _PI, _PI, _PI, _D, _I, _VP,

@@ -1355,45 +1355,6 @@ def _fused_s_planes(ctx, st, spec, kern: "_Kernel", prec: int) -> torch.Tensor:
     return S
 
 
-def _direct_ok(ctx, st, bw_rows: np.ndarray, npow: int) -> bool:
-    """Whether the direct (stencil) convolution serves these bandwidths: 2-D,
-    a separable kernel, at most 32 of them, stencils of at most 160 nodes."""
-    if st.d != 2 or st.kid not in (0, 1) or st.opts.get("_no_direct", False):
-        return False
-    g = st.geom
-    bw = np.ascontiguousarray(bw_rows, dtype=np.float64)
-    return ctx.lib.flpr_conv2d_direct_supported(
-        _lib.ivec(g.G), _lib.ivec(g.L), _lib.ivec(g.qout[0]), _lib.dvec(g.lo), _lib.dvec(g.hi),
-        bw.shape[0], npow, _lib.dvec(bw.ravel())) == 1
-
-
-def _conv_direct(ctx, st, bw_rows: np.ndarray, npow: int, scale: float, prods,
-                 add_eps: bool) -> torch.Tensor:
-    """Planes (nprod, M) of the products [(chan, hidx, pow)] by the direct
-    stencil convolution of the exact FP64 grid (flpr_conv2d_direct), one
-    call per bandwidth."""
-    g = st.geom
-    bw = np.ascontiguousarray(bw_rows, dtype=np.float64)
-    H = bw.shape[0]
-    out = ctx.empty((len(prods), g.M))
-    Lq = (_lib.ivec(g.G), _lib.ivec(g.L), _lib.ivec(g.qout[0]), _lib.dvec(g.lo),
-          _lib.dvec(g.hi))
-    groups: Dict[int, List[int]] = {}
-    for i, p in enumerate(prods):
-        groups.setdefault(int(p[1]), []).append(i)
-    for hk, idx in groups.items():
-        slots = {(int(prods[i][0]), int(prods[i][2][0])) for i in idx}
-        ws = ctx.ws(ctx.lib.flpr_conv2d_direct_ws(_lib.ivec(g.G), _lib.ivec(g.L), H, npow,
-                                                  len(slots)))
-        ctx.check(ctx.lib.flpr_conv2d_direct(
-            *Lq, H, npow, _lib.dvec(bw.ravel()), scale, st.grid64.data_ptr(), len(idx),
-            _lib.ivec([int(prods[i][0]) for i in idx]), _lib.ivec([hk] * len(idx)),
-            _lib.ivec([int(v) for i in idx for v in prods[i][2]]), _lib.ivec(idx),
-            1 if add_eps else 0, out.data_ptr(), ws.data_ptr(), ws.numel(), ctx.stream),
-            "flpr_conv2d_direct")
-    return out
-
-
 def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev, s64_all: bool = False) -> dict:
     """_evaluate_device with the first k64 bandwidths in FP64 (planes from
     the FP64 spectra) and the rest on the FP32 path; lambda (or max s) is
@@ -1421,23 +1382,9 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev, s64_all: bool = Fals
     # the FP64 group on the fused FP64 passes (S planes first: its lambda
     # floors the other group's), else on the cuFFT planes
     fused64 = _fused_ok(ctx, st, F64, max(k64, H32))
-    # bandwidths of a few grid cells: direct stencil sums instead of transforms
-    direct64 = k64 > 0 and _direct_ok(ctx, st, bw_k[:k64], npow)
     if k64:
         k64k = _kernel_rows(kern, keep[:k64], geom)
-        if direct64:
-            uniq = []
-            for e in epw:
-                if tuple(e) not in uniq:
-                    uniq.append(tuple(e))
-            Su = _conv_direct(ctx, st, bw_k[:k64], npow, kern.scale,
-                              [(0, hk, u) for u in uniq for hk in range(k64)], order == 0)
-            S64 = torch.cat([Su[uniq.index(tuple(e)) * k64:(uniq.index(tuple(e)) + 1) * k64]
-                             for e in epw], dim=0)
-            T64 = _conv_direct(ctx, st, bw_k[:k64], npow, kern.scale,
-                               [(1 + c, hk, epw[i]) for i in range(nt) for c in range(Cv)
-                                for hk in range(k64)], False)
-        elif fused64:
+        if fused64:
             S64 = _fused_s_planes(ctx, st, spec64, k64k, F64)
         else:
             S64 = _conv_s(ctx, geom, spec64, k64k, list(range(k64)), epw, F64, order == 0)
@@ -1493,7 +1440,7 @@ def _evaluate_split(ctx, st: _LprState, filt, k64: int, ev, s64_all: bool = Fals
     parts_dots, parts_s0 = [], []
     if k64:
         dots64 = ctx.empty((Cv, k64))
-        if fused64 and not direct64:
+        if fused64:
             ws = ctx.ws(lib.flpr_lpr2d_fused_ex_ws(F64, *Lq, k64, order, Cv))
             ctx.check(lib.flpr_lpr2d_fused_ex(F64, _FUSED_T, *Lq, k64, npow, order, Cv, ny,
                                               spec64.data_ptr(), k64k.data_ptr(), k64k.scale,

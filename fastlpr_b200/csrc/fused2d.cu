@@ -822,6 +822,10 @@ struct FusedTables {
   int s_nslots, t_nslots;
   ColArgs s_col, t_col;
   RowArgs s_row, t_row;
+  // S elements whose exponent an earlier element has (order 2: 6 of 21):
+  // the S pass computes each exponent once, then copies dup_src -> dup_dst
+  int ndup;
+  int dup_src[55], dup_dst[55];
 };
 
 static void design_powers2(int order, int pw[][2], int* nt) {
@@ -869,17 +873,35 @@ static int build_tables(int order, int C, FusedTables* t) {
     }
   }
   t->s_nslots = ns_slots;
+  // elements of distinct exponents (the first of each), the rest copied
+  int uq[55];
+  int nu = 0;
+  t->ndup = 0;
+  for (int e = 0; e < t->ns; ++e) {
+    int first = -1;
+    for (int f = 0; f < nu; ++f)
+      if (ep[uq[f]][0] == ep[e][0] && ep[uq[f]][1] == ep[e][1]) first = uq[f];
+    if (first < 0) {
+      uq[nu++] = e;
+    } else {
+      t->dup_src[t->ndup] = first;
+      t->dup_dst[t->ndup] = e;
+      ++t->ndup;
+    }
+  }
   int nj = 0;
-  for (int e = 0; e < t->ns; e += 2) {
+  for (int u = 0; u < nu; u += 2) {
     if (nj >= kMaxJobs) return FLPR_ERR_ARG;
+    const int e = uq[u];
     RowJob jb;
     jb.slot_a = (short)s_slot_of[ep[e][0]];
     jb.pow_a = (short)ep[e][1];
     jb.out_a = (short)e;
-    if (e + 1 < t->ns) {
-      jb.slot_b = (short)s_slot_of[ep[e + 1][0]];
-      jb.pow_b = (short)ep[e + 1][1];
-      jb.out_b = (short)(e + 1);
+    if (u + 1 < nu) {
+      const int e2 = uq[u + 1];
+      jb.slot_b = (short)s_slot_of[ep[e2][0]];
+      jb.pow_b = (short)ep[e2][1];
+      jb.out_b = (short)e2;
     } else {
       jb.slot_b = -1;
       jb.pow_b = 0;
@@ -1051,6 +1073,10 @@ static int run_fused(int mode, const FusedTables& tb, const FusedGeom& fg, int H
                                            s)));
       FLPR_TRY((launch_row_s<E1, T>(ra, hc, H, hc, b.W, F1f, b.tab1, kcut1, S, s)));
     }
+    for (int k = 0; k < tb.ndup; ++k)
+      FLPR_CUDA(cudaMemcpyAsync(S + (size_t)tb.dup_dst[k] * H * fg.M,
+                                S + (size_t)tb.dup_src[k] * H * fg.M,
+                                sizeof(T) * (size_t)H * fg.M, cudaMemcpyDeviceToDevice, s));
     if (mode == kSPass) return FLPR_OK;
     FLPR_TRY(global_scalar(order, nt, H, fg.M, S, scalar,
                            sizeof(T) == 4 ? FLPR_PREC_F32 : FLPR_PREC_F64, s));

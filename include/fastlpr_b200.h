@@ -221,29 +221,6 @@ int flpr_conv2d_sep(flpr_handle_t handle, const int* h_G, const int* h_L, const 
                     int add_eps, void* d_out, int prec, void* d_ws, size_t ws_bytes,
                     void* stream);
 
-/* (5a') flpr_conv2d_sep for short stencils, in FP64 from the real-space
- * grid: d_grid (C, L0, L1) float64 (e.g. flpr_spread_grid64), the
- * bandwidths on the host (h_bw, H x 2, as given to flpr_kernel_factors) and
- * the grid geometry (h_lo, h_hi: the kernel grid's ends per axis).  Each
- * product is the circular convolution of its channel with the sampled
- * factors (the samples flpr_kernel_factors transforms), summed over the
- * nodes with |g / h| <= 11 (the rest lie below 1e-22 of the peak), cropped
- * and times scale * L0 * L1: the planes of flpr_conv2d_sep without
- * transforms.  Products (h_chan, h_hidx, h_pow: nprod x 2 exponents) go to
- * planes h_out_index[p] (p when null) of d_out (planes of G0 x G1
- * float64).  Supported for H <= 32 and stencils of at most 160 nodes per
- * axis (flpr_conv2d_direct_supported); at most 128 products and 128
- * distinct (channel, axis-0 exponent, bandwidth) triples per call. */
-int flpr_conv2d_direct_supported(const int* h_G, const int* h_L, const int* h_qout,
-                                 const double* h_lo, const double* h_hi, int H, int npow,
-                                 const double* h_bw);
-size_t flpr_conv2d_direct_ws(const int* h_G, const int* h_L, int H, int npow, int nslots);
-int flpr_conv2d_direct(const int* h_G, const int* h_L, const int* h_qout, const double* h_lo,
-                       const double* h_hi, int H, int npow, const double* h_bw, double scale,
-                       const double* d_grid, int nprod, const int* h_chan, const int* h_hidx,
-                       const int* h_pow, const int* h_out_index, int add_eps, double* d_out,
-                       void* d_ws, size_t ws_bytes, void* stream);
-
 /* (5b) Non-separable (radial) kernels: kernel.py:310-431 (epanechnikov,
  * tricube, quartic/biweight, triweight, uniform; also gaussian and
  * gaussian_ft) for compute_kernel_fourier (convolution.py:318-652) and

@@ -350,30 +350,6 @@ def test_fused_2d_fp64_passes_match_cufft_path_and_oracle(cuda_ok, order, G):
     assert rel_err(fused.s0, o["s0"]) < 1e-9
 
 
-@pytest.mark.parametrize("order", [0, 1, 2])
-def test_sparse_bandwidths_direct_stencils_match_transforms(cuda_ok, order):
-    """The FP64 planes of the bandwidths whose kernel covers few points, by
-    direct stencil sums of the exact FP64 grid (flpr_conv2d_direct), agree
-    with the same planes by transforms and the fit with the oracle."""
-    rng = np.random.default_rng(90 + order)
-    n = 20000
-    x = rng.random((n, 2))
-    y = np.cos(2 * np.pi * x[:, 0]) * np.sin(np.pi * x[:, 1]) + 0.1 * rng.standard_normal(n)
-    hv = np.logspace(np.log10(0.004), np.log10(0.4), 12)
-    h = np.column_stack([hv, hv])
-    opts = {"order": order, "N": [200, 160]}
-    a = _fastlpr().cv_fastlpr(x, y, h, opts)
-    b = _fastlpr().cv_fastlpr(x, y, h, dict(opts, _no_direct=True))
-    assert a.metadata["fp64_bandwidths"] > 0
-    assert rel_err(a.yhat, b.yhat) < 1e-11
-    assert elem_rel_err(a.gcv_yhat["gcv_m"], b.gcv_yhat["gcv_m"]) < 1e-11
-    assert rel_err(a.gcv_yhat["dof"], b.gcv_yhat["dof"]) < 1e-11
-    o = oracle.cv_fastlpr(x, y, h, opts)
-    assert a.gcv_yhat["id1se"] == o["id1se"]
-    assert rel_err(a.yhat, o["yhat"]) < 1e-5
-    assert elem_rel_err(a.gcv_yhat["gcv_m"], o["gcv_m"]) < 1e-5
-
-
 @pytest.mark.parametrize("n,G", [(50000, [256, 256]), (300000, [200, 160])])
 def test_order2_2d_default_fp64_moment_planes_match_oracle(cuda_ok, n, G):
     """2-D local quadratic at the default precision: FP32 value channels on
