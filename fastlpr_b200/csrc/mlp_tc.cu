@@ -49,7 +49,8 @@ constexpr int kMaxLayersTc = 8;
 constexpr int kAChunk = kTM * 128;       // 16 KB
 constexpr int kBChunk = kHid * 128;      // 32 KB
 constexpr uint32_t kSpinLimit = 1u << 24;
-constexpr uint32_t kTmemCols = 256;
+constexpr int kHidChunks = kHid / kKC;   // 64-wide chunks of a hidden layer
+constexpr uint32_t kTmemCols = 2 * kHid;  // two accumulators: layer l uses columns (l % 2) * 256
 
 // instruction descriptor: D FP32, A and B BF16, both K-major, N = 256, M = 128
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) |
@@ -125,7 +126,8 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 }
 
 // bounded wait for the given phase parity of an mbarrier; gives up early
-// when another role of the CTA has given up (abort flag)
+// when another role of the CTA has given up (abort flag; null for the
+// drains of copies and products in flight, which run to the bound)
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
                                           const volatile int* abort_flag) {
   const uint32_t a = smem_u32(bar);
@@ -139,7 +141,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
-    if ((it & 1023u) == 1023u && *abort_flag) return false;
+    if (abort_flag != nullptr && (it & 1023u) == 1023u && *abort_flag) return false;
   }
   return false;
 }
@@ -210,12 +212,12 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t sA = base_u32 + pad;
   const uint32_t sB = sA + kMaxInChunks * kAChunk;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kMaxInChunks * kAChunk + kStages * kBChunk);
-  uint64_t* full = bars;                      // [kStages] chunk landed
-  uint64_t* empty = bars + kStages;           // [kStages] chunk's products done
-  uint64_t* in_full = bars + 2 * kStages;     // input rows landed
-  uint64_t* acc_full = in_full + 1;           // a layer's accumulator complete
-  uint64_t* a_ready = in_full + 2;            // next A operand written, accumulator read
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(in_full + 3);
+  uint64_t* full = bars;                       // [kStages] weight chunk landed
+  uint64_t* empty = bars + kStages;            // [kStages] chunk's products done
+  uint64_t* in_full = bars + 2 * kStages;      // [kMaxInChunks] input chunk landed
+  uint64_t* acc_full = in_full + kMaxInChunks; // a layer's accumulator complete
+  uint64_t* a_chunk = acc_full + 1;            // [kHidChunks] 64 activations of the next A written
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(a_chunk + kHidChunks);
   float* s_bias = reinterpret_cast<float*>(tmem_slot + 4);   // [nlayers - 1][256]
   float* s_wout = s_bias + (kMaxLayersTc - 1) * kHid;         // [256]
   __shared__ volatile int s_abort;
@@ -223,27 +225,32 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row0 = blockIdx.x * kTM;
   const int nhid = a.nlayers - 1;  // layers with 256 outputs
-  // the producer initialises the barriers and starts the first copies (the
-  // input rows and the first ring of weight chunks) before the CTA-wide
-  // set-up (tensor memory, bias cache) so their latency overlaps it
+  const int nin = a.nchunks[0];
+  // the producer initialises the barriers and starts the first copies
+  // (each input chunk beside the layer-0 weight chunk it meets, so the
+  // first products can start when the first pair has landed) before the
+  // CTA-wide set-up
   if (threadIdx.x == kProdWarp * 32) {
     s_abort = 0;
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(in_full, 1);
+    for (int k = 0; k < kMaxInChunks; ++k) mbar_init(&in_full[k], 1);
     mbar_init(acc_full, 1);
-    mbar_init(a_ready, kEpiWarps * 32);
+    for (int c = 0; c < kHidChunks; ++c) mbar_init(&a_chunk[c], kEpiWarps * 32);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    mbar_expect_tx(in_full, (uint32_t)(a.nchunks[0] * kAChunk));
-    for (int kc = 0; kc < a.nchunks[0]; ++kc)
-      tma_load_2d(sA + kc * kAChunk, &a.tm_x, kc * kKC, row0, in_full);
-    for (int j = 0; j < kStages && j < a.total_chunks; ++j) {
-      int l, kc;
-      chunk_of(a, j, &l, &kc);
-      mbar_expect_tx(&full[j], (uint32_t)kBChunk);
-      tma_load_2d(sB + j * kBChunk, &a.tm_w[l], kc * kKC, 0, &full[j]);
+    for (int k = 0; k < nin || (k < kStages && k < a.total_chunks); ++k) {
+      if (k < nin) {
+        mbar_expect_tx(&in_full[k], (uint32_t)kAChunk);
+        tma_load_2d(sA + k * kAChunk, &a.tm_x, k * kKC, row0, &in_full[k]);
+      }
+      if (k < kStages && k < a.total_chunks) {
+        int l, kc;
+        chunk_of(a, k, &l, &kc);
+        mbar_expect_tx(&full[k], (uint32_t)kBChunk);
+        tma_load_2d(sB + k * kBChunk, &a.tm_w[l], kc * kKC, 0, &full[k]);
+      }
     }
   }
   if (warp == 0) {
@@ -253,14 +260,6 @@ __global__ void __launch_bounds__(kThreads, 1)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
-  if (warp < kEpiWarps) {
-    for (int i = threadIdx.x; i < nhid * kHid; i += kEpiWarps * 32) {
-      const int l = i / kHid, c = i - l * kHid;
-      s_bias[i] = a.p32[a.b_off[l] + c];
-    }
-    const __nv_bfloat16* wout = a.p16 + a.w_off[a.nlayers - 1];
-    for (int c = threadIdx.x; c < kHid; c += kEpiWarps * 32) s_wout[c] = __bfloat162float(wout[c]);
-  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -269,8 +268,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == kProdWarp) {
     if (lane == 0) {
       // the rest of the weight chunks in order, each into the stage the
-      // products three chunks earlier have released (the input rows and
-      // the first three chunks were issued before the set-up)
+      // products kStages chunks earlier have released
       int issued = a.total_chunks < kStages ? a.total_chunks : kStages;
       for (int j = kStages; j < a.total_chunks; ++j) {
         const int s = j % kStages;
@@ -286,65 +284,71 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       // the copies in flight land before the CTA can leave
       for (int j = issued - 1; j >= 0 && j >= issued - kStages; --j)
-        mbar_wait(&full[j % kStages], (uint32_t)(j / kStages) & 1u, &s_abort);
-      mbar_wait(in_full, 0u, &s_abort);
+        mbar_wait(&full[j % kStages], (uint32_t)(j / kStages) & 1u, nullptr);
+      for (int k = 0; k < nin; ++k) mbar_wait(&in_full[k], 0u, nullptr);
     }
   } else if (warp == kMmaWarp) {
     if (lane == 0) {
       int last = -1;
-      if (!mbar_wait(in_full, 0u, &s_abort)) {
-        s_abort = 1;
-      } else {
-        for (int j = 0; j < a.total_chunks; ++j) {
-          const int s = j % kStages;
-          int l, kc;
-          chunk_of(a, j, &l, &kc);
-          // a new layer reads the A operand and overwrites the accumulator
-          // the previous layer's epilogue was working on
-          if (kc == 0 && l > 0 && !mbar_wait(a_ready, (uint32_t)(l - 1) & 1u, &s_abort)) {
-            s_abort = 1;
-            break;
-          }
-          if (!mbar_wait(&full[s], (uint32_t)(j / kStages) & 1u, &s_abort)) {
-            s_abort = 1;
-            break;
-          }
-          tc_fence_after();
-#pragma unroll
-          for (int kk = 0; kk < kKC / 16; ++kk) {
-            const uint64_t da = umma_desc(sA + kc * kAChunk + kk * 32);
-            const uint64_t db = umma_desc(sB + s * kBChunk + kk * 32);
-            umma_bf16(tmem, da, db, (kc > 0 || kk > 0) ? 1u : 0u);
-          }
-          umma_commit(&empty[s]);
-          if (kc == a.nchunks[l] - 1) umma_commit(acc_full);
-          last = j;
+      for (int j = 0; j < a.total_chunks; ++j) {
+        const int s = j % kStages;
+        int l, kc;
+        chunk_of(a, j, &l, &kc);
+        // the chunk's A operand: an input chunk for layer 0, else the 64
+        // activations of the previous layer's epilogue (which has also read
+        // this layer's accumulator as it was two layers back)
+        const bool a_ok = (l == 0) ? mbar_wait(&in_full[kc], 0u, &s_abort)
+                                   : mbar_wait(&a_chunk[kc], (uint32_t)(l - 1) & 1u, &s_abort);
+        if (!a_ok || !mbar_wait(&full[s], (uint32_t)(j / kStages) & 1u, &s_abort)) {
+          s_abort = 1;
+          break;
         }
+        tc_fence_after();
+        const uint32_t dacc = tmem + (uint32_t)((l & 1) * kHid);
+#pragma unroll
+        for (int kk = 0; kk < kKC / 16; ++kk) {
+          const uint64_t da = umma_desc(sA + kc * kAChunk + kk * 32);
+          const uint64_t db = umma_desc(sB + s * kBChunk + kk * 32);
+          umma_bf16(dacc, da, db, (kc > 0 || kk > 0) ? 1u : 0u);
+        }
+        umma_commit(&empty[s]);
+        if (kc == a.nchunks[l] - 1) umma_commit(acc_full);
+        last = j;
       }
       // every product issued is complete before the tensor memory is freed
       if (last >= 0)
-        mbar_wait(&empty[last % kStages], (uint32_t)(last / kStages) & 1u, &s_abort);
+        mbar_wait(&empty[last % kStages], (uint32_t)(last / kStages) & 1u, nullptr);
     }
   } else {
-    // epilogue warps: warp w reads TMEM lanes 32 w .. 32 w + 31 (its rows)
+    // epilogue warps: warp w reads TMEM lanes 32 w .. 32 w + 31 (its rows).
+    // The bias cache fills here, off the path of the first products.
+    for (int i = threadIdx.x; i < nhid * kHid; i += kEpiWarps * 32) {
+      const int l = i / kHid, c = i - l * kHid;
+      s_bias[i] = a.p32[a.b_off[l] + c];
+    }
+    const __nv_bfloat16* wout = a.p16 + a.w_off[a.nlayers - 1];
+    for (int c = threadIdx.x; c < kHid; c += kEpiWarps * 32) s_wout[c] = __bfloat162float(wout[c]);
+    asm volatile("bar.sync 1, %0;\n" ::"n"(kEpiWarps * 32) : "memory");
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
     const int m = warp * 32 + lane;
     float acc_out = 0.0f;
     bool ok = true;
     for (int l = 0; l < nhid; ++l) {
-      if (!mbar_wait(acc_full, (uint32_t)l & 1u, &s_abort)) {
+      ok = __all_sync(0xffffffffu, mbar_wait(acc_full, (uint32_t)l & 1u, &s_abort));
+      if (!ok) {
         s_abort = 1;
-        ok = false;
         break;
       }
       tc_fence_after();
       const float* bias = s_bias + l * kHid;
+      const uint32_t tacc = trow + (uint32_t)((l & 1) * kHid);
       const bool last_hidden = (l == nhid - 1);
-      if (last_hidden) acc_out = a.p32[a.b_off[l + 1]];
-      for (int c0 = 0; c0 < kHid; c0 += 64) {
+      // the output layer's dot product in eight independent partial sums
+      float part[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+      for (int c0 = 0; c0 < kHid; c0 += kKC) {
         uint32_t r[4][16];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) tmem_ld16(trow + (uint32_t)(c0 + 16 * q), r[q]);
+        for (int q = 0; q < 4; ++q) tmem_ld16(tacc + (uint32_t)(c0 + 16 * q), r[q]);
         tmem_wait_ld();
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -356,7 +360,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (last_hidden) {
 #pragma unroll
             for (int i = 0; i < 16; ++i)
-              acc_out += __bfloat162float(hv[i]) * s_wout[c0 + 16 * q + i];
+              part[(q & 1) * 4 + (i & 3)] += __bfloat162float(hv[i]) * s_wout[c0 + 16 * q + i];
           } else {
             // next layer's A operand: chunk c0 / 64, 16-byte columns 2q, 2q + 1
             unsigned char* dst = smem + (c0 / kKC) * kAChunk;
@@ -366,14 +370,18 @@ __global__ void __launch_bounds__(kThreads, 1)
                 *reinterpret_cast<const uint4*>(hv + 8);
           }
         }
+        if (!last_hidden) {
+          // generic-proxy writes of these 64 activations, and the
+          // accumulator reads so far, ordered before the next layer's
+          // products on this chunk
+          fence_async_shared();
+          tc_fence_before();
+          mbar_arrive(&a_chunk[c0 / kKC]);
+        }
       }
-      if (!last_hidden) {
-        // generic-proxy writes of the A operand, then the accumulator reads,
-        // ordered before the next layer's products
-        fence_async_shared();
-        tc_fence_before();
-        mbar_arrive(a_ready);
-      }
+      if (last_hidden)
+        acc_out = a.p32[a.b_off[l + 1]] + (((part[0] + part[1]) + (part[2] + part[3])) +
+                                           ((part[4] + part[5]) + (part[6] + part[7])));
     }
     if (ok && !s_abort) {
       const int gm = row0 + m;
@@ -392,7 +400,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 constexpr size_t kTcSmem = 1024 /* alignment */ + (size_t)kMaxInChunks * kAChunk +
-                           (size_t)kStages * kBChunk + (2 * kStages + 3) * sizeof(uint64_t) +
+                           (size_t)kStages * kBChunk +
+                           (2 * kStages + kMaxInChunks + 1 + kHidChunks) * sizeof(uint64_t) +
                            4 * sizeof(uint32_t) + sizeof(float) * (size_t)kMaxLayersTc * kHid;
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
