@@ -4,27 +4,31 @@
 // The network h_{l+1} = relu(h_l W_l^T + b_l) with hidden width 256 and one
 // output runs in ONE launch: a CTA takes 128 rows of the batch (the UMMA M),
 // keeps their activations in shared memory as the A operand of the next
-// layer (BF16, K-major, 128-byte swizzle) and accumulates every layer's
-// 128 x 256 product in tensor memory (256 FP32 columns).  The CTA is warp
-// specialised:
-//   - warp 4 (one lane) streams the weights through a ring of three 64-deep
-//     K chunks (256 rows x 128 bytes) with tensor-map copies
-//     (cp.async.bulk.tensor, 128-byte swizzle: the copy engine writes the
-//     UMMA operand layout itself, columns of W beyond its K read as zero),
-//     and the 128 input rows the same way;
-//   - warp 5 (one lane) issues the tcgen05.mma instructions (M = 128,
-//     N = 256, K = 16, BF16 x BF16 -> FP32) as soon as a chunk has landed,
-//     committing each chunk to its stage's "empty" barrier (the producer
-//     refills the stage after it) and each layer's last chunk to the
-//     accumulator barrier;
-//   - warps 0-3 (one per 32 TMEM lanes = rows) run each layer's epilogue:
-//     tcgen05.ld of the accumulator, FP32 bias (cached in shared memory),
-//     ReLU and rounding to BF16 into the next layer's A operand, then one
-//     arrival each on the "A ready" barrier the next layer's first MMA waits
-//     on; the last layer (one output) is a dot product of the last hidden
-//     row with the output weights in registers.
-// The weights of the next layer stream in while the epilogue runs.  Every
-// wait on an mbarrier is bounded: on expiry the CTA records
+// layer (BF16, K-major, 128-byte swizzle) and accumulates each layer's
+// 128 x 256 product in tensor memory, alternating between two 256-column
+// accumulators so that a layer's products can start while the previous
+// layer's epilogue is still reading its own.  The CTA is warp specialised:
+//   - warp 8 (one lane) issues the tensor-map copies (cp.async.bulk.tensor,
+//     128-byte swizzle: the copy engine writes the UMMA operand layout
+//     itself, columns beyond K read as zero): the input chunks (64 columns
+//     of the CTA's rows, each on its own barrier, the box only as tall as a
+//     batch smaller than the tile) beside the weights, which stream through
+//     a ring of three 64-deep K chunks (256 rows x 128 bytes);
+//   - warp 9 (one lane) issues the tcgen05.mma instructions (M = 128,
+//     N = 256, K = 16, BF16 x BF16 -> FP32) for a K chunk as soon as its
+//     weights and its 64 A columns are there, committing each chunk to its
+//     stage's "empty" barrier (the producer refills the stage after it) and
+//     each layer's last chunk to the accumulator barrier;
+//   - warps 0-7 run each layer's epilogue, warp w on TMEM lanes
+//     32 (w % 4) .. + 31 (its rows) and columns 128 (w / 4) .. + 127:
+//     tcgen05.ld of the accumulator, FP32 bias (cached in shared memory) on
+//     the packed two-lane adds, rounding to BF16 pairs and ReLU into the
+//     next layer's A operand, one arrival per 64 columns on the barrier the
+//     next layer's products on those K columns wait for; the last layer (one
+//     output) is a dot product of the last hidden row with the output
+//     weights on packed two-lane FMAs, the two column halves added in shared
+//     memory.
+// Every wait on an mbarrier is bounded: on expiry the CTA records
 // FLPR_ERR_TIMEOUT in the status word, the producer waits (bounded) for its
 // copies in flight, the MMA issuer for its products, and the tensor memory
 // is freed before the CTA returns.
@@ -41,10 +45,10 @@ constexpr int kHid = 256;                // hidden width (UMMA N)
 constexpr int kKC = 64;                  // K elements per chunk: one 128-byte swizzle row
 constexpr int kMaxInChunks = 7;          // input width <= 448
 constexpr int kStages = 3;               // weight chunk ring
-constexpr int kEpiWarps = 4;             // warps 0-3: TMEM lanes 0-127
-constexpr int kProdWarp = 4;             // tensor-map copies
-constexpr int kMmaWarp = 5;              // tcgen05.mma issue
-constexpr int kThreads = 32 * 6;
+constexpr int kEpiWarps = 8;             // warps 0-7: TMEM lanes 32 (w % 4) ..., columns half w / 4
+constexpr int kProdWarp = 8;             // tensor-map copies
+constexpr int kMmaWarp = 9;              // tcgen05.mma issue
+constexpr int kThreads = 32 * 10;
 constexpr int kMaxLayersTc = 8;
 constexpr int kAChunk = kTM * 128;       // 16 KB
 constexpr int kBChunk = kHid * 128;      // 32 KB
@@ -66,6 +70,7 @@ struct TcArgs {
   int nchunks[kMaxLayersTc];       // K chunks of each hidden layer
   int total_chunks;
   int batch;
+  int in_box_rows;                 // rows of each input box (the batch rounded up to 8, <= 128)
   const __nv_bfloat16* p16;
   const float* p32;
   float* out;
@@ -190,6 +195,47 @@ __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 }
 
+// FP32 pairs in one 64-bit register for the packed two-lane instructions
+// (each lane rounded as the scalar instruction)
+__device__ __forceinline__ unsigned long long f2_pack(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ float2 f2_unpack(unsigned long long r) {
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+  return v;
+}
+
+// relu(bf16(acc + bias)) of two adjacent columns as one BF16 pair, the
+// lower column in the low half: the sums on add.rn.f32x2, both roundings
+// to BF16 (nearest even) in one conversion, the ReLU on the pair (the same
+// values as rounding after the ReLU, up to the sign of a zero)
+__device__ __forceinline__ uint32_t bias_relu_bf16x2(uint32_t a0, uint32_t a1, float b0,
+                                                     float b1) {
+  unsigned long long sum;
+  asm("add.rn.f32x2 %0, %1, %2;"
+      : "=l"(sum)
+      : "l"(f2_pack(__uint_as_float(a0), __uint_as_float(a1))), "l"(f2_pack(b0, b1)));
+  const float2 v = f2_unpack(sum);
+  __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+  h = __hmax2(h, __float2bfloat162_rn(0.0f));
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+
+// acc (two FP32 lanes) += h * w on fma.rn.f32x2, the BF16 pair h widened
+// exactly to FP32
+__device__ __forceinline__ unsigned long long fma_bf16x2(uint32_t h, float w0, float w1,
+                                                         unsigned long long acc) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;"
+      : "=l"(d)
+      : "l"(f2_pack(__uint_as_float(h << 16), __uint_as_float(h & 0xffff0000u))),
+        "l"(f2_pack(w0, w1)), "l"(acc));
+  return d;
+}
+
 // the global chunk sequence: layer of chunk j and its K index within the layer
 __device__ __forceinline__ void chunk_of(const TcArgs& a, int j, int* layer, int* kc) {
   int l = 0;
@@ -218,8 +264,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* acc_full = in_full + kMaxInChunks; // a layer's accumulator complete
   uint64_t* a_chunk = acc_full + 1;            // [kHidChunks] 64 activations of the next A written
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(a_chunk + kHidChunks);
-  float* s_bias = reinterpret_cast<float*>(tmem_slot + 4);   // [nlayers - 1][256]
+  float* s_bias = reinterpret_cast<float*>(tmem_slot + 4);   // [nlayers - 1][256], 16-aligned
   float* s_wout = s_bias + (kMaxLayersTc - 1) * kHid;         // [256]
+  float* s_part = s_wout + kHid;                              // [128]
   __shared__ volatile int s_abort;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -238,11 +285,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     for (int k = 0; k < kMaxInChunks; ++k) mbar_init(&in_full[k], 1);
     mbar_init(acc_full, 1);
-    for (int c = 0; c < kHidChunks; ++c) mbar_init(&a_chunk[c], kEpiWarps * 32);
+    for (int c = 0; c < kHidChunks; ++c) mbar_init(&a_chunk[c], kEpiWarps * 16);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     for (int k = 0; k < nin || (k < kStages && k < a.total_chunks); ++k) {
       if (k < nin) {
-        mbar_expect_tx(&in_full[k], (uint32_t)kAChunk);
+        mbar_expect_tx(&in_full[k], (uint32_t)(a.in_box_rows * 128));
         tma_load_2d(sA + k * kAChunk, &a.tm_x, k * kKC, row0, &in_full[k]);
       }
       if (k < kStages && k < a.total_chunks) {
@@ -320,8 +367,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         mbar_wait(&empty[last % kStages], (uint32_t)(last / kStages) & 1u, nullptr);
     }
   } else {
-    // epilogue warps: warp w reads TMEM lanes 32 w .. 32 w + 31 (its rows).
-    // The bias cache fills here, off the path of the first products.
+    // epilogue warps: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its rows)
+    // and owns columns 128 (w / 4) .. + 127 of every layer.  The bias cache
+    // fills here, off the path of the first products.
     for (int i = threadIdx.x; i < nhid * kHid; i += kEpiWarps * 32) {
       const int l = i / kHid, c = i - l * kHid;
       s_bias[i] = a.p32[a.b_off[l] + c];
@@ -329,9 +377,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     const __nv_bfloat16* wout = a.p16 + a.w_off[a.nlayers - 1];
     for (int c = threadIdx.x; c < kHid; c += kEpiWarps * 32) s_wout[c] = __bfloat162float(wout[c]);
     asm volatile("bar.sync 1, %0;\n" ::"n"(kEpiWarps * 32) : "memory");
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-    const int m = warp * 32 + lane;
-    float acc_out = 0.0f;
+    const int quarter = warp & 3, half = warp >> 2;
+    const uint32_t trow = tmem + ((uint32_t)(quarter * 32) << 16);
+    const int m = quarter * 32 + lane;
+    float partial = 0.0f;  // this half's share of the output layer's dot product
     bool ok = true;
     for (int l = 0; l < nhid; ++l) {
       ok = __all_sync(0xffffffffu, mbar_wait(acc_full, (uint32_t)l & 1u, &s_abort));
@@ -344,30 +393,39 @@ __global__ void __launch_bounds__(kThreads, 1)
       const uint32_t tacc = trow + (uint32_t)((l & 1) * kHid);
       const bool last_hidden = (l == nhid - 1);
       // the output layer's dot product in eight independent partial sums
-      float part[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-      for (int c0 = 0; c0 < kHid; c0 += kKC) {
+      unsigned long long acc2[4] = {0ull, 0ull, 0ull, 0ull};
+#pragma unroll 1
+      for (int cc = 0; cc < kHidChunks / 2; ++cc) {
+        const int c0 = (half * (kHidChunks / 2) + cc) * kKC;
         uint32_t r[4][16];
 #pragma unroll
         for (int q = 0; q < 4; ++q) tmem_ld16(tacc + (uint32_t)(c0 + 16 * q), r[q]);
         tmem_wait_ld();
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          __align__(16) __nv_bfloat16 hv[16];
+          const float4* b4 = reinterpret_cast<const float4*>(bias + c0 + 16 * q);
+          uint32_t h2[8];
 #pragma unroll
-          for (int i = 0; i < 16; ++i)
-            hv[i] = __float2bfloat16_rn(
-                fmaxf(__uint_as_float(r[q][i]) + bias[c0 + 16 * q + i], 0.0f));
+          for (int t = 0; t < 4; ++t) {
+            const float4 bb = b4[t];
+            h2[2 * t] = bias_relu_bf16x2(r[q][4 * t], r[q][4 * t + 1], bb.x, bb.y);
+            h2[2 * t + 1] = bias_relu_bf16x2(r[q][4 * t + 2], r[q][4 * t + 3], bb.z, bb.w);
+          }
           if (last_hidden) {
+            const float4* w4 = reinterpret_cast<const float4*>(s_wout + c0 + 16 * q);
 #pragma unroll
-            for (int i = 0; i < 16; ++i)
-              part[(q & 1) * 4 + (i & 3)] += __bfloat162float(hv[i]) * s_wout[c0 + 16 * q + i];
+            for (int t = 0; t < 4; ++t) {
+              const float4 ww = w4[t];
+              acc2[(2 * t) & 3] = fma_bf16x2(h2[2 * t], ww.x, ww.y, acc2[(2 * t) & 3]);
+              acc2[(2 * t + 1) & 3] = fma_bf16x2(h2[2 * t + 1], ww.z, ww.w, acc2[(2 * t + 1) & 3]);
+            }
           } else {
             // next layer's A operand: chunk c0 / 64, 16-byte columns 2q, 2q + 1
             unsigned char* dst = smem + (c0 / kKC) * kAChunk;
             *reinterpret_cast<uint4*>(dst + sw128(m, 2 * q)) =
-                *reinterpret_cast<const uint4*>(hv);
+                make_uint4(h2[0], h2[1], h2[2], h2[3]);
             *reinterpret_cast<uint4*>(dst + sw128(m, 2 * q + 1)) =
-                *reinterpret_cast<const uint4*>(hv + 8);
+                make_uint4(h2[4], h2[5], h2[6], h2[7]);
           }
         }
         if (!last_hidden) {
@@ -379,13 +437,20 @@ __global__ void __launch_bounds__(kThreads, 1)
           mbar_arrive(&a_chunk[c0 / kKC]);
         }
       }
-      if (last_hidden)
-        acc_out = a.p32[a.b_off[l + 1]] + (((part[0] + part[1]) + (part[2] + part[3])) +
-                                           ((part[4] + part[5]) + (part[6] + part[7])));
+      if (last_hidden) {
+        float2 p[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) p[i] = f2_unpack(acc2[i]);
+        partial = ((p[0].x + p[0].y) + (p[1].x + p[1].y)) + ((p[2].x + p[2].y) + (p[3].x + p[3].y));
+      }
     }
-    if (ok && !s_abort) {
+    // the two halves' partial sums meet in shared memory (every epilogue
+    // thread reaches this barrier, also after a timeout)
+    if (half == 1) s_part[m] = partial;
+    asm volatile("bar.sync 1, %0;\n" ::"n"(kEpiWarps * 32) : "memory");
+    if (half == 0 && ok && !s_abort) {
       const int gm = row0 + m;
-      if (gm < a.batch) a.out[gm] = acc_out;
+      if (gm < a.batch) a.out[gm] = a.p32[a.b_off[nhid]] + (partial + s_part[m]);
     }
   }
   tc_fence_before();
@@ -402,7 +467,11 @@ __global__ void __launch_bounds__(kThreads, 1)
 constexpr size_t kTcSmem = 1024 /* alignment */ + (size_t)kMaxInChunks * kAChunk +
                            (size_t)kStages * kBChunk +
                            (2 * kStages + kMaxInChunks + 1 + kHidChunks) * sizeof(uint64_t) +
-                           4 * sizeof(uint32_t) + sizeof(float) * (size_t)kMaxLayersTc * kHid;
+                           4 * sizeof(uint32_t) + sizeof(float) * (size_t)(kMaxLayersTc * kHid + kTM);
+// the float4 reads of the bias cache need it on a 16-byte boundary
+static_assert(((size_t)kMaxInChunks * kAChunk + (size_t)kStages * kBChunk +
+               (2 * kStages + kMaxInChunks + 1 + kHidChunks) * sizeof(uint64_t) +
+               4 * sizeof(uint32_t)) % 16 == 0, "bias cache alignment");
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                    const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
@@ -490,7 +559,12 @@ int flpr_mlp_infer(int nlayers, const int* h_dims, const void* d_params16,
   const __nv_bfloat16* p16 = static_cast<const __nv_bfloat16*>(d_params16);
   for (int l = 0; l < nlayers - 1; ++l)
     FLPR_TRY(encode_bf16_2d(fn, &a.tm_w[l], p16 + a.w_off[l], h_dims[l], kHid, kHid));
-  FLPR_TRY(encode_bf16_2d(fn, &a.tm_x, d_x16, h_dims[0], batch, kTM));
+  // a batch smaller than the tile copies only its own rows (rounded up to
+  // 8): the tile's other rows hold stale values, whose products land in
+  // accumulator rows that no output reads (every row of D depends on its
+  // own row of A alone)
+  a.in_box_rows = batch >= kTM ? kTM : ((batch + 7) / 8) * 8;
+  FLPR_TRY(encode_bf16_2d(fn, &a.tm_x, d_x16, h_dims[0], batch, a.in_box_rows));
   a.batch = batch;
   a.p16 = p16;
   a.p32 = d_params32;
