@@ -437,7 +437,7 @@ def run_batched(args, dev, world: int = 1, rank: int = 0, barrier=lambda: None,
     s = torch.cuda.Event(enable_timing=True)
     e = torch.cuda.Event(enable_timing=True)
     s.record()
-    plan.graph.replay()
+    plan.replay()
     e.record()
     e.synchronize()
     replay_ms = s.elapsed_time(e)
@@ -506,7 +506,7 @@ def run_learned_batched(args, dev, plain_fits_per_s: float):
         s = torch.cuda.Event(enable_timing=True)
         e = torch.cuda.Event(enable_timing=True)
         s.record()
-        plan.graph.replay()
+        plan.replay()
         e.record()
         e.synchronize()
         replay_ms = s.elapsed_time(e)

@@ -14,14 +14,19 @@ reductions, the 1-SE choice, the fitted values at the chosen bandwidth and
 the copies of every output into pinned host buffers -- is captured once into
 a CUDA graph and replayed by ``run``.  The problems are spread over several
 streams inside the graph (largest first, each to the least loaded stream),
-so small and large data sets of uneven size run concurrently.  A run is one
-replay and one synchronisation for all problems.
+so small and large data sets of uneven size run concurrently.  A plan of
+many full-sweep problems is captured as a few graphs over consecutive
+parts of that order (about 1/8, 1/8, 1/4 and 1/2 of the response bytes),
+each replayed on its own stream as soon as its responses are staged: the
+host stages the later parts while the device fits the earlier ones.  A run
+is one replay of each graph and one synchronisation for all problems.
 
 ``cv_fastlpr_many`` runs a list of problems once (eagerly, on the same
 streams, no capture).
 """
 from __future__ import annotations
 
+import collections
 import os
 import time
 from concurrent.futures import ThreadPoolExecutor
@@ -36,6 +41,18 @@ from .structures import RegressionOutput
 
 class _Problem:
     pass
+
+
+class _Segment:
+    """One captured graph: the problems it fits (issue order), their
+    captured outputs, its NaN/Inf flag and the stream it replays on."""
+
+    def __init__(self, idx, graph, outs, finite, stream):
+        self.idx = idx
+        self.graph = graph
+        self.outs = outs
+        self.finite = finite
+        self.stream = stream
 
 
 def _cost(p) -> float:
@@ -124,7 +141,7 @@ class LprPlan:
             self._setup_learned()
             self._pool = None
             self._finite = None
-            self._write_y([p.su.y_arr for p in self.probs])
+            self._write_y([p.su.y_arr for p in self.probs], range(len(self.probs)))
             for p in self.probs:
                 self._check_finite(bool(np.all(np.isfinite(p.staging.numpy()))))
             # downloads of each problem's outputs, issued behind its last
@@ -135,8 +152,7 @@ class LprPlan:
             # (a rejected run leaves them there; a replay without new
             # responses would fit them)
             self._y_ok = True
-            self.graph = None
-            self.outs = None
+            self.segs = None
             self.tuning = None
             if autotune and graph:
                 self.tuning = self._autotune()
@@ -166,17 +182,50 @@ class LprPlan:
             load[k] += _cost(self.probs[i])
         self.order = order
 
+    def _segment_order(self) -> List[List[int]]:
+        """The issue order cut into consecutive parts of about 1/8, 1/8, 1/4
+        and 1/2 of the staged response bytes (one part for fewer than eight
+        problems or when the learned proposal chain joins all problems)."""
+        if self.prop is not None or len(self.order) < 8:
+            return [list(self.order)]
+        sizes = [self.probs[i].staging.numel() for i in self.order]
+        total = float(sum(sizes))
+        bounds = (total / 8, total / 4, total / 2)
+        segs = [[] for _ in range(len(bounds) + 1)]
+        acc = 0.0
+        for i, sz in zip(self.order, sizes):
+            segs[sum(acc >= b for b in bounds)].append(i)
+            acc += sz
+        return [sg for sg in segs if sg]
+
     def _capture(self) -> None:
         # eager pass: cuFFT plans, kernel attributes, output buffers
-        outs = self._issue()
+        outs = self._issue(self.order)
         torch.cuda.synchronize(self.device)
         del outs
-        self.graph = torch.cuda.CUDAGraph()
-        cap = torch.cuda.Stream(self.device)
-        cap.wait_stream(torch.cuda.current_stream(self.device))
-        with torch.cuda.graph(self.graph, stream=cap):
-            self.outs = self._issue()
+        # one graph per part, each with its own memory pool (the parts'
+        # replays overlap on the device)
+        self.segs = []
+        for idx in self._segment_order():
+            graph = torch.cuda.CUDAGraph()
+            cap = torch.cuda.Stream(self.device)
+            cap.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.graph(graph, stream=cap):
+                outs = self._issue(idx)
+            self.segs.append(_Segment(idx, graph, outs, self._finite,
+                                      torch.cuda.Stream(self.device)))
         torch.cuda.synchronize(self.device)
+
+    def replay(self) -> None:
+        """Replay every captured graph on the staged responses (each on its
+        stream, joined back into the current stream)."""
+        main = torch.cuda.current_stream(self.device)
+        for sg in self.segs:
+            sg.stream.wait_stream(main)
+            with torch.cuda.stream(sg.stream):
+                sg.graph.replay()
+        for sg in self.segs:
+            main.wait_stream(sg.stream)
 
     def _autotune(self) -> dict:
         """Streams x spread work-item size, timed as graph replays."""
@@ -194,9 +243,8 @@ class LprPlan:
             at.set_params({"spread_item_points": c["spread_item_points"]})
             self._set_streams(c["streams"])
             self._capture()
-            ms = at.time_ms(self.graph.replay, device=self.device)
-            self.graph = None
-            self.outs = None
+            ms = at.time_ms(self.replay, device=self.device)
+            self.segs = None
             return ms
 
         try:
@@ -272,11 +320,10 @@ class LprPlan:
         p.staging = torch.empty((nch, su.n), dtype=torch.float64, pin_memory=True)
         return p
 
-    def _write_y(self, ys) -> None:
-        """Copy the responses into the pinned staging rows (a few host threads:
-        numpy's copies release the GIL).  The upload to the device and the
-        NaN/Inf check are part of the issued work (_upload_y), so in a graph
-        they overlap the other problems' kernels."""
+    def _check_y(self, ys) -> list:
+        """The responses as (n, dy) arrays, checked against the plan."""
+        if len(ys) != len(self.probs):
+            raise ValueError(f"expected {len(self.probs)} responses, got {len(ys)}")
         arrs = []
         for p, y in zip(self.probs, ys):
             y_arr = np.asarray(y)
@@ -290,6 +337,14 @@ class LprPlan:
             if bool(np.iscomplexobj(y_arr)) != p.su.y_is_complex:
                 raise ValueError("a response changed between real and complex")
             arrs.append(y_arr)
+        return arrs
+
+    def _write_y(self, arrs, idx) -> None:
+        """Copy the responses of problems `idx` into their pinned staging
+        rows (a few host threads: numpy's copies release the GIL).  The
+        upload to the device and the NaN/Inf check are part of the issued
+        work (_upload_y), so in a graph they overlap the other problems'
+        kernels."""
 
         def stage(i):
             p, y_arr = self.probs[i], arrs[i]
@@ -303,7 +358,7 @@ class LprPlan:
 
         if self._pool is None:
             self._pool = ThreadPoolExecutor(max_workers=max(1, min(16, os.cpu_count() or 1)))
-        list(self._pool.map(stage, range(len(self.probs))))
+        list(self._pool.map(stage, idx))
 
     @staticmethod
     def _upload_y(p) -> torch.Tensor:
@@ -318,9 +373,10 @@ class LprPlan:
         if flag is not None and not bool(flag):
             raise ValueError("Response y contains NaN or Inf values")
 
-    def _issue(self):
-        """Enqueue the y-dependent stages of every problem on its stream, up
-        to its outputs in the pinned buffers.  Problems with the learned
+    def _issue(self, idx) -> dict:
+        """Enqueue the y-dependent stages of problems `idx` (issue order) on
+        their streams, up to their outputs in the pinned buffers; returns
+        {problem: (state, results, pending outputs)}.  Problems with the learned
         search stop after their binned sums; the proposal chain then runs
         once for all of them on the main stream, and each evaluates the
         window it chose (kernel factors gathered on the device) up to its
@@ -328,10 +384,10 @@ class LprPlan:
         main = torch.cuda.current_stream(self.device)
         for s in self.streams:
             s.wait_stream(main)
-        outs = [None] * len(self.probs)
+        outs = {}
         states = {}
         flags = []
-        for i in self.order:
+        for i in idx:
             p = self.probs[i]
             su = p.su
             if getattr(p, "done", None) is None:
@@ -366,7 +422,7 @@ class LprPlan:
             self.t_h.copy_(self.prop.t, non_blocking=True)
             for s in self.streams:
                 s.wait_stream(main)
-            for i in self.order:
+            for i in idx:
                 if i not in states:
                     continue
                 p, st = self.probs[i], states[i]
@@ -392,8 +448,10 @@ class LprPlan:
             timings: Optional[dict] = None) -> List[RegressionOutput]:
         """Fit every problem (with new responses `ys` if given).  timings
         (optional dict): accumulates host wall seconds of the stages
-        'stage' (responses into the pinned staging rows), 'enqueue' (replay
-        and downloads issued), 'wait' (device done) and 'results'."""
+        'stage' (responses into the pinned staging rows and the graphs
+        launched), 'enqueue' (downloads issued, results built as they
+        arrive), 'wait' (device done) and 'results' (the remaining
+        results)."""
         clock = [time.perf_counter()]
 
         def mark(name):
@@ -406,41 +464,82 @@ class LprPlan:
             if ys is None and not self._y_ok:
                 raise ValueError("Response y contains NaN or Inf values (the last responses "
                                  "given to run were rejected; pass new responses)")
-            if ys is not None:
-                if len(ys) != len(self.probs):
-                    raise ValueError(f"expected {len(self.probs)} responses, got {len(ys)}")
-                self._write_y(ys)
-            mark("stage")
-            if self.graph is not None:
-                self.graph.replay()
-                outs = self.outs
+            arrs = self._check_y(ys) if ys is not None else None
+            main = torch.cuda.current_stream(self.device)
+            if self.segs is not None:
+                # each part's graph starts as soon as its responses are staged
+                outs = {}
+                for sg in self.segs:
+                    if arrs is not None:
+                        self._write_y(arrs, sg.idx)
+                    sg.stream.wait_stream(main)
+                    with torch.cuda.stream(sg.stream):
+                        sg.graph.replay()
+                    outs.update(sg.outs)
+                for sg in self.segs:
+                    main.wait_stream(sg.stream)
+                flag = (self.segs[0].finite if len(self.segs) == 1 else
+                        torch.cat([sg.finite for sg in self.segs]).all().reshape(1))
             else:
-                outs = self._issue()
-            finite = api._to_host(self._finite)
+                if arrs is not None:
+                    self._write_y(arrs, range(len(self.probs)))
+                outs = self._issue(self.order)
+                flag = self._finite
+            mark("stage")
+            finite = api._to_host(flag)
             # each problem's outputs go into fresh pinned memory (no host
             # copies; the results stay valid after later runs) on the copy
-            # stream, as soon as that problem's last kernel is done
-            pends = []
+            # stream, as soon as that problem's last kernel is done (in issue
+            # order, which is about the order the problems finish).  The
+            # full-sweep results are built while the device still works on
+            # later problems; the NaN/Inf check of the responses comes after
+            # all of them (results of rejected responses are dropped, and a
+            # build that fails before the check is repeated after it).
+            pends, done = {}, {}
+            res = [None] * len(self.probs)
+            ready, deferred = collections.deque(), []
+            ev = api._PhaseEvents(None)
+
+            def build(i):
+                p = self.probs[i]
+                st, r, _ = outs[i]
+                return api._finalize_build(self._ctx, st, r, pends[i], ev,
+                                           dict(p.search) if p.search else None)
+
+            def drain(block):
+                while ready and (block or done[ready[0]].query()):
+                    i = ready.popleft()
+                    done[i].synchronize()
+                    try:
+                        res[i] = build(i)
+                    except Exception:  # noqa: BLE001 - repeated after the check
+                        deferred.append(i)
+
             with torch.cuda.stream(self._copy):
-                for p, (st, r, pend) in zip(self.probs, outs):
+                for i in self.order:
+                    p = self.probs[i]
+                    st, r, pend = outs[i]
                     self._copy.wait_event(p.done)
-                    pends.append({k: (api._to_host(v) if isinstance(v, torch.Tensor)
-                                      and v.is_cuda else v) for k, v in pend.items()})
+                    pends[i] = {k: (api._to_host(v) if isinstance(v, torch.Tensor)
+                                    and v.is_cuda else v) for k, v in pend.items()}
+                    if p.lidx is None:
+                        done[i] = torch.cuda.Event()
+                        done[i].record(self._copy)
+                        ready.append(i)
+                    drain(False)
             mark("enqueue")
-            torch.cuda.current_stream(self.device).synchronize()
+            main.synchronize()
             self._copy.synchronize()
             mark("wait")
+            drain(True)
             self._y_ok = bool(finite[0])
             self._check_finite(finite[0])
-            ev = api._PhaseEvents(None)
-            res = []
+            for i in deferred:
+                res[i] = build(i)
             for i, p in enumerate(self.probs):
-                st, r, _ = outs[i]
-                if p.lidx is None:
-                    res.append(api._finalize_build(self._ctx, st, r, pends[i], ev,
-                                                   dict(p.search) if p.search else None))
-                else:
-                    res.append(self._finish_learned(p, st, r, pends[i], ev))
+                if p.lidx is not None:
+                    st, r, _ = outs[i]
+                    res[i] = self._finish_learned(p, st, r, pends[i], ev)
             mark("results")
             return res
 

@@ -67,6 +67,10 @@ def test_plan_matches_single_fits(cuda_ok, graph):
     import fastlpr_b200
     probs = _problems()
     plan = fastlpr_b200.LprPlan(probs, graph=graph, streams=4)
+    if graph:
+        # ten problems: captured as several graphs, staged and replayed in turn
+        assert len(plan.segs) > 1
+        assert sorted(i for sg in plan.segs for i in sg.idx) == list(range(len(probs)))
     got = plan.run()
     for (x, y, h, o), g in zip(probs, got):
         ref = fastlpr_b200.cv_fastlpr(x, y, h, o)
@@ -96,6 +100,25 @@ def test_plan_replay_is_reproducible(cuda_ok):
     b = plan.run([p[1] for p in probs])
     for ra, rb in zip(a, b):
         _same(ra, rb, 1e-12)
+
+
+def test_segmented_plan_rejects_nonfinite_response_of_last_part(cuda_ok):
+    # a NaN in a problem of the last captured graph is caught like one in
+    # the first; the next finite run fits all problems again
+    import fastlpr_b200
+    probs = _problems()
+    plan = fastlpr_b200.LprPlan(probs, streams=4)
+    assert len(plan.segs) > 1
+    last = plan.segs[-1].idx[-1]
+    bad = [p[1].copy() for p in probs]
+    bad[last][3] = np.nan
+    with pytest.raises(ValueError, match="NaN or Inf"):
+        plan.run(bad)
+    with pytest.raises(ValueError, match="NaN or Inf"):
+        plan.run()
+    got = plan.run([p[1] for p in probs])
+    for (x, y, h, o), g in zip(probs, got):
+        _same(g, fastlpr_b200.cv_fastlpr(x, y, h, o), _tol(o))
 
 
 def test_plan_rejects_nonfinite_responses_and_recovers(cuda_ok):

@@ -223,3 +223,34 @@ def test_result_layout_matches_channel_rows(dy, cplx):
     ref = ref[0] if dy == 1 else ref.T
     assert got.shape == ref.shape and got.dtype == ref.dtype
     np.testing.assert_array_equal(got, ref)
+
+
+def test_plan_segments_cut_issue_order_by_staged_bytes():
+    # the captured graphs of a plan cover consecutive parts of the issue
+    # order, the first about 1/8 of the staged response bytes
+    import torch
+
+    from fastlpr_b200.plan import LprPlan, _Problem
+
+    rng = np.random.default_rng(3)
+    sizes = rng.integers(1000, 100000, 40)
+    stub = type("Stub", (), {})()
+    stub.prop = None
+    stub.probs = []
+    for n in sizes:
+        p = _Problem()
+        p.staging = torch.empty((1, int(n)), dtype=torch.float64)
+        stub.probs.append(p)
+    stub.order = sorted(range(len(sizes)), key=lambda i: -sizes[i])
+    segs = LprPlan._segment_order(stub)
+    assert len(segs) == 4
+    assert [i for sg in segs for i in sg] == stub.order
+    total = float(sizes.sum())
+    first = float(sum(sizes[i] for i in segs[0]))
+    assert first - sizes[segs[0][-1]] < total / 8 <= first
+    # few problems, or a learned proposal chain: one graph
+    stub.order = stub.order[:5]
+    assert LprPlan._segment_order(stub) == [stub.order]
+    stub.order = sorted(range(len(sizes)), key=lambda i: -sizes[i])
+    stub.prop = object()
+    assert LprPlan._segment_order(stub) == [stub.order]
