@@ -112,6 +112,26 @@ inline int sm_count() {
   return cached;
 }
 
+// Raise the dynamic shared-memory limit of `kernel` on the current device
+// to at least `bytes`.  The limit never goes down: a launch is checked
+// against the limit in force when it starts, so a launch captured in a CUDA
+// graph (or a profiler's replay of it) with a larger size stays valid after
+// a later launch of the same kernel asked for less.
+template <typename K>
+inline cudaError_t raise_dyn_smem(K kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> limit_of;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& lim = limit_of[std::make_pair(dev, reinterpret_cast<const void*>(kernel))];
+  if (bytes <= lim) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) lim = bytes;
+  return e;
+}
+
 // Shared-memory carveout of `kernel` sized for as many CTAs per SM as its
 // registers and `dyn_smem` allow at the largest carveout; the rest of the
 // unified L1/shared array stays L1.  Both attributes are set on every call
@@ -124,9 +144,7 @@ inline cudaError_t fit_carveout(K kernel, int threads, size_t dyn_smem) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)dyn_smem)) != cudaSuccess)
-    return e;
+  if ((e = raise_dyn_smem(kernel, dyn_smem)) != cudaSuccess) return e;
   const auto key = std::make_tuple(dev, reinterpret_cast<const void*>(kernel), dyn_smem, threads);
   int pct = -1;
   {

@@ -277,8 +277,7 @@ int flpr_learned_features(int B, const double* d_bins, const int* d_meta, const 
   FLPR_CHECK_ARG(d_bins && d_meta && d_fmean && d_fstd && d_x16,
                  "learned_features: null pointer");
   const size_t smem = sizeof(double) * 3 * kFeatCells;
-  FLPR_CUDA(cudaFuncSetAttribute(features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
+  FLPR_CUDA(raise_dyn_smem(features_kernel, smem));
   features_kernel<<<B, kFeatThreads, smem, as_stream(stream)>>>(
       d_bins, d_meta, d_fmean, d_fstd, d_feat, static_cast<__nv_bfloat16*>(d_x16));
   FLPR_LAUNCH_CHECK();

@@ -570,8 +570,7 @@ int flpr_mlp_infer(int nlayers, const int* h_dims, const void* d_params16,
   a.p32 = d_params32;
   a.out = d_out;
   a.status = d_status;
-  FLPR_CUDA(cudaFuncSetAttribute(mlp_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kTcSmem));
+  FLPR_CUDA(raise_dyn_smem(mlp_infer_tc_kernel, kTcSmem));
   const int grid = (batch + kTM - 1) / kTM;
   mlp_infer_tc_kernel<<<grid, kThreads, kTcSmem, as_stream(stream)>>>(a);
   FLPR_LAUNCH_CHECK();

@@ -959,7 +959,7 @@ static int launch_accumulate(const SpreadGeom& g, int64_t n, int nchan, int ones
                              cudaStream_t s) {
   if (fixed) {
     auto k = tile_accumulate_kernel<long long, double, NT1>;
-    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLPR_CUDA(raise_dyn_smem(k, smem));
     FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    cudaSharedmemCarveoutMaxShared));
     k<<<grid, kSpreadThreads, smem, s>>>(g, n, nchan, ones_channel, cg, w.offsets, w.items,
@@ -968,7 +968,7 @@ static int launch_accumulate(const SpreadGeom& g, int64_t n, int nchan, int ones
                                          (long long*)w.gacc);
   } else {
     auto k = tile_accumulate_kernel<double, double, NT1>;
-    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLPR_CUDA(raise_dyn_smem(k, smem));
     FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    cudaSharedmemCarveoutMaxShared));
     k<<<grid, kSpreadThreads, smem, s>>>(g, n, nchan, ones_channel, cg, w.offsets, w.items,
@@ -987,7 +987,7 @@ static int launch_accumulate_2d(const SpreadGeom& g, int64_t n, int nchan, int o
   const size_t smem = smem_2d(g.W[0], NT1, cg);
   if (fixed) {
     auto k = tile_accumulate_2d_kernel<long long, NT1>;
-    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLPR_CUDA(raise_dyn_smem(k, smem));
     FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    cudaSharedmemCarveoutMaxShared));
     k<<<grid, kBatch2, smem, s>>>(g, n, nchan, ones_channel, cg, w.offsets, w.items, w.rec_base,
@@ -995,7 +995,7 @@ static int launch_accumulate_2d(const SpreadGeom& g, int64_t n, int nchan, int o
                                   margin, (long long*)w.gacc);
   } else {
     auto k = tile_accumulate_2d_kernel<double, NT1>;
-    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLPR_CUDA(raise_dyn_smem(k, smem));
     FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    cudaSharedmemCarveoutMaxShared));
     k<<<grid, kBatch2, smem, s>>>(g, n, nchan, ones_channel, cg, w.offsets, w.items, w.rec_base,
@@ -1023,13 +1023,13 @@ static int launch_columns_3d(const SpreadGeom& g, int64_t n, int nchan, int ones
   const size_t smem = smem_3d(NT1);
   if (fixed) {
     auto k = tile_columns_3d_kernel<long long, NT1>;
-    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLPR_CUDA(raise_dyn_smem(k, smem));
     k<<<grid, kThreads3, smem, s>>>(g, n, ones_channel, w.offsets, w.items, w.rec_base,
                                     (const double*)w.rec_frac, (const double*)w.rec_val, w.absum,
                                     margin, (long long*)w.gacc);
   } else {
     auto k = tile_columns_3d_kernel<double, NT1>;
-    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLPR_CUDA(raise_dyn_smem(k, smem));
     k<<<grid, kThreads3, smem, s>>>(g, n, ones_channel, w.offsets, w.items, w.rec_base,
                                     (const double*)w.rec_frac, (const double*)w.rec_val, nullptr,
                                     margin, (double*)w.gacc);
@@ -1601,13 +1601,13 @@ int flpr_deposit_sorted(int d, int64_t n, const double* d_x, const int* h_L, int
   for (int c = 0; c < C; ++c) cp.col[c] = h_cols[c];
   if (d == 2) {
     auto k = tile_deposit_kernel<2>;
-    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLPR_CUDA(raise_dyn_smem(k, smem));
     k<<<(unsigned)nitems, kDepThreads, smem, s>>>(
         g, dg, n, d_x, w.offsets, w.items, w.rec_idx, (const double*)w.rec_val, w.absum,
         reinterpret_cast<unsigned long long*>(d_Q), reinterpret_cast<unsigned long long*>(d_B));
   } else {
     auto k = tile_deposit_kernel<1>;
-    FLPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLPR_CUDA(raise_dyn_smem(k, smem));
     k<<<(unsigned)nitems, kDepThreads, smem, s>>>(
         g, dg, n, d_x, w.offsets, w.items, w.rec_idx, (const double*)w.rec_val, w.absum,
         reinterpret_cast<unsigned long long*>(d_Q), reinterpret_cast<unsigned long long*>(d_B));

@@ -153,6 +153,7 @@ class LprPlan:
             # responses would fit them)
             self._y_ok = True
             self.segs = None
+            self._graph_downloads = False
             self.tuning = None
             if autotune and graph:
                 self.tuning = self._autotune()
@@ -202,6 +203,15 @@ class LprPlan:
         # eager pass: cuFFT plans, kernel attributes, output buffers
         outs = self._issue(self.order)
         torch.cuda.synchronize(self.device)
+        if self.prop is None:
+            # full sweeps: every output also gets a pinned buffer of the plan,
+            # so each problem's downloads are captured on its own stream
+            # right behind its last kernel
+            for i, p in enumerate(self.probs):
+                for k, t in outs[i][2].items():
+                    if isinstance(t, torch.Tensor) and t.is_cuda:
+                        p.bufs[k] = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            self._graph_downloads = True
         del outs
         # one graph per part, each with its own memory pool (the parts'
         # replays overlap on the device)
@@ -487,6 +497,8 @@ class LprPlan:
                 flag = self._finite
             mark("stage")
             finite = api._to_host(flag)
+            if self._graph_downloads:
+                return self._collect(outs, finite, main, mark)
             # each problem's outputs go into fresh pinned memory (no host
             # copies; the results stay valid after later runs) on the copy
             # stream, as soon as that problem's last kernel is done (in issue
@@ -542,6 +554,47 @@ class LprPlan:
                     res[i] = self._finish_learned(p, st, r, pends[i], ev)
             mark("results")
             return res
+
+    def _collect(self, outs, finite, main, mark) -> List[RegressionOutput]:
+        """Results of a replay whose downloads are in the graphs: as each
+        problem's event fires (issue order) a worker thread builds its
+        result, copying the outputs out of the plan's pinned buffers (the
+        results stay valid after later runs).  The NaN/Inf check of the
+        responses comes after all of them; a build that failed before it is
+        repeated after it."""
+        ev = api._PhaseEvents(None)
+
+        def build(i):
+            p = self.probs[i]
+            st, r, pend = outs[i]
+            return api._finalize_build(self._ctx, st, r, pend, ev,
+                                       dict(p.search) if p.search else None, copy=True)
+
+        def attempt(i):
+            try:
+                return build(i), None
+            except Exception as exc:  # noqa: BLE001 - repeated after the check
+                return None, exc
+
+        futs = {}
+        for i in self.order:
+            self.probs[i].done.synchronize()
+            futs[i] = self._pool.submit(attempt, i)
+        mark("enqueue")
+        main.synchronize()
+        mark("wait")
+        res = [None] * len(self.probs)
+        failed = []
+        for i, f in futs.items():
+            res[i], exc = f.result()
+            if exc is not None:
+                failed.append(i)
+        self._y_ok = bool(finite[0])
+        self._check_finite(finite[0])
+        for i in failed:
+            res[i] = build(i)
+        mark("results")
+        return res
 
     def _finish_learned(self, p, st, r, pend, ev) -> RegressionOutput:
         """Acceptance of a learned problem's window after the replay; the
