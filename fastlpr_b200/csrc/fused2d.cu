@@ -392,7 +392,7 @@ struct ColArgs {
 // cropped column in its own transpose buffer; the CTA then writes 8-column
 // row segments.
 template <int E, typename T>
-__global__ void __launch_bounds__(kColWarps * 32, (sizeof(T) == 4 || E <= 16) ? 2 : 1)
+__global__ void __launch_bounds__(kColWarps * 32, sizeof(T) == 4 ? (E <= 16 ? 3 : 2) : (E <= 16 ? 2 : 1))
 colpass_kernel(ColArgs ca, const typename Vec2<T>::V* __restrict__ Yt,
                const typename Vec2<T>::V* __restrict__ F0f,
                const typename Vec2<T>::V* __restrict__ tab, const int* __restrict__ kcut1,
@@ -537,7 +537,7 @@ __device__ __forceinline__ void row_fft(const RowArgs& ra, const RowJob& jb, int
 // (row, job).  S planes (ns, H, G0*G1) in the pass precision, written
 // straight from the registers (consecutive lanes hold consecutive x1).
 template <int E, typename T>
-__global__ void __launch_bounds__(kRowWarps * 32, (sizeof(T) == 4 || E <= 16) ? 2 : 1)
+__global__ void __launch_bounds__(kRowWarps * 32, sizeof(T) == 4 ? (E <= 16 ? 3 : 2) : (E <= 16 ? 2 : 1))
 rowpass_s_kernel(RowArgs ra, int H, int nslots_w, const typename Vec2<T>::V* __restrict__ W,
                  const typename Vec2<T>::V* __restrict__ F1f,
                  const typename Vec2<T>::V* __restrict__ tab, const int* __restrict__ kcut1,
@@ -695,7 +695,7 @@ __device__ __forceinline__ void rowpass_t_solve_body(
 
 // FP32: four CTAs of four warps per SM at the 112-register cap.
 template <int E, int NT>
-__global__ void __maxnreg__(112)
+__global__ void __maxnreg__(E <= 16 ? 80 : 112)
 rowpass_t_solve_kernel(RowArgs ra, int H, int nslots_w, const float2* __restrict__ W,
                        const float2* __restrict__ F1f, const float2* __restrict__ tab,
                        const int* __restrict__ kcut1, int C, int ny, const double* __restrict__ zg,
