@@ -635,7 +635,9 @@ def run_profile_case(args, dev):
     profiles: 'kde3d' (3-D KDE, grid 128^3), 'learned' (learned search on
     the benchmark data), 'cubic2d' (2-D, n = 3000: cubic GCV/DoF), 'order2'
     (2-D local quadratic, FP64 separable convolution), 'hetero2d' (the full
-    2-D local-quadratic mean + variance pair of config_workloads)."""
+    2-D local-quadratic mean + variance pair of config_workloads),
+    'batched64' (the first 64 problems of the batched workload through
+    cv_fastlpr_many: the plan's streams and kernels, launched eagerly)."""
     import torch
 
     import fastlpr_b200
@@ -644,6 +646,9 @@ def run_profile_case(args, dev):
     if case == "kde3d":
         x, h, o = kde3d_workload(args.points)
         r = fastlpr_b200.cv_fastkde(x, h, dict(o, device=str(dev)))
+    elif case == "batched64":
+        rs = fastlpr_b200.cv_fastlpr_many(batched_workload(count=512)[:64], device=dev)
+        r = rs[0]
     elif case == "hetero2d":
         x, y, h, o = config_workloads()["lpr2d_o2_hetero"]
         opts = dict(o, device=str(dev))
@@ -988,7 +993,8 @@ def main():
     ap.add_argument("--only-batched", action="store_true",
                     help="run only the batched workload leg (profiling)")
     ap.add_argument("--profile-case", default="",
-                    choices=["", "kde3d", "learned", "cubic2d", "order2", "hetero2d"],
+                    choices=["", "kde3d", "learned", "cubic2d", "order2", "hetero2d",
+                             "batched64"],
                     help="run one small fit of another kind (profiling)")
     ap.add_argument("--single-fit", action="store_true",
                     help="run one plain fit of the workload and exit (for profilers)")
