@@ -590,7 +590,7 @@ tile_accumulate_2d_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, 
       const int pos = off[lc] + rank;
       const int p = b0 + q;
       const double f0 = rec_frac[p], f1 = rec_frac[n + p];
-#pragma unroll
+#pragma unroll 1
       for (int j = 0; j < NT1; ++j) {
         const double d0 = f0 - hx0 * (double)(j - MSP);
         const double d1 = f1 - hx1 * (double)(j - MSP);
@@ -619,6 +619,7 @@ tile_accumulate_2d_kernel(SpreadGeom g, int64_t n, int nchan, int ones_channel, 
 #pragma unroll
       for (int cr = 0; cr < kT2; ++cr) {
         const int pe = off[rowbase + cr + 1];
+#pragma unroll 1
         for (int pp = off[rowbase + cr]; pp < pe; ++pp) {
           const double wyv = wy[pp * NT1 + jy];
           double v[kUnitCh];
