@@ -1007,7 +1007,7 @@ def _prepare_lpr(ctx, x_arr, y_arr, dy, opts, order, prec, variance, y_is_comple
                  bandwidths: Optional[np.ndarray] = None) -> _LprState:
     """Bandwidth-independent stage.  `hook(dx, ycols, stats, n, d, d_stats=None)`
     runs once the point statistics exist, before the spread is enqueued (the
-    learned search starts its data summary there, on a side stream); on the
+    learned search enqueues its data summary there, ahead of the spread); on the
     path whose knot maps are formed on the device it gets the device
     statistics (d_stats: minima then maxima) instead of the host ones.  With `stats` (the
     point statistics of these device inputs, already checked) nothing here
@@ -1710,44 +1710,29 @@ def _finalize_build(ctx, st: _LprState, r: dict, pend: dict, ev, search,
 _MAX_WALKS = 3
 
 
-_SIDE_STREAMS: Dict[int, torch.cuda.Stream] = {}
-
-
-def _side_stream(device: torch.device) -> torch.cuda.Stream:
-    idx = device.index if device.index is not None else torch.cuda.current_device()
-    if idx not in _SIDE_STREAMS:
-        _SIDE_STREAMS[idx] = torch.cuda.Stream(device=device)
-    return _SIDE_STREAMS[idx]
-
-
 def _start_summary(ctx, pending: dict, dx, ycols, stats, n, d, d_stats=None, model=None,
                    order: int = 0, log_h=None) -> None:
-    """The proposal chain on a side stream, overlapping the spread that the
-    main stream runs next: binned moment sums of the data, their feature
-    vector, the network and the window start in the bandwidth list
+    """The proposal chain, enqueued on the caller's stream ahead of the
+    spread: binned moment sums of the data, their feature vector, the
+    network and the window start in the bandwidth list
     (learned.DeviceProposal), copied to pinned host memory.  Nothing here
-    waits for the device."""
+    waits for the device.  (On a second stream beside the spread the fit was
+    1-1.5% slower: the binned sums' shared-memory atomics compete with the
+    spread's kernels for the same SMs.)"""
     from . import learned as _learned
     if len(ycols) != 1 or d > 2 or model is None or log_h is None:
         return
-    side = _side_stream(ctx.device)
-    ready = torch.cuda.Event()
-    ready.record()                                  # x, y and the statistics are on the device
-    with torch.cuda.stream(side):
-        side.wait_event(ready)
-        dx.record_stream(side)
-        ycols[0].record_stream(side)
-        if d_stats is None:
-            d_stats = ctx.upload(np.ascontiguousarray(stats[:2].ravel()))
-        prop = _learned.DeviceProposal(model, [(d, order, n)], [log_h], ctx.device)
-        _lib.check(ctx.lib.flpr_bin_moments(d, n, dx.data_ptr(), ycols[0].data_ptr(),
-                                            d_stats.data_ptr(), prop.bins.data_ptr(),
-                                            side.cuda_stream), "flpr_bin_moments")
-        prop.enqueue(side.cuda_stream)
-        lo_h, t_h = _to_host(prop.lo), _to_host(prop.t)
-        done = torch.cuda.Event()
-        done.record(side)
-    pending.update(side=side, prop=prop, lo=lo_h, t=t_h, done=done, keep=(d_stats,))
+    if d_stats is None:
+        d_stats = ctx.upload(np.ascontiguousarray(stats[:2].ravel()))
+    prop = _learned.DeviceProposal(model, [(d, order, n)], [log_h], ctx.device)
+    _lib.check(ctx.lib.flpr_bin_moments(d, n, dx.data_ptr(), ycols[0].data_ptr(),
+                                        d_stats.data_ptr(), prop.bins.data_ptr(), ctx.stream),
+               "flpr_bin_moments")
+    prop.enqueue(ctx.stream)
+    lo_h, t_h = _to_host(prop.lo), _to_host(prop.t)
+    done = torch.cuda.Event()
+    done.record()
+    pending.update(prop=prop, lo=lo_h, t=t_h, done=done, keep=(d_stats,))
 
 
 def _window_filter(ctx, st: _LprState, filt_all, lo_dev: torch.Tensor, W: int):
@@ -1783,7 +1768,7 @@ def _learned_search(ctx, st: _LprState, bandwidths: np.ndarray, model, ev, pendi
     next window shares the edge bandwidth) at most _MAX_WALKS times; returns
     (evaluation, search record, pending outputs or None) or None when the
     full sweep must run.  The first window is chosen and evaluated without a
-    host round trip: the proposal chain ran on the side stream
+    host round trip: the proposal chain was enqueued ahead of the spread
     (_start_summary), the window's kernel factors are gathered on the device
     at the start index it wrote, and GCV, the 1-SE choice and the output
     stage are enqueued behind them; one synchronisation brings back the
