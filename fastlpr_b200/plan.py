@@ -162,6 +162,13 @@ class LprPlan:
             if graph:
                 self._capture()
 
+    def _workers(self) -> ThreadPoolExecutor:
+        """The host threads that stage responses and build results (started
+        again after close)."""
+        if self._pool is None:
+            self._pool = ThreadPoolExecutor(max_workers=max(1, min(16, os.cpu_count() or 1)))
+        return self._pool
+
     def close(self) -> None:
         """Stop the staging threads (also done when the plan is collected)."""
         pool, self._pool = getattr(self, "_pool", None), None
@@ -366,9 +373,7 @@ class LprPlan:
                 else:
                     st[c] = y_arr[:, c]
 
-        if self._pool is None:
-            self._pool = ThreadPoolExecutor(max_workers=max(1, min(16, os.cpu_count() or 1)))
-        list(self._pool.map(stage, idx))
+        list(self._workers().map(stage, idx))
 
     @staticmethod
     def _upload_y(p) -> torch.Tensor:
@@ -579,7 +584,7 @@ class LprPlan:
         futs = {}
         for i in self.order:
             self.probs[i].done.synchronize()
-            futs[i] = self._pool.submit(attempt, i)
+            futs[i] = self._workers().submit(attempt, i)
         mark("enqueue")
         main.synchronize()
         mark("wait")

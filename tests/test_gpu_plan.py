@@ -119,6 +119,12 @@ def test_segmented_plan_rejects_nonfinite_response_of_last_part(cuda_ok):
     got = plan.run([p[1] for p in probs])
     for (x, y, h, o), g in zip(probs, got):
         _same(g, fastlpr_b200.cv_fastlpr(x, y, h, o), _tol(o))
+    # after close() the host threads start again for the next run, and the
+    # results of the earlier run stay as they were
+    plan.close()
+    again = plan.run()
+    for a, b in zip(got, again):
+        _same(a, b, 1e-12)
 
 
 def test_plan_rejects_nonfinite_responses_and_recovers(cuda_ok):
