@@ -918,6 +918,8 @@ def run_ours(args):
                       "peak": hbm, "unit": "GB/s",
                       "frac": conv_bytes / (conv_ms / 1000.0) / 1e9 / hbm,
                       "traffic": CONV_STAGE_TRAFFIC,
+                      # what the stage's measured DRAM traffic uses of the peak
+                      "traffic_frac": CONV_STAGE_TRAFFIC / (conv_ms / 1000.0) / 1e9 / hbm,
                       "scope": (f"fused convolution + solve stage (colpass/rowpass kernels) of one "
                                 f"fit: algorithmic {conv_bytes / 1e9:.2f} GB (B_fit intermediates + "
                                 f"m) over {conv_ms:.3f} ms; peak "
