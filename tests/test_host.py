@@ -254,3 +254,29 @@ def test_plan_segments_cut_issue_order_by_staged_bytes():
     stub.order = sorted(range(len(sizes)), key=lambda i: -sizes[i])
     stub.prop = object()
     assert LprPlan._segment_order(stub) == [stub.order]
+
+
+def test_plan_checks_new_responses_against_the_plan():
+    # new responses must keep each problem's shape and real/complex kind; a
+    # 1 x n row is taken as a column (as cv_fastlpr takes it)
+    from fastlpr_b200.plan import LprPlan, _Problem
+
+    stub = type("Stub", (), {})()
+    stub.probs = []
+    for shape, cplx in (((5, 1), False), ((4, 2), False), ((3, 1), True)):
+        p = _Problem()
+        p.su = type("Setup", (), {})()
+        p.su.y_arr = np.zeros(shape, dtype=complex if cplx else float)
+        p.su.y_is_complex = cplx
+        stub.probs.append(p)
+    good = [np.arange(5.0), np.ones((4, 2)), np.ones(3) * (1 + 2j)]
+    arrs = LprPlan._check_y(stub, good)
+    assert [a.shape for a in arrs] == [(5, 1), (4, 2), (3, 1)]
+    row = [np.arange(5.0)[None, :], np.ones((4, 2)), np.ones(3) * 1j]
+    assert LprPlan._check_y(stub, row)[0].shape == (5, 1)
+    with pytest.raises(ValueError, match="expected 3 responses"):
+        LprPlan._check_y(stub, good[:2])
+    with pytest.raises(ValueError, match="differs from the planned"):
+        LprPlan._check_y(stub, [np.arange(6.0), good[1], good[2]])
+    with pytest.raises(ValueError, match="real and complex"):
+        LprPlan._check_y(stub, [good[0], good[1], np.ones(3)])
