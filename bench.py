@@ -972,7 +972,8 @@ def run_ours(args):
     return 0
 
 
-def main():
+def build_parser() -> argparse.ArgumentParser:
+    """The command-line options of this benchmark."""
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -1004,6 +1005,11 @@ def main():
                     help="points per fit (profiling of smaller cases only)")
     ap.add_argument("--grid", type=int, default=0, help="grid per axis (default 512)")
     ap.add_argument("--bandwidths", type=int, default=0, help="subset of the 32 bandwidths")
+    return ap
+
+
+def main():
+    ap = build_parser()
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
